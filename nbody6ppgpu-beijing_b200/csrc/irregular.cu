@@ -1,0 +1,434 @@
+// irregular.cu -- irregular (neighbour) force + jerk + nearest neighbour
+// behind the reference's irr_simd_* C ABI (irr.avx.cpp:568-606), with the
+// GPUIRR_* names of the NBODY6/GPU interface as aliases (the calls the
+// reference keeps commented out in fpoly0.F:42,70,202,383).
+//
+// State lives on the device: one 128-byte record per particle
+// (x0, x0dot, F = a/2, FDOT = adot/6, mass, t0, all FP64) and one neighbour
+// row per particle ([nnb, 0-based ids...], stride lmax).  irr_simd_set_jp_ /
+// irr_simd_set_list_ are called once per particle by the Fortran driver, so
+// they only write into pinned host staging (a later call for the same
+// particle overwrites its staged entry); irr_simd_firr_vec_ uploads what is
+// staged, scatters it, and runs one warp per active particle: lanes walk the
+// list, predict each j to ti in FP64 (jpred_int.f:16-25), form the
+// differences in FP64, do the pair math in FP32 with rsqrt + one Newton step
+// and sum in FP64; the nearest neighbour is the minimum FP64 r2 with the
+// smallest index on ties (irr.avx.cpp:320-323 packs (r2, idx) the same way).
+#include "nb6_common.cuh"
+
+#include <algorithm>
+#include <string.h>
+#include <vector>
+
+namespace {
+
+constexpr int IRR_WARPS = 4;
+
+struct Rec {           // 16 doubles = 128 bytes, one cache line per gather
+    double x[3], v[3], f[3], fd[3], m, t0, pad0, pad1;
+};
+
+NB6_DEV void predict(const Rec &r, double ti, double *x, double *v) {
+    const double s = ti - r.t0;
+    const double s1 = 1.5 * s, s2 = 2.0 * s;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        x[k] = ((r.fd[k] * s + r.f[k]) * s + r.v[k]) * s + r.x[k];
+        v[k] = (r.fd[k] * s1 + r.f[k]) * s2 + r.v[k];
+    }
+}
+
+NB6_DEV void load_rec(const Rec *__restrict__ p, Rec &r) {
+    const double2 *q = reinterpret_cast<const double2 *>(p);
+    double2 a = __ldg(q + 0), b = __ldg(q + 1), c = __ldg(q + 2), d = __ldg(q + 3);
+    double2 e = __ldg(q + 4), f = __ldg(q + 5), g = __ldg(q + 6);
+    r.x[0] = a.x; r.x[1] = a.y; r.x[2] = b.x;
+    r.v[0] = b.y; r.v[1] = c.x; r.v[2] = c.y;
+    r.f[0] = d.x; r.f[1] = d.y; r.f[2] = e.x;
+    r.fd[0] = e.y; r.fd[1] = f.x; r.fd[2] = f.y;
+    r.m = g.x; r.t0 = g.y;
+}
+
+__global__ void __launch_bounds__(IRR_WARPS * 32)
+    irr_kernel(int ni, const int *__restrict__ addr, double ti, const Rec *__restrict__ rec,
+               const int *__restrict__ lists, int ls, int nmax, double *__restrict__ out,
+               int *__restrict__ outid) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int k = blockIdx.x * IRR_WARPS + warp;
+    if (k >= ni) return;
+    const int i = addr[k] - 1;
+    Rec ri;
+    load_rec(rec + i, ri);
+    double xi[3], vi[3];
+    predict(ri, ti, xi, vi);
+    const int *row = lists + (size_t)i * ls;
+    const int nnb = row[0];
+    double ax = 0, ay = 0, az = 0, jx = 0, jy = 0, jz = 0;
+    double rmin = 1.0e300;
+    int jmin = 0x7fffffff;
+    for (int l = lane; l < nnb; l += 32) {
+        const int j = row[1 + l];
+        if (j < 0 || j >= nmax) continue;   // ids are checked at set_list time
+        Rec rj;
+        load_rec(rec + j, rj);
+        double xj[3], vj[3];
+        predict(rj, ti, xj, vj);
+        const double dxd = xj[0] - xi[0], dyd = xj[1] - xi[1], dzd = xj[2] - xi[2];
+        const double r2d = dxd * dxd + dyd * dyd + dzd * dzd;
+        if (r2d < rmin || (r2d == rmin && j < jmin)) {
+            rmin = r2d;
+            jmin = j;
+        }
+        const float dx = (float)dxd, dy = (float)dyd, dz = (float)dzd;
+        const float dvx = (float)(vj[0] - vi[0]);
+        const float dvy = (float)(vj[1] - vi[1]);
+        const float dvz = (float)(vj[2] - vi[2]);
+        const float r2 = (float)r2d;
+        const float y = rsqrt2_nr(r2);             // 2/r
+        const float y2 = y * y;
+        const float my3 = (float)rj.m * y * y2;    // 8 m / r^3
+        const float al = (y2 * -0.75f) * fmaf(dz, dvz, fmaf(dy, dvy, dx * dvx));
+        ax += (double)(my3 * dx);
+        ay += (double)(my3 * dy);
+        az += (double)(my3 * dz);
+        jx += (double)(my3 * fmaf(al, dx, dvx));
+        jy += (double)(my3 * fmaf(al, dy, dvy));
+        jz += (double)(my3 * fmaf(al, dz, dvz));
+    }
+    ax = warp_sum_d(ax);
+    ay = warp_sum_d(ay);
+    az = warp_sum_d(az);
+    jx = warp_sum_d(jx);
+    jy = warp_sum_d(jy);
+    jz = warp_sum_d(jz);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double r2 = __shfl_xor_sync(0xffffffffu, rmin, o);
+        const int j2 = __shfl_xor_sync(0xffffffffu, jmin, o);
+        if (r2 < rmin || (r2 == rmin && j2 < jmin)) {
+            rmin = r2;
+            jmin = j2;
+        }
+    }
+    if (lane == 0) {
+        double *o = out + (size_t)k * 6;
+        o[0] = ax * 0.125;
+        o[1] = ay * 0.125;
+        o[2] = az * 0.125;
+        o[3] = jx * 0.125;
+        o[4] = jy * 0.125;
+        o[5] = jz * 0.125;
+        outid[k] = (nnb > 0 && jmin != 0x7fffffff) ? jmin + 1 : -1;
+    }
+}
+
+// Scatter staged records: slot s goes to particle saddr[s].
+__global__ void irr_scatter_jp(int ns, const int *__restrict__ saddr, const Rec *__restrict__ src,
+                               Rec *__restrict__ rec) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < ns) rec[saddr[s]] = src[s];
+}
+
+// Scatter staged lists: entry e starts at off[e] in `stage` as [addr, nnb, ids].
+__global__ void irr_scatter_list(int ne, const int *__restrict__ off, const int *__restrict__ stage,
+                                 int *__restrict__ lists, int ls) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= ne) return;
+    const int *e = stage + off[warp];
+    const int a = e[0], nnb = e[1];
+    int *row = lists + (size_t)a * ls;
+    if (lane == 0) row[0] = nnb;
+    for (int l = lane; l < nnb; l += 32) row[1 + l] = e[2 + l];
+}
+
+struct IrrState {
+    bool open = false;
+    int nmax = 0, lmax = 0;
+    DevBuf<Rec> rec;
+    DevBuf<int> lists;
+    DevBuf<Rec> dstage_rec;
+    DevBuf<int> dstage_addr, dstage_list, dstage_off, daddr, dnnbid;
+    DevBuf<double> dout;
+    HostBuf<Rec> hstage_rec;
+    HostBuf<int> hstage_addr, hstage_list, hstage_off, haddr, hnnbid;
+    HostBuf<double> hout;
+    std::vector<int> jp_slot, list_slot;  // staged slot per particle, -1 if none
+    int njp = 0, nlist = 0;
+    size_t list_words = 0;
+    double time_grav = 0;
+    unsigned long long num_inter = 0, num_fcall = 0, num_steps = 0;
+};
+IrrState I;
+
+void irr_open_impl(int nmax, int lmax, int rank) {
+    nb6_devinit_once(rank);
+    if (I.open) {
+        fprintf(stderr, "irr_simd: it is already open\n");
+        return;
+    }
+    if (nmax <= 0 || lmax < 1) {
+        nb6_fatal(NB6_ERR_BAD_ARG);
+        return;
+    }
+    I.open = true;
+    I.nmax = nmax;
+    I.lmax = lmax;
+    I.rec.reserve((size_t)nmax + 1);
+    I.lists.reserve((size_t)nmax * lmax);
+    NB6_CUDA_CHECK(cudaMemsetAsync(I.rec.ptr, 0, sizeof(Rec) * ((size_t)nmax + 1), nb6_stream()));
+    NB6_CUDA_CHECK(cudaMemsetAsync(I.lists.ptr, 0, sizeof(int) * (size_t)nmax * lmax, nb6_stream()));
+    I.jp_slot.assign(nmax, -1);
+    I.list_slot.assign(nmax, -1);
+    I.njp = I.nlist = 0;
+    I.list_words = 0;
+    I.time_grav = 0;
+    I.num_inter = I.num_fcall = I.num_steps = 0;
+    if (getenv("NB6_VERBOSE"))
+        fprintf(stderr, "# Opening IRR lib. GPU ver. - rank: %d; nmax: %d, lmax: %d\n", rank, nmax, lmax);
+}
+
+void irr_close_impl() {
+    if (!I.open) {
+        fprintf(stderr, "irr_simd: it is already close\n");
+        return;
+    }
+    I.open = false;
+    I.rec.release();
+    I.lists.release();
+    I.dstage_rec.release();
+    I.dstage_addr.release();
+    I.dstage_list.release();
+    I.dstage_off.release();
+    I.daddr.release();
+    I.dnnbid.release();
+    I.dout.release();
+    I.hstage_rec.release();
+    I.hstage_addr.release();
+    I.hstage_list.release();
+    I.hstage_off.release();
+    I.haddr.release();
+    I.hnnbid.release();
+    I.hout.release();
+    I.jp_slot.clear();
+    I.list_slot.clear();
+}
+
+void irr_set_jp_impl(int a, const double *pos, const double *vel, const double *acc2,
+                     const double *jrk6, double mass, double time) {
+    if (!I.open) {
+        nb6_fatal(NB6_ERR_NOT_OPEN);
+        return;
+    }
+    if (a < 0 || a >= I.nmax) {
+        fprintf(stderr, "irr_simd_set_jp: address %d outside [1, %d]\n", a + 1, I.nmax);
+        nb6_fatal(NB6_ERR_BAD_ARG);
+        return;
+    }
+    int s = I.jp_slot[a];
+    if (s < 0) {
+        s = I.njp++;
+        I.jp_slot[a] = s;
+        if ((size_t)I.njp > I.hstage_rec.cap) {
+            // grow pinned staging, keeping staged content
+            HostBuf<Rec> nr;
+            HostBuf<int> na;
+            nr.reserve((size_t)I.njp * 2);
+            na.reserve((size_t)I.njp * 2);
+            if (I.njp > 1) {
+                memcpy(nr.ptr, I.hstage_rec.ptr, sizeof(Rec) * (I.njp - 1));
+                memcpy(na.ptr, I.hstage_addr.ptr, sizeof(int) * (I.njp - 1));
+            }
+            I.hstage_rec.release();
+            I.hstage_addr.release();
+            I.hstage_rec = nr;
+            I.hstage_addr = na;
+        }
+        I.hstage_addr.ptr[s] = a;
+    }
+    Rec &r = I.hstage_rec.ptr[s];
+    for (int k = 0; k < 3; ++k) {
+        r.x[k] = pos[k];
+        r.v[k] = vel[k];
+        r.f[k] = acc2[k];
+        r.fd[k] = jrk6[k];
+    }
+    r.m = mass;
+    r.t0 = time;
+    r.pad0 = r.pad1 = 0.0;
+}
+
+void irr_set_list_impl(int a, const int *nblist) {
+    if (!I.open) {
+        nb6_fatal(NB6_ERR_NOT_OPEN);
+        return;
+    }
+    const int nnb = nblist[0];
+    if (a < 0 || a >= I.nmax || nnb < 0 || nnb > I.lmax - 1) {
+        fprintf(stderr, "irr_simd_set_list: address %d or nnb %d outside the opened sizes\n", a + 1, nnb);
+        nb6_fatal(NB6_ERR_BAD_ARG);
+        return;
+    }
+    for (int l = 1; l <= nnb; ++l) {
+        if (nblist[l] < 1 || nblist[l] > I.nmax) {
+            fprintf(stderr, "irr_simd_set_list: neighbour id %d outside [1, %d]\n", nblist[l], I.nmax);
+            nb6_fatal(NB6_ERR_BAD_ARG);
+            return;
+        }
+    }
+    // Entries are appended; a re-set of the same particle before the next
+    // flush supersedes the earlier entry (list_slot keeps the latest).
+    const size_t need = I.list_words + 2 + nnb;
+    if (need > I.hstage_list.cap) {
+        HostBuf<int> nl;
+        nl.reserve(std::max(need * 2, (size_t)4096));
+        if (I.list_words) memcpy(nl.ptr, I.hstage_list.ptr, sizeof(int) * I.list_words);
+        I.hstage_list.release();
+        I.hstage_list = nl;
+    }
+    int *e = I.hstage_list.ptr + I.list_words;
+    e[0] = a;
+    e[1] = nnb;
+    for (int l = 0; l < nnb; ++l) e[2 + l] = nblist[1 + l] - 1;
+    I.list_slot[a] = (int)I.list_words;
+    I.list_words = need;
+    I.nlist++;
+}
+
+// Upload and scatter everything staged since the last flush.
+void irr_flush(cudaStream_t st) {
+    if (I.njp > 0) {
+        I.dstage_rec.reserve(I.njp);
+        I.dstage_addr.reserve(I.njp);
+        NB6_CUDA_CHECK(cudaMemcpyAsync(I.dstage_rec.ptr, I.hstage_rec.ptr, sizeof(Rec) * I.njp,
+                                       cudaMemcpyHostToDevice, st));
+        NB6_CUDA_CHECK(cudaMemcpyAsync(I.dstage_addr.ptr, I.hstage_addr.ptr, sizeof(int) * I.njp,
+                                       cudaMemcpyHostToDevice, st));
+        irr_scatter_jp<<<(I.njp + 255) / 256, 256, 0, st>>>(I.njp, I.dstage_addr.ptr, I.dstage_rec.ptr,
+                                                           I.rec.ptr);
+        NB6_CUDA_CHECK(cudaGetLastError());
+        for (int s = 0; s < I.njp; ++s) I.jp_slot[I.hstage_addr.ptr[s]] = -1;
+        I.njp = 0;
+    }
+    if (I.nlist > 0) {
+        // keep only the latest entry per particle
+        I.hstage_off.reserve(I.nlist);
+        int ne = 0;
+        size_t w = 0;
+        while (w < I.list_words) {
+            const int a = I.hstage_list.ptr[w];
+            const int nnb = I.hstage_list.ptr[w + 1];
+            if (I.list_slot[a] == (int)w) {
+                I.hstage_off.ptr[ne++] = (int)w;
+                I.list_slot[a] = -1;
+            }
+            w += 2 + nnb;
+        }
+        I.dstage_list.reserve(I.list_words);
+        I.dstage_off.reserve(ne);
+        NB6_CUDA_CHECK(cudaMemcpyAsync(I.dstage_list.ptr, I.hstage_list.ptr, sizeof(int) * I.list_words,
+                                       cudaMemcpyHostToDevice, st));
+        NB6_CUDA_CHECK(cudaMemcpyAsync(I.dstage_off.ptr, I.hstage_off.ptr, sizeof(int) * ne,
+                                       cudaMemcpyHostToDevice, st));
+        const int threads = 256;
+        const int blocks = (int)(((size_t)ne * 32 + threads - 1) / threads);
+        irr_scatter_list<<<blocks, threads, 0, st>>>(ne, I.dstage_off.ptr, I.dstage_list.ptr,
+                                                     I.lists.ptr, I.lmax);
+        NB6_CUDA_CHECK(cudaGetLastError());
+        I.nlist = 0;
+        I.list_words = 0;
+    }
+}
+
+void irr_firr_vec_impl(double ti, int ni, const int *addr, double (*acc)[3], double (*jrk)[3],
+                       int *nnbid) {
+    if (!I.open) {
+        nb6_fatal(NB6_ERR_NOT_OPEN);
+        return;
+    }
+    if (ni <= 0) return;
+    for (int k = 0; k < ni; ++k) {
+        if (addr[k] < 1 || addr[k] > I.nmax) {
+            fprintf(stderr, "irr_simd_firr_vec: address %d outside [1, %d]\n", addr[k], I.nmax);
+            nb6_fatal(NB6_ERR_BAD_ARG);
+            return;
+        }
+    }
+    const double t0 = nb6_wtime();
+    cudaStream_t st = nb6_stream();
+    // the staged records must reach the device before we clear the staging,
+    // which the stream order guarantees (copies precede the next host write
+    // only after this call's synchronize below)
+    irr_flush(st);
+    I.haddr.reserve(ni);
+    I.daddr.reserve(ni);
+    I.dout.reserve((size_t)ni * 6);
+    I.dnnbid.reserve(ni);
+    I.hout.reserve((size_t)ni * 6);
+    I.hnnbid.reserve(ni);
+    memcpy(I.haddr.ptr, addr, sizeof(int) * ni);
+    NB6_CUDA_CHECK(cudaMemcpyAsync(I.daddr.ptr, I.haddr.ptr, sizeof(int) * ni, cudaMemcpyHostToDevice, st));
+    irr_kernel<<<(ni + IRR_WARPS - 1) / IRR_WARPS, IRR_WARPS * 32, 0, st>>>(
+        ni, I.daddr.ptr, ti, I.rec.ptr, I.lists.ptr, I.lmax, I.nmax, I.dout.ptr, I.dnnbid.ptr);
+    NB6_CUDA_CHECK(cudaGetLastError());
+    NB6_CUDA_CHECK(cudaMemcpyAsync(I.hout.ptr, I.dout.ptr, sizeof(double) * 6 * ni,
+                                   cudaMemcpyDeviceToHost, st));
+    NB6_CUDA_CHECK(cudaMemcpyAsync(I.hnnbid.ptr, I.dnnbid.ptr, sizeof(int) * ni, cudaMemcpyDeviceToHost, st));
+    NB6_CUDA_CHECK(cudaStreamSynchronize(st));
+    if (nb6_check_dev_status() != 0) return;
+    unsigned long long inter = 0;
+    for (int k = 0; k < ni; ++k) {
+        const double *o = I.hout.ptr + (size_t)k * 6;
+        acc[k][0] = o[0];
+        acc[k][1] = o[1];
+        acc[k][2] = o[2];
+        jrk[k][0] = o[3];
+        jrk[k][1] = o[4];
+        jrk[k][2] = o[5];
+        nnbid[k] = I.hnnbid.ptr[k];
+    }
+    (void)inter;
+    I.time_grav += nb6_wtime() - t0;
+    I.num_fcall++;
+    I.num_steps += ni;
+}
+
+void irr_profile_impl(int rank) {
+    if (I.open && I.num_fcall) {
+        const double gf = I.time_grav > 0 ? 60.0 * (double)I.num_inter * 1e-9 / I.time_grav : 0.0;
+        fprintf(stderr, "[R.%d GPU Irr.F ] Ncall: %llu <NI>: %d grav: %f s, %f Gflops, %f usec\n", rank,
+                I.num_fcall, (int)(I.num_steps / I.num_fcall), I.time_grav, gf,
+                1e6 * I.time_grav / (double)I.num_fcall);
+    }
+    I.time_grav = 0;
+    I.num_inter = I.num_fcall = I.num_steps = 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+void irr_simd_open_(int *nmax, int *lmax, int *rank) { irr_open_impl(*nmax, *lmax, *rank); }
+void irr_simd_close_(int *rank) { (void)rank; irr_close_impl(); }
+void irr_simd_profile_(int *rank) { irr_profile_impl(*rank); }
+void irr_simd_set_jp_(int *addr, double pos[3], double vel[3], double acc2[3], double jrk6[3],
+                      double *mass, double *time) {
+    irr_set_jp_impl(*addr - 1, pos, vel, acc2, jrk6, *mass, *time);
+}
+void irr_simd_set_list_(int *addr, int *nblist) { irr_set_list_impl(*addr - 1, nblist); }
+void irr_simd_firr_vec_(double *ti, int *ni, int addr[], double acc[][3], double jrk[][3],
+                        int nnbid[]) {
+    irr_firr_vec_impl(*ti, *ni, addr, acc, jrk, nnbid);
+}
+
+// NBODY6/GPU names (fpoly0.F:42,70,202,383, intgrt.F:1329 -- commented out
+// in the reference): same arguments, rank 0.
+void gpuirr_open_(int *nmax, int *lmax) { irr_open_impl(*nmax, *lmax, 0); }
+void gpuirr_close_() { irr_close_impl(); }
+void gpuirr_set_jp_(int *addr, double pos[3], double vel[3], double acc2[3], double jrk6[3],
+                    double *mass, double *time) {
+    irr_set_jp_impl(*addr - 1, pos, vel, acc2, jrk6, *mass, *time);
+}
+void gpuirr_set_list_(int *addr, int *nblist) { irr_set_list_impl(*addr - 1, nblist); }
+
+}  // extern "C"

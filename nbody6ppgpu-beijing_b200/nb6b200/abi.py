@@ -1,0 +1,179 @@
+"""ctypes mirror of the reference's Fortran-callable force ABI.
+
+The reference's driver calls (``util_gpu.F:59``, ``fpoly0.F:31,79,131,381``,
+``energy.F:33``, ``intgrt.F:533,1229``) pass every argument by pointer and
+arrays in Fortran column-major order, i.e. ``X(3,N)`` is C ``double[N][3]``.
+:class:`ForceLib` binds those symbols on any shared object that exports them
+-- this package's ``libnb6b200.so`` or, in the tests, the reference's own CPU
+libraries -- and offers numpy-level calls with the reference's argument
+meaning:
+
+* ``gpunb_open(nbmax, irank)``, ``gpunb_send(m, x, v)``,
+  ``gpunb_regf(h2, dtr, xi, vi, lmax, nnbmax, m_flag)`` ->
+  ``(acc, jrk, pot, list)`` (``gpunb.velocity.cu:905-940``);
+* ``gpupot(irank, istart, ni, m, x)`` -> ``pot`` (``gpupot.gpu.cu:116-127``);
+* ``irr_simd_open/set_jp/set_list/firr_vec/close``
+  (``irr.avx.cpp:568-606``).
+
+Nothing here computes forces; it only marshals arrays.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+_d = C.POINTER(C.c_double)
+_i = C.POINTER(C.c_int)
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(_d)
+
+
+def _ip(a: np.ndarray):
+    return a.ctypes.data_as(_i)
+
+
+def _f64(a, shape=None) -> np.ndarray:
+    out = np.ascontiguousarray(a, dtype=np.float64)
+    if shape is not None:
+        out = out.reshape(shape)
+    return out
+
+
+def _ci(v: int):
+    return C.byref(C.c_int(int(v)))
+
+
+def _cd(v: float):
+    return C.byref(C.c_double(float(v)))
+
+
+class ForceLib:
+    """Numpy-level calls onto a shared object exporting the reference ABI."""
+
+    # Pad i-arrays to a multiple of 4: the reference AVX library reads four
+    # i-particles at a time (reg.avx.cpp:204-226), past ni for ragged ni.
+    IPAD = 4
+
+    def __init__(self, lib: C.CDLL, name: str = "lib"):
+        self.lib = lib
+        self.name = name
+        self.has_gpunb = hasattr(lib, "gpunb_regf_")
+        self.has_gpupot = hasattr(lib, "gpupot_")
+        self.has_irr = hasattr(lib, "irr_simd_firr_vec_")
+        for fn in ("gpunb_open_", "gpunb_close_", "gpunb_send_", "gpunb_regf_",
+                   "gpunb_profile_", "gpunb_devinit_", "gpupot_", "irr_simd_open_",
+                   "irr_simd_close_", "irr_simd_set_jp_", "irr_simd_set_list_",
+                   "irr_simd_firr_vec_", "irr_simd_profile_"):
+            if hasattr(lib, fn):
+                getattr(lib, fn).restype = None
+
+    # ------------------------------------------------------------------ gpunb
+    def gpunb_open(self, nbmax: int, irank: int = 0) -> None:
+        self.lib.gpunb_open_(_ci(nbmax), _ci(irank))
+
+    def gpunb_close(self) -> None:
+        self.lib.gpunb_close_()
+
+    def gpunb_profile(self, irank: int = 0) -> None:
+        self.lib.gpunb_profile_(_ci(irank))
+
+    def gpunb_send(self, m, x, v) -> None:
+        m = _f64(m)
+        n = m.shape[0]
+        x = _f64(x, (n, 3))
+        v = _f64(v, (n, 3))
+        self.lib.gpunb_send_(_ci(n), _dp(m), _dp(x), _dp(v))
+
+    def gpunb_regf(self, h2, dtr, xi, vi, lmax: int, nnbmax: int, m_flag: int = 0):
+        h2 = _f64(h2)
+        ni = h2.shape[0]
+        pad = (-ni) % self.IPAD
+        npad = ni + pad
+
+        def padv(a, cols=None):
+            a = _f64(a, (ni,) if cols is None else (ni, cols))
+            if pad == 0:
+                return np.ascontiguousarray(a)
+            shape = (npad,) if cols is None else (npad, cols)
+            out = np.zeros(shape)
+            out[:ni] = a
+            return out
+
+        h2p, dtrp = padv(h2), padv(dtr)
+        xip, vip = padv(xi, 3), padv(vi, 3)
+        acc = np.zeros((npad, 3))
+        jrk = np.zeros((npad, 3))
+        pot = np.zeros(npad)
+        lst = np.zeros((npad, lmax), dtype=np.int32)
+        self.lib.gpunb_regf_(_ci(ni), _dp(h2p), _dp(dtrp), _dp(xip), _dp(vip), _dp(acc),
+                             _dp(jrk), _dp(pot), _ci(lmax), _ci(nnbmax), _ip(lst), _ci(m_flag))
+        return acc[:ni], jrk[:ni], pot[:ni], lst[:ni]
+
+    # ----------------------------------------------------------------- gpupot
+    def gpupot(self, m, x, istart: int = 1, ni: int | None = None, irank: int = 0,
+               absolute_output: bool = False) -> np.ndarray:
+        """pot[k] = potential at particle istart-1+k (the GPU library's and
+        energy_mpi.F:216's convention).  The reference's CPU pot.avx.cpp
+        writes pot[istart-1+k] instead (pot.avx.cpp:343); pass
+        absolute_output=True for that library."""
+        m = _f64(m)
+        n = m.shape[0]
+        x = _f64(x, (n, 3))
+        if ni is None:
+            ni = n - (istart - 1)
+        off = (istart - 1) if absolute_output else 0
+        # The AVX library writes 8 i at a time (pot.avx.cpp:296-343); pad by 8.
+        pot = np.zeros(off + ni + 8)
+        self.lib.gpupot_(_ci(irank), _ci(istart), _ci(ni), _ci(n), _dp(m), _dp(x), _dp(pot))
+        return pot[off:off + ni].copy()
+
+    # -------------------------------------------------------------- irregular
+    def irr_open(self, nmax: int, lmax: int, rank: int = 0) -> None:
+        self.lib.irr_simd_open_(_ci(nmax), _ci(lmax), _ci(rank))
+
+    def irr_close(self, rank: int = 0) -> None:
+        self.lib.irr_simd_close_(_ci(rank))
+
+    def irr_profile(self, rank: int = 0) -> None:
+        self.lib.irr_simd_profile_(_ci(rank))
+
+    def irr_set_jp(self, addr: int, pos, vel, acc2, jrk6, mass: float, time: float) -> None:
+        """addr is 1-based (Fortran particle index)."""
+        p = _f64(pos, (3,))
+        v = _f64(vel, (3,))
+        a = _f64(acc2, (3,))
+        j = _f64(jrk6, (3,))
+        self.lib.irr_simd_set_jp_(_ci(addr), _dp(p), _dp(v), _dp(a), _dp(j), _cd(mass), _cd(time))
+
+    def irr_set_jp_all(self, pos, vel, acc2, jrk6, mass, time, first: int = 1) -> None:
+        pos = _f64(pos)
+        n = pos.shape[0]
+        vel, acc2, jrk6 = _f64(vel), _f64(acc2), _f64(jrk6)
+        mass, time = _f64(mass), _f64(time)
+        fn = self.lib.irr_simd_set_jp_
+        for k in range(n):
+            fn(_ci(first + k), _dp(pos[k]), _dp(vel[k]), _dp(acc2[k]), _dp(jrk6[k]),
+               C.byref(C.c_double(mass[k])), C.byref(C.c_double(time[k])))
+
+    def irr_set_list(self, addr: int, nblist) -> None:
+        """nblist = [nnb, j1, ..., jnnb] with 1-based j (Fortran LIST(1,I)).
+
+        The reference reads ids in blocks of 8 (irr.avx.cpp:468-489), so the
+        row handed over is padded to a multiple of 8 past nnb."""
+        row = np.asarray(nblist, dtype=np.int32)
+        nnb = int(row[0])
+        padded = np.zeros(1 + max(8, ((nnb + 7) // 8) * 8), dtype=np.int32)
+        padded[: row.shape[0]] = row[: padded.shape[0]]
+        self.lib.irr_simd_set_list_(_ci(addr), _ip(padded))
+
+    def irr_firr_vec(self, ti: float, addr) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+        addr = np.ascontiguousarray(addr, dtype=np.int32)
+        ni = addr.shape[0]
+        acc = np.zeros((max(ni, 1), 3))
+        jrk = np.zeros((max(ni, 1), 3))
+        nnbid = np.zeros(max(ni, 1), dtype=np.int32)
+        self.lib.irr_simd_firr_vec_(_cd(ti), _ci(ni), _ip(addr), _dp(acc), _dp(jrk), _ip(nnbid))
+        return acc[:ni], jrk[:ni], nnbid[:ni]

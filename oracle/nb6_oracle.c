@@ -1,0 +1,160 @@
+/*
+ * nb6_oracle.c -- FP64 CPU restatement of the Nbody6++GPU force hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY (the checker, never the product).  Each function
+ * cites the reference lines it restates; arithmetic is plain IEEE double with
+ * no reassociation tricks, so it is the "FP64 direct-sum oracle" that the
+ * CUDA kernels' relative errors are stated against.
+ */
+#include "nb6_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+
+long orc_regf(int nj, const double *mj, const double *xj, const double *vj,
+              int ni, const double *h2, const double *dtr,
+              const double *xi, const double *vi,
+              int lmax, int nnbmax, int m_flag,
+              double *acc, double *jrk, double *pot, int *list)
+{
+    long total = 0;
+#pragma omp parallel for schedule(dynamic, 4) reduction(+ : total)
+    for (int i = 0; i < ni; i++) {
+        const double x0 = xi[3 * i], x1 = xi[3 * i + 1], x2 = xi[3 * i + 2];
+        const double v0 = vi[3 * i], v1 = vi[3 * i + 1], v2 = vi[3 * i + 2];
+        const double hh = h2[i], dt = dtr[i];
+        double ax = 0, ay = 0, az = 0, jx = 0, jy = 0, jz = 0, po = 0;
+        int *row = list + (long)i * lmax;
+        int nnb = 0;
+        const int cap = (nnbmax < lmax - 1) ? nnbmax : lmax - 1;
+        /* ids go to scratch first: an overflowed row gets no ids */
+        int *ids = (int *)malloc(sizeof(int) * (size_t)(cap > 0 ? cap : 1));
+        for (int j = 0; j < nj; j++) {
+            /* gpunb.velocity.cu:169-185 / regint.f:41-58 */
+            const double dx = xj[3 * j] - x0;
+            const double dy = xj[3 * j + 1] - x1;
+            const double dz = xj[3 * j + 2] - x2;
+            const double dvx = vj[3 * j] - v0;
+            const double dvy = vj[3 * j + 1] - v1;
+            const double dvz = vj[3 * j + 2] - v2;
+            const double r2 = dx * dx + dy * dy + dz * dz;
+            const double px = dx + dt * dvx, py = dy + dt * dvy, pz = dz + dt * dvz;
+            const double r2p = px * px + py * py + pz * pz;
+            const double rmin = (r2 < r2p) ? r2 : r2p;
+            const double crit = m_flag ? mj[j] * hh : hh;
+            if (rmin < crit) {
+                /* neighbour: recorded, contributes nothing (:188-193) */
+                if (nnb < cap) ids[nnb] = j;
+                nnb++;
+                continue;
+            }
+            const double rv = dx * dvx + dy * dvy + dz * dvz;
+            const double rinv2 = 1.0 / r2;
+            const double rinv = sqrt(rinv2);
+            const double mr = mj[j] * rinv;
+            const double mr3 = mr * rinv2;
+            const double alpha = -3.0 * rv * rinv2;
+            po += mr;
+            ax += mr3 * dx;
+            ay += mr3 * dy;
+            az += mr3 * dz;
+            jx += mr3 * (dvx + alpha * dx);
+            jy += mr3 * (dvy + alpha * dy);
+            jz += mr3 * (dvz + alpha * dz);
+        }
+        acc[3 * i] = ax; acc[3 * i + 1] = ay; acc[3 * i + 2] = az;
+        jrk[3 * i] = jx; jrk[3 * i + 1] = jy; jrk[3 * i + 2] = jz;
+        pot[i] = po;
+        /* overflow contract: reg.avx.cpp:320-327 (negative count) */
+        row[0] = (nnb > cap) ? -nnb : nnb;
+        if (nnb <= cap)
+            for (int k = 0; k < nnb; k++) row[1 + k] = ids[k];
+        free(ids);
+        total += nnb;
+    }
+    return total;
+}
+
+void orc_pot(int n, const double *m, const double *x, int istart, int ni,
+             double *pot)
+{
+    const int i0 = istart - 1;
+#pragma omp parallel for schedule(dynamic, 8)
+    for (int k = 0; k < ni; k++) {
+        const int i = i0 + k;
+        const double x0 = x[3 * i], x1 = x[3 * i + 1], x2 = x[3 * i + 2];
+        double p = 0.0;
+        for (int j = 0; j < n; j++) {
+            const double dx = x[3 * j] - x0;
+            const double dy = x[3 * j + 1] - x1;
+            const double dz = x[3 * j + 2] - x2;
+            const double r2 = dx * dx + dy * dy + dz * dz;
+            if (r2 > 0.0) p += m[j] / sqrt(r2); /* gpupot.gpu.cu:48-52 */
+        }
+        pot[k] = p;
+    }
+}
+
+static inline void pred1(double s, const double *x0, const double *x0dot,
+                         const double *f, const double *fdot, double *x,
+                         double *xd)
+{
+    /* xbpredall.F:50-59 */
+    const double s1 = 1.5 * s, s2 = 2.0 * s;
+    for (int k = 0; k < 3; k++) {
+        x[k] = ((fdot[k] * s + f[k]) * s + x0dot[k]) * s + x0[k];
+        xd[k] = (fdot[k] * s1 + f[k]) * s2 + x0dot[k];
+    }
+}
+
+void orc_predict(int n, double time, const double *t0, const double *x0,
+                 const double *x0dot, const double *f, const double *fdot,
+                 double *x, double *xdot)
+{
+#pragma omp parallel for schedule(static)
+    for (int j = 0; j < n; j++)
+        pred1(time - t0[j], x0 + 3 * j, x0dot + 3 * j, f + 3 * j,
+              fdot + 3 * j, x + 3 * j, xdot + 3 * j);
+}
+
+void orc_firr(double ti, int ni, const int *addr, int nmax,
+              const double *x0, const double *v0, const double *acc2,
+              const double *jrk6, const double *mass, const double *t0,
+              const int *lists, int lmax,
+              double *acc, double *jrk, int *nnbid)
+{
+    (void)nmax;
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int k = 0; k < ni; k++) {
+        const int i = addr[k] - 1;
+        double xi[3], vi[3];
+        pred1(ti - t0[i], x0 + 3 * i, v0 + 3 * i, acc2 + 3 * i, jrk6 + 3 * i,
+              xi, vi);
+        const int *row = lists + (long)i * lmax;
+        const int nnb = row[0];
+        double ax = 0, ay = 0, az = 0, jx = 0, jy = 0, jz = 0;
+        double rmin = INFINITY;
+        int imin = -1;
+        for (int l = 1; l <= nnb; l++) {
+            /* nbint.F:133-158 */
+            const int j = row[l] - 1;
+            double xj[3], vj[3];
+            pred1(ti - t0[j], x0 + 3 * j, v0 + 3 * j, acc2 + 3 * j,
+                  jrk6 + 3 * j, xj, vj);
+            const double dx = xj[0] - xi[0], dy = xj[1] - xi[1], dz = xj[2] - xi[2];
+            const double dvx = vj[0] - vi[0], dvy = vj[1] - vi[1], dvz = vj[2] - vi[2];
+            const double r2 = dx * dx + dy * dy + dz * dz;
+            if (r2 < rmin) { rmin = r2; imin = j + 1; }
+            const double rinv2 = 1.0 / r2;
+            const double mr3 = mass[j] * rinv2 * sqrt(rinv2);
+            const double drdp = 3.0 * (dx * dvx + dy * dvy + dz * dvz) * rinv2;
+            ax += dx * mr3; ay += dy * mr3; az += dz * mr3;
+            jx += (dvx - dx * drdp) * mr3;
+            jy += (dvy - dy * drdp) * mr3;
+            jz += (dvz - dz * drdp) * mr3;
+        }
+        acc[3 * k] = ax; acc[3 * k + 1] = ay; acc[3 * k + 2] = az;
+        jrk[3 * k] = jx; jrk[3 * k + 1] = jy; jrk[3 * k + 2] = jz;
+        nnbid[k] = imin;
+    }
+}

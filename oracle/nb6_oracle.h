@@ -1,0 +1,66 @@
+/*
+ * nb6_oracle.h -- FP64 CPU restatement of the Nbody6++GPU force hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is the parity checker for the CUDA library,
+ * never the thing measured or shipped: only tests/, __graft_entry__.smoke()
+ * and bench.py's cpu_baseline leg load it.
+ *
+ * Parity pin: the restatement is checked against the reference's own CPU
+ * libraries (reg.avx.cpp, pot.avx.cpp, irr.avx.cpp compiled from their
+ * sources into oracle/_ref) on seeded inputs; the committed fixtures under
+ * tests/golden/ were produced by those libraries (tests/golden/make_golden.py).
+ *
+ * Arrays follow the reference ABI: Fortran X(3,N) == C double[N][3] (AoS),
+ * list rows are list[i*lmax + k].
+ */
+#ifndef NB6_ORACLE_H
+#define NB6_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Regular force + jerk + potential + neighbour list, gpunb_regf_ semantics
+ * (gpunb.velocity.cu:163-258 pair rule; FP64 loop form of regint.f:39-79).
+ * j runs over all nj particles (self included as a neighbour, r2 = 0).
+ * Neighbour:  min(r2, |dx + dtr*dv|^2) < h2      (m_flag == 0)
+ *             min(r2, |dx + dtr*dv|^2) < m_j*h2  (m_flag != 0)
+ * acc/jrk/pot sum over non-neighbours only; pot is positive (sum m/r).
+ * list[i*lmax] = nnb, list[i*lmax+1..nnb] = 0-based ascending j; on overflow
+ * (nnb > nnbmax or nnb > lmax-1) list[i*lmax] = -nnb and no ids are written.
+ * Returns the total neighbour count over all i. */
+long orc_regf(int nj, const double *mj, const double *xj, const double *vj,
+              int ni, const double *h2, const double *dtr,
+              const double *xi, const double *vi,
+              int lmax, int nnbmax, int m_flag,
+              double *acc, double *jrk, double *pot, int *list);
+
+/* N^2 potential, gpupot_ semantics (gpupot.gpu.cu:32-57; FP64 form of
+ * energy.F:65-99): pot[k] = sum_{j: r2>0} m_j / r_ij for
+ * i = istart-1+k, k in [0, ni); istart is 1-based. */
+void orc_pot(int n, const double *m, const double *x, int istart, int ni,
+             double *pot);
+
+/* Hermite predictor of all particles (xbpredall.F:49-61, jpred_int.f:16-25):
+ * s = time - t0[j]; x = ((fdot*s + f)*s + x0dot)*s + x0;
+ * xdot = (fdot*1.5s + f)*2s + x0dot.  f = a/2, fdot = adot/6. */
+void orc_predict(int n, double time, const double *t0, const double *x0,
+                 const double *x0dot, const double *f, const double *fdot,
+                 double *x, double *xdot);
+
+/* Irregular force + jerk + nearest neighbour over resident lists,
+ * irr_simd_firr_vec_ semantics (irr.avx.cpp:499-565) computed in FP64 as in
+ * nbint.F:121-159 with jpred_int.f prediction of both i and j to ti.
+ * addr[] and list ids are 1-based (Fortran); lists[(a-1)*lmax] = nnb,
+ * lists[(a-1)*lmax + 1..nnb] = 1-based j.  nnbid = 1-based j of the minimum
+ * r2 (first in list order on ties), or -1 for an empty list. */
+void orc_firr(double ti, int ni, const int *addr, int nmax,
+              const double *x0, const double *v0, const double *acc2,
+              const double *jrk6, const double *mass, const double *t0,
+              const int *lists, int lmax,
+              double *acc, double *jrk, int *nnbid);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,128 @@
+"""ctypes access to the parity checkers (TEST INFRASTRUCTURE ONLY).
+
+* :func:`fp64` -- the FP64 C restatement (``oracle/liboracle.so``) of the
+  reference's force loops, see ``nb6_oracle.h`` for the cited lines.
+* :func:`ref_lib` -- the reference's own CPU force libraries
+  (``oracle/_ref/libref_{reg,pot,irr}_avx.so``) compiled from their sources by
+  ``oracle/Makefile``.  Each is loaded RTLD_LOCAL and was linked -Bsymbolic,
+  so its ``gpunb_*`` / ``gpupot_`` / ``irr_simd_*`` never bind to the
+  product's symbols of the same name.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
+module; the product path never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_DIR = os.path.join(HERE, "_ref")
+
+_d = C.POINTER(C.c_double)
+_i = C.POINTER(C.c_int)
+
+
+def build(ref: bool = True) -> None:
+    """Run oracle/Makefile (the reference libraries only if their sources exist)."""
+    subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
+    if ref:
+        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+
+
+_FP64 = None
+
+
+def fp64():
+    global _FP64
+    if _FP64 is None:
+        if not os.path.exists(ORACLE_SO):
+            build(ref=False)
+        lib = C.CDLL(ORACLE_SO, mode=C.RTLD_LOCAL)
+        lib.orc_regf.restype = C.c_long
+        lib.orc_pot.restype = None
+        lib.orc_predict.restype = None
+        lib.orc_firr.restype = None
+        _FP64 = lib
+    return _FP64
+
+
+def ref_path(name: str) -> str:
+    return os.path.join(REF_DIR, f"libref_{name}_avx.so")
+
+
+def ref_available(name: str) -> bool:
+    return os.path.exists(ref_path(name))
+
+
+def ref_lib(name: str) -> C.CDLL:
+    """name in {"reg", "pot", "irr"}."""
+    p = ref_path(name)
+    if not os.path.exists(p):
+        raise FileNotFoundError(p)
+    return C.CDLL(p, mode=C.RTLD_LOCAL)
+
+
+def _f(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def regf(mj, xj, vj, h2, dtr, xi, vi, lmax, nnbmax, m_flag=0):
+    """FP64 regular force (gpunb_regf_ semantics).  Returns acc, jrk, pot, list."""
+    mj, xj, vj = _f(mj), _f(xj), _f(vj)
+    h2, dtr, xi, vi = _f(h2), _f(dtr), _f(xi), _f(vi)
+    nj, ni = mj.shape[0], h2.shape[0]
+    acc = np.zeros((ni, 3))
+    jrk = np.zeros((ni, 3))
+    pot = np.zeros(ni)
+    lst = np.zeros((ni, lmax), dtype=np.int32)
+    fp64().orc_regf(nj, mj.ctypes.data_as(_d), xj.ctypes.data_as(_d), vj.ctypes.data_as(_d),
+                    ni, h2.ctypes.data_as(_d), dtr.ctypes.data_as(_d),
+                    xi.ctypes.data_as(_d), vi.ctypes.data_as(_d), lmax, nnbmax, m_flag,
+                    acc.ctypes.data_as(_d), jrk.ctypes.data_as(_d), pot.ctypes.data_as(_d),
+                    lst.ctypes.data_as(_i))
+    return acc, jrk, pot, lst
+
+
+def pot(m, x, istart=1, ni=None):
+    m, x = _f(m), _f(x)
+    n = m.shape[0]
+    if ni is None:
+        ni = n - istart + 1
+    out = np.zeros(ni)
+    fp64().orc_pot(n, m.ctypes.data_as(_d), x.ctypes.data_as(_d), istart, ni,
+                   out.ctypes.data_as(_d))
+    return out
+
+
+def predict(time, t0, x0, x0dot, f, fdot):
+    t0, x0, x0dot, f, fdot = _f(t0), _f(x0), _f(x0dot), _f(f), _f(fdot)
+    n = t0.shape[0]
+    x = np.zeros((n, 3))
+    xd = np.zeros((n, 3))
+    fp64().orc_predict(n, float(time), t0.ctypes.data_as(_d), x0.ctypes.data_as(_d),
+                       x0dot.ctypes.data_as(_d), f.ctypes.data_as(_d), fdot.ctypes.data_as(_d),
+                       x.ctypes.data_as(_d), xd.ctypes.data_as(_d))
+    return x, xd
+
+
+def firr(ti, addr, x0, v0, acc2, jrk6, mass, t0, lists):
+    """lists: (nmax, lmax) int32 rows [nnb, 1-based j...]; addr 1-based."""
+    x0, v0, acc2, jrk6, mass, t0 = map(_f, (x0, v0, acc2, jrk6, mass, t0))
+    lists = np.ascontiguousarray(lists, dtype=np.int32)
+    addr = np.ascontiguousarray(addr, dtype=np.int32)
+    nmax, lmax = lists.shape
+    ni = addr.shape[0]
+    acc = np.zeros((ni, 3))
+    jrk = np.zeros((ni, 3))
+    nnbid = np.zeros(ni, dtype=np.int32)
+    fp64().orc_firr(C.c_double(ti), ni, addr.ctypes.data_as(_i), nmax, x0.ctypes.data_as(_d),
+                    v0.ctypes.data_as(_d), acc2.ctypes.data_as(_d), jrk6.ctypes.data_as(_d),
+                    mass.ctypes.data_as(_d), t0.ctypes.data_as(_d), lists.ctypes.data_as(_i),
+                    lmax, acc.ctypes.data_as(_d), jrk.ctypes.data_as(_d),
+                    nnbid.ctypes.data_as(_i))
+    return acc, jrk, nnbid

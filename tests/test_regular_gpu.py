@@ -1,0 +1,191 @@
+"""Regular force + jerk + potential + neighbour list: CUDA library vs oracle.
+
+Called through the C ABI exactly as util_gpu.F:59 / fpoly0.F:131 call
+gpunb_regf.  Tolerances (stated per the contract):
+
+* force, jerk, potential vs the FP64 oracle: relative error per particle
+  <= 1e-6 (acc, pot) and <= 1e-5 (jerk, which carries a cancelling
+  (r.v) r term) after list alignment;
+* neighbour lists vs the FP64 oracle: identical (the kernel re-decides every
+  candidate in FP64 with the oracle's operation order);
+* neighbour lists vs the reference's own CPU library (golden fixtures):
+  identical except pairs within 1e-4 of the radius boundary (the reference
+  rounds absolute coordinates to FP32).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from parity import align_to_lists, compare_lists, rel_err_vec
+
+pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+TOL_ACC = 1e-6
+TOL_POT = 1e-6
+TOL_JRK = 1e-5
+
+
+def _load(name):
+    return dict(np.load(os.path.join(GOLD, name + ".npz")))
+
+
+def run_gpu(nb6, mj, xj, vj, h2, dtr, xi, vi, lmax, nnbmax, m_flag, nbmax=None):
+    nb6.gpunb_open(nbmax or (len(mj) + 10), 0)
+    try:
+        nb6.gpunb_send(mj, xj, vj)
+        return nb6.gpunb_regf(h2, dtr, xi, vi, lmax, nnbmax, m_flag)
+    finally:
+        nb6.gpunb_close()
+
+
+def check_vs_oracle(orc, inp, out, exact_lists=True):
+    acc, jrk, pot, lst = out
+    oa, oj, op, ol = orc.regf(inp["mj"], inp["xj"], inp["vj"], inp["h2"], inp["dtr"],
+                              inp["xi"], inp["vi"], int(inp["lmax"]), int(inp["nnbmax"]),
+                              int(inp["m_flag"]))
+    np.testing.assert_array_equal(lst[:, 0], ol[:, 0])
+    res = compare_lists(lst, ol, inp, band=1e-12, m_flag=int(inp["m_flag"]))
+    if exact_lists:
+        assert res["pairs_in_band"] + res["pairs_out_of_band"] == 0, res
+    assert res["unsorted_rows"] == 0, res
+    oa, oj, op = align_to_lists(oa, oj, op, ol, lst, inp)
+    ok = lst[:, 0] >= 0
+    ea = rel_err_vec(acc[ok], oa[ok])
+    ej = rel_err_vec(jrk[ok], oj[ok])
+    ep = rel_err_vec(pot[ok], op[ok])
+    assert ea.max() <= TOL_ACC, (ea.max(), np.median(ea))
+    assert ej.max() <= TOL_JRK, (ej.max(), np.median(ej))
+    assert ep.max() <= TOL_POT, (ep.max(), np.median(ep))
+    # rows that overflowed carry no ids in either
+    return ea, ej, ep
+
+
+@pytest.mark.parametrize("case", ["reg_plummer1k", "reg_plummer1k_overflow",
+                                  "reg_kroupa2k_mflag"])
+def test_regular_golden_cases(nb6, orc, case):
+    g = _load(case)
+    out = run_gpu(nb6, g["mj"], g["xj"], g["vj"], g["h2"], g["dtr"], g["xi"], g["vi"],
+                  int(g["lmax"]), int(g["nnbmax"]), int(g["m_flag"]))
+    check_vs_oracle(orc, g, out)
+    # against the reference's own library: lists equal outside the FP32 band
+    res = compare_lists(out[3], g["list"], g, band=1e-4, m_flag=int(g["m_flag"]))
+    assert res["pairs_out_of_band"] == 0, res
+    assert res["overflow_mismatch"] == 0, res
+    acc, jrk, pot = align_to_lists(out[0], out[1], out[2], out[3], g["list"], g)
+    ok = (out[3][:, 0] >= 0) & (g["list"][:, 0] >= 0)
+    assert np.median(rel_err_vec(acc[ok], g["acc"][ok])) < 2e-5
+
+
+def _inputs(cl, isel, lmax, nnbmax, m_flag):
+    return {"mj": cl.mass, "xj": cl.pos, "vj": cl.vel, "h2": cl.h2(m_flag)[isel],
+            "dtr": cl.dtr[isel], "xi": cl.pos[isel], "vi": cl.vel[isel], "lmax": lmax,
+            "nnbmax": nnbmax, "m_flag": m_flag}
+
+
+@pytest.mark.parametrize("n,ni", [(1, 1), (2, 1), (130, 3), (1000, 129), (1000, 1000),
+                                  (4097, 257), (8192, 1024)])
+def test_regular_ragged_sizes(nb6, orc, n, ni):
+    from nb6b200 import ics
+    cl = ics.plummer(max(n, 2), seed=100 + n, imf=True, nnbopt=min(50, max(n - 1, 1)))
+    if n == 1:
+        cl.mass, cl.pos, cl.vel = cl.mass[:1], cl.pos[:1], cl.vel[:1]
+        cl.rs, cl.dtr = cl.rs[:1], cl.dtr[:1]
+    isel = np.sort(np.random.default_rng(n).choice(cl.n, size=ni, replace=False))
+    for m_flag in (0, 1):
+        inp = _inputs(cl, isel, 512, 400, m_flag)
+        out = run_gpu(nb6, **inp)
+        check_vs_oracle(orc, inp, out)
+
+
+def test_regular_self_is_listed_and_ascending(nb6):
+    from nb6b200 import ics
+    cl = ics.plummer(3000, seed=5)
+    isel = np.arange(0, 3000, 7)
+    inp = _inputs(cl, isel, 512, 400, 0)
+    acc, jrk, pot, lst = run_gpu(nb6, **inp)
+    for r, i in enumerate(isel):
+        n = lst[r, 0]
+        assert n >= 1
+        ids = lst[r, 1:1 + n]
+        assert i in ids                    # self included (util_gpu.F:105 strips it)
+        assert np.all(np.diff(ids) > 0)    # ascending (regcor_gpu.F:284-321)
+        assert ids.min() >= 0 and ids.max() < cl.n
+
+
+def test_regular_overflow_contract(nb6, orc):
+    from nb6b200 import ics
+    cl = ics.plummer(2048, seed=9)
+    isel = np.arange(2048)
+    for nnbmax, lmax in ((10, 600), (400, 20), (0, 8)):
+        inp = _inputs(cl, isel, lmax, nnbmax, 0)
+        acc, jrk, pot, lst = run_gpu(nb6, **inp)
+        _, _, _, ol = orc.regf(cl.mass, cl.pos, cl.vel, inp["h2"], inp["dtr"], inp["xi"],
+                               inp["vi"], lmax, nnbmax, 0)
+        np.testing.assert_array_equal(lst[:, 0], ol[:, 0])
+        cap = min(nnbmax, lmax - 1)
+        assert np.all((lst[:, 0] < 0) == (np.abs(ol[:, 0]) > cap))
+        # overflowed rows: -nnb, nothing else written
+        bad = lst[:, 0] < 0
+        assert np.all(lst[bad, 1:] == 0)
+
+
+def test_regular_repeated_calls_and_resend(nb6, orc):
+    """Counters and buffers are reset per call; a second send replaces j."""
+    from nb6b200 import ics
+    a = ics.plummer(5000, seed=1)
+    b = ics.plummer(3001, seed=2, imf=True)
+    nb6.gpunb_open(6000, 0)
+    try:
+        for cl in (a, b, a):
+            nb6.gpunb_send(cl.mass, cl.pos, cl.vel)
+            for isel in (np.arange(0, cl.n, 3), np.arange(17)):
+                inp = _inputs(cl, isel, 300, 250, 0)
+                out = nb6.gpunb_regf(inp["h2"], inp["dtr"], inp["xi"], inp["vi"], 300, 250, 0)
+                check_vs_oracle(orc, inp, out)
+    finally:
+        nb6.gpunb_close()
+
+
+def test_regular_i_not_in_j_set(nb6, orc):
+    """i-particles need not be members of the sent j set (no self pair)."""
+    from nb6b200 import ics
+    cl = ics.plummer(2000, seed=3)
+    other = ics.plummer(300, seed=4)
+    inp = {"mj": cl.mass, "xj": cl.pos, "vj": cl.vel, "h2": other.rs ** 2, "dtr": other.dtr,
+           "xi": other.pos, "vi": other.vel, "lmax": 512, "nnbmax": 400, "m_flag": 0}
+    out = run_gpu(nb6, **inp)
+    check_vs_oracle(orc, inp, out)
+
+
+def test_regular_mid_size_kroupa(nb6, orc):
+    """N = 65,536 Plummer + Kroupa (config 2's model), 1024 active."""
+    from nb6b200 import ics
+    cl = ics.plummer(65536, seed=2026, imf=True)
+    isel = np.sort(np.random.default_rng(0).choice(cl.n, 1024, replace=False))
+    for m_flag in (0, 1):
+        inp = _inputs(cl, isel, 512, 400, m_flag)
+        out = run_gpu(nb6, **inp)
+        ea, ej, ep = check_vs_oracle(orc, inp, out)
+        print(f"N=65536 m_flag={m_flag}: acc rel max {ea.max():.2e} med {np.median(ea):.2e}; "
+              f"jrk max {ej.max():.2e}; pot max {ep.max():.2e}")
+
+
+def test_regular_nan_input_rejected(nb6):
+    import nb6b200
+    from nb6b200 import ics
+    cl = ics.plummer(256, seed=8)
+    nb6b200.set_abort_on_error(False)
+    try:
+        nb6.gpunb_open(300, 0)
+        nb6.gpunb_send(cl.mass, cl.pos, cl.vel)
+        nb6b200.last_status()
+        x = cl.pos[:4].copy()
+        x[1, 2] = np.nan
+        nb6.gpunb_regf(cl.rs[:4] ** 2, cl.dtr[:4], x, cl.vel[:4], 64, 50, 0)
+        assert nb6b200.last_status() == 3     # NB6_ERR_NAN_INPUT
+        nb6.gpunb_close()
+    finally:
+        nb6b200.set_abort_on_error(True)
