@@ -1,0 +1,421 @@
+#!/usr/bin/env python
+"""Benchmark: regular force + jerk + neighbour list, pair interactions/s at N=1M.
+
+Workload (one "step" = one full regular evaluation, as FPOLY0 does it,
+fpoly0.F:100-206): a King W0=6 cluster of N = 1,048,576 stars with a Kroupa
+IMF and 5% primordial binaries entering as centre-of-mass bodies
+(996,147 bodies), seeded synthetic data.  Every body is an i-particle against
+all bodies as j, issued in calls of 1024 i (util_gpu.F:7,33-60), NNBMAX = 400,
+LMAX = 512, neighbour radii at NNBOPT = 50.
+
+Reported on one JSON line (rank 0):
+  value      pairs/s with inputs resident in HBM (nb6_regf_device_), CUDA
+             events on the library stream, L2 flushed between timed steps;
+  e2e        the same metric through gpunb_send_ + gpunb_regf_ with host
+             buffers, all host<->device copies inside the timed region;
+  roofline   the force kernel against the FP32 FMA pipe: 60 flops per pair
+             (the reference's convention, gpunb.velocity.cu:895) over the
+             kernel's own CUDA-event time, peak = measured FP32 FMA rate;
+  cpu_baseline  the reference's own reg.avx.cpp (oracle/_ref) on the host
+             cores, bounded sample of the same workload;
+  err_vs_fp64   force/jerk/potential error against the FP64 oracle on a
+             sample of i-particles.
+
+--impl reference runs the reference's CPU library (the timed CPU arm).
+Multi-GPU (torchrun, --gpus N): every rank evaluates its own cluster of the
+same size (independent clusters, weak scaling), no data-path collective.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [os.path.join(ROOT, "nbody6ppgpu-beijing_b200"), os.path.join(ROOT, "oracle")]
+os.environ.setdefault("OMP_NUM_THREADS", str(min(32, os.cpu_count() or 1)))
+
+import numpy as np  # noqa: E402
+
+METRIC = "Regular force+jerk+nbr pair interactions/s at N=1M"
+FLOPS_PER_PAIR = 60          # gpunb.velocity.cu:895, reg.avx.cpp:343
+# DRAM bytes per regf_kernel launch (1024 i x 996,147 j), from the ncu capture
+# summarised in profiles/regf_kernel_king1m.md; None until captured.
+NCU_TRAFFIC_PER_LAUNCH = None
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=1048576, help="stars (before folding binaries)")
+    ap.add_argument("--chunk", type=int, default=1024)
+    ap.add_argument("--nnbmax", type=int, default=400)
+    ap.add_argument("--lmax", type=int, default=512)
+    ap.add_argument("--m-flag", type=int, default=0)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--seed", type=int, default=20260)
+    return ap.parse_args()
+
+
+def workload(n: int, seed: int):
+    path = f"/tmp/nb6_king_w6_n{n}_s{seed}.npz"
+    if os.path.exists(path):
+        d = np.load(path)
+        return d["m"], d["x"], d["v"], d["rs"], d["dtr"]
+    from nb6b200 import ics
+    c = ics.king(n, w0=6.0, seed=seed, imf=True, binary_fraction=0.05, nnbopt=50)
+    try:
+        np.savez(path, m=c.mass, x=c.pos, v=c.vel, rs=c.rs, dtr=c.dtr)
+    except OSError:
+        pass
+    return c.mass, c.pos, c.vel, c.rs, c.dtr
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region (the recipe's clocks line)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, pw, reasons = [], [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [q.strip() for q in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax.append(float(p[2]))
+                pw.append(float(p[3]))
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if p[5 + k].lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        load = [s for s, w in zip(sm, pw) if w > 0.3 * max(pw)] or sm
+        return {"sm_mhz": float(np.median(load)), "sm_max_mhz": float(max(smax)),
+                "reasons": sorted(reasons), "samples": len(sm),
+                "power_w_max": float(max(pw))}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_reference_rate(m, x, v, rs, dtr, args, seconds: float, max_calls: int | None = None):
+    """Time the reference's reg.avx.cpp gpunb_regf_ on the host cores over a
+    bounded sample of 1024-i calls of the same workload."""
+    import oracle
+    from nb6b200.abi import ForceLib
+    if not oracle.ref_available("reg"):
+        oracle.build(ref=True)
+    lib = ForceLib(oracle.ref_lib("reg"), "ref-reg-avx")
+    n = m.shape[0]
+    lib.gpunb_open(n + 10, 0)
+    lib.gpunb_send(m, x, v)
+    h2 = rs ** 2 if not args.m_flag else rs ** 2 / m.mean()
+    pairs, t_used, calls = 0, 0.0, 0
+    rng = np.random.default_rng(1)
+    starts = rng.permutation(n // args.chunk) * args.chunk
+    for s in starts:
+        sl = slice(s, min(n, s + args.chunk))
+        t0 = time.perf_counter()
+        lib.gpunb_regf(h2[sl], dtr[sl], x[sl], v[sl], args.lmax, args.nnbmax, args.m_flag)
+        t_used += time.perf_counter() - t0
+        pairs += (sl.stop - sl.start) * n
+        calls += 1
+        if t_used >= seconds or (max_calls and calls >= max_calls):
+            break
+    lib.gpunb_close()
+    threads = int(os.environ.get("OMP_NUM_THREADS", "1"))
+    return pairs / t_used, threads, calls, t_used
+
+
+def run_reference(args):
+    world, rank, _ = dist_setup(args)
+    if rank != 0:
+        return 0
+    m, x, v, rs, dtr = workload(args.n, args.seed)
+    n = m.shape[0]
+    # each step: a bounded sample of the workload (a few seconds of CPU)
+    _, threads, _, t1 = cpu_reference_rate(m, x, v, rs, dtr, args, seconds=0.0, max_calls=1)
+    calls = max(1, int(2.0 / max(t1, 1e-3)))
+    for _ in range(args.warmup):
+        cpu_reference_rate(m, x, v, rs, dtr, args, seconds=1e9, max_calls=1)
+    rates, times = [], []
+    for _ in range(args.steps):
+        r, threads, c, t = cpu_reference_rate(m, x, v, rs, dtr, args, seconds=1e9, max_calls=calls)
+        rates.append(r)
+        times.append(t)
+    value = float(np.sum([r * t for r, t in zip(rates, times)]) / np.sum(times))
+    sample = f"{calls} calls x {args.chunk} i x {n} j per step (reg.avx.cpp gpunb_regf_)"
+    out = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "pairs/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * float(np.mean(times)), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic King W0=6, Kroupa IMF, 5% binaries as c.m. bodies",
+        "config": {"workload": f"king-w0=6 N={args.n} ({n} c.m. bodies), 1024-i gpunb_regf calls",
+                   "n_bodies": n, "chunk": args.chunk, "nnbmax": args.nnbmax,
+                   "lmax": args.lmax, "m_flag": args.m_flag},
+        "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": threads,
+                         "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    world, rank, local = dist_setup(args)
+    os.environ["NB_GPU_DEVICE"] = str(local)
+    import torch
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+
+    import nb6b200
+    lib = nb6b200.load()
+    raw = lib.lib
+    m, x, v, rs, dtr = workload(args.n, args.seed + 7919 * rank)
+    n = m.shape[0]
+    h2 = rs ** 2 if not args.m_flag else rs ** 2 / m.mean()
+    lib.gpunb_open(n + 10, 0)
+    lib.gpunb_send(m, x, v)
+    stream = torch.cuda.ExternalStream(raw.nb6_stream_())
+    dev = torch.device("cuda", local)
+    d_h2 = torch.tensor(h2, dtype=torch.float64, device=dev)
+    d_dtr = torch.tensor(dtr, dtype=torch.float64, device=dev)
+    d_x = torch.tensor(x, dtype=torch.float64, device=dev).contiguous()
+    d_v = torch.tensor(v, dtype=torch.float64, device=dev).contiguous()
+    torch.cuda.synchronize()
+    chunks = [(s, min(n, s + args.chunk)) for s in range(0, n, args.chunk)]
+    ci = C.c_int
+    lmax, nnbmax, mflag = ci(args.lmax), ci(args.nnbmax), ci(args.m_flag)
+
+    def dev_step():
+        for s, e in chunks:
+            raw.nb6_regf_device_(C.byref(ci(e - s)), C.c_void_p(d_h2.data_ptr() + 8 * s),
+                                 C.c_void_p(d_dtr.data_ptr() + 8 * s),
+                                 C.c_void_p(d_x.data_ptr() + 24 * s),
+                                 C.c_void_p(d_v.data_ptr() + 24 * s),
+                                 C.byref(lmax), C.byref(nnbmax), C.byref(mflag))
+
+    flush_buf = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def flush_l2():
+        with torch.cuda.stream(stream):
+            flush_buf.fill_(1.0)
+        stream.synchronize()
+
+    def barrier():
+        if pg is not None:
+            pg.barrier()
+        torch.cuda.synchronize()
+
+    # warm-up
+    for _ in range(args.warmup):
+        dev_step()
+    raw.nb6_sync_()
+    peak_tf = float(raw.nb6_fp32_peak_probe_(C.byref(ci(20000))))
+
+    # kernel-only launch time of the force kernel (live CUDA events on the
+    # library stream around regf_kernel alone), over a sample of full calls
+    kms = []
+    for s, e in chunks[: min(64, len(chunks))]:
+        raw.nb6_regf_device_(C.byref(ci(e - s)), C.c_void_p(d_h2.data_ptr() + 8 * s),
+                             C.c_void_p(d_dtr.data_ptr() + 8 * s),
+                             C.c_void_p(d_x.data_ptr() + 24 * s),
+                             C.c_void_p(d_v.data_ptr() + 24 * s),
+                             C.byref(lmax), C.byref(nnbmax), C.byref(mflag))
+        kms.append(float(raw.nb6_regf_last_kernel_ms_()))
+    geom = (ci * 3)()
+    raw.nb6_regf_last_geometry_(geom)
+    kernel_ms = float(np.median(kms))
+
+    # timed region: K steps, L2 flushed between steps, events on the library stream
+    clocks = Clocks(local)
+    step_ms = []
+    clocks.start()
+    for _ in range(args.steps):
+        flush_l2()
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        dev_step()
+        e1.record(stream)
+        e1.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+    barrier()
+    clk = clocks.stop()
+    ms = float(np.mean(step_ms))
+    total_ms = float(np.sum(step_ms))
+    if pg is not None:
+        t = torch.tensor([total_ms], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        total_ms = float(t.item())
+    pairs_step = float(n) * float(n)
+    value = world * pairs_step * args.steps / (total_ms * 1e-3)
+
+    # e2e through the C ABI with host buffers: gpunb_send_ + gpunb_regf_ calls
+    e2e = None
+    if not args.no_e2e:
+        lst = np.zeros((args.chunk, args.lmax), dtype=np.int32)
+        acc = np.zeros((args.chunk, 3))
+        jrk = np.zeros((args.chunk, 3))
+        pot = np.zeros(args.chunk)
+        dp = C.POINTER(C.c_double)
+        ip = C.POINTER(C.c_int)
+
+        def e2e_step():
+            lib.gpunb_send(m, x, v)
+            for s, e in chunks:
+                raw.gpunb_regf_(C.byref(ci(e - s)), h2[s:e].ctypes.data_as(dp),
+                                dtr[s:e].ctypes.data_as(dp), x[s:e].ctypes.data_as(dp),
+                                v[s:e].ctypes.data_as(dp), acc.ctypes.data_as(dp),
+                                jrk.ctypes.data_as(dp), pot.ctypes.data_as(dp), C.byref(lmax),
+                                C.byref(nnbmax), lst.ctypes.data_as(ip), C.byref(mflag))
+        e2e_step()
+        barrier()
+        t0 = time.perf_counter()
+        e2e_steps = max(1, min(args.steps, 2))
+        for _ in range(e2e_steps):
+            e2e_step()
+        e2e_s = (time.perf_counter() - t0) / e2e_steps
+        if pg is not None:
+            t = torch.tensor([e2e_s], device=dev)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        W = min(args.nnbmax, args.lmax - 1) + 1
+        e2e = {"value": world * pairs_step / e2e_s, "unit": "pairs/s",
+               "h2d_bytes_per_step": int(n * (8 + 24 + 24) + n * 64),
+               "d2h_bytes_per_step": int(n * 64 + n * W * 4),
+               "steps": e2e_steps, "timing": "wall clock around synchronous ABI calls"}
+
+    # accuracy against the FP64 oracle on a sample of i (rank 0)
+    err = None
+    cpu = None
+    if rank == 0:
+        import oracle
+        rng = np.random.default_rng(5)
+        isel = np.sort(rng.choice(n, 64, replace=False))
+        a_g, j_g, p_g, l_g = lib.gpunb_regf(h2[isel], dtr[isel], x[isel], v[isel], args.lmax,
+                                            args.nnbmax, args.m_flag)
+        a_o, j_o, p_o, l_o = oracle.regf(m, x, v, h2[isel], dtr[isel], x[isel], v[isel],
+                                         args.lmax, args.nnbmax, args.m_flag)
+        ok = l_o[:, 0] >= 0
+
+        def rel(a, b):
+            if a.ndim == 1:
+                return np.abs(a - b) / np.abs(b)
+            return np.sqrt(((a - b) ** 2).sum(1) / (b ** 2).sum(1))
+        err = {"sample_i": int(len(isel)), "acc_rel_max": float(rel(a_g, a_o)[ok].max()),
+               "jrk_rel_max": float(rel(j_g, j_o)[ok].max()),
+               "pot_rel_max": float(rel(p_g, p_o)[ok].max()),
+               "lists_identical": bool(np.array_equal(l_g, l_o)),
+               "nnb_mean": float(l_o[ok, 0].mean())}
+        if not args.no_cpu_baseline:
+            rate, threads, calls, t_used = cpu_reference_rate(m, x, v, rs, dtr, args,
+                                                              seconds=args.cpu_seconds)
+            cpu = {"value": rate, "unit": "pairs/s", "cores": threads, "kind": "reference",
+                   "sample": f"{calls} calls x {args.chunk} i x {n} j of the same workload, "
+                             f"reg.avx.cpp gpunb_regf_ (oracle/_ref), {t_used:.1f} s"}
+
+    lib.gpunb_close()
+    achieved = FLOPS_PER_PAIR * args.chunk * n / (kernel_ms * 1e-3) / 1e12
+    nominal = 2 * 128 * 148 * (clk.get("sm_max_mhz") or 1965.0) * 1e6 / 1e12
+    roof = {"bound": "fp32", "achieved": achieved, "peak": peak_tf, "unit": "TFLOP/s",
+            "frac": achieved / peak_tf if peak_tf else None,
+            "traffic": NCU_TRAFFIC_PER_LAUNCH,
+            "kernel": "regf_kernel", "kernel_ms_per_launch": kernel_ms,
+            "flops_per_launch": FLOPS_PER_PAIR * args.chunk * n,
+            "algorithmic_bytes_per_launch": 48 * n + 64 * args.chunk,
+            "peak_source": "measured: FFMA probe kernel in the library, same process "
+                           "(MEASURED_PEAKS.json carries no FP32 figure)",
+            "frac_of_nominal_fp32": achieved / nominal,
+            "geometry": {"i_per_thread": geom[0], "i_tiles": geom[1], "j_slices": geom[2]}}
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic King W0=6 (seeded), Kroupa IMF 0.08-100 Msun, 5% binaries "
+                    "as c.m. bodies, Henon units",
+            "config": {"workload": f"king-w0=6 N={args.n} ({n} c.m. bodies), full regular "
+                                   f"evaluation in {args.chunk}-i calls",
+                       "n_bodies": n, "chunk": args.chunk, "calls_per_step": len(chunks),
+                       "nnbopt": 50, "nnbmax": args.nnbmax, "lmax": args.lmax,
+                       "m_flag": args.m_flag, "parallelism": f"replicas x{world}",
+                       "l2": "flushed (256 MiB write) between timed steps"},
+            "gpu_launches": int(args.steps * len(chunks) * 2),
+            "clocks": clk, "roofline": roof, "e2e": e2e, "cpu_baseline": cpu,
+            "err_vs_fp64": err,
+            "pct_fp32_peak": 100.0 * FLOPS_PER_PAIR * pairs_step / (ms * 1e-3) / 1e12 / peak_tf,
+        }
+        print(json.dumps(out), flush=True)
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

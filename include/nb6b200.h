@@ -1,0 +1,158 @@
+/*
+ * nb6b200.h -- C ABI of libnb6b200.so, the sm_100a (B200) force hot path of
+ * Nbody6++GPU.
+ *
+ * The first three groups are drop-in replacements for the reference's
+ * Fortran-callable libraries: every argument by pointer, Fortran name
+ * mangling (lower case, trailing underscore), Fortran X(3,N) arrays passed as
+ * C double[N][3].  A Fortran build links this library in place of
+ * gpunb.velocity.o / gpunb.gpu.o / gpupot.gpu.o / irr.avx.o; no caller change
+ * is needed.  Error behaviour follows the reference (bad input aborts) unless
+ * nb6_set_abort_on_error_(0) switches to record-and-return.
+ *
+ * The last group (nb6_*) are extensions with no reference counterpart.
+ */
+#ifndef NB6B200_H
+#define NB6B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Regular force + jerk + potential + neighbour list                         */
+/* replaces gpunb.velocity.cu:905-940 (and gpunb.gpu.cu:820-849,            */
+/* reg.avx.cpp:353-385)                                                      */
+/* ------------------------------------------------------------------------ */
+
+/* Pick the device: GPU_LIST (first id), NB_GPU_DEVICE, else irank % ngpu.
+ * replaces GPUNB_devinit, gpunb.velocity.cu:575-627,906-908 */
+void gpunb_devinit_(int *irank);
+
+/* Allocate for up to nbmax j-particles.  gpunb.velocity.cu:629-667,909-911 */
+void gpunb_open_(int *nbmax, int *irank);
+
+/* Release device buffers.  gpunb.velocity.cu:669-702,912-914 */
+void gpunb_close_(void);
+
+/* Copy nj j-particles (mass, position, velocity) to the device; the caller
+ * may overwrite its arrays on return.  gpunb.velocity.cu:704-730,915-921 */
+void gpunb_send_(int *nj, double *mj, double (*xj)[3], double (*vj)[3]);
+
+/* For ni i-particles against the last-sent j set: regular acceleration,
+ * jerk (adot) and potential (positive, sum m/r) over non-neighbours, and the
+ * neighbour list list[i*lmax + 0] = nnb, list[i*lmax + 1..nnb] = 0-based j
+ * ascending, self included.  Neighbour: min(r2, |dx + dtr*dv|^2) < h2
+ * (m_flag == 0) or < m_j*h2 (m_flag != 0).  If nnb > nnbmax (or lmax-1):
+ * list[i*lmax] = -nnb and no ids are written.
+ * gpunb.velocity.cu:732-881,922-936 */
+void gpunb_regf_(int *ni, double *h2, double *dtr, double (*xi)[3], double (*vi)[3],
+                 double (*acc)[3], double (*jrk)[3], double *pot, int *lmax, int *nnbmax,
+                 int *list, int *m_flag);
+
+/* Print the "[R.x GPU Reg.F ] ..." line (60 flops per pair) and reset the
+ * counters.  gpunb.velocity.cu:883-903,937-939 */
+void gpunb_profile_(int *irank);
+
+/* ------------------------------------------------------------------------ */
+/* N^2 potential                                                             */
+/* replaces gpupot.gpu.cu:116-127 (pot.avx.cpp:354-365)                     */
+/* ------------------------------------------------------------------------ */
+
+/* pot[k] = sum_{j: r2 > 0} m_j / r_ij for i = istart-1+k, k in [0, ni);
+ * istart is 1-based.  gpupot.gpu.cu:61-114 */
+void gpupot_(int *irank, int *istart, int *ni, int *n, double *m, double (*x)[3],
+             double *pot);
+
+/* ------------------------------------------------------------------------ */
+/* Irregular force + jerk + nearest neighbour over resident lists           */
+/* replaces irr.avx.cpp:568-606 (irr.sse.cpp)                               */
+/* ------------------------------------------------------------------------ */
+
+/* Allocate state for nmax particles, lists of up to lmax-1 ids.
+ * irr.avx.cpp:368-405,569-571 */
+void irr_simd_open_(int *nmax, int *lmax, int *rank);
+
+/* irr.avx.cpp:424-438,572-574 */
+void irr_simd_close_(int *rank);
+
+/* Print "[R.x GPU Irr.F ] ..." and reset counters.  irr.avx.cpp:407-422,575-577 */
+void irr_simd_profile_(int *rank);
+
+/* Set particle addr (1-based): position, velocity, acc2 = F = a/2,
+ * jrk6 = FDOT = adot/6, mass, time of last step.  irr.avx.cpp:440-450,579-589 */
+void irr_simd_set_jp_(int *addr, double pos[3], double vel[3], double acc2[3], double jrk6[3],
+                      double *mass, double *time);
+
+/* Set the neighbour list of addr: nblist[0] = nnb, nblist[1..nnb] = 1-based
+ * ids (Fortran LIST(1,I)).  irr.avx.cpp:452-497,590-595 */
+void irr_simd_set_list_(int *addr, int *nblist);
+
+/* For ni particles addr[] (1-based): predict them and their neighbours to ti,
+ * sum acceleration and jerk over the list; nnbid = 1-based id of the nearest
+ * neighbour (-1 for an empty list).  irr.avx.cpp:499-565,596-605 */
+void irr_simd_firr_vec_(double *ti, int *ni, int addr[], double acc[][3], double jrk[][3],
+                        int nnbid[]);
+
+/* NBODY6/GPU names of the same library, the calls commented out in
+ * fpoly0.F:42,70,202,383 and intgrt.F:1329.  gpuirr_open_(nmax, lmax) and
+ * gpuirr_close_() use rank 0. */
+void gpuirr_open_(int *nmax, int *lmax);
+void gpuirr_close_(void);
+void gpuirr_set_jp_(int *addr, double pos[3], double vel[3], double acc2[3], double jrk6[3],
+                    double *mass, double *time);
+void gpuirr_set_list_(int *addr, int *nblist);
+
+/* ------------------------------------------------------------------------ */
+/* Extensions (no reference counterpart)                                     */
+/* ------------------------------------------------------------------------ */
+
+/* Error policy: flag != 0 aborts on bad input (the reference's behaviour,
+ * default), 0 records the code and returns.  nb6_last_status_ returns and
+ * clears the first recorded code (0 = ok, 2 bad argument, 3 NaN input,
+ * 4 CUDA error, 5 not open, 6 too large, 1 device wait timeout). */
+void nb6_set_abort_on_error_(int *flag);
+int nb6_last_status_(void);
+int nb6_device_(void);
+
+/* gpunb_regf_ on DEVICE arrays (same layout), results kept on the device:
+ * nb6_regf_outputs_ returns outf [ni][8] = (acc3, jrk3, pot, 0) and
+ * outl [ni][W], W = min(nnbmax, lmax-1) + 1.  Enqueued, no sync. */
+void nb6_regf_device_(int *ni, const double *d_h2, const double *d_dtr, const double *d_x,
+                      const double *d_v, int *lmax, int *nnbmax, int *m_flag);
+void nb6_regf_outputs_(double **d_outf, int **d_outl);
+float nb6_regf_last_kernel_ms_(void);
+void nb6_regf_last_geometry_(int *geom);
+void nb6_regf_tune_(int *ni_per_thread, int *nslices);
+
+/* Synchronise the library stream (and check the device status); the stream
+ * handle itself for callers that record events on it. */
+void nb6_sync_(void);
+void *nb6_stream_(void);
+
+/* gpupot_ on DEVICE arrays; *d_out receives the device result pointer. */
+void nb6_pot_device_(int *istart, int *ni, int *n, const double *d_m, const double *d_x,
+                     double **d_out);
+float nb6_pot_last_kernel_ms_(void);
+
+/* Device-resident Hermite state and predictor (xbpredall.F:48-62 on the GPU).
+ * nb6_predict_send_ predicts bodies [ifirst, ifirst+nn) and packs them as the
+ * gpunb j set: XBPREDALL + GPUNB_SEND without host traffic. */
+void nb6_state_open_(int *nmax);
+void nb6_state_close_(void);
+void nb6_state_set_(int *n, double *body, double *t0, double (*x0)[3], double (*x0dot)[3],
+                    double (*f)[3], double (*fdot)[3]);
+void nb6_state_update_(int *nu, int *idx, double *body, double *t0, double (*x0)[3],
+                       double (*x0dot)[3], double (*f)[3], double (*fdot)[3]);
+void nb6_predict_(double *time, double (*x)[3], double (*xdot)[3]);
+void nb6_predict_device_(double *time, double **d_x, double **d_xdot);
+void nb6_predict_send_(double *time, int *ifirst, int *nn);
+float nb6_predict_last_kernel_ms_(void);
+
+/* Measured FP32 FMA throughput (TFLOP/s) of the current GPU. */
+double nb6_fp32_peak_probe_(int *iters);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NB6B200_H */

@@ -10,9 +10,10 @@
 // they only write into pinned host staging (a later call for the same
 // particle overwrites its staged entry); irr_simd_firr_vec_ uploads what is
 // staged, scatters it, and runs one warp per active particle: lanes walk the
-// list, predict each j to ti in FP64 (jpred_int.f:16-25), form the
-// differences in FP64, do the pair math in FP32 with rsqrt + one Newton step
-// and sum in FP64; the nearest neighbour is the minimum FP64 r2 with the
+// list, predict each j to ti in FP64 (jpred_int.f:16-25) and do the pair
+// math and the sums in FP64 -- the walk is bound by the 128-byte record
+// gathers, so FP64 costs nothing here and is more accurate than the
+// reference's FP32 (irr.avx.cpp:303-332); the nearest neighbour is the minimum FP64 r2 with the
 // smallest index on ties (irr.avx.cpp:320-323 packs (r2, idx) the same way).
 #include "nb6_common.cuh"
 
@@ -79,21 +80,19 @@ __global__ void __launch_bounds__(IRR_WARPS * 32)
             rmin = r2d;
             jmin = j;
         }
-        const float dx = (float)dxd, dy = (float)dyd, dz = (float)dzd;
-        const float dvx = (float)(vj[0] - vi[0]);
-        const float dvy = (float)(vj[1] - vi[1]);
-        const float dvz = (float)(vj[2] - vi[2]);
-        const float r2 = (float)r2d;
-        const float y = rsqrt2_nr(r2);             // 2/r
-        const float y2 = y * y;
-        const float my3 = (float)rj.m * y * y2;    // 8 m / r^3
-        const float al = (y2 * -0.75f) * fmaf(dz, dvz, fmaf(dy, dvy, dx * dvx));
-        ax += (double)(my3 * dx);
-        ay += (double)(my3 * dy);
-        az += (double)(my3 * dz);
-        jx += (double)(my3 * fmaf(al, dx, dvx));
-        jy += (double)(my3 * fmaf(al, dy, dvy));
-        jz += (double)(my3 * fmaf(al, dz, dvz));
+        // The list walk is bound by the record gathers, not by arithmetic,
+        // so the pair math stays in FP64 (nbint.F:143-158).
+        const double dvx = vj[0] - vi[0], dvy = vj[1] - vi[1], dvz = vj[2] - vi[2];
+        const double rinv = rsqrt(r2d);
+        const double rinv2 = rinv * rinv;
+        const double mr3 = rj.m * rinv * rinv2;
+        const double al = -3.0 * (dxd * dvx + dyd * dvy + dzd * dvz) * rinv2;
+        ax += mr3 * dxd;
+        ay += mr3 * dyd;
+        az += mr3 * dzd;
+        jx += mr3 * (dvx + al * dxd);
+        jy += mr3 * (dvy + al * dyd);
+        jz += mr3 * (dvz + al * dzd);
     }
     ax = warp_sum_d(ax);
     ay = warp_sum_d(ay);
@@ -112,12 +111,12 @@ __global__ void __launch_bounds__(IRR_WARPS * 32)
     }
     if (lane == 0) {
         double *o = out + (size_t)k * 6;
-        o[0] = ax * 0.125;
-        o[1] = ay * 0.125;
-        o[2] = az * 0.125;
-        o[3] = jx * 0.125;
-        o[4] = jy * 0.125;
-        o[5] = jz * 0.125;
+        o[0] = ax;
+        o[1] = ay;
+        o[2] = az;
+        o[3] = jx;
+        o[4] = jy;
+        o[5] = jz;
         outid[k] = (nnb > 0 && jmin != 0x7fffffff) ? jmin + 1 : -1;
     }
 }
@@ -154,6 +153,7 @@ struct IrrState {
     HostBuf<int> hstage_addr, hstage_list, hstage_off, haddr, hnnbid;
     HostBuf<double> hout;
     std::vector<int> jp_slot, list_slot;  // staged slot per particle, -1 if none
+    std::vector<int> nnb_host;            // list lengths, for the profile counters
     int njp = 0, nlist = 0;
     size_t list_words = 0;
     double time_grav = 0;
@@ -180,6 +180,7 @@ void irr_open_impl(int nmax, int lmax, int rank) {
     NB6_CUDA_CHECK(cudaMemsetAsync(I.lists.ptr, 0, sizeof(int) * (size_t)nmax * lmax, nb6_stream()));
     I.jp_slot.assign(nmax, -1);
     I.list_slot.assign(nmax, -1);
+    I.nnb_host.assign(nmax, 0);
     I.njp = I.nlist = 0;
     I.list_words = 0;
     I.time_grav = 0;
@@ -291,6 +292,7 @@ void irr_set_list_impl(int a, const int *nblist) {
     e[1] = nnb;
     for (int l = 0; l < nnb; ++l) e[2 + l] = nblist[1 + l] - 1;
     I.list_slot[a] = (int)I.list_words;
+    I.nnb_host[a] = nnb;
     I.list_words = need;
     I.nlist++;
 }
@@ -377,6 +379,8 @@ void irr_firr_vec_impl(double ti, int ni, const int *addr, double (*acc)[3], dou
     NB6_CUDA_CHECK(cudaStreamSynchronize(st));
     if (nb6_check_dev_status() != 0) return;
     unsigned long long inter = 0;
+    for (int k = 0; k < ni; ++k) inter += (unsigned long long)I.nnb_host[addr[k] - 1];
+    I.num_inter += inter;
     for (int k = 0; k < ni; ++k) {
         const double *o = I.hout.ptr + (size_t)k * 6;
         acc[k][0] = o[0];
@@ -387,7 +391,6 @@ void irr_firr_vec_impl(double ti, int ni, const int *addr, double (*acc)[3], dou
         jrk[k][2] = o[5];
         nnbid[k] = I.hnnbid.ptr[k];
     }
-    (void)inter;
     I.time_grav += nb6_wtime() - t0;
     I.num_fcall++;
     I.num_steps += ni;

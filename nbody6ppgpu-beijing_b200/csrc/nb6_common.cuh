@@ -192,7 +192,6 @@ template <class T> struct HostBuf {
     void release();
 };
 
-#ifndef __CUDA_ARCH__
 template <class T> void DevBuf<T>::reserve(size_t n) {
     if (n <= cap) return;
     if (ptr) NB6_CUDA_CHECK(cudaFree(ptr));
@@ -217,4 +216,3 @@ template <class T> void HostBuf<T>::release() {
     ptr = nullptr;
     cap = 0;
 }
-#endif

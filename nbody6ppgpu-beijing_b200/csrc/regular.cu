@@ -39,6 +39,18 @@ constexpr float CAND_SLACK = 1.01f;
 constexpr unsigned long long WAIT_NS = 2000000000ull;  // 2 s per wait
 constexpr int FIN_WARPS = 4;
 
+// j unroll of the hot loop: large enough for ILP, small enough that the
+// loop body stays resident in the instruction cache.
+#ifndef UNROLL_J
+#define UNROLL_J 8
+#endif
+constexpr int kUnrollJ = UNROLL_J;
+// The rare candidate path is kept out of line by default so that it does not
+// inflate the register allocation of the hot loop.
+#ifndef FLUSH_INLINE
+#define FLUSH_INLINE __noinline__
+#endif
+
 struct RegArgs {
     const float4 *__restrict__ posH;  // (xH, yH, zH, m)
     const float4 *__restrict__ posL;  // (xL, yL, zL, 0)
@@ -69,25 +81,43 @@ struct Sums {
 
 NB6_DEV void zero(Sums &s) { s.ax = s.ay = s.az = s.jx = s.jy = s.jz = s.po = 0.f; }
 
+// The FP32 candidate test, shared verbatim by the hot loop and the rare path
+// so both always classify a pair the same way (explicit fmaf/__fmul_rn: no
+// contraction freedom).  Candidate: min(r2, |dx + dt dv|^2) < 1.01 crit.
+struct PairGeom {
+    float dx, dy, dz, dvx, dvy, dvz, r2;
+    bool cand;
+};
+
+template <bool MFLAG>
+NB6_DEV PairGeom reg_geom(const IPart &ip, const float4 &a, const float4 &b, const float4 &c) {
+    PairGeom g;
+    g.dx = (a.x - ip.xh) + (b.x - ip.xl);
+    g.dy = (a.y - ip.yh) + (b.y - ip.yl);
+    g.dz = (a.z - ip.zh) + (b.z - ip.zl);
+    g.dvx = c.x - ip.vx;
+    g.dvy = c.y - ip.vy;
+    g.dvz = c.z - ip.vz;
+    g.r2 = fmaf(g.dz, g.dz, fmaf(g.dy, g.dy, __fmul_rn(g.dx, g.dx)));
+    const float px = fmaf(ip.dt, g.dvx, g.dx);
+    const float py = fmaf(ip.dt, g.dvy, g.dy);
+    const float pz = fmaf(ip.dt, g.dvz, g.dz);
+    const float rp2 = fmaf(pz, pz, fmaf(py, py, __fmul_rn(px, px)));
+    const float crit = MFLAG ? __fmul_rn(a.w, ip.h2c) : ip.h2c;
+    g.cand = fminf(g.r2, rp2) < crit;
+    return g;
+}
+
 // Pair interaction in FP32; returns whether j is a neighbour candidate.
 // Sums are kept scaled: pot x2, acc and jerk x8 (see rsqrt2_nr).
 template <bool MFLAG>
 NB6_DEV bool reg_pair(const IPart &ip, const float4 &a, const float4 &b, const float4 &c,
                       Sums &s) {
-    const float dx = (a.x - ip.xh) + (b.x - ip.xl);
-    const float dy = (a.y - ip.yh) + (b.y - ip.yl);
-    const float dz = (a.z - ip.zh) + (b.z - ip.zl);
-    const float dvx = c.x - ip.vx;
-    const float dvy = c.y - ip.vy;
-    const float dvz = c.z - ip.vz;
-    const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+    const PairGeom g = reg_geom<MFLAG>(ip, a, b, c);
+    const float dx = g.dx, dy = g.dy, dz = g.dz, dvx = g.dvx, dvy = g.dvy, dvz = g.dvz;
+    const float r2 = g.r2;
+    const bool cand = g.cand;
     const float rv = fmaf(dz, dvz, fmaf(dy, dvy, dx * dvx));
-    const float px = fmaf(ip.dt, dvx, dx);
-    const float py = fmaf(ip.dt, dvy, dy);
-    const float pz = fmaf(ip.dt, dvz, dz);
-    const float rp2 = fmaf(pz, pz, fmaf(py, py, px * px));
-    const float crit = MFLAG ? a.w * ip.h2c : ip.h2c;
-    const bool cand = fminf(r2, rp2) < crit;
     float y = rsqrt2_nr(r2);
     y = cand ? 0.0f : y;
     const float y2 = y * y;
@@ -104,18 +134,18 @@ NB6_DEV bool reg_pair(const IPart &ip, const float4 &a, const float4 &b, const f
     return cand;
 }
 
-// Exact FP64 decision for the candidates of one 32-j group (rare path).
-// Operation order matches the FP64 rule of regint.f:41-65 with the strict
-// "<" of gpunb.velocity.cu:188,236; no FMA contraction.
+// Rare path for one i and one 32-j group that held at least one candidate:
+// re-derive the candidates with the same FP32 test, then decide each exactly
+// in FP64.  Operation order matches the FP64 rule of regint.f:41-65 with the
+// strict "<" of gpunb.velocity.cu:188,236; no FMA contraction.
 template <bool MFLAG>
-__device__ __forceinline__ void reg_flush(const RegArgs &a, int i, uint32_t mask, int jbase,
-                                       Sums &s) {
+__device__ FLUSH_INLINE Sums reg_flush(const RegArgs &a, const IPart ip, int i, const float4 *A,
+                                       const float4 *B, const float4 *Cv, int jbase, Sums s) {
     const double xi0 = a.ix[3 * i], xi1 = a.ix[3 * i + 1], xi2 = a.ix[3 * i + 2];
     const double vi0 = a.iv[3 * i], vi1 = a.iv[3 * i + 1], vi2 = a.iv[3 * i + 2];
     const double h2 = a.ih2[i], dt = a.idtr[i];
-    while (mask) {
-        const int b = __ffs(mask) - 1;
-        mask &= mask - 1;
+    for (int b = 0; b < 32; ++b) {
+        if (!reg_geom<MFLAG>(ip, A[b], B[b], Cv[b]).cand) continue;
         const int j = jbase + b;
         if (j >= a.nj) continue;  // padding slots are never neighbours
         const double dx = __dsub_rn(a.jx[3 * j], xi0);
@@ -153,6 +183,7 @@ __device__ __forceinline__ void reg_flush(const RegArgs &a, int i, uint32_t mask
             s.jz += (float)(8.0 * mr3 * (dvz + al * dz));
         }
     }
+    return s;
 }
 
 NB6_DEV void issue_tile(const RegArgs &a, float4 (*stage)[JT], uint64_t *bar, int tile) {
@@ -234,21 +265,21 @@ __global__ void __launch_bounds__(NT) regf_kernel(const RegArgs a) {
         const int jt0 = (t_begin + t) * JT;
 #pragma unroll 1
         for (int g = 0; g < JT / 32; ++g) {
-            uint32_t m[NI];
+            bool anyc[NI];
 #pragma unroll
-            for (int k = 0; k < NI; ++k) m[k] = 0u;
-#pragma unroll
+            for (int k = 0; k < NI; ++k) anyc[k] = false;
+            const float4 *Ag = A + g * 32, *Bg = B + g * 32, *Cg = C + g * 32;
+#pragma unroll kUnrollJ
             for (int q = 0; q < 32; ++q) {
-                const float4 pa = A[g * 32 + q];
-                const float4 pb = B[g * 32 + q];
-                const float4 pc = C[g * 32 + q];
+                const float4 pa = Ag[q];
+                const float4 pb = Bg[q];
+                const float4 pc = Cg[q];
 #pragma unroll
-                for (int k = 0; k < NI; ++k)
-                    if (reg_pair<MFLAG>(ip[k], pa, pb, pc, s[k])) m[k] |= (1u << q);
+                for (int k = 0; k < NI; ++k) anyc[k] |= reg_pair<MFLAG>(ip[k], pa, pb, pc, s[k]);
             }
 #pragma unroll
             for (int k = 0; k < NI; ++k)
-                if (m[k]) reg_flush<MFLAG>(a, ii[k], m[k], jt0 + g * 32, s[k]);
+                if (anyc[k]) s[k] = reg_flush<MFLAG>(a, ip[k], ii[k], Ag, Bg, Cg, jt0 + g * 32, s[k]);
         }
 #pragma unroll
         for (int k = 0; k < NI; ++k) {
@@ -403,6 +434,7 @@ struct RegState {
     float last_kernel_ms = 0.f;
     int forced_ni_per_thread = 0;   // 0 = autotune
     int forced_slices = 0;
+    int last_geometry[3] = {0, 0, 0};  // NI, i-tiles, j-slices of the last launch
 };
 RegState R;
 
@@ -507,6 +539,13 @@ static void regf_device(int ni, const double *d_h2, const double *d_dtr, const d
     a.lcap = std::max(cap, 1);
     a.status = nb6_dev_status();
 
+    if (!R.ev0) {
+        NB6_CUDA_CHECK(cudaEventCreate(&R.ev0));
+        NB6_CUDA_CHECK(cudaEventCreate(&R.ev1));
+    }
+    // kernel-only timing of the main force kernel (read by
+    // nb6_regf_last_kernel_ms_ after the stream has drained)
+    NB6_CUDA_CHECK(cudaEventRecord(R.ev0, st));
     if (mflag) {
         if (NI == 1) launch_regf<1, true>(a, nitile, st);
         else if (NI == 2) launch_regf<2, true>(a, nitile, st);
@@ -517,6 +556,10 @@ static void regf_device(int ni, const double *d_h2, const double *d_dtr, const d
         else launch_regf<4, false>(a, nitile, st);
     }
     NB6_CUDA_CHECK(cudaGetLastError());
+    NB6_CUDA_CHECK(cudaEventRecord(R.ev1, st));
+    R.last_geometry[0] = NI;
+    R.last_geometry[1] = nitile;
+    R.last_geometry[2] = nslices;
 
     int pmax = 32;
     while (pmax < cap) pmax <<= 1;
@@ -628,6 +671,46 @@ void gpunb_send_(int *nj, double *mj, double (*xj)[3], double (*vj)[3]) {
     R.time_send += nb6_wtime();
 }
 
+}  // extern "C"
+
+// Internal hook for the device-resident predictor (predictor.cu): a send whose
+// j data are produced on the device.  Sizes the j buffers for n bodies, makes
+// them current, and hands out the arrays to fill (FP64 m, x, v for the exact
+// neighbour recheck and the float4 tiles, padded to *npad with far massless
+// bodies by the caller's kernel).
+bool regular_bind_j(int n, double **jm, double **jx, double **jv, float4 **posH, float4 **posL,
+                    float4 **vel, int *npad) {
+    if (!R.open) {
+        nb6_fatal(NB6_ERR_NOT_OPEN);
+        return false;
+    }
+    if (n < 0 || n > R.nbodymax) {
+        fprintf(stderr, "nb6_predict_send: n=%d outside [0, nbmax=%d]\n", n, R.nbodymax);
+        nb6_fatal(NB6_ERR_TOO_LARGE);
+        return false;
+    }
+    R.isend++;
+    R.nj = n;
+    R.ntile = std::max(1, (n + JT - 1) / JT);
+    const size_t np = (size_t)R.ntile * JT;
+    R.posH.reserve(np);
+    R.posL.reserve(np);
+    R.vel.reserve(np);
+    R.jm.reserve(np);
+    R.jx.reserve(3 * np);
+    R.jv.reserve(3 * np);
+    *jm = R.jm.ptr;
+    *jx = R.jx.ptr;
+    *jv = R.jv.ptr;
+    *posH = R.posH.ptr;
+    *posL = R.posL.ptr;
+    *vel = R.vel.ptr;
+    *npad = (int)np;
+    return true;
+}
+
+extern "C" {
+
 void gpunb_regf_(int *ni_, double *h2, double *dtr, double (*xi)[3], double (*vi)[3],
                  double (*acc)[3], double (*jrk)[3], double *pot, int *lmax_, int *nnbmax_,
                  int *list, int *m_flag) {
@@ -669,9 +752,7 @@ void gpunb_regf_(int *ni_, double *h2, double *dtr, double (*xi)[3], double (*vi
     const double *d = R.iin.ptr;
 
     int W = 0;
-    NB6_CUDA_CHECK(cudaEventRecord(R.ev0, st));
     regf_device(ni, d, d + ni, d + 2 * (size_t)ni, d + 5 * (size_t)ni, lmax, nnbmax, *m_flag, st, W);
-    NB6_CUDA_CHECK(cudaEventRecord(R.ev1, st));
 
     R.houtf.reserve((size_t)ni * 8);
     R.houtl.reserve((size_t)ni * W);
@@ -741,7 +822,19 @@ void nb6_regf_outputs_(double **d_outf, int **d_outl) {
 }
 
 // Kernel-only device time (ms) of the last gpunb_regf_ call.
-float nb6_regf_last_kernel_ms_() { return R.last_kernel_ms; }
+float nb6_regf_last_kernel_ms_() {
+    if (!R.ev1) return 0.f;
+    NB6_CUDA_CHECK(cudaEventSynchronize(R.ev1));
+    NB6_CUDA_CHECK(cudaEventElapsedTime(&R.last_kernel_ms, R.ev0, R.ev1));
+    return R.last_kernel_ms;
+}
+
+// Launch geometry of the last regf launch: i per thread, i-tiles, j-slices.
+void nb6_regf_last_geometry_(int *geom) {
+    geom[0] = R.last_geometry[0];
+    geom[1] = R.last_geometry[1];
+    geom[2] = R.last_geometry[2];
+}
 
 // Launch-geometry override for tuning sweeps: i per thread (1, 2, 4; 0 =
 // automatic) and j-slice count (0 = automatic).

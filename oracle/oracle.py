@@ -80,9 +80,10 @@ def regf(mj, xj, vj, h2, dtr, xi, vi, lmax, nnbmax, m_flag=0):
     jrk = np.zeros((ni, 3))
     pot = np.zeros(ni)
     lst = np.zeros((ni, lmax), dtype=np.int32)
-    fp64().orc_regf(nj, mj.ctypes.data_as(_d), xj.ctypes.data_as(_d), vj.ctypes.data_as(_d),
-                    ni, h2.ctypes.data_as(_d), dtr.ctypes.data_as(_d),
-                    xi.ctypes.data_as(_d), vi.ctypes.data_as(_d), lmax, nnbmax, m_flag,
+    fp64().orc_regf(int(nj), mj.ctypes.data_as(_d), xj.ctypes.data_as(_d), vj.ctypes.data_as(_d),
+                    int(ni), h2.ctypes.data_as(_d), dtr.ctypes.data_as(_d),
+                    xi.ctypes.data_as(_d), vi.ctypes.data_as(_d), int(lmax), int(nnbmax),
+                    int(m_flag),
                     acc.ctypes.data_as(_d), jrk.ctypes.data_as(_d), pot.ctypes.data_as(_d),
                     lst.ctypes.data_as(_i))
     return acc, jrk, pot, lst
@@ -93,8 +94,8 @@ def pot(m, x, istart=1, ni=None):
     n = m.shape[0]
     if ni is None:
         ni = n - istart + 1
-    out = np.zeros(ni)
-    fp64().orc_pot(n, m.ctypes.data_as(_d), x.ctypes.data_as(_d), istart, ni,
+    out = np.zeros(int(ni))
+    fp64().orc_pot(int(n), m.ctypes.data_as(_d), x.ctypes.data_as(_d), int(istart), int(ni),
                    out.ctypes.data_as(_d))
     return out
 
@@ -104,7 +105,7 @@ def predict(time, t0, x0, x0dot, f, fdot):
     n = t0.shape[0]
     x = np.zeros((n, 3))
     xd = np.zeros((n, 3))
-    fp64().orc_predict(n, float(time), t0.ctypes.data_as(_d), x0.ctypes.data_as(_d),
+    fp64().orc_predict(int(n), C.c_double(float(time)), t0.ctypes.data_as(_d), x0.ctypes.data_as(_d),
                        x0dot.ctypes.data_as(_d), f.ctypes.data_as(_d), fdot.ctypes.data_as(_d),
                        x.ctypes.data_as(_d), xd.ctypes.data_as(_d))
     return x, xd
@@ -120,9 +121,10 @@ def firr(ti, addr, x0, v0, acc2, jrk6, mass, t0, lists):
     acc = np.zeros((ni, 3))
     jrk = np.zeros((ni, 3))
     nnbid = np.zeros(ni, dtype=np.int32)
-    fp64().orc_firr(C.c_double(ti), ni, addr.ctypes.data_as(_i), nmax, x0.ctypes.data_as(_d),
+    fp64().orc_firr(C.c_double(float(ti)), int(ni), addr.ctypes.data_as(_i), int(nmax),
+                    x0.ctypes.data_as(_d),
                     v0.ctypes.data_as(_d), acc2.ctypes.data_as(_d), jrk6.ctypes.data_as(_d),
                     mass.ctypes.data_as(_d), t0.ctypes.data_as(_d), lists.ctypes.data_as(_i),
-                    lmax, acc.ctypes.data_as(_d), jrk.ctypes.data_as(_d),
+                    int(lmax), acc.ctypes.data_as(_d), jrk.ctypes.data_as(_d),
                     nnbid.ctypes.data_as(_i))
     return acc, jrk, nnbid
