@@ -122,8 +122,17 @@ void nb6_regf_device_(int *ni, const double *d_h2, const double *d_dtr, const do
                       const double *d_v, int *lmax, int *nnbmax, int *m_flag);
 void nb6_regf_outputs_(double **d_outf, int **d_outl);
 float nb6_regf_last_kernel_ms_(void);
+/* geom = (variant, i-grid, j-slices) of the last launch; variant > 0 is the
+ * i-parallel kernel with that many i per thread, variant < 0 the j-parallel
+ * kernel with -variant i per CTA. */
 void nb6_regf_last_geometry_(int *geom);
-void nb6_regf_tune_(int *ni_per_thread, int *nslices);
+/* Force a variant (1, 2, 4, -1, -2, -4, -8; 0 = automatic) and a slice count
+ * (0 = automatic). */
+void nb6_regf_tune_(int *variant, int *nslices);
+/* Measured autotuner keyed on (log2 N_active, log2 N_j, m_flag): 1 on
+ * (default, or NB6_AUTOTUNE=0 in the environment for off), 0 off, -1 clears
+ * the cached choices. */
+void nb6_regf_autotune_(int *flag);
 
 /* Synchronise the library stream (and check the device status); the stream
  * handle itself for callers that record events on it. */

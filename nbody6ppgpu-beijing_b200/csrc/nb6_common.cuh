@@ -44,6 +44,55 @@ NB6_DEV void split_hl(double x, float &hi, float &lo) {
     lo = __double2float_rn(x - (double)hi);
 }
 
+// Regular-force j set in HBM, written by the send/predict pack kernels.
+// Two layouts of the same data:
+//   posH/posL/vel  float4 per j: (xH,yH,zH,m), (xL,yL,zL,0), (vx,vy,vz,0) --
+//                  read per j by the j-parallel kernel;
+//   comp           10 float arrays of npad entries, component-major
+//                  (xH,yH,zH,m,xL,yL,zL,vx,vy,vz) -- tiles of it are bulk-copied
+//                  to shared memory so that one LDS.128 yields 4 consecutive j
+//                  of one component, the operand shape of packed f32x2 math.
+// Padding slots (j >= n) are massless and far away: never neighbours.
+constexpr int NB6_NCOMP = 10;
+
+struct JSetOut {
+    float4 *posH, *posL, *vel;
+    float *comp;
+    size_t npad;
+};
+
+NB6_DEV void write_j(const JSetOut &o, size_t j, bool real, double x0, double x1, double x2,
+                     double m, double v0, double v1, double v2) {
+    float4 h, l, v;
+    if (real) {
+        split_hl(x0, h.x, l.x);
+        split_hl(x1, h.y, l.y);
+        split_hl(x2, h.z, l.z);
+        h.w = (float)m;
+        l.w = 0.f;
+        v = make_float4((float)v0, (float)v1, (float)v2, 0.f);
+    } else {
+        h = make_float4(1.0e15f, 1.0e15f, 1.0e15f, 0.f);
+        l = make_float4(0.f, 0.f, 0.f, 0.f);
+        v = l;
+    }
+    o.posH[j] = h;
+    o.posL[j] = l;
+    o.vel[j] = v;
+    float *c = o.comp + j;
+    const size_t s = o.npad;
+    c[0] = h.x;
+    c[s] = h.y;
+    c[2 * s] = h.z;
+    c[3 * s] = h.w;
+    c[4 * s] = l.x;
+    c[5 * s] = l.y;
+    c[6 * s] = l.z;
+    c[7 * s] = v.x;
+    c[8 * s] = v.y;
+    c[9 * s] = v.z;
+}
+
 // Error-free sum (Knuth TwoSum): s + e == a + b exactly.
 NB6_DEV void two_sum(float a, float b, float &s, float &e) {
     s = __fadd_rn(a, b);
@@ -93,6 +142,11 @@ NB6_DEV void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
         "mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
         "r"(bytes)
         : "memory");
+}
+
+// Plain arrival (count 1) on an mbarrier.
+NB6_DEV void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
 // 1-D bulk copy global -> shared, completion counted on `bar` (bytes must be a

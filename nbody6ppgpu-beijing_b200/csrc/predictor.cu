@@ -26,8 +26,7 @@
 
 #include <algorithm>
 
-bool regular_bind_j(int n, double **jm, double **jx, double **jv, float4 **posH, float4 **posL,
-                    float4 **vel, int *npad);
+bool regular_bind_j(int n, double **jm, double **jx, double **jv, JSetOut *out);
 
 namespace {
 
@@ -72,39 +71,28 @@ __global__ void predict_kernel(int n, double time, const double *__restrict__ t0
 }
 
 // Predict bodies [j0, j0+n) and write the regular-force j set (FP64 copy and
-// hi/lo float4 tiles, padded to npad with far massless bodies).
-__global__ void predict_pack_kernel(int j0, int n, int npad, double time,
-                                    const double *__restrict__ t0, const double *__restrict__ x0,
-                                    const double *__restrict__ x0dot, const double *__restrict__ f,
-                                    const double *__restrict__ fdot, const double *__restrict__ body,
-                                    double *__restrict__ jm, double *__restrict__ jx,
-                                    double *__restrict__ jv, float4 *__restrict__ posH,
-                                    float4 *__restrict__ posL, float4 *__restrict__ vel) {
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < npad; q += gridDim.x * blockDim.x) {
-        if (q < n) {
+// the float layouts, padded with far massless bodies).
+__global__ void predict_pack_kernel(int j0, int n, double time, const double *__restrict__ t0,
+                                    const double *__restrict__ x0, const double *__restrict__ x0dot,
+                                    const double *__restrict__ f, const double *__restrict__ fdot,
+                                    const double *__restrict__ body, double *__restrict__ jm,
+                                    double *__restrict__ jx, double *__restrict__ jv, JSetOut o) {
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < o.npad;
+         q += (size_t)gridDim.x * blockDim.x) {
+        if (q < (size_t)n) {
             const size_t j = (size_t)j0 + q;
             double x[3], v[3];
             pred3(time - t0[j], x0, x0dot, f, fdot, j, x, v);
             const double m = body[j];
             jm[q] = m;
-            float4 h, l;
-            split_hl(x[0], h.x, l.x);
-            split_hl(x[1], h.y, l.y);
-            split_hl(x[2], h.z, l.z);
-            h.w = (float)m;
-            l.w = 0.f;
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
-                jx[3 * (size_t)q + k] = x[k];
-                jv[3 * (size_t)q + k] = v[k];
+                jx[3 * q + k] = x[k];
+                jv[3 * q + k] = v[k];
             }
-            posH[q] = h;
-            posL[q] = l;
-            vel[q] = make_float4((float)v[0], (float)v[1], (float)v[2], 0.f);
+            write_j(o, q, true, x[0], x[1], x[2], m, v[0], v[1], v[2]);
         } else {
-            posH[q] = make_float4(1.0e15f, 1.0e15f, 1.0e15f, 0.f);
-            posL[q] = make_float4(0.f, 0.f, 0.f, 0.f);
-            vel[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+            write_j(o, q, false, 0, 0, 0, 0, 0, 0, 0);
         }
     }
 }
@@ -279,14 +267,13 @@ void nb6_predict_send_(double *time, int *ifirst, int *nn) {
         return;
     }
     double *jm, *jx, *jv;
-    float4 *ph, *pl, *pv;
-    int npad;
-    if (!regular_bind_j(n, &jm, &jx, &jv, &ph, &pl, &pv, &npad)) return;
+    JSetOut o;
+    if (!regular_bind_j(n, &jm, &jx, &jv, &o)) return;
     cudaStream_t st = nb6_stream();
     NB6_CUDA_CHECK(cudaEventRecord(S.ev0, st));
-    predict_pack_kernel<<<grid_for(npad), 256, 0, st>>>(j0, n, npad, *time, S.t0.ptr, S.x0.ptr,
-                                                        S.x0dot.ptr, S.f.ptr, S.fdot.ptr, S.body.ptr,
-                                                        jm, jx, jv, ph, pl, pv);
+    predict_pack_kernel<<<grid_for(o.npad), 256, 0, st>>>(j0, n, *time, S.t0.ptr, S.x0.ptr,
+                                                          S.x0dot.ptr, S.f.ptr, S.fdot.ptr,
+                                                          S.body.ptr, jm, jx, jv, o);
     NB6_CUDA_CHECK(cudaGetLastError());
     NB6_CUDA_CHECK(cudaEventRecord(S.ev1, st));
 }

@@ -27,6 +27,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <map>
 #include <math.h>
 #include <string.h>
 
@@ -45,16 +46,23 @@ constexpr int FIN_WARPS = 4;
 #define UNROLL_J 8
 #endif
 constexpr int kUnrollJ = UNROLL_J;
-// The rare candidate path is kept out of line by default so that it does not
-// inflate the register allocation of the hot loop.
+// Minimum resident CTAs per SM requested for the packed kernel with one i
+// per thread (halved for two): bounds its register allocation.
+#ifndef X2_MINB
+#define X2_MINB 4
+#endif
+// The rare candidate path is inlined: an out-of-line call forces the
+// accumulators through a stack frame.
 #ifndef FLUSH_INLINE
-#define FLUSH_INLINE __noinline__
+#define FLUSH_INLINE __forceinline__
 #endif
 
 struct RegArgs {
     const float4 *__restrict__ posH;  // (xH, yH, zH, m)
     const float4 *__restrict__ posL;  // (xL, yL, zL, 0)
     const float4 *__restrict__ vel;   // (vx, vy, vz, 0)
+    const float *__restrict__ comp;   // component-major copy (NB6_NCOMP x npad)
+    size_t npad;
     const double *__restrict__ jm;    // FP64 copies for the exact recheck
     const double *__restrict__ jx;
     const double *__restrict__ jv;
@@ -134,20 +142,16 @@ NB6_DEV bool reg_pair(const IPart &ip, const float4 &a, const float4 &b, const f
     return cand;
 }
 
-// Rare path for one i and one 32-j group that held at least one candidate:
-// re-derive the candidates with the same FP32 test, then decide each exactly
-// in FP64.  Operation order matches the FP64 rule of regint.f:41-65 with the
-// strict "<" of gpunb.velocity.cu:188,236; no FMA contraction.
+// Exact FP64 decision for one candidate pair (i, j): record j as a neighbour
+// or, if it is not one, add its contribution (which the hot loop masked).
+// Operation order matches the FP64 rule of regint.f:41-65 with the strict
+// "<" of gpunb.velocity.cu:188,236; no FMA contraction.
 template <bool MFLAG>
-__device__ FLUSH_INLINE Sums reg_flush(const RegArgs &a, const IPart ip, int i, const float4 *A,
-                                       const float4 *B, const float4 *Cv, int jbase, Sums s) {
+NB6_DEV void reg_exact(const RegArgs &a, int i, int j, Sums &s) {
     const double xi0 = a.ix[3 * i], xi1 = a.ix[3 * i + 1], xi2 = a.ix[3 * i + 2];
     const double vi0 = a.iv[3 * i], vi1 = a.iv[3 * i + 1], vi2 = a.iv[3 * i + 2];
     const double h2 = a.ih2[i], dt = a.idtr[i];
-    for (int b = 0; b < 32; ++b) {
-        if (!reg_geom<MFLAG>(ip, A[b], B[b], Cv[b]).cand) continue;
-        const int j = jbase + b;
-        if (j >= a.nj) continue;  // padding slots are never neighbours
+    {
         const double dx = __dsub_rn(a.jx[3 * j], xi0);
         const double dy = __dsub_rn(a.jx[3 * j + 1], xi1);
         const double dz = __dsub_rn(a.jx[3 * j + 2], xi2);
@@ -183,6 +187,19 @@ __device__ FLUSH_INLINE Sums reg_flush(const RegArgs &a, const IPart ip, int i, 
             s.jz += (float)(8.0 * mr3 * (dvz + al * dz));
         }
     }
+}
+
+// Rare path for one i and one 32-j group that held at least one candidate:
+// re-derive the candidates with the same FP32 test, decide each in FP64.
+template <bool MFLAG>
+__device__ FLUSH_INLINE Sums reg_flush(const RegArgs &a, const IPart ip, int i, const float4 *A,
+                                       const float4 *B, const float4 *Cv, int jbase, Sums s) {
+    for (int b = 0; b < 32; ++b) {
+        if (!reg_geom<MFLAG>(ip, A[b], B[b], Cv[b]).cand) continue;
+        const int j = jbase + b;
+        if (j >= a.nj) continue;  // padding slots are never neighbours
+        reg_exact<MFLAG>(a, i, j, s);
+    }
     return s;
 }
 
@@ -198,6 +215,7 @@ template <int NI, bool MFLAG>
 __global__ void __launch_bounds__(NT) regf_kernel(const RegArgs a) {
     __shared__ __align__(128) float4 sj[NSTAGE][3][JT];
     __shared__ __align__(8) uint64_t bar[NSTAGE];
+    __shared__ __align__(8) uint64_t ebar[NSTAGE];
 
     const int tid = threadIdx.x;
     const int slice = blockIdx.y;
@@ -232,32 +250,37 @@ __global__ void __launch_bounds__(NT) regf_kernel(const RegArgs a) {
         }
     }
 
+    // Ring of NSTAGE tiles.  bar[st] completes when a tile's bulk copies have
+    // landed; ebar[st] when every warp has finished reading it.  Warps release
+    // stages independently, so they can drift up to NSTAGE-1 tiles apart and
+    // only the producer (thread 0) ever waits for the slowest warp.
+    const int lane = tid & 31;
     if (tid == 0) {
 #pragma unroll
-        for (int st = 0; st < NSTAGE; ++st) mbar_init(&bar[st], 1);
+        for (int st = 0; st < NSTAGE; ++st) {
+            mbar_init(&bar[st], 1);
+            mbar_init(&ebar[st], NT / 32);
+        }
         fence_mbar_init();
     }
     __syncthreads();
+    int issued = 0;  // tiles issued so far (thread 0 only)
     if (tid == 0) {
         for (int st = 0; st < NSTAGE && st < nt; ++st) issue_tile(a, sj[st], &bar[st], t_begin + st);
+        issued = min(nt, NSTAGE);
     }
 
     for (int t = 0; t < nt; ++t) {
         const int st = t % NSTAGE;
-        const bool ok = mbar_wait_timed(&bar[st], (uint32_t)((t / NSTAGE) & 1), WAIT_NS);
-        if (__syncthreads_or(!ok)) {
-            if (tid == 0) {
-                set_status(a.status, NB6_ERR_WAIT_TIMEOUT);
-                // drain copies still in flight before the CTA's smem goes away
-                const int issued = min(nt, NSTAGE + max(t - 1, 0));
+        const uint32_t par = (uint32_t)((t / NSTAGE) & 1);
+        const bool ok = __all_sync(0xffffffffu, mbar_wait_timed(&bar[st], par, WAIT_NS));
+        if (!ok) {
+            set_status(a.status, NB6_ERR_WAIT_TIMEOUT);
+            if (tid == 0)  // drain copies still in flight before the CTA's smem goes away
                 for (int u = t; u < issued; ++u)
                     mbar_wait_timed(&bar[u % NSTAGE], (uint32_t)((u / NSTAGE) & 1), WAIT_NS / 8);
-            }
             return;
         }
-        // every thread finished tile t-1: its stage can be refilled
-        if (tid == 0 && t >= 1 && t - 1 + NSTAGE < nt)
-            issue_tile(a, sj[(t - 1) % NSTAGE], &bar[(t - 1) % NSTAGE], t_begin + t - 1 + NSTAGE);
 
         const float4 *A = sj[st][0];
         const float4 *B = sj[st][1];
@@ -265,9 +288,9 @@ __global__ void __launch_bounds__(NT) regf_kernel(const RegArgs a) {
         const int jt0 = (t_begin + t) * JT;
 #pragma unroll 1
         for (int g = 0; g < JT / 32; ++g) {
-            bool anyc[NI];
+            unsigned anyc[NI];
 #pragma unroll
-            for (int k = 0; k < NI; ++k) anyc[k] = false;
+            for (int k = 0; k < NI; ++k) anyc[k] = 0u;
             const float4 *Ag = A + g * 32, *Bg = B + g * 32, *Cg = C + g * 32;
 #pragma unroll kUnrollJ
             for (int q = 0; q < 32; ++q) {
@@ -275,11 +298,25 @@ __global__ void __launch_bounds__(NT) regf_kernel(const RegArgs a) {
                 const float4 pb = Bg[q];
                 const float4 pc = Cg[q];
 #pragma unroll
-                for (int k = 0; k < NI; ++k) anyc[k] |= reg_pair<MFLAG>(ip[k], pa, pb, pc, s[k]);
+                for (int k = 0; k < NI; ++k) anyc[k] += reg_pair<MFLAG>(ip[k], pa, pb, pc, s[k]) ? 1u : 0u;
             }
 #pragma unroll
             for (int k = 0; k < NI; ++k)
                 if (anyc[k]) s[k] = reg_flush<MFLAG>(a, ip[k], ii[k], Ag, Bg, Cg, jt0 + g * 32, s[k]);
+        }
+        // this warp is done with the stage
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&ebar[st]);
+        if (tid == 0 && t + NSTAGE < nt) {
+            // once every warp has released tile t, refill its stage
+            if (!mbar_wait_timed(&ebar[st], par, WAIT_NS)) {
+                set_status(a.status, NB6_ERR_WAIT_TIMEOUT);
+                for (int u = t + 1; u < issued; ++u)
+                    mbar_wait_timed(&bar[u % NSTAGE], (uint32_t)((u / NSTAGE) & 1), WAIT_NS / 8);
+                return;
+            }
+            issue_tile(a, sj[st], &bar[st], t_begin + t + NSTAGE);
+            issued = t + NSTAGE + 1;
         }
 #pragma unroll
         for (int k = 0; k < NI; ++k) {
@@ -303,6 +340,361 @@ __global__ void __launch_bounds__(NT) regf_kernel(const RegArgs a) {
             p[1] = make_float4(H[k].az, L[k].az, H[k].jx, L[k].jx);
             p[2] = make_float4(H[k].jy, L[k].jy, H[k].jz, L[k].jz);
             p[3] = make_float4(H[k].po, L[k].po, 0.f, 0.f);
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------
+// Packed variant: two j per instruction in the f32x2 lanes (fma/add/mul.f32x2
+// of sm_100).  Each FP32 add/mul/fma of the pair math processes two pairs per
+// issue slot, which moves the kernel from issue-bound to FMA-pipe-bound.  The
+// j tile sits in shared memory component-major (NB6_NCOMP rows of JT floats),
+// so one LDS.128 brings four consecutive j of one component.  The arithmetic
+// is the scalar reg_pair's, operation for operation (negated i operands turn
+// subtractions into adds; sums are kept negated), so candidates and results
+// are bit-identical to the scalar kernels.
+// ----------------------------------------------------------------------------
+struct IP2 {
+    float2 nxh, nyh, nzh, nxl, nyl, nzl, nvx, nvy, nvz, h2c, dt;  // i data, negated, duplicated
+};
+
+struct S2 {
+    float2 ax, ay, az, jx, jy, jz, po;  // -(scaled sums), lane = j parity
+};
+
+NB6_DEV float2 dup2(float v) { return make_float2(v, v); }
+
+NB6_DEV void zero2(S2 &s) {
+    s.ax = s.ay = s.az = s.jx = s.jy = s.jz = s.po = make_float2(0.f, 0.f);
+}
+
+// Returns the candidate flags of the two lanes as bits 0 and 1.
+template <bool MFLAG>
+NB6_DEV unsigned pair_x2(const IP2 &ip, float2 xh, float2 yh, float2 zh, float2 m, float2 xl,
+                         float2 yl, float2 zl, float2 vx, float2 vy, float2 vz, S2 &s) {
+    const float2 dx = __fadd2_rn(__fadd2_rn(xh, ip.nxh), __fadd2_rn(xl, ip.nxl));
+    const float2 dy = __fadd2_rn(__fadd2_rn(yh, ip.nyh), __fadd2_rn(yl, ip.nyl));
+    const float2 dz = __fadd2_rn(__fadd2_rn(zh, ip.nzh), __fadd2_rn(zl, ip.nzl));
+    const float2 dvx = __fadd2_rn(vx, ip.nvx);
+    const float2 dvy = __fadd2_rn(vy, ip.nvy);
+    const float2 dvz = __fadd2_rn(vz, ip.nvz);
+    const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+    const float2 px = __ffma2_rn(ip.dt, dvx, dx);
+    const float2 py = __ffma2_rn(ip.dt, dvy, dy);
+    const float2 pz = __ffma2_rn(ip.dt, dvz, dz);
+    const float2 rp2 = __ffma2_rn(pz, pz, __ffma2_rn(py, py, __fmul2_rn(px, px)));
+    const float2 crit = MFLAG ? __fmul2_rn(m, ip.h2c) : ip.h2c;
+    const bool c0 = fminf(r2.x, rp2.x) < crit.x;
+    const bool c1 = fminf(r2.y, rp2.y) < crit.y;
+    const float2 rv = __ffma2_rn(dz, dvz, __ffma2_rn(dy, dvy, __fmul2_rn(dx, dvx)));
+    float2 y0;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y0.x) : "f"(r2.x));
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y0.y) : "f"(r2.y));
+    const float2 ra = __fmul2_rn(r2, y0);
+    const float2 nb = __ffma2_rn(ra, y0, dup2(-3.0f));   // -(3 - r2 y0^2)
+    float2 ny = __fmul2_rn(y0, nb);                      // -2/r
+    ny.x = c0 ? 0.0f : ny.x;
+    ny.y = c1 ? 0.0f : ny.y;
+    const float2 y2 = __fmul2_rn(ny, ny);
+    const float2 nmy = __fmul2_rn(m, ny);
+    const float2 nmy3 = __fmul2_rn(nmy, y2);
+    const float2 al = __fmul2_rn(__fmul2_rn(y2, dup2(-0.75f)), rv);
+    s.po = __fadd2_rn(s.po, nmy);
+    s.ax = __ffma2_rn(nmy3, dx, s.ax);
+    s.ay = __ffma2_rn(nmy3, dy, s.ay);
+    s.az = __ffma2_rn(nmy3, dz, s.az);
+    s.jx = __ffma2_rn(nmy3, __ffma2_rn(al, dx, dvx), s.jx);
+    s.jy = __ffma2_rn(nmy3, __ffma2_rn(al, dy, dvy), s.jy);
+    s.jz = __ffma2_rn(nmy3, __ffma2_rn(al, dz, dvz), s.jz);
+    return (c0 ? 1u : 0u) | (c1 ? 2u : 0u);
+}
+
+// Rare path: the candidates of one 32-j group, as recorded bit by bit by the
+// hot loop, each decided exactly in FP64.
+template <bool MFLAG>
+NB6_DEV Sums reg_flush_mask(const RegArgs &a, int i, unsigned mask, int jbase, Sums s) {
+    while (mask) {
+        const int b = __ffs(mask) - 1;
+        mask &= mask - 1;
+        const int j = jbase + b;
+        if (j >= a.nj) continue;  // padding slots are never neighbours
+        reg_exact<MFLAG>(a, i, j, s);
+    }
+    return s;
+}
+
+NB6_DEV void issue_tile_soa(const RegArgs &a, float (*stage)[JT], uint64_t *bar, int tile) {
+    const size_t off = (size_t)tile * JT;
+    mbar_arrive_expect_tx(bar, (uint32_t)(NB6_NCOMP * JT * sizeof(float)));
+#pragma unroll
+    for (int c = 0; c < NB6_NCOMP; ++c)
+        bulk_g2s(stage[c], a.comp + (size_t)c * a.npad + off, JT * sizeof(float), bar);
+}
+
+template <int NI, bool MFLAG>
+__global__ void __launch_bounds__(NT, X2_MINB / NI) regf_x2_kernel(const RegArgs a) {
+    __shared__ __align__(128) float sj[NSTAGE][NB6_NCOMP][JT];
+    __shared__ __align__(8) uint64_t bar[NSTAGE];
+    __shared__ __align__(8) uint64_t ebar[NSTAGE];
+    // double-single accumulators, touched once per tile: kept in shared
+    // memory (thread-private slots) to free registers for the pair math
+    __shared__ float2 dsum[NI][7][NT];
+
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int slice = blockIdx.y;
+    const int t_begin = (int)(((long long)slice * a.ntile) / a.nslices);
+    const int t_end = (int)(((long long)(slice + 1) * a.ntile) / a.nslices);
+    const int nt = t_end - t_begin;
+
+    IP2 ip[NI];
+    S2 s[NI];
+    Sums fx[NI];
+    int ii[NI];
+#pragma unroll
+    for (int k = 0; k < NI; ++k) {
+        const int i = blockIdx.x * (NT * NI) + k * NT + tid;
+        ii[k] = i;
+        zero2(s[k]);
+        zero(fx[k]);
+#pragma unroll
+        for (int c = 0; c < 7; ++c) dsum[k][c][tid] = make_float2(0.f, 0.f);
+        IPart p;
+        if (i < a.ni) {
+            split_hl(a.ix[3 * i], p.xh, p.xl);
+            split_hl(a.ix[3 * i + 1], p.yh, p.yl);
+            split_hl(a.ix[3 * i + 2], p.zh, p.zl);
+            p.vx = (float)a.iv[3 * i];
+            p.vy = (float)a.iv[3 * i + 1];
+            p.vz = (float)a.iv[3 * i + 2];
+            p.h2c = (float)a.ih2[i] * CAND_SLACK;
+            p.dt = (float)a.idtr[i];
+        } else {
+            p.xh = p.yh = p.zh = p.xl = p.yl = p.zl = p.vx = p.vy = p.vz = 0.f;
+            p.h2c = 0.f;  // padding lanes: never a candidate
+            p.dt = 0.f;
+        }
+        ip[k].nxh = dup2(-p.xh);
+        ip[k].nyh = dup2(-p.yh);
+        ip[k].nzh = dup2(-p.zh);
+        ip[k].nxl = dup2(-p.xl);
+        ip[k].nyl = dup2(-p.yl);
+        ip[k].nzl = dup2(-p.zl);
+        ip[k].nvx = dup2(-p.vx);
+        ip[k].nvy = dup2(-p.vy);
+        ip[k].nvz = dup2(-p.vz);
+        ip[k].h2c = dup2(p.h2c);
+        ip[k].dt = dup2(p.dt);
+    }
+
+    if (tid == 0) {
+#pragma unroll
+        for (int st = 0; st < NSTAGE; ++st) {
+            mbar_init(&bar[st], 1);
+            mbar_init(&ebar[st], NT / 32);
+        }
+        fence_mbar_init();
+    }
+    __syncthreads();
+    int issued = 0;
+    if (tid == 0) {
+        for (int st = 0; st < NSTAGE && st < nt; ++st) issue_tile_soa(a, sj[st], &bar[st], t_begin + st);
+        issued = min(nt, NSTAGE);
+    }
+
+    for (int t = 0; t < nt; ++t) {
+        const int st = t % NSTAGE;
+        const uint32_t par = (uint32_t)((t / NSTAGE) & 1);
+        const bool ok = __all_sync(0xffffffffu, mbar_wait_timed(&bar[st], par, WAIT_NS));
+        if (!ok) {
+            set_status(a.status, NB6_ERR_WAIT_TIMEOUT);
+            if (tid == 0)
+                for (int u = t; u < issued; ++u)
+                    mbar_wait_timed(&bar[u % NSTAGE], (uint32_t)((u / NSTAGE) & 1), WAIT_NS / 8);
+            return;
+        }
+        const float(*S)[JT] = sj[st];
+        const int jt0 = (t_begin + t) * JT;
+#pragma unroll 1
+        for (int g = 0; g < JT / 32; ++g) {
+            unsigned cnt[NI];
+#pragma unroll
+            for (int k = 0; k < NI; ++k) cnt[k] = 0u;
+            // fully unrolled: every candidate flag lands on a fixed mask bit
+#pragma unroll
+            for (int u = 0; u < 32; u += 4) {
+                const int q = g * 32 + u;
+                const float4 XH = *reinterpret_cast<const float4 *>(&S[0][q]);
+                const float4 YH = *reinterpret_cast<const float4 *>(&S[1][q]);
+                const float4 ZH = *reinterpret_cast<const float4 *>(&S[2][q]);
+                const float4 MM = *reinterpret_cast<const float4 *>(&S[3][q]);
+                const float4 XL = *reinterpret_cast<const float4 *>(&S[4][q]);
+                const float4 YL = *reinterpret_cast<const float4 *>(&S[5][q]);
+                const float4 ZL = *reinterpret_cast<const float4 *>(&S[6][q]);
+                const float4 VX = *reinterpret_cast<const float4 *>(&S[7][q]);
+                const float4 VY = *reinterpret_cast<const float4 *>(&S[8][q]);
+                const float4 VZ = *reinterpret_cast<const float4 *>(&S[9][q]);
+#pragma unroll
+                for (int k = 0; k < NI; ++k) {
+                    const unsigned c01 =
+                        pair_x2<MFLAG>(ip[k], make_float2(XH.x, XH.y), make_float2(YH.x, YH.y),
+                                       make_float2(ZH.x, ZH.y), make_float2(MM.x, MM.y),
+                                       make_float2(XL.x, XL.y), make_float2(YL.x, YL.y),
+                                       make_float2(ZL.x, ZL.y), make_float2(VX.x, VX.y),
+                                       make_float2(VY.x, VY.y), make_float2(VZ.x, VZ.y), s[k]);
+                    const unsigned c23 =
+                        pair_x2<MFLAG>(ip[k], make_float2(XH.z, XH.w), make_float2(YH.z, YH.w),
+                                       make_float2(ZH.z, ZH.w), make_float2(MM.z, MM.w),
+                                       make_float2(XL.z, XL.w), make_float2(YL.z, YL.w),
+                                       make_float2(ZL.z, ZL.w), make_float2(VX.z, VX.w),
+                                       make_float2(VY.z, VY.w), make_float2(VZ.z, VZ.w), s[k]);
+                    cnt[k] |= (c01 | (c23 << 2)) << u;
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < NI; ++k)
+                if (cnt[k]) fx[k] = reg_flush_mask<MFLAG>(a, ii[k], cnt[k], jt0 + g * 32, fx[k]);
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&ebar[st]);
+        if (tid == 0 && t + NSTAGE < nt) {
+            if (!mbar_wait_timed(&ebar[st], par, WAIT_NS)) {
+                set_status(a.status, NB6_ERR_WAIT_TIMEOUT);
+                for (int u = t + 1; u < issued; ++u)
+                    mbar_wait_timed(&bar[u % NSTAGE], (uint32_t)((u / NSTAGE) & 1), WAIT_NS / 8);
+                return;
+            }
+            issue_tile_soa(a, sj[st], &bar[st], t_begin + t + NSTAGE);
+            issued = t + NSTAGE + 1;
+        }
+        // fold: positive partial = rare-path sums - packed (negated) lane sums
+#pragma unroll
+        for (int k = 0; k < NI; ++k) {
+            const float p[7] = {fx[k].ax - (s[k].ax.x + s[k].ax.y), fx[k].ay - (s[k].ay.x + s[k].ay.y),
+                                fx[k].az - (s[k].az.x + s[k].az.y), fx[k].jx - (s[k].jx.x + s[k].jx.y),
+                                fx[k].jy - (s[k].jy.x + s[k].jy.y), fx[k].jz - (s[k].jz.x + s[k].jz.y),
+                                fx[k].po - (s[k].po.x + s[k].po.y)};
+#pragma unroll
+            for (int c = 0; c < 7; ++c) {
+                float2 d = dsum[k][c][tid];
+                ds_fold(d.x, d.y, p[c]);
+                dsum[k][c][tid] = d;
+            }
+            zero2(s[k]);
+            zero(fx[k]);
+        }
+    }
+
+#pragma unroll
+    for (int k = 0; k < NI; ++k) {
+        const int i = ii[k];
+        if (i < a.ni) {
+            float2 d[7];
+#pragma unroll
+            for (int c = 0; c < 7; ++c) d[c] = dsum[k][c][tid];
+            float4 *p = a.part + ((size_t)slice * a.ni_pad + i) * 4;
+            p[0] = make_float4(d[0].x, d[0].y, d[1].x, d[1].y);
+            p[1] = make_float4(d[2].x, d[2].y, d[3].x, d[3].y);
+            p[2] = make_float4(d[4].x, d[4].y, d[5].x, d[5].y);
+            p[3] = make_float4(d[6].x, d[6].y, 0.f, 0.f);
+        }
+    }
+}
+
+// j-parallel variant for few active particles (blocksteps with small
+// N_active): a CTA takes IB i-particles (hi/lo split into shared memory) and
+// a j-slice; each thread streams its own j's straight from global memory
+// (coalesced float4 loads) and runs them against all IB i's, so every SM is
+// busy even for ni = 1.  Same pair math, candidate test and exact FP64 rare
+// path as regf_kernel; the per-thread FP32 partials are reduced over the CTA
+// in FP64 and written as (hi, lo) slice partials for regf_finalize.
+constexpr int JPAR_NT = 256;
+
+template <int IB, bool MFLAG>
+__global__ void __launch_bounds__(JPAR_NT) regf_jpar_kernel(const RegArgs a) {
+    __shared__ float4 sip[IB][3];
+    __shared__ double red[JPAR_NT / 32][IB][7];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int i0 = blockIdx.x * IB;
+    if (tid < IB) {
+        const int i = i0 + tid;
+        float4 p = make_float4(0.f, 0.f, 0.f, 0.f), q = p, r = p;  // padding: never a candidate
+        if (i < a.ni) {
+            split_hl(a.ix[3 * i], p.x, q.x);
+            split_hl(a.ix[3 * i + 1], p.y, q.y);
+            split_hl(a.ix[3 * i + 2], p.z, q.z);
+            p.w = (float)a.ih2[i] * CAND_SLACK;
+            q.w = (float)a.idtr[i];
+            r = make_float4((float)a.iv[3 * i], (float)a.iv[3 * i + 1], (float)a.iv[3 * i + 2], 0.f);
+        }
+        sip[tid][0] = p;
+        sip[tid][1] = q;
+        sip[tid][2] = r;
+    }
+    __syncthreads();
+    const int j_begin = (int)(((long long)blockIdx.y * a.nj) / a.nslices);
+    const int j_end = (int)(((long long)(blockIdx.y + 1) * a.nj) / a.nslices);
+    Sums s[IB];
+#pragma unroll
+    for (int k = 0; k < IB; ++k) zero(s[k]);
+    for (int j = j_begin + tid; j < j_end; j += JPAR_NT) {
+        const float4 pa = __ldg(a.posH + j);
+        const float4 pb = __ldg(a.posL + j);
+        const float4 pc = __ldg(a.vel + j);
+        bool any = false;
+#pragma unroll
+        for (int k = 0; k < IB; ++k) {
+            const float4 p = sip[k][0], q = sip[k][1], r = sip[k][2];
+            IPart ip;
+            ip.xh = p.x; ip.yh = p.y; ip.zh = p.z; ip.h2c = p.w;
+            ip.xl = q.x; ip.yl = q.y; ip.zl = q.z; ip.dt = q.w;
+            ip.vx = r.x; ip.vy = r.y; ip.vz = r.z;
+            any |= reg_pair<MFLAG>(ip, pa, pb, pc, s[k]);
+        }
+        if (any) {
+            for (int k = 0; k < IB; ++k) {
+                const float4 p = sip[k][0], q = sip[k][1], r = sip[k][2];
+                IPart ip;
+                ip.xh = p.x; ip.yh = p.y; ip.zh = p.z; ip.h2c = p.w;
+                ip.xl = q.x; ip.yl = q.y; ip.zl = q.z; ip.dt = q.w;
+                ip.vx = r.x; ip.vy = r.y; ip.vz = r.z;
+                if (reg_geom<MFLAG>(ip, pa, pb, pc).cand) reg_exact<MFLAG>(a, i0 + k, j, s[k]);
+            }
+        }
+    }
+    // CTA reduction in FP64: warp shuffles, then across warps in shared memory
+#pragma unroll
+    for (int k = 0; k < IB; ++k) {
+        double v[7] = {s[k].ax, s[k].ay, s[k].az, s[k].jx, s[k].jy, s[k].jz, s[k].po};
+#pragma unroll
+        for (int c = 0; c < 7; ++c) {
+            const double w = warp_sum_d(v[c]);
+            if (lane == 0) red[warp][k][c] = w;
+        }
+    }
+    __syncthreads();
+    if (tid < IB * 7) {
+        const int k = tid / 7, c = tid % 7;
+        double w = 0.0;
+#pragma unroll
+        for (int q = 0; q < JPAR_NT / 32; ++q) w += red[q][k][c];
+        red[0][k][c] = w;
+    }
+    __syncthreads();
+    if (tid < IB) {
+        const int i = i0 + tid;
+        if (i < a.ni) {
+            float hv[7], lv[7];
+#pragma unroll
+            for (int c = 0; c < 7; ++c) {
+                const double w = red[0][tid][c];
+                hv[c] = (float)w;
+                lv[c] = (float)(w - (double)hv[c]);
+            }
+            float4 *p = a.part + ((size_t)blockIdx.y * a.ni_pad + i) * 4;
+            p[0] = make_float4(hv[0], lv[0], hv[1], lv[1]);
+            p[1] = make_float4(hv[2], lv[2], hv[3], lv[3]);
+            p[2] = make_float4(hv[4], lv[4], hv[5], lv[5]);
+            p[3] = make_float4(hv[6], lv[6], 0.f, 0.f);
         }
     }
 }
@@ -379,31 +771,20 @@ __global__ void __launch_bounds__(FIN_WARPS * 32)
 }
 
 // FP64 (m, x, v) -> SoA float4 tiles; padding slots are massless and far.
-__global__ void regf_pack_j(int nj, int npad, const double *__restrict__ m,
-                            const double *__restrict__ x, const double *__restrict__ v,
-                            float4 *__restrict__ posH, float4 *__restrict__ posL,
-                            float4 *__restrict__ vel, int *status) {
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < npad; j += gridDim.x * blockDim.x) {
-        if (j < nj) {
+__global__ void regf_pack_j(int nj, JSetOut o, const double *__restrict__ m,
+                            const double *__restrict__ x, const double *__restrict__ v, int *status) {
+    for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < o.npad;
+         j += (size_t)gridDim.x * blockDim.x) {
+        if (j < (size_t)nj) {
             const double x0 = x[3 * j], x1 = x[3 * j + 1], x2 = x[3 * j + 2];
             const double v0 = v[3 * j], v1 = v[3 * j + 1], v2 = v[3 * j + 2];
             const double mj = m[j];
             if (x0 != x0 || x1 != x1 || x2 != x2 || v0 != v0 || v1 != v1 || v2 != v2 ||
                 mj != mj)
                 set_status(status, NB6_ERR_NAN_INPUT);
-            float4 h, l;
-            split_hl(x0, h.x, l.x);
-            split_hl(x1, h.y, l.y);
-            split_hl(x2, h.z, l.z);
-            h.w = (float)mj;
-            l.w = 0.f;
-            posH[j] = h;
-            posL[j] = l;
-            vel[j] = make_float4((float)v0, (float)v1, (float)v2, 0.f);
+            write_j(o, j, true, x0, x1, x2, mj, v0, v1, v2);
         } else {
-            posH[j] = make_float4(1.0e15f, 1.0e15f, 1.0e15f, 0.f);
-            posL[j] = make_float4(0.f, 0.f, 0.f, 0.f);
-            vel[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+            write_j(o, j, false, 0, 0, 0, 0, 0, 0, 0);
         }
     }
 }
@@ -411,12 +792,26 @@ __global__ void regf_pack_j(int nj, int npad, const double *__restrict__ m,
 // ----------------------------------------------------------------------------
 // host state
 // ----------------------------------------------------------------------------
+
+// Measured autotuner keyed on (log2 N_active, log2 N_j, m_flag): the first
+// call in a bucket times every admissible variant on the caller's own data
+// (kernel-only CUDA events) and caches the fastest.  NB6_AUTOTUNE=0 turns it
+// off (default_variant is used); nb6_regf_tune_ forces a variant.
+struct TuneKey {
+    int li, lj, mf;
+    bool operator<(const TuneKey &o) const {
+        return li != o.li ? li < o.li : lj != o.lj ? lj < o.lj : mf < o.mf;
+    }
+};
+
 struct RegState {
     bool open = false;
     int nbodymax = 0;
     int nj = 0;
     int ntile = 0;
     DevBuf<float4> posH, posL, vel;
+    DevBuf<float> comp;              // NB6_NCOMP x npad, component-major
+    size_t npad = 0;
     DevBuf<double> jm, jx, jv;
     DevBuf<double> iin;
     DevBuf<float4> part;
@@ -432,62 +827,115 @@ struct RegState {
     // kernel-only device time of the last regf launch pair (ms)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     float last_kernel_ms = 0.f;
-    int forced_ni_per_thread = 0;   // 0 = autotune
+    int forced_ni_per_thread = 0;   // forced variant (see Plan); 0 = automatic
     int forced_slices = 0;
-    int last_geometry[3] = {0, 0, 0};  // NI, i-tiles, j-slices of the last launch
+    int last_geometry[3] = {0, 0, 0};  // variant, i-grid, j-slices of the last launch
+    int autotune = -1;                 // -1 = read NB6_AUTOTUNE on first use
+    std::map<TuneKey, int> tuned;      // bucket -> best variant
+    cudaEvent_t tev0 = nullptr, tev1 = nullptr;
 };
 RegState R;
 
-template <int NI, bool MF> int occupancy() {
-    static int occ = -1;
-    if (occ < 0) {
-        NB6_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, regf_kernel<NI, MF>, NT, 0));
-        if (occ < 1) occ = 1;
+// A launch plan.  variant > 0: regf_kernel with NI = variant i per thread
+// (i-parallel tiles); variant < 0: regf_jpar_kernel with IB = -variant
+// i-particles per CTA (j-parallel).
+struct Plan {
+    int variant = 1;
+    int igrid = 1;   // i-tiles or i-groups
+    int nslices = 1;
+};
+
+template <class K> int occ_of(K kern, int threads) {
+    int occ = 0;
+    NB6_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, 0));
+    return occ < 1 ? 1 : occ;
+}
+
+// Variants: 1, 2, 4 = regf_kernel with that many i per thread; 11, 12 =
+// regf_x2_kernel (packed f32x2) with 1 or 2 i per thread; -1, -2, -4, -8 =
+// regf_jpar_kernel with that many i per CTA.
+bool valid_variant(int v) {
+    return v == 1 || v == 2 || v == 4 || v == 11 || v == 12 || v == -1 || v == -2 || v == -4 ||
+           v == -8;
+}
+
+int i_per_thread(int v) { return v > 10 ? v - 10 : v; }
+
+template <bool MF> int occupancy_t(int variant) {
+    switch (variant) {
+        case 1: return occ_of(regf_kernel<1, MF>, NT);
+        case 2: return occ_of(regf_kernel<2, MF>, NT);
+        case 4: return occ_of(regf_kernel<4, MF>, NT);
+        case 11: return occ_of(regf_x2_kernel<1, MF>, NT);
+        case 12: return occ_of(regf_x2_kernel<2, MF>, NT);
+        case -1: return occ_of(regf_jpar_kernel<1, MF>, JPAR_NT);
+        case -2: return occ_of(regf_jpar_kernel<2, MF>, JPAR_NT);
+        case -4: return occ_of(regf_jpar_kernel<4, MF>, JPAR_NT);
+        default: return occ_of(regf_jpar_kernel<8, MF>, JPAR_NT);
     }
-    return occ;
 }
 
-template <int NI, bool MF>
-void launch_regf(RegArgs a, int nitile, cudaStream_t st) {
-    dim3 grid(nitile, a.nslices);
-    regf_kernel<NI, MF><<<grid, NT, 0, st>>>(a);
+int occupancy(int variant, bool mf) {
+    static std::map<int, int> cache;
+    const int key = variant * 2 + (mf ? 1 : 0);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    const int c = mf ? occupancy_t<true>(variant) : occupancy_t<false>(variant);
+    cache[key] = c;
+    return c;
 }
 
-int occ_for(int NI, bool mf) {
-    if (mf) {
-        if (NI == 1) return occupancy<1, true>();
-        if (NI == 2) return occupancy<2, true>();
-        return occupancy<4, true>();
-    }
-    if (NI == 1) return occupancy<1, false>();
-    if (NI == 2) return occupancy<2, false>();
-    return occupancy<4, false>();
-}
-
-// Launch geometry: i-per-thread and j-slice count.  Picks the largest NI whose
-// i-tiles stay >= 90% full, then enough slices to fill every SM once.
-void pick_geometry(int ni, int ntile, bool mf, int &NI, int &nitile, int &nslices) {
-    NI = 1;
-    if (R.forced_ni_per_thread == 1 || R.forced_ni_per_thread == 2 || R.forced_ni_per_thread == 4) {
-        NI = R.forced_ni_per_thread;
+// Geometry of one variant: enough CTAs for one full wave.
+Plan make_plan(int variant, int ni, int nj, int ntile, bool mf, int forced_slices) {
+    Plan p;
+    p.variant = variant;
+    const int target = nb6_num_sms() * occupancy(variant, mf);
+    if (variant > 0) {
+        const int tile = NT * i_per_thread(variant);
+        p.igrid = (ni + tile - 1) / tile;
+        p.nslices = std::max(1, target / p.igrid);
+        p.nslices = std::min(p.nslices, ntile);
     } else {
-        const int cands[3] = {4, 2, 1};
-        for (int c : cands) {
-            const int tile = NT * c;
-            const int nit = (ni + tile - 1) / tile;
-            if ((double)ni / ((double)nit * tile) >= 0.9 || c == 1) {
-                NI = c;
-                break;
-            }
-        }
+        const int ib = -variant;
+        p.igrid = (ni + ib - 1) / ib;
+        // at least 4 j per thread so the per-CTA set-up and reduction amortise
+        const int maxsl = std::max(1, nj / (JPAR_NT * 4));
+        p.nslices = std::max(1, std::min(target / p.igrid, maxsl));
     }
-    const int tile = NT * NI;
-    nitile = (ni + tile - 1) / tile;
-    const int target = nb6_num_sms() * occ_for(NI, mf);
-    nslices = std::max(1, target / nitile);
-    if (R.forced_slices > 0) nslices = R.forced_slices;
-    nslices = std::min(nslices, ntile);
-    nslices = std::max(nslices, 1);
+    if (forced_slices > 0) p.nslices = variant > 0 ? std::min(forced_slices, ntile) : forced_slices;
+    p.nslices = std::max(p.nslices, 1);
+    return p;
+}
+
+// Default plan without measurement: the packed i-parallel kernel with one i
+// per thread once a 128-thread tile is full, otherwise the j-parallel kernel
+// with the smallest CTA i-group that covers ni (at most 8).
+int default_variant(int ni) {
+    if (ni >= NT) return 11;
+    int ib = 1;
+    while (ib < ni && ib < 8) ib <<= 1;
+    return -ib;
+}
+
+template <bool MF> void launch_plan(const Plan &p, const RegArgs &a, cudaStream_t st) {
+    dim3 grid(p.igrid, p.nslices);
+    switch (p.variant) {
+        case 1: regf_kernel<1, MF><<<grid, NT, 0, st>>>(a); break;
+        case 2: regf_kernel<2, MF><<<grid, NT, 0, st>>>(a); break;
+        case 4: regf_kernel<4, MF><<<grid, NT, 0, st>>>(a); break;
+        case 11: regf_x2_kernel<1, MF><<<grid, NT, 0, st>>>(a); break;
+        case 12: regf_x2_kernel<2, MF><<<grid, NT, 0, st>>>(a); break;
+        case -1: regf_jpar_kernel<1, MF><<<grid, JPAR_NT, 0, st>>>(a); break;
+        case -2: regf_jpar_kernel<2, MF><<<grid, JPAR_NT, 0, st>>>(a); break;
+        case -4: regf_jpar_kernel<4, MF><<<grid, JPAR_NT, 0, st>>>(a); break;
+        default: regf_jpar_kernel<8, MF><<<grid, JPAR_NT, 0, st>>>(a); break;
+    }
+}
+
+int ilog2(int v) {
+    int r = 0;
+    while ((1 << (r + 1)) <= v) ++r;
+    return r;
 }
 
 bool any_nan(const double *p, size_t n) {
@@ -497,6 +945,28 @@ bool any_nan(const double *p, size_t n) {
 }
 
 }  // namespace
+
+// Make n bodies the current j set: tile count, padded length and buffers for
+// both float layouts plus the FP64 copies.
+static JSetOut size_j_buffers(int n) {
+    R.nj = n;
+    R.ntile = std::max(1, (n + JT - 1) / JT);
+    R.npad = (size_t)R.ntile * JT;
+    R.posH.reserve(R.npad);
+    R.posL.reserve(R.npad);
+    R.vel.reserve(R.npad);
+    R.comp.reserve((size_t)NB6_NCOMP * R.npad);
+    R.jm.reserve(R.npad);
+    R.jx.reserve(3 * R.npad);
+    R.jv.reserve(3 * R.npad);
+    JSetOut o;
+    o.posH = R.posH.ptr;
+    o.posL = R.posL.ptr;
+    o.vel = R.vel.ptr;
+    o.comp = R.comp.ptr;
+    o.npad = R.npad;
+    return o;
+}
 
 // ----------------------------------------------------------------------------
 // device-side regular force on resident i data (used by the ABI and by the
@@ -508,9 +978,44 @@ static void regf_device(int ni, const double *d_h2, const double *d_dtr, const d
     const int cap = std::max(0, std::min(nnbmax, lmax - 1));
     W = cap + 1;
     const int ni_pad = ni;
-    int NI, nitile, nslices;
-    pick_geometry(ni, R.ntile, mflag != 0, NI, nitile, nslices);
-    R.part.reserve((size_t)nslices * ni_pad * 4);
+    const bool mf = mflag != 0;
+    if (R.autotune < 0) {
+        const char *e = getenv("NB6_AUTOTUNE");
+        R.autotune = (e && atoi(e) == 0) ? 0 : 1;
+    }
+    int variant = default_variant(ni);
+    const TuneKey key{ilog2(std::max(ni, 1)), ilog2(std::max(R.nj, 1)), mf ? 1 : 0};
+    bool tune_now = false;
+    if (R.forced_ni_per_thread != 0) {
+        variant = R.forced_ni_per_thread;
+    } else if (R.autotune) {
+        auto it = R.tuned.find(key);
+        if (it != R.tuned.end()) variant = it->second;
+        else tune_now = true;
+    }
+    // admissible variants for this bucket
+    int cands[12], ncand = 0;
+    if (tune_now) {
+        if (ni >= NT / 2) {
+            cands[ncand++] = 1;
+            cands[ncand++] = 11;
+            if (ni >= NT * 2) {
+                cands[ncand++] = 2;
+                cands[ncand++] = 12;
+            }
+        }
+        if (ni <= 2048)
+            for (int ib : {1, 2, 4, 8})
+                if (ib <= 2 * ni) cands[ncand++] = -ib;
+        if (ncand == 0) tune_now = false;
+    }
+    Plan plan = make_plan(variant, ni, R.nj, R.ntile, mf, R.forced_slices);
+    size_t max_slices = plan.nslices;
+    if (tune_now)
+        for (int c = 0; c < ncand; ++c)
+            max_slices = std::max<size_t>(max_slices,
+                                          make_plan(cands[c], ni, R.nj, R.ntile, mf, 0).nslices);
+    R.part.reserve(max_slices * ni_pad * 4);
     R.nbcnt.reserve(ni);
     R.nbbuf.reserve((size_t)ni * std::max(cap, 1));
     R.outf.reserve((size_t)ni * 8);
@@ -521,12 +1026,14 @@ static void regf_device(int ni, const double *d_h2, const double *d_dtr, const d
     a.posH = R.posH.ptr;
     a.posL = R.posL.ptr;
     a.vel = R.vel.ptr;
+    a.comp = R.comp.ptr;
+    a.npad = R.npad;
     a.jm = R.jm.ptr;
     a.jx = R.jx.ptr;
     a.jv = R.jv.ptr;
     a.nj = R.nj;
     a.ntile = R.ntile;
-    a.nslices = nslices;
+    a.nslices = plan.nslices;
     a.ih2 = d_h2;
     a.idtr = d_dtr;
     a.ix = d_x;
@@ -543,23 +1050,54 @@ static void regf_device(int ni, const double *d_h2, const double *d_dtr, const d
         NB6_CUDA_CHECK(cudaEventCreate(&R.ev0));
         NB6_CUDA_CHECK(cudaEventCreate(&R.ev1));
     }
+    if (!R.tev0) {
+        NB6_CUDA_CHECK(cudaEventCreate(&R.tev0));
+        NB6_CUDA_CHECK(cudaEventCreate(&R.tev1));
+    }
+    if (tune_now) {
+        // time each candidate once (twice for the first, to skip cold
+        // effects); neighbour counters are reset before every trial
+        float best = 1e30f;
+        int bestv = variant;
+        for (int c = -1; c < ncand; ++c) {
+            const int v = cands[c < 0 ? 0 : c];
+            Plan p = make_plan(v, ni, R.nj, R.ntile, mf, 0);
+            RegArgs t = a;
+            t.nslices = p.nslices;
+            NB6_CUDA_CHECK(cudaMemsetAsync(R.nbcnt.ptr, 0, sizeof(int) * ni, st));
+            NB6_CUDA_CHECK(cudaEventRecord(R.tev0, st));
+            if (mf) launch_plan<true>(p, t, st);
+            else launch_plan<false>(p, t, st);
+            NB6_CUDA_CHECK(cudaGetLastError());
+            NB6_CUDA_CHECK(cudaEventRecord(R.tev1, st));
+            NB6_CUDA_CHECK(cudaEventSynchronize(R.tev1));
+            float ms = 0.f;
+            NB6_CUDA_CHECK(cudaEventElapsedTime(&ms, R.tev0, R.tev1));
+            if (c >= 0 && ms < best) {
+                best = ms;
+                bestv = v;
+            }
+        }
+        R.tuned[key] = bestv;
+        variant = bestv;
+        plan = make_plan(variant, ni, R.nj, R.ntile, mf, R.forced_slices);
+        a.nslices = plan.nslices;
+        NB6_CUDA_CHECK(cudaMemsetAsync(R.nbcnt.ptr, 0, sizeof(int) * ni, st));
+        if (getenv("NB6_VERBOSE"))
+            fprintf(stderr, "# nb6 autotune: ni~2^%d nj~2^%d mflag %d -> variant %d (%.3f ms)\n",
+                    key.li, key.lj, key.mf, bestv, best);
+    }
     // kernel-only timing of the main force kernel (read by
     // nb6_regf_last_kernel_ms_ after the stream has drained)
     NB6_CUDA_CHECK(cudaEventRecord(R.ev0, st));
-    if (mflag) {
-        if (NI == 1) launch_regf<1, true>(a, nitile, st);
-        else if (NI == 2) launch_regf<2, true>(a, nitile, st);
-        else launch_regf<4, true>(a, nitile, st);
-    } else {
-        if (NI == 1) launch_regf<1, false>(a, nitile, st);
-        else if (NI == 2) launch_regf<2, false>(a, nitile, st);
-        else launch_regf<4, false>(a, nitile, st);
-    }
+    if (mf) launch_plan<true>(plan, a, st);
+    else launch_plan<false>(plan, a, st);
     NB6_CUDA_CHECK(cudaGetLastError());
     NB6_CUDA_CHECK(cudaEventRecord(R.ev1, st));
-    R.last_geometry[0] = NI;
-    R.last_geometry[1] = nitile;
-    R.last_geometry[2] = nslices;
+    const int nslices = plan.nslices;
+    R.last_geometry[0] = plan.variant;
+    R.last_geometry[1] = plan.igrid;
+    R.last_geometry[2] = plan.nslices;
 
     int pmax = 32;
     while (pmax < cap) pmax <<= 1;
@@ -596,13 +1134,8 @@ void gpunb_open_(int *nbmax, int *irank) {
     }
     R.open = true;
     R.nbodymax = *nbmax;
-    const size_t npad = ((size_t)std::max(*nbmax, 1) + JT - 1) / JT * JT;
-    R.posH.reserve(npad);
-    R.posL.reserve(npad);
-    R.vel.reserve(npad);
-    R.jm.reserve(npad);
-    R.jx.reserve(3 * npad);
-    R.jv.reserve(3 * npad);
+    size_j_buffers(std::max(*nbmax, 1));
+    R.nj = 0;
     if (!R.ev0) {
         NB6_CUDA_CHECK(cudaEventCreate(&R.ev0));
         NB6_CUDA_CHECK(cudaEventCreate(&R.ev1));
@@ -620,6 +1153,7 @@ void gpunb_close_() {
     R.posH.release();
     R.posL.release();
     R.vel.release();
+    R.comp.release();
     R.jm.release();
     R.jx.release();
     R.jv.release();
@@ -650,23 +1184,14 @@ void gpunb_send_(int *nj, double *mj, double (*xj)[3], double (*vj)[3]) {
     R.time_send -= nb6_wtime();
     R.isend++;
     cudaStream_t st = nb6_stream();
-    R.nj = n;
-    R.ntile = std::max(1, (n + JT - 1) / JT);
-    const size_t npad = (size_t)R.ntile * JT;
-    R.posH.reserve(npad);
-    R.posL.reserve(npad);
-    R.vel.reserve(npad);
-    R.jm.reserve(npad);
-    R.jx.reserve(3 * npad);
-    R.jv.reserve(3 * npad);
+    const JSetOut o = size_j_buffers(n);
     if (n > 0) {
         NB6_CUDA_CHECK(cudaMemcpyAsync(R.jm.ptr, mj, sizeof(double) * n, cudaMemcpyHostToDevice, st));
         NB6_CUDA_CHECK(cudaMemcpyAsync(R.jx.ptr, xj, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, st));
         NB6_CUDA_CHECK(cudaMemcpyAsync(R.jv.ptr, vj, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, st));
     }
-    const int blocks = (int)std::min<size_t>((npad + 255) / 256, (size_t)nb6_num_sms() * 8);
-    regf_pack_j<<<blocks, 256, 0, st>>>(n, (int)npad, R.jm.ptr, R.jx.ptr, R.jv.ptr, R.posH.ptr,
-                                        R.posL.ptr, R.vel.ptr, nb6_dev_status());
+    const int blocks = (int)std::min<size_t>((o.npad + 255) / 256, (size_t)nb6_num_sms() * 8);
+    regf_pack_j<<<blocks, 256, 0, st>>>(n, o, R.jm.ptr, R.jx.ptr, R.jv.ptr, nb6_dev_status());
     NB6_CUDA_CHECK(cudaGetLastError());
     R.time_send += nb6_wtime();
 }
@@ -675,11 +1200,10 @@ void gpunb_send_(int *nj, double *mj, double (*xj)[3], double (*vj)[3]) {
 
 // Internal hook for the device-resident predictor (predictor.cu): a send whose
 // j data are produced on the device.  Sizes the j buffers for n bodies, makes
-// them current, and hands out the arrays to fill (FP64 m, x, v for the exact
-// neighbour recheck and the float4 tiles, padded to *npad with far massless
-// bodies by the caller's kernel).
-bool regular_bind_j(int n, double **jm, double **jx, double **jv, float4 **posH, float4 **posL,
-                    float4 **vel, int *npad) {
+// them current, and hands out the arrays to fill: FP64 m, x, v for the exact
+// neighbour recheck and the float layouts (JSetOut), which the caller's
+// kernel writes for j < npad with write_j.
+bool regular_bind_j(int n, double **jm, double **jx, double **jv, JSetOut *out) {
     if (!R.open) {
         nb6_fatal(NB6_ERR_NOT_OPEN);
         return false;
@@ -690,22 +1214,10 @@ bool regular_bind_j(int n, double **jm, double **jx, double **jv, float4 **posH,
         return false;
     }
     R.isend++;
-    R.nj = n;
-    R.ntile = std::max(1, (n + JT - 1) / JT);
-    const size_t np = (size_t)R.ntile * JT;
-    R.posH.reserve(np);
-    R.posL.reserve(np);
-    R.vel.reserve(np);
-    R.jm.reserve(np);
-    R.jx.reserve(3 * np);
-    R.jv.reserve(3 * np);
+    *out = size_j_buffers(n);
     *jm = R.jm.ptr;
     *jx = R.jx.ptr;
     *jv = R.jv.ptr;
-    *posH = R.posH.ptr;
-    *posL = R.posL.ptr;
-    *vel = R.vel.ptr;
-    *npad = (int)np;
     return true;
 }
 
@@ -838,9 +1350,24 @@ void nb6_regf_last_geometry_(int *geom) {
 
 // Launch-geometry override for tuning sweeps: i per thread (1, 2, 4; 0 =
 // automatic) and j-slice count (0 = automatic).
-void nb6_regf_tune_(int *ni_per_thread, int *nslices) {
-    R.forced_ni_per_thread = *ni_per_thread;
+void nb6_regf_tune_(int *variant, int *nslices) {
+    const int v = *variant;
+    const bool ok = v == 0 || valid_variant(v);
+    if (!ok || *nslices < 0) {
+        nb6_fatal(NB6_ERR_BAD_ARG);
+        return;
+    }
+    R.forced_ni_per_thread = v;
     R.forced_slices = *nslices;
+}
+
+// Enable (1) or disable (0) the measured autotuner; -1 clears its cache.
+void nb6_regf_autotune_(int *flag) {
+    if (*flag < 0) {
+        R.tuned.clear();
+        return;
+    }
+    R.autotune = *flag ? 1 : 0;
 }
 
 void nb6_sync_() { NB6_CUDA_CHECK(cudaStreamSynchronize(nb6_stream())); nb6_check_dev_status(); }

@@ -100,6 +100,30 @@ def test_regular_ragged_sizes(nb6, orc, n, ni):
         check_vs_oracle(orc, inp, out)
 
 
+@pytest.mark.parametrize("variant", [1, 2, 4, 11, 12, -1, -2, -4, -8])
+def test_regular_every_kernel_variant(nb6, orc, variant):
+    """Each launch variant (i-parallel with 1/2/4 i per thread, packed f32x2
+    with 1/2 i per thread, j-parallel with 1..8 i per CTA) matches the oracle,
+    whatever the autotuner would pick."""
+    import ctypes as C
+    from nb6b200 import ics
+    cl = ics.plummer(6000, seed=77, imf=True)
+    raw = nb6.lib
+    raw.nb6_regf_tune_(C.byref(C.c_int(variant)), C.byref(C.c_int(0)))
+    try:
+        for ni in (1, 5, 130, 700):
+            isel = np.sort(np.random.default_rng(ni).choice(cl.n, ni, replace=False))
+            for m_flag in (0, 1):
+                inp = _inputs(cl, isel, 512, 400, m_flag)
+                out = run_gpu(nb6, **inp)
+                geom = (C.c_int * 3)()
+                raw.nb6_regf_last_geometry_(geom)
+                assert geom[0] == variant
+                check_vs_oracle(orc, inp, out)
+    finally:
+        raw.nb6_regf_tune_(C.byref(C.c_int(0)), C.byref(C.c_int(0)))
+
+
 def test_regular_self_is_listed_and_ascending(nb6):
     from nb6b200 import ics
     cl = ics.plummer(3000, seed=5)
