@@ -58,6 +58,7 @@ constexpr int NB6_NCOMP = 10;
 struct JSetOut {
     float4 *posH, *posL, *vel;
     float *comp;
+    double *compd;  // FP64 positions, component-major (x, y, z) x npad
     size_t npad;
 };
 
@@ -91,6 +92,10 @@ NB6_DEV void write_j(const JSetOut &o, size_t j, bool real, double x0, double x1
     c[7 * s] = v.x;
     c[8 * s] = v.y;
     c[9 * s] = v.z;
+    double *d = o.compd + j;
+    d[0] = real ? x0 : 1.0e15;
+    d[s] = real ? x1 : 1.0e15;
+    d[2 * s] = real ? x2 : 1.0e15;
 }
 
 // Error-free sum (Knuth TwoSum): s + e == a + b exactly.

@@ -62,6 +62,7 @@ struct RegArgs {
     const float4 *__restrict__ posL;  // (xL, yL, zL, 0)
     const float4 *__restrict__ vel;   // (vx, vy, vz, 0)
     const float *__restrict__ comp;   // component-major copy (NB6_NCOMP x npad)
+    const double *__restrict__ compd; // FP64 positions, component-major (3 x npad)
     size_t npad;
     const double *__restrict__ jm;    // FP64 copies for the exact recheck
     const double *__restrict__ jx;
@@ -409,6 +410,49 @@ NB6_DEV unsigned pair_x2(const IP2 &ip, float2 xh, float2 yh, float2 zh, float2 
     return (c0 ? 1u : 0u) | (c1 ? 2u : 0u);
 }
 
+// Same pair math with the coordinate differences formed in FP64 and rounded
+// once to FP32 (DADD + F2F on the FP64 pipe instead of three FP32 adds per
+// component on the FMA pipe).  xi/yi/zi are the i position in FP64.
+template <bool MFLAG>
+NB6_DEV unsigned pair_x2d(const IP2 &ip, double xi, double yi, double zi, double2 xj, double2 yj,
+                          double2 zj, float2 m, float2 vx, float2 vy, float2 vz, S2 &s) {
+    const float2 dx = make_float2(__double2float_rn(xj.x - xi), __double2float_rn(xj.y - xi));
+    const float2 dy = make_float2(__double2float_rn(yj.x - yi), __double2float_rn(yj.y - yi));
+    const float2 dz = make_float2(__double2float_rn(zj.x - zi), __double2float_rn(zj.y - zi));
+    const float2 dvx = __fadd2_rn(vx, ip.nvx);
+    const float2 dvy = __fadd2_rn(vy, ip.nvy);
+    const float2 dvz = __fadd2_rn(vz, ip.nvz);
+    const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+    const float2 px = __ffma2_rn(ip.dt, dvx, dx);
+    const float2 py = __ffma2_rn(ip.dt, dvy, dy);
+    const float2 pz = __ffma2_rn(ip.dt, dvz, dz);
+    const float2 rp2 = __ffma2_rn(pz, pz, __ffma2_rn(py, py, __fmul2_rn(px, px)));
+    const float2 crit = MFLAG ? __fmul2_rn(m, ip.h2c) : ip.h2c;
+    const bool c0 = fminf(r2.x, rp2.x) < crit.x;
+    const bool c1 = fminf(r2.y, rp2.y) < crit.y;
+    const float2 rv = __ffma2_rn(dz, dvz, __ffma2_rn(dy, dvy, __fmul2_rn(dx, dvx)));
+    float2 y0;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y0.x) : "f"(r2.x));
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y0.y) : "f"(r2.y));
+    const float2 ra = __fmul2_rn(r2, y0);
+    const float2 nb = __ffma2_rn(ra, y0, dup2(-3.0f));
+    float2 ny = __fmul2_rn(y0, nb);
+    ny.x = c0 ? 0.0f : ny.x;
+    ny.y = c1 ? 0.0f : ny.y;
+    const float2 y2 = __fmul2_rn(ny, ny);
+    const float2 nmy = __fmul2_rn(m, ny);
+    const float2 nmy3 = __fmul2_rn(nmy, y2);
+    const float2 al = __fmul2_rn(__fmul2_rn(y2, dup2(-0.75f)), rv);
+    s.po = __fadd2_rn(s.po, nmy);
+    s.ax = __ffma2_rn(nmy3, dx, s.ax);
+    s.ay = __ffma2_rn(nmy3, dy, s.ay);
+    s.az = __ffma2_rn(nmy3, dz, s.az);
+    s.jx = __ffma2_rn(nmy3, __ffma2_rn(al, dx, dvx), s.jx);
+    s.jy = __ffma2_rn(nmy3, __ffma2_rn(al, dy, dvy), s.jy);
+    s.jz = __ffma2_rn(nmy3, __ffma2_rn(al, dz, dvz), s.jz);
+    return (c0 ? 1u : 0u) | (c1 ? 2u : 0u);
+}
+
 // Rare path: the candidates of one 32-j group, as recorded bit by bit by the
 // hot loop, each decided exactly in FP64.
 template <bool MFLAG>
@@ -423,15 +467,29 @@ NB6_DEV Sums reg_flush_mask(const RegArgs &a, int i, unsigned mask, int jbase, S
     return s;
 }
 
+// One tile into a stage of NB6_NCOMP float rows.  FP32 layout: the ten float
+// components.  FP64 layout: x, y, z as doubles in row pairs (0,1) (2,3) (4,5),
+// then m, vx, vy, vz in rows 6..9 -- the same 10*JT*4 bytes.
+template <bool F64DX>
 NB6_DEV void issue_tile_soa(const RegArgs &a, float (*stage)[JT], uint64_t *bar, int tile) {
     const size_t off = (size_t)tile * JT;
     mbar_arrive_expect_tx(bar, (uint32_t)(NB6_NCOMP * JT * sizeof(float)));
+    if constexpr (F64DX) {
 #pragma unroll
-    for (int c = 0; c < NB6_NCOMP; ++c)
-        bulk_g2s(stage[c], a.comp + (size_t)c * a.npad + off, JT * sizeof(float), bar);
+        for (int c = 0; c < 3; ++c)
+            bulk_g2s(stage[2 * c], a.compd + (size_t)c * a.npad + off, JT * sizeof(double), bar);
+        bulk_g2s(stage[6], a.comp + (size_t)3 * a.npad + off, JT * sizeof(float), bar);
+#pragma unroll
+        for (int c = 7; c < 10; ++c)
+            bulk_g2s(stage[c], a.comp + (size_t)c * a.npad + off, JT * sizeof(float), bar);
+    } else {
+#pragma unroll
+        for (int c = 0; c < NB6_NCOMP; ++c)
+            bulk_g2s(stage[c], a.comp + (size_t)c * a.npad + off, JT * sizeof(float), bar);
+    }
 }
 
-template <int NI, bool MFLAG>
+template <int NI, bool MFLAG, bool F64DX = false>
 __global__ void __launch_bounds__(NT, X2_MINB / NI) regf_x2_kernel(const RegArgs a) {
     __shared__ __align__(128) float sj[NSTAGE][NB6_NCOMP][JT];
     __shared__ __align__(8) uint64_t bar[NSTAGE];
@@ -450,6 +508,7 @@ __global__ void __launch_bounds__(NT, X2_MINB / NI) regf_x2_kernel(const RegArgs
     S2 s[NI];
     Sums fx[NI];
     int ii[NI];
+    double xd[NI], yd[NI], zd[NI];  // FP64 i position (F64DX layout)
 #pragma unroll
     for (int k = 0; k < NI; ++k) {
         const int i = blockIdx.x * (NT * NI) + k * NT + tid;
@@ -458,6 +517,9 @@ __global__ void __launch_bounds__(NT, X2_MINB / NI) regf_x2_kernel(const RegArgs
         zero(fx[k]);
 #pragma unroll
         for (int c = 0; c < 7; ++c) dsum[k][c][tid] = make_float2(0.f, 0.f);
+        xd[k] = i < a.ni ? a.ix[3 * i] : 0.0;
+        yd[k] = i < a.ni ? a.ix[3 * i + 1] : 0.0;
+        zd[k] = i < a.ni ? a.ix[3 * i + 2] : 0.0;
         IPart p;
         if (i < a.ni) {
             split_hl(a.ix[3 * i], p.xh, p.xl);
@@ -497,7 +559,8 @@ __global__ void __launch_bounds__(NT, X2_MINB / NI) regf_x2_kernel(const RegArgs
     __syncthreads();
     int issued = 0;
     if (tid == 0) {
-        for (int st = 0; st < NSTAGE && st < nt; ++st) issue_tile_soa(a, sj[st], &bar[st], t_begin + st);
+        for (int st = 0; st < NSTAGE && st < nt; ++st)
+            issue_tile_soa<F64DX>(a, sj[st], &bar[st], t_begin + st);
         issued = min(nt, NSTAGE);
     }
 
@@ -523,6 +586,32 @@ __global__ void __launch_bounds__(NT, X2_MINB / NI) regf_x2_kernel(const RegArgs
 #pragma unroll
             for (int u = 0; u < 32; u += 4) {
                 const int q = g * 32 + u;
+                if constexpr (F64DX) {
+                    const double *SX = reinterpret_cast<const double *>(S[0]);
+                    const double *SY = reinterpret_cast<const double *>(S[2]);
+                    const double *SZ = reinterpret_cast<const double *>(S[4]);
+                    const double2 X0 = *reinterpret_cast<const double2 *>(SX + q);
+                    const double2 X1 = *reinterpret_cast<const double2 *>(SX + q + 2);
+                    const double2 Y0 = *reinterpret_cast<const double2 *>(SY + q);
+                    const double2 Y1 = *reinterpret_cast<const double2 *>(SY + q + 2);
+                    const double2 Z0 = *reinterpret_cast<const double2 *>(SZ + q);
+                    const double2 Z1 = *reinterpret_cast<const double2 *>(SZ + q + 2);
+                    const float4 MM = *reinterpret_cast<const float4 *>(&S[6][q]);
+                    const float4 VX = *reinterpret_cast<const float4 *>(&S[7][q]);
+                    const float4 VY = *reinterpret_cast<const float4 *>(&S[8][q]);
+                    const float4 VZ = *reinterpret_cast<const float4 *>(&S[9][q]);
+#pragma unroll
+                    for (int k = 0; k < NI; ++k) {
+                        const unsigned c01 = pair_x2d<MFLAG>(
+                            ip[k], xd[k], yd[k], zd[k], X0, Y0, Z0, make_float2(MM.x, MM.y),
+                            make_float2(VX.x, VX.y), make_float2(VY.x, VY.y), make_float2(VZ.x, VZ.y), s[k]);
+                        const unsigned c23 = pair_x2d<MFLAG>(
+                            ip[k], xd[k], yd[k], zd[k], X1, Y1, Z1, make_float2(MM.z, MM.w),
+                            make_float2(VX.z, VX.w), make_float2(VY.z, VY.w), make_float2(VZ.z, VZ.w), s[k]);
+                        cnt[k] |= (c01 | (c23 << 2)) << u;
+                    }
+                    continue;
+                }
                 const float4 XH = *reinterpret_cast<const float4 *>(&S[0][q]);
                 const float4 YH = *reinterpret_cast<const float4 *>(&S[1][q]);
                 const float4 ZH = *reinterpret_cast<const float4 *>(&S[2][q]);
@@ -563,7 +652,7 @@ __global__ void __launch_bounds__(NT, X2_MINB / NI) regf_x2_kernel(const RegArgs
                     mbar_wait_timed(&bar[u % NSTAGE], (uint32_t)((u / NSTAGE) & 1), WAIT_NS / 8);
                 return;
             }
-            issue_tile_soa(a, sj[st], &bar[st], t_begin + t + NSTAGE);
+            issue_tile_soa<F64DX>(a, sj[st], &bar[st], t_begin + t + NSTAGE);
             issued = t + NSTAGE + 1;
         }
         // fold: positive partial = rare-path sums - packed (negated) lane sums
@@ -811,6 +900,7 @@ struct RegState {
     int ntile = 0;
     DevBuf<float4> posH, posL, vel;
     DevBuf<float> comp;              // NB6_NCOMP x npad, component-major
+    DevBuf<double> compd;            // 3 x npad FP64 positions, component-major
     size_t npad = 0;
     DevBuf<double> jm, jx, jv;
     DevBuf<double> iin;
@@ -855,11 +945,11 @@ template <class K> int occ_of(K kern, int threads) {
 // regf_x2_kernel (packed f32x2) with 1 or 2 i per thread; -1, -2, -4, -8 =
 // regf_jpar_kernel with that many i per CTA.
 bool valid_variant(int v) {
-    return v == 1 || v == 2 || v == 4 || v == 11 || v == 12 || v == -1 || v == -2 || v == -4 ||
+    return v == 1 || v == 2 || v == 4 || v == 11 || v == 12 || v == 13 || v == -1 || v == -2 || v == -4 ||
            v == -8;
 }
 
-int i_per_thread(int v) { return v > 10 ? v - 10 : v; }
+int i_per_thread(int v) { return v == 13 ? 1 : v > 10 ? v - 10 : v; }
 
 template <bool MF> int occupancy_t(int variant) {
     switch (variant) {
@@ -868,6 +958,7 @@ template <bool MF> int occupancy_t(int variant) {
         case 4: return occ_of(regf_kernel<4, MF>, NT);
         case 11: return occ_of(regf_x2_kernel<1, MF>, NT);
         case 12: return occ_of(regf_x2_kernel<2, MF>, NT);
+        case 13: return occ_of(regf_x2_kernel<1, MF, true>, NT);
         case -1: return occ_of(regf_jpar_kernel<1, MF>, JPAR_NT);
         case -2: return occ_of(regf_jpar_kernel<2, MF>, JPAR_NT);
         case -4: return occ_of(regf_jpar_kernel<4, MF>, JPAR_NT);
@@ -925,6 +1016,7 @@ template <bool MF> void launch_plan(const Plan &p, const RegArgs &a, cudaStream_
         case 4: regf_kernel<4, MF><<<grid, NT, 0, st>>>(a); break;
         case 11: regf_x2_kernel<1, MF><<<grid, NT, 0, st>>>(a); break;
         case 12: regf_x2_kernel<2, MF><<<grid, NT, 0, st>>>(a); break;
+        case 13: regf_x2_kernel<1, MF, true><<<grid, NT, 0, st>>>(a); break;
         case -1: regf_jpar_kernel<1, MF><<<grid, JPAR_NT, 0, st>>>(a); break;
         case -2: regf_jpar_kernel<2, MF><<<grid, JPAR_NT, 0, st>>>(a); break;
         case -4: regf_jpar_kernel<4, MF><<<grid, JPAR_NT, 0, st>>>(a); break;
@@ -956,6 +1048,7 @@ static JSetOut size_j_buffers(int n) {
     R.posL.reserve(R.npad);
     R.vel.reserve(R.npad);
     R.comp.reserve((size_t)NB6_NCOMP * R.npad);
+    R.compd.reserve((size_t)3 * R.npad);
     R.jm.reserve(R.npad);
     R.jx.reserve(3 * R.npad);
     R.jv.reserve(3 * R.npad);
@@ -964,6 +1057,7 @@ static JSetOut size_j_buffers(int n) {
     o.posL = R.posL.ptr;
     o.vel = R.vel.ptr;
     o.comp = R.comp.ptr;
+    o.compd = R.compd.ptr;
     o.npad = R.npad;
     return o;
 }
@@ -999,6 +1093,7 @@ static void regf_device(int ni, const double *d_h2, const double *d_dtr, const d
         if (ni >= NT / 2) {
             cands[ncand++] = 1;
             cands[ncand++] = 11;
+            cands[ncand++] = 13;
             if (ni >= NT * 2) {
                 cands[ncand++] = 2;
                 cands[ncand++] = 12;
@@ -1027,6 +1122,7 @@ static void regf_device(int ni, const double *d_h2, const double *d_dtr, const d
     a.posL = R.posL.ptr;
     a.vel = R.vel.ptr;
     a.comp = R.comp.ptr;
+    a.compd = R.compd.ptr;
     a.npad = R.npad;
     a.jm = R.jm.ptr;
     a.jx = R.jx.ptr;
@@ -1154,6 +1250,7 @@ void gpunb_close_() {
     R.posL.release();
     R.vel.release();
     R.comp.release();
+    R.compd.release();
     R.jm.release();
     R.jx.release();
     R.jv.release();

@@ -100,7 +100,7 @@ def test_regular_ragged_sizes(nb6, orc, n, ni):
         check_vs_oracle(orc, inp, out)
 
 
-@pytest.mark.parametrize("variant", [1, 2, 4, 11, 12, -1, -2, -4, -8])
+@pytest.mark.parametrize("variant", [1, 2, 4, 11, 12, 13, -1, -2, -4, -8])
 def test_regular_every_kernel_variant(nb6, orc, variant):
     """Each launch variant (i-parallel with 1/2/4 i per thread, packed f32x2
     with 1/2 i per thread, j-parallel with 1..8 i per CTA) matches the oracle,
