@@ -161,6 +161,25 @@ float nb6_predict_last_kernel_ms_(void);
 /* Measured FP32 FMA throughput (TFLOP/s) of the current GPU. */
 double nb6_fp32_peak_probe_(int *iters);
 
+/* Regular force + jerk + potential + neighbour list that allocates nothing.
+ * No counterpart in the reference.  It is for callers that cannot let the
+ * library allocate device memory, because another allocator owns the GPU's
+ * memory or the run's allocation state must not change mid-run.  Inputs and
+ * outputs are caller-provided device-accessible arrays in the gpunb_regf_
+ * layouts: j set m[nj], x[nj][3], v[nj][3]; i set h2, dtr, x[ni][3],
+ * v[ni][3]; outputs acc[ni][3], jrk[ni][3], pot[ni], list[ni][lmax].
+ * Working memory is one fixed 12 MiB device array inside the library,
+ * resident on each GPU that loads it until exit.  That bounds a call to
+ * ni <= 1024 and min(nnbmax, lmax-1) <= 511; larger sizes are rejected.
+ * Work is enqueued on `stream` (a cudaStream_t, 0 = default stream) without
+ * waiting.  The first call on a device looks up the array's address, so make
+ * it before any stream capture.  Calls share the array: calls that overlap on
+ * the GPU race and must not be issued. */
+void nb6_regf_noalloc_(int *nj, const double *d_mj, const double *d_xj, const double *d_vj,
+                       int *ni, const double *d_h2, const double *d_dtr, const double *d_xi,
+                       const double *d_vi, double *d_acc, double *d_jrk, double *d_pot, int *lmax,
+                       int *nnbmax, int *d_list, int *m_flag, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1472,3 +1472,284 @@ void nb6_sync_() { NB6_CUDA_CHECK(cudaStreamSynchronize(nb6_stream())); nb6_chec
 void *nb6_stream_() { return (void *)nb6_stream(); }
 
 }  // extern "C"
+
+// ============================================================================
+// Regular force without any device allocation.
+//
+// Some callers cannot let this library allocate device memory: a simulation
+// whose GPU memory is entirely owned by another allocator (a framework's
+// caching pool, or a fixed per-rank budget set when the run starts), or a
+// driver that must not change the device's allocation state in the middle of
+// a run.  nb6_regf_noalloc_ serves them: the caller passes device-accessible
+// inputs and outputs, and the only working memory is the fixed array below,
+// which is part of the library image.  Nothing is allocated or freed, not
+// even a stream or an event.
+//
+// The array is NB6_NOALLOC_SCRATCH_BYTES (12 MiB) per GPU and stays resident
+// on every GPU that loads the library until the process exits.  It bounds a
+// call to ni <= 1024 active particles and a list cap min(nnbmax, lmax-1) <=
+// 511; larger requests are rejected.  Every call shares it and it keeps the
+// previous call's contents (the neighbour counters are cleared at the start
+// of each call): calls that overlap on the GPU -- different streams, or
+// different host threads without ordering -- race on it and must not be
+// issued.
+// ============================================================================
+
+constexpr size_t NB6_NOALLOC_SCRATCH_BYTES = 12u << 20;
+constexpr int NA_NIMAX = 1024;
+constexpr int NA_CAPMAX = 511;
+constexpr int NA_SLICES_MAX = 128;
+constexpr int NA_IB = 4;  // i-particles per CTA of the j-parallel kernel
+
+// Layout inside the array: neighbour counters [NA_NIMAX], neighbour ids
+// [NA_NIMAX][NA_CAPMAX], slice partials [NA_SLICES_MAX][NA_NIMAX][4] float4.
+constexpr size_t NA_OFF_CNT = 0;
+constexpr size_t NA_OFF_IDS = 4096;
+constexpr size_t NA_OFF_PART = NA_OFF_IDS + (size_t)NA_NIMAX * NA_CAPMAX * sizeof(int) + 4096;
+static_assert(NA_OFF_PART % 256 == 0, "alignment");
+static_assert(NA_OFF_PART + (size_t)NA_SLICES_MAX * NA_NIMAX * 4 * sizeof(float4) <=
+                  NB6_NOALLOC_SCRATCH_BYTES,
+              "scratch layout exceeds the array");
+
+static __device__ __align__(256) unsigned char nb6_noalloc_scratch[NB6_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+__global__ void na_clear_counts(int *cnt, int ni) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < ni) cnt[i] = 0;
+}
+
+// j-parallel regular force reading the caller's FP64 j arrays directly
+// (hi/lo split on the fly); pair math, candidate test and exact FP64
+// re-decision are those of the other regular kernels.
+template <bool MFLAG>
+__global__ void __launch_bounds__(JPAR_NT) regf_na_kernel(const RegArgs a) {
+    __shared__ float4 sip[NA_IB][3];
+    __shared__ double red[JPAR_NT / 32][NA_IB][7];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int i0 = blockIdx.x * NA_IB;
+    if (tid < NA_IB) {
+        const int i = i0 + tid;
+        float4 p = make_float4(0.f, 0.f, 0.f, 0.f), q = p, r = p;  // padding: never a candidate
+        if (i < a.ni) {
+            split_hl(a.ix[3 * i], p.x, q.x);
+            split_hl(a.ix[3 * i + 1], p.y, q.y);
+            split_hl(a.ix[3 * i + 2], p.z, q.z);
+            p.w = (float)a.ih2[i] * CAND_SLACK;
+            q.w = (float)a.idtr[i];
+            r = make_float4((float)a.iv[3 * i], (float)a.iv[3 * i + 1], (float)a.iv[3 * i + 2], 0.f);
+        }
+        sip[tid][0] = p;
+        sip[tid][1] = q;
+        sip[tid][2] = r;
+    }
+    __syncthreads();
+    const int j_begin = (int)(((long long)blockIdx.y * a.nj) / a.nslices);
+    const int j_end = (int)(((long long)(blockIdx.y + 1) * a.nj) / a.nslices);
+    Sums s[NA_IB];
+#pragma unroll
+    for (int k = 0; k < NA_IB; ++k) zero(s[k]);
+    for (int j = j_begin + tid; j < j_end; j += JPAR_NT) {
+        float4 pa, pb;
+        split_hl(a.jx[3 * (size_t)j], pa.x, pb.x);
+        split_hl(a.jx[3 * (size_t)j + 1], pa.y, pb.y);
+        split_hl(a.jx[3 * (size_t)j + 2], pa.z, pb.z);
+        pa.w = (float)a.jm[j];
+        pb.w = 0.f;
+        const float4 pc = make_float4((float)a.jv[3 * (size_t)j], (float)a.jv[3 * (size_t)j + 1],
+                                      (float)a.jv[3 * (size_t)j + 2], 0.f);
+        bool any = false;
+        IPart ips[NA_IB];
+#pragma unroll
+        for (int k = 0; k < NA_IB; ++k) {
+            const float4 p = sip[k][0], q = sip[k][1], r = sip[k][2];
+            IPart &ip = ips[k];
+            ip.xh = p.x; ip.yh = p.y; ip.zh = p.z; ip.h2c = p.w;
+            ip.xl = q.x; ip.yl = q.y; ip.zl = q.z; ip.dt = q.w;
+            ip.vx = r.x; ip.vy = r.y; ip.vz = r.z;
+            any |= reg_pair<MFLAG>(ip, pa, pb, pc, s[k]);
+        }
+        if (any) {
+            for (int k = 0; k < NA_IB; ++k)
+                if (reg_geom<MFLAG>(ips[k], pa, pb, pc).cand) reg_exact<MFLAG>(a, i0 + k, j, s[k]);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < NA_IB; ++k) {
+        double v[7] = {s[k].ax, s[k].ay, s[k].az, s[k].jx, s[k].jy, s[k].jz, s[k].po};
+#pragma unroll
+        for (int c = 0; c < 7; ++c) {
+            const double w = warp_sum_d(v[c]);
+            if (lane == 0) red[warp][k][c] = w;
+        }
+    }
+    __syncthreads();
+    if (tid < NA_IB * 7) {
+        const int k = tid / 7, c = tid % 7;
+        double w = 0.0;
+#pragma unroll
+        for (int q = 0; q < JPAR_NT / 32; ++q) w += red[q][k][c];
+        const int i = i0 + k;
+        if (i < a.ni) {
+            float *p = reinterpret_cast<float *>(a.part + ((size_t)blockIdx.y * a.ni_pad + i) * 4);
+            const float hi = (float)w;
+            p[2 * c] = hi;
+            p[2 * c + 1] = (float)(w - (double)hi);
+        }
+    }
+}
+
+// One warp per i: FP64 sum of the slice partials into the caller's acc, jrk
+// and pot rows, and the sorted neighbour ids into the caller's list row.
+__global__ void __launch_bounds__(FIN_WARPS * 32)
+    regf_na_finalize(const float4 *__restrict__ part, int nslices, int ni,
+                     const int *__restrict__ nbcnt, const int *__restrict__ nbbuf, int lcap, int cap,
+                     int lmax, double *__restrict__ acc, double *__restrict__ jrk,
+                     double *__restrict__ pot, int *__restrict__ list) {
+    __shared__ int sbuf[FIN_WARPS][512];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i = blockIdx.x * FIN_WARPS + warp;
+    if (i >= ni) return;
+    double v[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (int sl = lane; sl < nslices; sl += 32) {
+        const float *p = reinterpret_cast<const float *>(part + ((size_t)sl * ni + i) * 4);
+#pragma unroll
+        for (int c = 0; c < 7; ++c) v[c] += (double)p[2 * c] + (double)p[2 * c + 1];
+    }
+#pragma unroll
+    for (int c = 0; c < 7; ++c) v[c] = warp_sum_d(v[c]);
+    if (lane == 0) {
+        acc[3 * (size_t)i] = v[0] * 0.125;
+        acc[3 * (size_t)i + 1] = v[1] * 0.125;
+        acc[3 * (size_t)i + 2] = v[2] * 0.125;
+        jrk[3 * (size_t)i] = v[3] * 0.125;
+        jrk[3 * (size_t)i + 1] = v[4] * 0.125;
+        jrk[3 * (size_t)i + 2] = v[5] * 0.125;
+        pot[i] = v[6] * 0.5;
+    }
+    const int n = nbcnt[i];
+    int *row = list + (size_t)i * lmax;
+    if (n > cap) {
+        if (lane == 0) row[0] = -n;
+        return;
+    }
+    int *sb = sbuf[warp];
+    int P = 32;
+    while (P < n) P <<= 1;
+    const int *src = nbbuf + (size_t)i * lcap;
+    for (int k = lane; k < P; k += 32) sb[k] = (k < n) ? src[k] : INT_MAX;
+    __syncwarp();
+    for (int kk = 2; kk <= P; kk <<= 1) {
+        for (int jj = kk >> 1; jj > 0; jj >>= 1) {
+            for (int x = lane; x < P; x += 32) {
+                const int y = x ^ jj;
+                if (y > x) {
+                    const int p0 = sb[x], p1 = sb[y];
+                    const bool up = (x & kk) == 0;
+                    if ((p0 > p1) == up) {
+                        sb[x] = p1;
+                        sb[y] = p0;
+                    }
+                }
+            }
+            __syncwarp();
+        }
+    }
+    if (lane == 0) row[0] = n;
+    for (int k = lane; k < n; k += 32) row[1 + k] = sb[k];
+}
+
+// Device address of the scratch array, looked up once per device (up to 64
+// devices) with that device current.
+unsigned char *na_scratch_address(int dev) {
+    static unsigned char *addr[64] = {nullptr};
+    if (dev < 0 || dev >= 64) return nullptr;
+    if (!addr[dev]) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, nb6_noalloc_scratch);
+        if (e != cudaSuccess) {
+            fprintf(stderr, "nb6_regf_noalloc: cudaGetSymbolAddress failed: %s\n", cudaGetErrorString(e));
+            return nullptr;
+        }
+        addr[dev] = static_cast<unsigned char *>(p);
+    }
+    return addr[dev];
+}
+
+}  // namespace
+
+extern "C" {
+
+// Regular force + jerk + potential + neighbour list (gpunb_regf_ semantics)
+// that allocates nothing.  All array arguments are device-accessible
+// pointers in the gpunb_regf_ layouts: j set m[nj], x[nj][3], v[nj][3];
+// i set h2[ni], dtr[ni], x[ni][3], v[ni][3]; outputs acc[ni][3], jrk[ni][3],
+// pot[ni] and list[ni][lmax] (list[i*lmax] = nnb or -nnb, ids 0-based and
+// ascending after it).  Work is enqueued on `stream` (0 = the legacy default
+// stream) and the call returns without waiting.  The first call on a device
+// looks up the scratch array's device address (cudaGetSymbolAddress, with
+// that device current); make that first call before any stream capture.
+// Limits: ni <= 1024, min(nnbmax, lmax-1) <= 511.
+void nb6_regf_noalloc_(int *nj_, const double *d_mj, const double *d_xj, const double *d_vj,
+                       int *ni_, const double *d_h2, const double *d_dtr, const double *d_xi,
+                       const double *d_vi, double *d_acc, double *d_jrk, double *d_pot, int *lmax_,
+                       int *nnbmax_, int *d_list, int *m_flag, void *stream) {
+    const int nj = *nj_, ni = *ni_, lmax = *lmax_, nnbmax = *nnbmax_;
+    const int cap = std::max(0, std::min(nnbmax, lmax - 1));
+    if (ni <= 0 || ni > NA_NIMAX || nj <= 0 || lmax < 1 || cap > NA_CAPMAX) {
+        fprintf(stderr,
+                "nb6_regf_noalloc: ni=%d (1..%d), nj=%d (>=1), list cap min(nnbmax,lmax-1)=%d (<=%d) "
+                "outside the fixed scratch limits\n",
+                ni, NA_NIMAX, nj, cap, NA_CAPMAX);
+        nb6_fatal(NB6_ERR_TOO_LARGE);
+        return;
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        nb6_fatal(NB6_ERR_CUDA);
+        return;
+    }
+    unsigned char *base = na_scratch_address(dev);
+    if (!base) {
+        nb6_fatal(NB6_ERR_CUDA);
+        return;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+        nb6_fatal(NB6_ERR_CUDA);
+        return;
+    }
+    RegArgs a = {};
+    a.jm = d_mj;
+    a.jx = d_xj;
+    a.jv = d_vj;
+    a.nj = nj;
+    a.ih2 = d_h2;
+    a.idtr = d_dtr;
+    a.ix = d_xi;
+    a.iv = d_vi;
+    a.ni = ni;
+    a.ni_pad = ni;
+    a.nbcnt = reinterpret_cast<int *>(base + NA_OFF_CNT);
+    a.nbbuf = reinterpret_cast<int *>(base + NA_OFF_IDS);
+    a.lcap = std::max(cap, 1);
+    a.part = reinterpret_cast<float4 *>(base + NA_OFF_PART);
+    const int igroups = (ni + NA_IB - 1) / NA_IB;
+    a.nslices = std::max(1, std::min(std::min(2 * sms / igroups, nj / (JPAR_NT * 4)), NA_SLICES_MAX));
+
+    na_clear_counts<<<(ni + 255) / 256, 256, 0, st>>>(a.nbcnt, ni);
+    dim3 grid(igroups, a.nslices);
+    if (*m_flag) regf_na_kernel<true><<<grid, JPAR_NT, 0, st>>>(a);
+    else regf_na_kernel<false><<<grid, JPAR_NT, 0, st>>>(a);
+    regf_na_finalize<<<(ni + FIN_WARPS - 1) / FIN_WARPS, FIN_WARPS * 32, 0, st>>>(
+        a.part, a.nslices, ni, a.nbcnt, a.nbbuf, a.lcap, cap, lmax, d_acc, d_jrk, d_pot, d_list);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        fprintf(stderr, "nb6_regf_noalloc: launch failed: %s\n", cudaGetErrorString(e));
+        nb6_fatal(NB6_ERR_CUDA);
+    }
+}
+
+}  // extern "C"

@@ -33,6 +33,7 @@ ABI_SYMBOLS = (
     "nb6_predict_device_", "nb6_predict_send_", "nb6_predict_last_kernel_ms_",
     "nb6_state_close_",
     "nb6_fp32_peak_probe_",
+    "nb6_regf_noalloc_",
 )
 
 _LIB: C.CDLL | None = None

@@ -1,0 +1,105 @@
+"""nb6_regf_noalloc_: the regular-force entry point for callers that cannot
+let the library allocate device memory (their GPU memory belongs to another
+allocator, or the run's allocation state must stay fixed).  It must give the
+same results as gpunb_regf_ on the same inputs -- lists identical, forces
+within the 1e-6 (acc, pot) / 1e-5 (jerk) relative tolerances of the parity
+tests -- and keep doing so on a second call in a row, since every call reuses
+the same fixed working array.
+
+The arrays handed to it are allocated here by the test (the caller), with
+torch; the entry point itself allocates nothing.  This file is named to be
+collected last.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from parity import rel_err_vec
+
+pytestmark = pytest.mark.gpu
+
+dp = C.c_void_p
+
+
+def _run_noalloc(raw, torch, dev, cl, isel, lmax, nnbmax, m_flag):
+    t = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float64, device=dev)
+    mj, xj, vj = t(cl.mass), t(cl.pos), t(cl.vel)
+    h2, dtr = t(cl.h2(m_flag)[isel]), t(cl.dtr[isel])
+    xi, vi = t(cl.pos[isel]), t(cl.vel[isel])
+    ni = len(isel)
+    acc = torch.zeros((ni, 3), dtype=torch.float64, device=dev)
+    jrk = torch.zeros((ni, 3), dtype=torch.float64, device=dev)
+    pot = torch.zeros(ni, dtype=torch.float64, device=dev)
+    lst = torch.zeros((ni, lmax), dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    ci = lambda v: C.byref(C.c_int(v))
+    raw.nb6_regf_noalloc_(ci(cl.n), dp(mj.data_ptr()), dp(xj.data_ptr()), dp(vj.data_ptr()),
+                          ci(ni), dp(h2.data_ptr()), dp(dtr.data_ptr()), dp(xi.data_ptr()),
+                          dp(vi.data_ptr()), dp(acc.data_ptr()), dp(jrk.data_ptr()),
+                          dp(pot.data_ptr()), ci(lmax), ci(nnbmax), dp(lst.data_ptr()),
+                          ci(m_flag), dp(stream.cuda_stream))
+    stream.synchronize()
+    return acc.cpu().numpy(), jrk.cpu().numpy(), pot.cpu().numpy(), lst.cpu().numpy()
+
+
+def _run_reference_entry(nb6, cl, isel, lmax, nnbmax, m_flag):
+    nb6.gpunb_open(cl.n + 10, 0)
+    try:
+        nb6.gpunb_send(cl.mass, cl.pos, cl.vel)
+        return nb6.gpunb_regf(cl.h2(m_flag)[isel], cl.dtr[isel], cl.pos[isel], cl.vel[isel],
+                              lmax, nnbmax, m_flag)
+    finally:
+        nb6.gpunb_close()
+
+
+def _compare(a, b):
+    acc, jrk, pot, lst = a
+    acc2, jrk2, pot2, lst2 = b
+    np.testing.assert_array_equal(lst[:, 0], lst2[:, 0])
+    for r in range(lst.shape[0]):
+        n = lst[r, 0]
+        if n > 0:
+            np.testing.assert_array_equal(lst[r, 1:1 + n], lst2[r, 1:1 + n])
+    ok = lst[:, 0] >= 0
+    assert rel_err_vec(acc[ok], acc2[ok]).max() <= 1e-6
+    assert rel_err_vec(pot[ok], pot2[ok]).max() <= 1e-6
+    assert rel_err_vec(jrk[ok], jrk2[ok]).max() <= 1e-5
+
+
+def test_noalloc_matches_gpunb_regf_twice_in_a_row(nb6):
+    import torch
+    from nb6b200 import ics
+    dev = torch.device("cuda", 0)
+    raw = nb6.lib
+    cases = [
+        (ics.plummer(3000, seed=21, imf=True), 777, 512, 400, 0),
+        (ics.plummer(5000, seed=22), 1024, 256, 200, 1),
+    ]
+    for cl, ni, lmax, nnbmax, m_flag in cases:
+        isel = np.sort(np.random.default_rng(ni).choice(cl.n, ni, replace=False))
+        want = _run_reference_entry(nb6, cl, isel, lmax, nnbmax, m_flag)
+        first = _run_noalloc(raw, torch, dev, cl, isel, lmax, nnbmax, m_flag)
+        second = _run_noalloc(raw, torch, dev, cl, isel, lmax, nnbmax, m_flag)
+        _compare(first, want)
+        _compare(second, want)
+
+
+def test_noalloc_rejects_sizes_beyond_its_array(nb6):
+    import nb6b200
+    raw = nb6.lib
+    nb6b200.set_abort_on_error(False)
+    try:
+        nb6b200.last_status()
+        ci = lambda v: C.byref(C.c_int(v))
+        null = dp(0)
+        # ni above 1024: rejected on the host before anything is launched
+        raw.nb6_regf_noalloc_(ci(10), null, null, null, ci(1025), null, null, null, null, null,
+                              null, null, ci(64), ci(50), null, ci(0), null)
+        assert nb6b200.last_status() == 6
+        # list cap above 511
+        raw.nb6_regf_noalloc_(ci(10), null, null, null, ci(8), null, null, null, null, null,
+                              null, null, ci(1000), ci(900), null, ci(0), null)
+        assert nb6b200.last_status() == 6
+    finally:
+        nb6b200.set_abort_on_error(True)
