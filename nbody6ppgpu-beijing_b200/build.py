@@ -47,7 +47,27 @@ def _stale() -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+DRIVER_SRC = os.path.join(HERE, "driver", "blockstep.cpp")
+DRIVER_LIB = os.path.join(HERE, "libnb6drive.so")
+
+
+def build_driver(force: bool = False, verbose: bool = False) -> str:
+    """The C++ block-step driver (host code only, loads force backends with dlopen)."""
+    if (not force and os.path.exists(DRIVER_LIB)
+            and os.path.getmtime(DRIVER_LIB) >= os.path.getmtime(DRIVER_SRC)):
+        return DRIVER_LIB
+    cxx = shutil.which("g++") or "g++"
+    cmd = [cxx, "-O2", "-std=c++17", "-fPIC", "-shared", "-Wall", "-o", DRIVER_LIB + ".tmp",
+           DRIVER_SRC, "-ldl"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    os.replace(DRIVER_LIB + ".tmp", DRIVER_LIB)
+    return DRIVER_LIB
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
+    build_driver(force=force, verbose=verbose)
     if not force and not _stale():
         return LIB
     os.makedirs(BUILD_DIR, exist_ok=True)
