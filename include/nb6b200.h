@@ -133,6 +133,52 @@ void nb6_regf_tune_(int *variant, int *nslices);
  * (default, or NB6_AUTOTUNE=0 in the environment for off), 0 off, -1 clears
  * the cached choices. */
 void nb6_regf_autotune_(int *flag);
+/* Regular-force calls (gpunb_regf_, nb6_regf_device_) are submitted as one
+ * CUDA graph launch each: the graph of a call kind is built once and its
+ * nodes re-parameterised per call.  flag 1 = on (default; NB6_GRAPHS=0 in
+ * the environment for off), 0 = off (plain launches), other values leave it
+ * unchanged.  counts[3] receives {graphs built, graph launches, on}. */
+void nb6_regf_graphs_(int *flag, long long *counts);
+
+/* Segmented regular force for ensembles of independent clusters sent
+ * together (one persistent launch for all of them).  Segment c is the j
+ * range [seg_j0[c], seg_j0[c+1]) of the last send; active particle k belongs
+ * to segment iseg[k] (non-decreasing) and interacts with that segment only.
+ * Outputs as gpunb_regf_ (reference layout), list ids relative to
+ * seg_j0[iseg[k]].  No reference counterpart: the reference runs one cluster
+ * per process. */
+void nb6_regf_seg_(int *ni, int *iseg, double *h2, double *dtr, double (*xi)[3], double (*vi)[3],
+                   double (*acc)[3], double (*jrk)[3], double *pot, int *lmax, int *nnbmax,
+                   int *list, int *m_flag, int *nseg, int *seg_j0);
+
+/* The regular-force j set made on the device from the irregular library's
+ * resident records (irr_simd_set_jp_), predicted to *t: segment s is the
+ * count[s] records from 1-based address addr0[s], laid out back to back.
+ * Replaces XBPREDALL + GPUNB_SEND (intgrt.F:866-882) without host
+ * prediction or j upload.  Needs gpunb_open_ and irr_simd_open_. */
+void nb6_irr_predict_send_(double *t, int *nseg, int *addr0, int *count);
+
+/* Learned neighbour radius (no reference counterpart; its fallback is the
+ * reference's Ahmad-Cohen rule, regcor_gpu.F:131-196).  A 5-64-64-1 SiLU
+ * network, bf16 parameters, FP32 sums, proposing dlog = log(RS_next / RS)
+ * from a particle's regular-step features: log(1+nnb), log RS,
+ * log(1+nnb) - 1.5 log h2, log|a_reg|, -log2 dtr.  A model is
+ * nb6_mlp_size_() floats: 4609 parameters then in_mean[5], in_scale[5],
+ * out_mean, out_std.  Training runs on the GPU (Adam, mean squared error in
+ * standardised units); x is [n][5], y [n]. */
+int nb6_mlp_size_(void);
+void nb6_mlp_init_(int *seed);
+void nb6_mlp_set_(const float *model);
+void nb6_mlp_get_(float *model);
+void nb6_mlp_grad_(int *n, const float *x, const float *y, float *grad, float *loss);
+void nb6_mlp_train_(int *n, const float *x, const float *y, int *epochs, int *batch, float *lr,
+                    int *seed, float *loss_hist);
+void nb6_mlp_predict_(int *n, const float *x, float *y);
+/* 1: every regular-force call also evaluates the model in its epilogue on
+ * its own results; nb6_regf_proposals_ returns the last call's dlog per
+ * active particle.  0: off (default). */
+void nb6_mlp_enable_(int *flag);
+void nb6_regf_proposals_(int *ni, double *out);
 
 /* Synchronise the library stream (and check the device status); the stream
  * handle itself for callers that record events on it. */

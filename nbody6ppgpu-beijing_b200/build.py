@@ -47,18 +47,20 @@ def _stale() -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-DRIVER_SRC = os.path.join(HERE, "driver", "blockstep.cpp")
+DRIVER_SRCS = [os.path.join(HERE, "driver", f) for f in ("blockstep.cpp", "ensemble.cpp")]
+DRIVER_DEPS = DRIVER_SRCS + [os.path.join(HERE, "driver", "hermite.h")]
 DRIVER_LIB = os.path.join(HERE, "libnb6drive.so")
 
 
 def build_driver(force: bool = False, verbose: bool = False) -> str:
-    """The C++ block-step driver (host code only, loads force backends with dlopen)."""
+    """The C++ block-step drivers, single cluster and ensemble (host code only,
+    loads force backends with dlopen)."""
     if (not force and os.path.exists(DRIVER_LIB)
-            and os.path.getmtime(DRIVER_LIB) >= os.path.getmtime(DRIVER_SRC)):
+            and all(os.path.getmtime(DRIVER_LIB) >= os.path.getmtime(d) for d in DRIVER_DEPS)):
         return DRIVER_LIB
     cxx = shutil.which("g++") or "g++"
     cmd = [cxx, "-O2", "-std=c++17", "-fPIC", "-shared", "-Wall", "-o", DRIVER_LIB + ".tmp",
-           DRIVER_SRC, "-ldl"]
+           *DRIVER_SRCS, "-ldl"]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)

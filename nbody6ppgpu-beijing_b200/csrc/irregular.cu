@@ -18,8 +18,11 @@
 #include "nb6_common.cuh"
 
 #include <algorithm>
+#include <climits>
 #include <string.h>
 #include <vector>
+
+bool regular_bind_j(int n, double **jm, double **jx, double **jv, JSetOut *out);
 
 namespace {
 
@@ -141,6 +144,53 @@ __global__ void irr_scatter_list(int ne, const int *__restrict__ off, const int 
     for (int l = lane; l < nnb; l += 32) row[1 + l] = e[2 + l];
 }
 
+// Predict resident records to time t and write them as the regular-force j
+// set: output body q lies in segment s with segoff[s] <= q < segoff[s+1] and
+// is record addr0[s] + (q - segoff[s]).  The predictor is xbpredall.F:50-59
+// with every operation rounded separately (no FMA contraction), so the
+// values equal a host FP64 prediction of the same state bit for bit.
+__global__ void irr_predict_pack(int n, double t, int nseg, const int *__restrict__ segoff,
+                                 const int *__restrict__ addr0, const Rec *__restrict__ rec,
+                                 double *__restrict__ jm, double *__restrict__ jx,
+                                 double *__restrict__ jv, JSetOut o, int *status) {
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < o.npad;
+         q += (size_t)gridDim.x * blockDim.x) {
+        if (q >= (size_t)n) {
+            write_j(o, q, false, 0, 0, 0, 0, 0, 0, 0);
+            continue;
+        }
+        int lo = 0, hi = nseg - 1;  // last segment with segoff <= q
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (segoff[mid] <= (int)q) lo = mid;
+            else hi = mid - 1;
+        }
+        Rec r;
+        load_rec(rec + addr0[lo] + ((int)q - segoff[lo]), r);
+        const double s = __dsub_rn(t, r.t0);
+        const double s1 = __dmul_rn(1.5, s), s2 = __dmul_rn(2.0, s);
+        double x[3], v[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            x[k] = __dadd_rn(__dmul_rn(__dadd_rn(__dmul_rn(__dadd_rn(__dmul_rn(r.fd[k], s), r.f[k]), s),
+                                                 r.v[k]),
+                                       s),
+                             r.x[k]);
+            v[k] = __dadd_rn(__dmul_rn(__dadd_rn(__dmul_rn(r.fd[k], s1), r.f[k]), s2), r.v[k]);
+        }
+        if (x[0] != x[0] || x[1] != x[1] || x[2] != x[2] || v[0] != v[0] || v[1] != v[1] ||
+            v[2] != v[2] || r.m != r.m)
+            set_status(status, NB6_ERR_NAN_INPUT);
+        jm[q] = r.m;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            jx[3 * q + k] = x[k];
+            jv[3 * q + k] = v[k];
+        }
+        write_j(o, q, true, x[0], x[1], x[2], r.m, v[0], v[1], v[2]);
+    }
+}
+
 struct IrrState {
     bool open = false;
     int nmax = 0, lmax = 0;
@@ -149,6 +199,8 @@ struct IrrState {
     DevBuf<Rec> dstage_rec;
     DevBuf<int> dstage_addr, dstage_list, dstage_off, daddr, dnnbid;
     DevBuf<double> dout;
+    DevBuf<int> dseg;      // predict-send segment tables
+    HostBuf<int> hseg;
     HostBuf<Rec> hstage_rec;
     HostBuf<int> hstage_addr, hstage_list, hstage_off, haddr, hnnbid;
     HostBuf<double> hout;
@@ -204,6 +256,8 @@ void irr_close_impl() {
     I.daddr.release();
     I.dnnbid.release();
     I.dout.release();
+    I.dseg.release();
+    I.hseg.release();
     I.hstage_rec.release();
     I.hstage_addr.release();
     I.hstage_list.release();
@@ -396,6 +450,48 @@ void irr_firr_vec_impl(double ti, int ni, const int *addr, double (*acc)[3], dou
     I.num_steps += ni;
 }
 
+// The regular-force j set from the resident records: segments of
+// consecutive addresses, predicted to t on the device (see irr_predict_pack).
+void irr_predict_send_impl(double t, int nseg, const int *addr0, const int *count) {
+    if (!I.open) {
+        nb6_fatal(NB6_ERR_NOT_OPEN);
+        return;
+    }
+    long long n = 0;
+    bool bad = nseg <= 0;
+    for (int s = 0; s < nseg && !bad; ++s) {
+        bad = count[s] < 0 || addr0[s] < 1 || (long long)addr0[s] - 1 + count[s] > I.nmax;
+        n += count[s];
+    }
+    if (bad || n > INT_MAX / 4) {
+        fprintf(stderr, "nb6_irr_predict_send: segment outside [1, %d]\n", I.nmax);
+        nb6_fatal(NB6_ERR_BAD_ARG);
+        return;
+    }
+    cudaStream_t st = nb6_stream();
+    irr_flush(st);  // records staged by set_jp must be on the device first
+    double *jm, *jx, *jv;
+    JSetOut o;
+    if (!regular_bind_j((int)n, &jm, &jx, &jv, &o)) return;
+    // [segoff (nseg+1) | addr0 - 1 (nseg)]
+    I.hseg.reserve(2 * (size_t)nseg + 1);
+    I.dseg.reserve(2 * (size_t)nseg + 1);
+    int *h = I.hseg.ptr;
+    h[0] = 0;
+    for (int s = 0; s < nseg; ++s) {
+        h[s + 1] = h[s] + count[s];
+        h[nseg + 1 + s] = addr0[s] - 1;
+    }
+    NB6_CUDA_CHECK(cudaMemcpyAsync(I.dseg.ptr, h, sizeof(int) * (2 * (size_t)nseg + 1),
+                                   cudaMemcpyHostToDevice, st));
+    const int blocks = (int)std::min<size_t>((o.npad + 255) / 256, (size_t)nb6_num_sms() * 8);
+    irr_predict_pack<<<blocks, 256, 0, st>>>((int)n, t, nseg, I.dseg.ptr, I.dseg.ptr + nseg + 1, I.rec.ptr,
+                                             jm, jx, jv, o, nb6_dev_status());
+    NB6_CUDA_CHECK(cudaGetLastError());
+    // the host table may be rewritten by the next call: wait for the copy
+    NB6_CUDA_CHECK(cudaStreamSynchronize(st));
+}
+
 void irr_profile_impl(int rank) {
     if (I.open && I.num_fcall) {
         const double gf = I.time_grav > 0 ? 60.0 * (double)I.num_inter * 1e-9 / I.time_grav : 0.0;
@@ -433,5 +529,15 @@ void gpuirr_set_jp_(int *addr, double pos[3], double vel[3], double acc2[3], dou
     irr_set_jp_impl(*addr - 1, pos, vel, acc2, jrk6, *mass, *time);
 }
 void gpuirr_set_list_(int *addr, int *nblist) { irr_set_list_impl(*addr - 1, nblist); }
+
+// Extension (no reference counterpart): make the regular-force j set (what
+// gpunb_send_ sends) from the resident irregular records, predicted to *t on
+// the device.  Segment s is the count[s] records from 1-based address
+// addr0[s]; segments are laid out back to back in the j set.  Records staged
+// by irr_simd_set_jp_ are uploaded first.  Replaces XBPREDALL + GPUNB_SEND
+// (intgrt.F:866-882) with no host prediction and no j upload.
+void nb6_irr_predict_send_(double *t, int *nseg, int *addr0, int *count) {
+    irr_predict_send_impl(*t, *nseg, addr0, count);
+}
 
 }  // extern "C"

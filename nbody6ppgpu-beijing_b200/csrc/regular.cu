@@ -24,12 +24,16 @@
 // sent, ascending, self included; nnb > nnbmax -> list[0] = -nnb and no ids
 // (reg.avx.cpp:320-327).
 #include "nb6_common.cuh"
+#include "mlp.cuh"
 
 #include <algorithm>
 #include <climits>
 #include <map>
+#include <vector>
 #include <math.h>
 #include <string.h>
+
+MlpArgs nb6_mlp_args(const double *h2, const double *dtr);  // mlp.cu
 
 namespace {
 
@@ -148,7 +152,7 @@ NB6_DEV bool reg_pair(const IPart &ip, const float4 &a, const float4 &b, const f
 // Operation order matches the FP64 rule of regint.f:41-65 with the strict
 // "<" of gpunb.velocity.cu:188,236; no FMA contraction.
 template <bool MFLAG>
-NB6_DEV void reg_exact(const RegArgs &a, int i, int j, Sums &s) {
+NB6_DEV void reg_exact(const RegArgs &a, int i, int j, Sums &s, int joff = 0) {
     const double xi0 = a.ix[3 * i], xi1 = a.ix[3 * i + 1], xi2 = a.ix[3 * i + 2];
     const double vi0 = a.iv[3 * i], vi1 = a.iv[3 * i + 1], vi2 = a.iv[3 * i + 2];
     const double h2 = a.ih2[i], dt = a.idtr[i];
@@ -170,7 +174,7 @@ NB6_DEV void reg_exact(const RegArgs &a, int i, int j, Sums &s) {
         const double crit = MFLAG ? __dmul_rn(a.jm[j], h2) : h2;
         if (rmin < crit) {
             const int pos = atomicAdd(&a.nbcnt[i], 1);
-            if (pos < a.lcap) a.nbbuf[(size_t)i * a.lcap + pos] = j;
+            if (pos < a.lcap) a.nbbuf[(size_t)i * a.lcap + pos] = j - joff;
         } else {
             // inside the slack band but not a neighbour: add it here
             const double rinv2 = 1.0 / r2;
@@ -788,31 +792,25 @@ __global__ void __launch_bounds__(JPAR_NT) regf_jpar_kernel(const RegArgs a) {
     }
 }
 
-// One warp per i: FP64 sum over slices in a fixed order, then the neighbour
-// ids sorted ascending.  outf row = (ax, ay, az, jx, jy, jz, pot, 0).
-__global__ void __launch_bounds__(FIN_WARPS * 32)
-    regf_finalize(const float4 *__restrict__ part, int nslices, int ni, int ni_pad,
-                  const int *__restrict__ nbcnt, const int *__restrict__ nbbuf, int lcap,
-                  int cap, int W, int pmax, double *__restrict__ outf,
-                  int *__restrict__ outl) {
-    extern __shared__ int sbuf[];
-    const int warp = threadIdx.x >> 5;
-    const int lane = threadIdx.x & 31;
-    const int i = blockIdx.x * FIN_WARPS + warp;
-    if (i >= ni) return;
+// Accumulate one (hi, lo) slice partial into FP64 sums.
+NB6_DEV void add_partial(const float4 *p, double *v) {
+    const float4 q0 = p[0], q1 = p[1], q2 = p[2], q3 = p[3];
+    v[0] += (double)q0.x + (double)q0.y;
+    v[1] += (double)q0.z + (double)q0.w;
+    v[2] += (double)q1.x + (double)q1.y;
+    v[3] += (double)q1.z + (double)q1.w;
+    v[4] += (double)q2.x + (double)q2.y;
+    v[5] += (double)q2.z + (double)q2.w;
+    v[6] += (double)q3.x + (double)q3.y;
+}
 
-    double v[7] = {0, 0, 0, 0, 0, 0, 0};
-    for (int sl = lane; sl < nslices; sl += 32) {
-        const float4 *p = part + ((size_t)sl * ni_pad + i) * 4;
-        const float4 q0 = p[0], q1 = p[1], q2 = p[2], q3 = p[3];
-        v[0] += (double)q0.x + (double)q0.y;
-        v[1] += (double)q0.z + (double)q0.w;
-        v[2] += (double)q1.x + (double)q1.y;
-        v[3] += (double)q1.z + (double)q1.w;
-        v[4] += (double)q2.x + (double)q2.y;
-        v[5] += (double)q2.z + (double)q2.w;
-        v[6] += (double)q3.x + (double)q3.y;
-    }
+// Second half of a finalize row (one warp, one i): reduce the lanes' FP64
+// sums, write outf, reset the neighbour counter, and write the list row
+// sorted ascending (warp bitonic sort in shared memory) or -nnb on overflow.
+NB6_DEV void finalize_row(int i, int lane, double *v, int *__restrict__ nbcnt,
+                          const int *__restrict__ nbbuf, int lcap, int cap, int W, int *sb,
+                          double *__restrict__ outf, int *__restrict__ outl, const MlpArgs &mlp,
+                          const __nv_bfloat16 *sw) {
 #pragma unroll
     for (int c = 0; c < 7; ++c) v[c] = warp_sum_d(v[c]);
     if (lane == 0) {
@@ -828,12 +826,22 @@ __global__ void __launch_bounds__(FIN_WARPS * 32)
     }
 
     const int n = nbcnt[i];
+    __syncwarp();
+    if (lane == 0) nbcnt[i] = 0;
+    if (mlp.on) {
+        // learned radius proposal from this call's own results (out slot 7)
+        float fe[MLP_IN];
+        const double ax = v[0] * 0.125, ay = v[1] * 0.125, az = v[2] * 0.125;
+        mlp_features((double)n, mlp.h2[i], ax * ax + ay * ay + az * az, mlp.dtr[i], fe);
+        MlpAct act;
+        const float out = mlp_forward_warp(sw, mlp.norm, fe, lane, act);
+        if (lane == 0) outf[(size_t)i * 8 + 7] = (double)(out * mlp.norm[2 * MLP_IN + 1] + mlp.norm[2 * MLP_IN]);
+    }
     int *row = outl + (size_t)i * W;
     if (n > cap) {
         if (lane == 0) row[0] = -n;
         return;
     }
-    int *sb = sbuf + warp * pmax;
     int P = 32;
     while (P < n) P <<= 1;
     const int *src = nbbuf + (size_t)i * lcap;
@@ -857,6 +865,160 @@ __global__ void __launch_bounds__(FIN_WARPS * 32)
     }
     if (lane == 0) row[0] = n;
     for (int k = lane; k < n; k += 32) row[1 + k] = sb[k];
+}
+
+// One warp per i: FP64 sum over slices in a fixed order, then the neighbour
+// ids sorted ascending.  outf row = (ax, ay, az, jx, jy, jz, pot, 0).  The
+// neighbour counter of i is reset to zero once read, so the next call starts
+// from clean counters without a memset.
+__global__ void __launch_bounds__(FIN_WARPS * 32)
+    regf_finalize(const float4 *__restrict__ part, int nslices, int ni, int ni_pad,
+                  int *__restrict__ nbcnt, const int *__restrict__ nbbuf, int lcap,
+                  int cap, int W, int pmax, double *__restrict__ outf,
+                  int *__restrict__ outl, const MlpArgs mlp) {
+    extern __shared__ __align__(16) int sbuf[];
+    __nv_bfloat16 *sw = reinterpret_cast<__nv_bfloat16 *>(sbuf + FIN_WARPS * pmax);
+    if (mlp.on) {
+        mlp_load(sw, mlp.w);
+        __syncthreads();
+    }
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int i = blockIdx.x * FIN_WARPS + warp;
+    if (i >= ni) return;
+    double v[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (int sl = lane; sl < nslices; sl += 32) add_partial(part + ((size_t)sl * ni_pad + i) * 4, v);
+    finalize_row(i, lane, v, nbcnt, nbbuf, lcap, cap, W, sbuf + warp * pmax, outf, outl, mlp, sw);
+}
+
+// ----------------------------------------------------------------------------
+// Segmented regular force (ensembles of independent clusters in one call).
+//
+// The j set holds several clusters back to back; segment c is the j range
+// [seg_j0[c], seg_j0[c+1]).  Every active i belongs to one segment and sees
+// only that segment's j: the same force, jerk, potential and neighbour rule
+// as gpunb_regf_ with that cluster alone sent, list ids relative to the
+// segment's first j.  The work is a list of items (segment, group of up to IB
+// consecutive i of that segment, j chunk), built on the host with the costly
+// items first; one persistent launch of SMs x occupancy CTAs walks the list
+// (grid-stride), each item running the j-parallel inner loop of
+// regf_jpar_kernel (threads over j, the IB i in shared memory).  Item q of an
+// i writes its (hi, lo) partial to slot pinfo[i].x + q; regf_finalize_seg
+// sums the pinfo[i].y slots of each i in order.
+// ----------------------------------------------------------------------------
+struct SegItem {
+    int i0, ni, j0, j1, jbase, q, pad0, pad1;
+};
+
+template <int IB, bool MFLAG>
+__global__ void __launch_bounds__(JPAR_NT)
+    regf_seg_kernel(const RegArgs a, const SegItem *__restrict__ items, const int *__restrict__ nitems_p,
+                    const int2 *__restrict__ pinfo) {
+    __shared__ float4 sip[IB][3];
+    __shared__ double red[JPAR_NT / 32][IB][7];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nitems = *nitems_p;
+    for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
+        const SegItem it = items[w];
+        __syncthreads();  // the previous item is done with sip and red
+        if (tid < IB) {
+            float4 p = make_float4(0.f, 0.f, 0.f, 0.f), q = p, r = p;  // padding: never a candidate
+            if (tid < it.ni) {
+                const int i = it.i0 + tid;
+                split_hl(a.ix[3 * i], p.x, q.x);
+                split_hl(a.ix[3 * i + 1], p.y, q.y);
+                split_hl(a.ix[3 * i + 2], p.z, q.z);
+                p.w = (float)a.ih2[i] * CAND_SLACK;
+                q.w = (float)a.idtr[i];
+                r = make_float4((float)a.iv[3 * i], (float)a.iv[3 * i + 1], (float)a.iv[3 * i + 2], 0.f);
+            }
+            sip[tid][0] = p;
+            sip[tid][1] = q;
+            sip[tid][2] = r;
+        }
+        __syncthreads();
+        Sums s[IB];
+#pragma unroll
+        for (int k = 0; k < IB; ++k) zero(s[k]);
+        for (int j = it.j0 + tid; j < it.j1; j += JPAR_NT) {
+            const float4 pa = __ldg(a.posH + j);
+            const float4 pb = __ldg(a.posL + j);
+            const float4 pc = __ldg(a.vel + j);
+            bool any = false;
+#pragma unroll
+            for (int k = 0; k < IB; ++k) {
+                const float4 p = sip[k][0], q = sip[k][1], r = sip[k][2];
+                IPart ip;
+                ip.xh = p.x; ip.yh = p.y; ip.zh = p.z; ip.h2c = p.w;
+                ip.xl = q.x; ip.yl = q.y; ip.zl = q.z; ip.dt = q.w;
+                ip.vx = r.x; ip.vy = r.y; ip.vz = r.z;
+                any |= reg_pair<MFLAG>(ip, pa, pb, pc, s[k]);
+            }
+            if (any) {
+                for (int k = 0; k < it.ni && k < IB; ++k) {
+                    const float4 p = sip[k][0], q = sip[k][1], r = sip[k][2];
+                    IPart ip;
+                    ip.xh = p.x; ip.yh = p.y; ip.zh = p.z; ip.h2c = p.w;
+                    ip.xl = q.x; ip.yl = q.y; ip.zl = q.z; ip.dt = q.w;
+                    ip.vx = r.x; ip.vy = r.y; ip.vz = r.z;
+                    if (reg_geom<MFLAG>(ip, pa, pb, pc).cand) reg_exact<MFLAG>(a, it.i0 + k, j, s[k], it.jbase);
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < IB; ++k) {
+            double v[7] = {s[k].ax, s[k].ay, s[k].az, s[k].jx, s[k].jy, s[k].jz, s[k].po};
+#pragma unroll
+            for (int c = 0; c < 7; ++c) {
+                const double wsum = warp_sum_d(v[c]);
+                if (lane == 0) red[warp][k][c] = wsum;
+            }
+        }
+        __syncthreads();
+        if (tid < IB * 7) {
+            const int k = tid / 7, c = tid % 7;
+            double wsum = 0.0;
+#pragma unroll
+            for (int q = 0; q < JPAR_NT / 32; ++q) wsum += red[q][k][c];
+            red[0][k][c] = wsum;
+        }
+        __syncthreads();
+        if (tid < it.ni && tid < IB) {
+            const int i = it.i0 + tid;
+            float hv[7], lv[7];
+#pragma unroll
+            for (int c = 0; c < 7; ++c) {
+                const double wsum = red[0][tid][c];
+                hv[c] = (float)wsum;
+                lv[c] = (float)(wsum - (double)hv[c]);
+            }
+            float4 *p = a.part + ((size_t)pinfo[i].x + it.q) * 4;
+            p[0] = make_float4(hv[0], lv[0], hv[1], lv[1]);
+            p[1] = make_float4(hv[2], lv[2], hv[3], lv[3]);
+            p[2] = make_float4(hv[4], lv[4], hv[5], lv[5]);
+            p[3] = make_float4(hv[6], lv[6], 0.f, 0.f);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(FIN_WARPS * 32)
+    regf_finalize_seg(const float4 *__restrict__ part, const int2 *__restrict__ pinfo, int ni,
+                      int *__restrict__ nbcnt, const int *__restrict__ nbbuf, int lcap, int cap, int W,
+                      int pmax, double *__restrict__ outf, int *__restrict__ outl, const MlpArgs mlp) {
+    extern __shared__ __align__(16) int sbuf[];
+    __nv_bfloat16 *sw = reinterpret_cast<__nv_bfloat16 *>(sbuf + FIN_WARPS * pmax);
+    if (mlp.on) {
+        mlp_load(sw, mlp.w);
+        __syncthreads();
+    }
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int i = blockIdx.x * FIN_WARPS + warp;
+    if (i >= ni) return;
+    const int2 pi = pinfo[i];
+    double v[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (int q = lane; q < pi.y; q += 32) add_partial(part + ((size_t)pi.x + q) * 4, v);
+    finalize_row(i, lane, v, nbcnt, nbbuf, lcap, cap, W, sbuf + warp * pmax, outf, outl, mlp, sw);
 }
 
 // FP64 (m, x, v) -> SoA float4 tiles; padding slots are massless and far.
@@ -923,6 +1085,20 @@ struct RegState {
     int autotune = -1;                 // -1 = read NB6_AUTOTUNE on first use
     std::map<TuneKey, int> tuned;      // bucket -> best variant
     cudaEvent_t tev0 = nullptr, tev1 = nullptr;
+    // CUDA graphs of one call: [0] device-resident i data, [1] host i data
+    // with the copies in the graph.  Built once, then re-parameterised per
+    // call (launch geometry, kernel, pointers, copy sizes).
+    struct Graph {
+        cudaGraph_t g = nullptr;
+        cudaGraphExec_t x = nullptr;
+        cudaGraphNode_t h2d = nullptr, kmain = nullptr, kfin = nullptr, d2hf = nullptr, d2hl = nullptr;
+    } graph[2];
+    int use_graphs = -1;               // -1 = read NB6_GRAPHS on first use
+    long long graph_builds = 0, graph_launches = 0;
+    bool nbcnt_dirty = true;           // neighbour counters not known to be zero
+    // segmented calls: work list and per-i partial slots, staged as ints
+    HostBuf<int> hseg;
+    DevBuf<int> dseg;
 };
 RegState R;
 
@@ -1024,6 +1200,22 @@ template <bool MF> void launch_plan(const Plan &p, const RegArgs &a, cudaStream_
     }
 }
 
+// The kernel launch_plan would launch, as a function handle for graph nodes.
+template <bool MF> const void *kernel_of(int variant) {
+    switch (variant) {
+        case 1: return (const void *)regf_kernel<1, MF>;
+        case 2: return (const void *)regf_kernel<2, MF>;
+        case 4: return (const void *)regf_kernel<4, MF>;
+        case 11: return (const void *)regf_x2_kernel<1, MF>;
+        case 12: return (const void *)regf_x2_kernel<2, MF>;
+        case 13: return (const void *)regf_x2_kernel<1, MF, true>;
+        case -1: return (const void *)regf_jpar_kernel<1, MF>;
+        case -2: return (const void *)regf_jpar_kernel<2, MF>;
+        case -4: return (const void *)regf_jpar_kernel<4, MF>;
+        default: return (const void *)regf_jpar_kernel<8, MF>;
+    }
+}
+
 int ilog2(int v) {
     int r = 0;
     while ((1 << (r + 1)) <= v) ++r;
@@ -1063,14 +1255,52 @@ static JSetOut size_j_buffers(int n) {
 }
 
 // ----------------------------------------------------------------------------
-// device-side regular force on resident i data (used by the ABI and by the
-// benchmark's kernel-only timing)
+// One regular-force call on resident i data, in three steps:
+//   regf_prepare  pick the launch plan (autotuner), size the buffers;
+//   regf_eager    memset + force kernel + finalize (+ copies) as launches;
+//   regf_submit   the same work as one CUDA graph launch.
+// The graph of each call kind is built once and re-parameterised per call
+// (cudaGraphExec*SetParams: kernel, grid, arguments, copy sizes), so calls
+// of any ni replay it without a new capture.  The neighbour counters are
+// zeroed by regf_finalize itself, which keeps memsets out of the graph.
 // ----------------------------------------------------------------------------
-static void regf_device(int ni, const double *d_h2, const double *d_dtr, const double *d_x,
-                        const double *d_v, int lmax, int nnbmax, int mflag, cudaStream_t st,
-                        int &W) {
+struct RegLaunch {
+    Plan plan;
+    RegArgs a;
+    int ni = 0, W = 1, cap = 0, pmax = 32, fblocks = 1;
+    size_t smem = 0;
+    bool mf = false;
+    MlpArgs mlp{};
+    // host staging (graph node of kind 1)
+    const double *hin = nullptr;
+    size_t in_bytes = 0;
+};
+
+// Arguments of regf_finalize, addressable for a kernel node.
+struct FinArgs {
+    const float4 *part;
+    int nslices, ni, ni_pad;
+    int *nbcnt;
+    const int *nbbuf;
+    int lcap, cap, W, pmax;
+    double *outf;
+    int *outl;
+    MlpArgs mlp;
+    void *p[13];
+    explicit FinArgs(const RegLaunch &L)
+        : part(L.a.part), nslices(L.plan.nslices), ni(L.ni), ni_pad(L.a.ni_pad), nbcnt(L.a.nbcnt),
+          nbbuf(L.a.nbbuf), lcap(L.a.lcap), cap(L.cap), W(L.W), pmax(L.pmax), outf(R.outf.ptr),
+          outl(R.outl.ptr), mlp(L.mlp) {
+        void *q[13] = {&part, &nslices, &ni, &ni_pad, &nbcnt, &nbbuf, &lcap, &cap, &W, &pmax, &outf, &outl, &mlp};
+        memcpy(p, q, sizeof(q));
+    }
+};
+
+static void regf_prepare(int ni, const double *d_h2, const double *d_dtr, const double *d_x,
+                         const double *d_v, int lmax, int nnbmax, int mflag, cudaStream_t st,
+                         RegLaunch &L) {
     const int cap = std::max(0, std::min(nnbmax, lmax - 1));
-    W = cap + 1;
+    const int W = cap + 1;
     const int ni_pad = ni;
     const bool mf = mflag != 0;
     if (R.autotune < 0) {
@@ -1111,11 +1341,13 @@ static void regf_device(int ni, const double *d_h2, const double *d_dtr, const d
             max_slices = std::max<size_t>(max_slices,
                                           make_plan(cands[c], ni, R.nj, R.ntile, mf, 0).nslices);
     R.part.reserve(max_slices * ni_pad * 4);
+    const int *cnt_before = R.nbcnt.ptr;
+    const size_t cnt_cap_before = R.nbcnt.cap;
     R.nbcnt.reserve(ni);
+    if (R.nbcnt.ptr != cnt_before || R.nbcnt.cap != cnt_cap_before) R.nbcnt_dirty = true;
     R.nbbuf.reserve((size_t)ni * std::max(cap, 1));
     R.outf.reserve((size_t)ni * 8);
     R.outl.reserve((size_t)ni * W);
-    NB6_CUDA_CHECK(cudaMemsetAsync(R.nbcnt.ptr, 0, sizeof(int) * ni, st));
 
     RegArgs a;
     a.posH = R.posH.ptr;
@@ -1151,6 +1383,9 @@ static void regf_device(int ni, const double *d_h2, const double *d_dtr, const d
         NB6_CUDA_CHECK(cudaEventCreate(&R.tev1));
     }
     if (tune_now) {
+        // the trials read the i data: stage it first when the call brings it
+        if (L.hin)
+            NB6_CUDA_CHECK(cudaMemcpyAsync(R.iin.ptr, L.hin, L.in_bytes, cudaMemcpyHostToDevice, st));
         // time each candidate once (twice for the first, to skip cold
         // effects); neighbour counters are reset before every trial
         float best = 1e30f;
@@ -1174,38 +1409,197 @@ static void regf_device(int ni, const double *d_h2, const double *d_dtr, const d
                 bestv = v;
             }
         }
+        R.nbcnt_dirty = true;
         R.tuned[key] = bestv;
         variant = bestv;
         plan = make_plan(variant, ni, R.nj, R.ntile, mf, R.forced_slices);
         a.nslices = plan.nslices;
-        NB6_CUDA_CHECK(cudaMemsetAsync(R.nbcnt.ptr, 0, sizeof(int) * ni, st));
         if (getenv("NB6_VERBOSE"))
             fprintf(stderr, "# nb6 autotune: ni~2^%d nj~2^%d mflag %d -> variant %d (%.3f ms)\n",
                     key.li, key.lj, key.mf, bestv, best);
     }
-    // kernel-only timing of the main force kernel (read by
-    // nb6_regf_last_kernel_ms_ after the stream has drained)
-    NB6_CUDA_CHECK(cudaEventRecord(R.ev0, st));
-    if (mf) launch_plan<true>(plan, a, st);
-    else launch_plan<false>(plan, a, st);
-    NB6_CUDA_CHECK(cudaGetLastError());
-    NB6_CUDA_CHECK(cudaEventRecord(R.ev1, st));
-    const int nslices = plan.nslices;
     R.last_geometry[0] = plan.variant;
     R.last_geometry[1] = plan.igrid;
     R.last_geometry[2] = plan.nslices;
 
     int pmax = 32;
     while (pmax < cap) pmax <<= 1;
-    const int fblocks = (ni + FIN_WARPS - 1) / FIN_WARPS;
-    const size_t smem = (size_t)FIN_WARPS * pmax * sizeof(int);
+    const MlpArgs mlp = nb6_mlp_args(d_h2, d_dtr);
+    const size_t smem = (size_t)FIN_WARPS * pmax * sizeof(int) + (mlp.on ? MLP_SMEM_BYTES : 0);
     if (smem > 48 * 1024)
         NB6_CUDA_CHECK(cudaFuncSetAttribute(regf_finalize, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)smem));
-    regf_finalize<<<fblocks, FIN_WARPS * 32, smem, st>>>(R.part.ptr, nslices, ni, ni_pad,
-                                                        R.nbcnt.ptr, R.nbbuf.ptr, a.lcap, cap, W,
-                                                        pmax, R.outf.ptr, R.outl.ptr);
+    L.mlp = mlp;
+    L.plan = plan;
+    L.a = a;
+    L.ni = ni;
+    L.W = W;
+    L.cap = cap;
+    L.pmax = pmax;
+    L.smem = smem;
+    L.fblocks = (ni + FIN_WARPS - 1) / FIN_WARPS;
+    L.mf = mf;
+}
+
+// Copies back to the host staging buffers (kind 1 only).
+static void regf_copy_out(const RegLaunch &L, cudaStream_t st) {
+    NB6_CUDA_CHECK(cudaMemcpyAsync(R.houtf.ptr, R.outf.ptr, sizeof(double) * 8 * L.ni,
+                                   cudaMemcpyDeviceToHost, st));
+    NB6_CUDA_CHECK(cudaMemcpyAsync(R.houtl.ptr, R.outl.ptr, sizeof(int) * (size_t)L.W * L.ni,
+                                   cudaMemcpyDeviceToHost, st));
+}
+
+static void regf_eager(const RegLaunch &L, cudaStream_t st) {
+    if (L.hin)
+        NB6_CUDA_CHECK(cudaMemcpyAsync(R.iin.ptr, L.hin, L.in_bytes, cudaMemcpyHostToDevice, st));
+    NB6_CUDA_CHECK(cudaMemsetAsync(R.nbcnt.ptr, 0, sizeof(int) * L.ni, st));
+    // kernel-only timing of the main force kernel (read by
+    // nb6_regf_last_kernel_ms_ after the stream has drained)
+    NB6_CUDA_CHECK(cudaEventRecord(R.ev0, st));
+    if (L.mf) launch_plan<true>(L.plan, L.a, st);
+    else launch_plan<false>(L.plan, L.a, st);
     NB6_CUDA_CHECK(cudaGetLastError());
+    NB6_CUDA_CHECK(cudaEventRecord(R.ev1, st));
+    regf_finalize<<<L.fblocks, FIN_WARPS * 32, L.smem, st>>>(
+        L.a.part, L.plan.nslices, L.ni, L.a.ni_pad, R.nbcnt.ptr, R.nbbuf.ptr, L.a.lcap, L.cap, L.W,
+        L.pmax, R.outf.ptr, R.outl.ptr, L.mlp);
+    NB6_CUDA_CHECK(cudaGetLastError());
+    if (L.hin) regf_copy_out(L, st);
+    R.nbcnt_dirty = false;
+}
+
+static cudaKernelNodeParams main_node(const RegLaunch &L, void **args) {
+    cudaKernelNodeParams k{};
+    k.func = (void *)(L.mf ? kernel_of<true>(L.plan.variant) : kernel_of<false>(L.plan.variant));
+    k.gridDim = dim3(L.plan.igrid, L.plan.nslices);
+    k.blockDim = dim3(L.plan.variant > 0 ? NT : JPAR_NT);
+    k.sharedMemBytes = 0;
+    k.kernelParams = args;
+    return k;
+}
+
+static cudaKernelNodeParams fin_node(const RegLaunch &L, FinArgs &f) {
+    cudaKernelNodeParams k{};
+    k.func = (void *)regf_finalize;
+    k.gridDim = dim3(L.fblocks);
+    k.blockDim = dim3(FIN_WARPS * 32);
+    k.sharedMemBytes = (unsigned)L.smem;
+    k.kernelParams = f.p;
+    return k;
+}
+
+#define NB6_GRAPH_TRY(call)              \
+    do {                                 \
+        if ((call) != cudaSuccess) return false; \
+    } while (0)
+
+static bool graph_build(RegState::Graph &G, const RegLaunch &L) {
+    const bool io = L.hin != nullptr;
+    NB6_GRAPH_TRY(cudaGraphCreate(&G.g, 0));
+    cudaGraphNode_t prev = nullptr, n = nullptr;
+    auto deps = [&]() { return prev ? &prev : (cudaGraphNode_t *)nullptr; };
+    auto ndeps = [&]() { return (size_t)(prev ? 1 : 0); };
+    if (io) {
+        NB6_GRAPH_TRY(cudaGraphAddMemcpyNode1D(&G.h2d, G.g, deps(), ndeps(), R.iin.ptr, L.hin, L.in_bytes,
+                                               cudaMemcpyHostToDevice));
+        prev = G.h2d;
+    }
+    NB6_GRAPH_TRY(cudaGraphAddEventRecordNode(&n, G.g, deps(), ndeps(), R.ev0));
+    prev = n;
+    RegArgs a = L.a;
+    void *margs[1] = {&a};
+    const cudaKernelNodeParams km = main_node(L, margs);
+    NB6_GRAPH_TRY(cudaGraphAddKernelNode(&G.kmain, G.g, deps(), ndeps(), &km));
+    prev = G.kmain;
+    NB6_GRAPH_TRY(cudaGraphAddEventRecordNode(&n, G.g, deps(), ndeps(), R.ev1));
+    prev = n;
+    FinArgs f(L);
+    const cudaKernelNodeParams kf = fin_node(L, f);
+    NB6_GRAPH_TRY(cudaGraphAddKernelNode(&G.kfin, G.g, deps(), ndeps(), &kf));
+    prev = G.kfin;
+    if (io) {
+        NB6_GRAPH_TRY(cudaGraphAddMemcpyNode1D(&G.d2hf, G.g, deps(), ndeps(), R.houtf.ptr, R.outf.ptr,
+                                               sizeof(double) * 8 * L.ni, cudaMemcpyDeviceToHost));
+        prev = G.d2hf;
+        NB6_GRAPH_TRY(cudaGraphAddMemcpyNode1D(&G.d2hl, G.g, deps(), ndeps(), R.houtl.ptr, R.outl.ptr,
+                                               sizeof(int) * (size_t)L.W * L.ni, cudaMemcpyDeviceToHost));
+    }
+    NB6_GRAPH_TRY(cudaGraphInstantiate(&G.x, G.g, 0));
+    R.graph_builds++;
+    return true;
+}
+
+static bool graph_update(RegState::Graph &G, const RegLaunch &L) {
+    const bool io = L.hin != nullptr;
+    if (io)
+        NB6_GRAPH_TRY(cudaGraphExecMemcpyNodeSetParams1D(G.x, G.h2d, R.iin.ptr, L.hin, L.in_bytes,
+                                                         cudaMemcpyHostToDevice));
+    RegArgs a = L.a;
+    void *margs[1] = {&a};
+    const cudaKernelNodeParams km = main_node(L, margs);
+    NB6_GRAPH_TRY(cudaGraphExecKernelNodeSetParams(G.x, G.kmain, &km));
+    FinArgs f(L);
+    const cudaKernelNodeParams kf = fin_node(L, f);
+    NB6_GRAPH_TRY(cudaGraphExecKernelNodeSetParams(G.x, G.kfin, &kf));
+    if (io) {
+        NB6_GRAPH_TRY(cudaGraphExecMemcpyNodeSetParams1D(G.x, G.d2hf, R.houtf.ptr, R.outf.ptr,
+                                                         sizeof(double) * 8 * L.ni, cudaMemcpyDeviceToHost));
+        NB6_GRAPH_TRY(cudaGraphExecMemcpyNodeSetParams1D(G.x, G.d2hl, R.houtl.ptr, R.outl.ptr,
+                                                         sizeof(int) * (size_t)L.W * L.ni,
+                                                         cudaMemcpyDeviceToHost));
+    }
+    return true;
+}
+#undef NB6_GRAPH_TRY
+
+static void clear_graphs() {
+    for (auto &G : R.graph) {
+        if (G.x) cudaGraphExecDestroy(G.x);
+        if (G.g) cudaGraphDestroy(G.g);
+        G = RegState::Graph{};
+    }
+}
+
+// Enqueue one call: as a graph launch when graphs are on (NB6_GRAPHS=0 or
+// nb6_regf_graphs_(0) turns them off), else as individual launches.  A graph
+// API error turns graphs off for the rest of the run and falls back to
+// launches for this call.
+static void regf_submit(const RegLaunch &L, cudaStream_t st) {
+    if (R.use_graphs < 0) {
+        const char *e = getenv("NB6_GRAPHS");
+        R.use_graphs = (e && atoi(e) == 0) ? 0 : 1;
+    }
+    if (!R.use_graphs) {
+        regf_eager(L, st);
+        return;
+    }
+    RegState::Graph &G = R.graph[L.hin ? 1 : 0];
+    bool ok = G.x ? graph_update(G, L) : graph_build(G, L);
+    if (ok) {
+        if (R.nbcnt_dirty) NB6_CUDA_CHECK(cudaMemsetAsync(R.nbcnt.ptr, 0, sizeof(int) * L.ni, st));
+        ok = cudaGraphLaunch(G.x, st) == cudaSuccess;
+    }
+    if (!ok) {
+        const cudaError_t e = cudaGetLastError();
+        fprintf(stderr, "libnb6b200: CUDA graph path unavailable (%s); using plain launches\n",
+                cudaGetErrorName(e));
+        clear_graphs();
+        R.use_graphs = 0;
+        regf_eager(L, st);
+        return;
+    }
+    R.nbcnt_dirty = false;
+    R.graph_launches++;
+}
+
+// Device-resident regular force (i data already on the device).
+static void regf_device(int ni, const double *d_h2, const double *d_dtr, const double *d_x,
+                        const double *d_v, int lmax, int nnbmax, int mflag, cudaStream_t st,
+                        int &W) {
+    RegLaunch L;
+    regf_prepare(ni, d_h2, d_dtr, d_x, d_v, lmax, nnbmax, mflag, st, L);
+    W = L.W;
+    regf_submit(L, st);
 }
 
 // ----------------------------------------------------------------------------
@@ -1246,6 +1640,8 @@ void gpunb_close_() {
         return;
     }
     R.open = false;
+    clear_graphs();
+    R.nbcnt_dirty = true;
     R.posH.release();
     R.posL.release();
     R.vel.release();
@@ -1318,6 +1714,70 @@ bool regular_bind_j(int n, double **jm, double **jx, double **jv, JSetOut *out) 
     return true;
 }
 
+// Results of a finished call, from the pinned staging into the caller's
+// arrays (reference layout: acc/jrk [ni][3], pot [ni], list rows of lmax).
+static void unpack_results(int ni, int W, int lmax, double (*acc)[3], double (*jrk)[3], double *pot,
+                           int *list) {
+    const double *of = R.houtf.ptr;
+    const int *ol = R.houtl.ptr;
+    for (int i = 0; i < ni; ++i) {
+        acc[i][0] = of[8 * i + 0];
+        acc[i][1] = of[8 * i + 1];
+        acc[i][2] = of[8 * i + 2];
+        jrk[i][0] = of[8 * i + 3];
+        jrk[i][1] = of[8 * i + 4];
+        jrk[i][2] = of[8 * i + 5];
+        pot[i] = of[8 * i + 6];
+        const int *src = ol + (size_t)i * W;
+        int *dst = list + (size_t)i * lmax;
+        const int nnb = src[0];
+        dst[0] = nnb;
+        if (nnb > 0) memcpy(dst + 1, src + 1, sizeof(int) * nnb);
+    }
+}
+
+template <bool MF> static const void *seg_kernel_of(int ib) {
+    switch (ib) {
+        case 1: return (const void *)regf_seg_kernel<1, MF>;
+        case 2: return (const void *)regf_seg_kernel<2, MF>;
+        case 4: return (const void *)regf_seg_kernel<4, MF>;
+        default: return (const void *)regf_seg_kernel<8, MF>;
+    }
+}
+
+static int seg_occupancy(int ib, bool mf) {
+    static std::map<int, int> cache;
+    const int key = ib * 2 + (mf ? 1 : 0);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    int occ = 0;
+    NB6_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &occ, mf ? seg_kernel_of<true>(ib) : seg_kernel_of<false>(ib), JPAR_NT, 0));
+    occ = std::max(occ, 1);
+    cache[key] = occ;
+    return occ;
+}
+
+template <int IB, bool MF>
+static void launch_seg_t(int grid, const RegArgs &a, const SegItem *items, const int *nit,
+                         const int2 *pinfo, cudaStream_t st) {
+    regf_seg_kernel<IB, MF><<<grid, JPAR_NT, 0, st>>>(a, items, nit, pinfo);
+}
+
+static void launch_seg(int ib, bool mf, int grid, const RegArgs &a, const SegItem *items, const int *nit,
+                       const int2 *pinfo, cudaStream_t st) {
+    switch (ib * 2 + (mf ? 1 : 0)) {
+        case 2: launch_seg_t<1, false>(grid, a, items, nit, pinfo, st); break;
+        case 3: launch_seg_t<1, true>(grid, a, items, nit, pinfo, st); break;
+        case 4: launch_seg_t<2, false>(grid, a, items, nit, pinfo, st); break;
+        case 5: launch_seg_t<2, true>(grid, a, items, nit, pinfo, st); break;
+        case 8: launch_seg_t<4, false>(grid, a, items, nit, pinfo, st); break;
+        case 9: launch_seg_t<4, true>(grid, a, items, nit, pinfo, st); break;
+        case 16: launch_seg_t<8, false>(grid, a, items, nit, pinfo, st); break;
+        default: launch_seg_t<8, true>(grid, a, items, nit, pinfo, st); break;
+    }
+}
+
 extern "C" {
 
 void gpunb_regf_(int *ni_, double *h2, double *dtr, double (*xi)[3], double (*vi)[3],
@@ -1357,41 +1817,219 @@ void gpunb_regf_(int *ni_, double *h2, double *dtr, double (*xi)[3], double (*vi
     memcpy(h + ni, dtr, sizeof(double) * ni);
     memcpy(h + 2 * (size_t)ni, xi, sizeof(double) * 3 * ni);
     memcpy(h + 5 * (size_t)ni, vi, sizeof(double) * 3 * ni);
-    NB6_CUDA_CHECK(cudaMemcpyAsync(R.iin.ptr, h, sizeof(double) * nin, cudaMemcpyHostToDevice, st));
     const double *d = R.iin.ptr;
 
-    int W = 0;
-    regf_device(ni, d, d + ni, d + 2 * (size_t)ni, d + 5 * (size_t)ni, lmax, nnbmax, *m_flag, st, W);
-
+    // one submission: H2D of the staged i data, force kernel, finalize and
+    // the D2H of the results (a graph launch unless graphs are off)
+    RegLaunch L;
+    L.hin = h;
+    L.in_bytes = sizeof(double) * nin;
+    regf_prepare(ni, d, d + ni, d + 2 * (size_t)ni, d + 5 * (size_t)ni, lmax, nnbmax, *m_flag, st, L);
+    const int W = L.W;
     R.houtf.reserve((size_t)ni * 8);
     R.houtl.reserve((size_t)ni * W);
-    NB6_CUDA_CHECK(cudaMemcpyAsync(R.houtf.ptr, R.outf.ptr, sizeof(double) * 8 * ni,
-                                   cudaMemcpyDeviceToHost, st));
-    NB6_CUDA_CHECK(cudaMemcpyAsync(R.houtl.ptr, R.outl.ptr, sizeof(int) * (size_t)W * ni,
-                                   cudaMemcpyDeviceToHost, st));
+    regf_submit(L, st);
     NB6_CUDA_CHECK(cudaStreamSynchronize(st));
     NB6_CUDA_CHECK(cudaEventElapsedTime(&R.last_kernel_ms, R.ev0, R.ev1));
     const double wt = nb6_wtime();
     R.time_grav += wt;
     R.time_reduce -= wt;
-    if (nb6_check_dev_status() != 0) return;
-
-    const double *of = R.houtf.ptr;
-    const int *ol = R.houtl.ptr;
-    for (int i = 0; i < ni; ++i) {
-        acc[i][0] = of[8 * i + 0];
-        acc[i][1] = of[8 * i + 1];
-        acc[i][2] = of[8 * i + 2];
-        jrk[i][0] = of[8 * i + 3];
-        jrk[i][1] = of[8 * i + 4];
-        jrk[i][2] = of[8 * i + 5];
-        pot[i] = of[8 * i + 6];
-        const int *src = ol + (size_t)i * W;
-        int *dst = list + (size_t)i * lmax;
-        const int nnb = src[0];
-        dst[0] = nnb;
-        if (nnb > 0) memcpy(dst + 1, src + 1, sizeof(int) * nnb);
+    if (nb6_check_dev_status() != 0) {
+        R.nbcnt_dirty = true;
+        return;
     }
+
+    unpack_results(ni, W, lmax, acc, jrk, pot, list);
+    R.time_reduce += nb6_wtime();
+}
+
+// Segmented regular force: gpunb_regf_ for an ensemble of independent
+// clusters sent together.  Segment c is the j range [seg_j0[c], seg_j0[c+1])
+// of the last send; active particle k belongs to segment iseg[k] (iseg
+// non-decreasing, so each cluster's active particles are contiguous) and
+// interacts with that segment only.  Outputs as gpunb_regf_, neighbour ids
+// relative to seg_j0[iseg[k]].  One persistent kernel launch covers every
+// cluster.
+void nb6_regf_seg_(int *ni_, int *iseg, double *h2, double *dtr, double (*xi)[3], double (*vi)[3],
+                   double (*acc)[3], double (*jrk)[3], double *pot, int *lmax_, int *nnbmax_,
+                   int *list, int *m_flag, int *nseg_, int *seg_j0) {
+    if (!R.open) {
+        nb6_fatal(NB6_ERR_NOT_OPEN);
+        return;
+    }
+    const int ni = *ni_, lmax = *lmax_, nnbmax = *nnbmax_, nseg = *nseg_;
+    bool bad = ni <= 0 || lmax < 1 || std::min(nnbmax, lmax - 1) > 8191 || nseg <= 0 ||
+               seg_j0[0] < 0 || seg_j0[nseg] > R.nj;
+    for (int c = 0; c < nseg && !bad; ++c) bad = seg_j0[c + 1] < seg_j0[c];
+    for (int k = 0; k < ni && !bad; ++k)
+        bad = iseg[k] < 0 || iseg[k] >= nseg || (k > 0 && iseg[k] < iseg[k - 1]);
+    if (bad) {
+        fprintf(stderr, "nb6_regf_seg: bad ni, lmax, list cap, segment bounds or segment order\n");
+        nb6_fatal(NB6_ERR_BAD_ARG);
+        return;
+    }
+    if (any_nan(h2, ni) || any_nan(dtr, ni) || any_nan(&xi[0][0], 3 * (size_t)ni) ||
+        any_nan(&vi[0][0], 3 * (size_t)ni)) {
+        fprintf(stderr, "nb6_regf_seg: NaN in i-particle input\n");
+        nb6_fatal(NB6_ERR_NAN_INPUT);
+        return;
+    }
+    R.time_grav -= nb6_wtime();
+    R.ini += ni;
+    R.icall++;
+    cudaStream_t st = nb6_stream();
+    const int cap = std::max(0, std::min(nnbmax, lmax - 1));
+    const int W = cap + 1;
+    const bool mf = *m_flag != 0;
+
+    // i data: [h2 | dtr | x | v], as in gpunb_regf_
+    const size_t nin = (size_t)8 * ni;
+    R.hin.reserve(nin);
+    R.iin.reserve(nin);
+    double *h = R.hin.ptr;
+    memcpy(h, h2, sizeof(double) * ni);
+    memcpy(h + ni, dtr, sizeof(double) * ni);
+    memcpy(h + 2 * (size_t)ni, xi, sizeof(double) * 3 * ni);
+    memcpy(h + 5 * (size_t)ni, vi, sizeof(double) * 3 * ni);
+
+    // runs of active particles per segment, and the CTA i-group size
+    std::vector<int> run_k0, run_c;
+    for (int k = 0; k < ni; ++k)
+        if (k == 0 || iseg[k] != iseg[k - 1]) {
+            run_k0.push_back(k);
+            run_c.push_back(iseg[k]);
+        }
+    const int nrun = (int)run_k0.size();
+    run_k0.push_back(ni);
+    int ib = 1;
+    while (ib < 8 && ib * nrun < ni) ib <<= 1;
+    const int grid_max = nb6_num_sms() * seg_occupancy(ib, mf);
+    double work = 0.0;
+    for (int r = 0; r < nrun; ++r)
+        work += (double)(run_k0[r + 1] - run_k0[r]) * (seg_j0[run_c[r] + 1] - seg_j0[run_c[r]]);
+    R.numInter += (long long)work;
+    // items of about a quarter wave's share of the work each, at least 4 j
+    // per thread
+    const double wt = std::max(work / (4.0 * grid_max), (double)ib * JPAR_NT * 4);
+    std::vector<SegItem> items;
+    std::vector<int2> pinfo(ni);
+    long long slots = 0;
+    for (int r = 0; r < nrun; ++r) {
+        const int c = run_c[r], k0 = run_k0[r], k1 = run_k0[r + 1];
+        const int j0 = seg_j0[c], nc = seg_j0[c + 1] - seg_j0[c];
+        const int g = std::min(ib, k1 - k0);
+        int Q = 0;
+        if (nc > 0) {
+            const int qmax = (nc + JPAR_NT * 4 - 1) / (JPAR_NT * 4);
+            Q = std::max(1, std::min(qmax, (int)std::ceil((double)g * nc / wt)));
+        }
+        for (int k = k0; k < k1; ++k) pinfo[k] = make_int2((int)(slots + (long long)(k - k0) * Q), Q);
+        slots += (long long)(k1 - k0) * Q;
+        for (int i0 = k0; i0 < k1; i0 += ib)
+            for (int q = 0; q < Q; ++q) {
+                SegItem it;
+                it.i0 = i0;
+                it.ni = std::min(ib, k1 - i0);
+                it.j0 = j0 + (int)((long long)nc * q / Q);
+                it.j1 = j0 + (int)((long long)nc * (q + 1) / Q);
+                it.jbase = j0;
+                it.q = q;
+                it.pad0 = it.pad1 = 0;
+                items.push_back(it);
+            }
+    }
+    std::stable_sort(items.begin(), items.end(), [](const SegItem &x, const SegItem &y) {
+        return (long long)x.ni * (x.j1 - x.j0) > (long long)y.ni * (y.j1 - y.j0);
+    });
+    const int nitems = (int)items.size();
+    if (slots > INT_MAX / 4) {
+        fprintf(stderr, "nb6_regf_seg: too many partial slots (%lld)\n", slots);
+        nb6_fatal(NB6_ERR_TOO_LARGE);
+        return;
+    }
+    // int staging: [nitems, 0, 0, 0 | items (8 ints each) | pinfo (2 ints each)]
+    const size_t nint = 4 + (size_t)8 * nitems + (size_t)2 * ni;
+    R.hseg.reserve(nint);
+    R.dseg.reserve(nint);
+    int *hs = R.hseg.ptr;
+    hs[0] = nitems;
+    hs[1] = hs[2] = hs[3] = 0;
+    if (nitems) memcpy(hs + 4, items.data(), sizeof(SegItem) * nitems);
+    memcpy(hs + 4 + (size_t)8 * nitems, pinfo.data(), sizeof(int2) * ni);
+    const SegItem *d_items = reinterpret_cast<const SegItem *>(R.dseg.ptr + 4);
+    const int2 *d_pinfo = reinterpret_cast<const int2 *>(R.dseg.ptr + 4 + (size_t)8 * nitems);
+
+    R.part.reserve((size_t)std::max<long long>(slots, 1) * 4);
+    R.nbcnt.reserve(ni);
+    R.nbbuf.reserve((size_t)ni * std::max(cap, 1));
+    R.outf.reserve((size_t)ni * 8);
+    R.outl.reserve((size_t)ni * W);
+    R.houtf.reserve((size_t)ni * 8);
+    R.houtl.reserve((size_t)ni * W);
+    if (!R.ev0) {
+        NB6_CUDA_CHECK(cudaEventCreate(&R.ev0));
+        NB6_CUDA_CHECK(cudaEventCreate(&R.ev1));
+    }
+    RegArgs a{};
+    a.posH = R.posH.ptr;
+    a.posL = R.posL.ptr;
+    a.vel = R.vel.ptr;
+    a.comp = R.comp.ptr;
+    a.compd = R.compd.ptr;
+    a.npad = R.npad;
+    a.jm = R.jm.ptr;
+    a.jx = R.jx.ptr;
+    a.jv = R.jv.ptr;
+    a.nj = R.nj;
+    a.ntile = R.ntile;
+    a.nslices = 1;
+    const double *d = R.iin.ptr;
+    a.ih2 = d;
+    a.idtr = d + ni;
+    a.ix = d + 2 * (size_t)ni;
+    a.iv = d + 5 * (size_t)ni;
+    a.ni = ni;
+    a.ni_pad = ni;
+    a.part = R.part.ptr;
+    a.nbcnt = R.nbcnt.ptr;
+    a.nbbuf = R.nbbuf.ptr;
+    a.lcap = std::max(cap, 1);
+    a.status = nb6_dev_status();
+
+    NB6_CUDA_CHECK(cudaMemcpyAsync(R.iin.ptr, h, sizeof(double) * nin, cudaMemcpyHostToDevice, st));
+    NB6_CUDA_CHECK(cudaMemcpyAsync(R.dseg.ptr, hs, sizeof(int) * nint, cudaMemcpyHostToDevice, st));
+    NB6_CUDA_CHECK(cudaMemsetAsync(R.nbcnt.ptr, 0, sizeof(int) * ni, st));
+    NB6_CUDA_CHECK(cudaEventRecord(R.ev0, st));
+    if (nitems > 0)
+        launch_seg(ib, mf, std::min(nitems, grid_max), a, d_items, R.dseg.ptr, d_pinfo, st);
+    NB6_CUDA_CHECK(cudaGetLastError());
+    NB6_CUDA_CHECK(cudaEventRecord(R.ev1, st));
+    R.last_geometry[0] = -ib;
+    R.last_geometry[1] = std::min(nitems, grid_max);
+    R.last_geometry[2] = nitems;
+    int pmax = 32;
+    while (pmax < cap) pmax <<= 1;
+    const MlpArgs mlp = nb6_mlp_args(a.ih2, a.idtr);
+    const size_t smem = (size_t)FIN_WARPS * pmax * sizeof(int) + (mlp.on ? MLP_SMEM_BYTES : 0);
+    if (smem > 48 * 1024)
+        NB6_CUDA_CHECK(cudaFuncSetAttribute(regf_finalize_seg, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)smem));
+    regf_finalize_seg<<<(ni + FIN_WARPS - 1) / FIN_WARPS, FIN_WARPS * 32, smem, st>>>(
+        R.part.ptr, d_pinfo, ni, R.nbcnt.ptr, R.nbbuf.ptr, a.lcap, cap, W, pmax, R.outf.ptr, R.outl.ptr, mlp);
+    NB6_CUDA_CHECK(cudaGetLastError());
+    NB6_CUDA_CHECK(cudaMemcpyAsync(R.houtf.ptr, R.outf.ptr, sizeof(double) * 8 * ni, cudaMemcpyDeviceToHost, st));
+    NB6_CUDA_CHECK(cudaMemcpyAsync(R.houtl.ptr, R.outl.ptr, sizeof(int) * (size_t)W * ni,
+                                   cudaMemcpyDeviceToHost, st));
+    NB6_CUDA_CHECK(cudaStreamSynchronize(st));
+    NB6_CUDA_CHECK(cudaEventElapsedTime(&R.last_kernel_ms, R.ev0, R.ev1));
+    const double wt2 = nb6_wtime();
+    R.time_grav += wt2;
+    R.time_reduce -= wt2;
+    if (nb6_check_dev_status() != 0) {
+        R.nbcnt_dirty = true;
+        return;
+    }
+    unpack_results(ni, W, lmax, acc, jrk, pot, list);
     R.time_reduce += nb6_wtime();
 }
 
@@ -1465,6 +2103,31 @@ void nb6_regf_autotune_(int *flag) {
         return;
     }
     R.autotune = *flag ? 1 : 0;
+}
+
+// Learned radius proposals of the last gpunb_regf_ / nb6_regf_seg_ call:
+// out[k] = dlog RS for active particle k (0 when proposals are off).
+void nb6_regf_proposals_(int *ni, double *out) {
+    for (int k = 0; k < *ni; ++k) out[k] = R.houtf.ptr ? R.houtf.ptr[8 * (size_t)k + 7] : 0.0;
+}
+
+// CUDA-graph submission of regular-force calls: flag 1 turns it on, 0 off
+// (plain launches), any other value leaves it as it is.  counts receives
+// {graphs built, graph launches, 1 if on else 0}.
+void nb6_regf_graphs_(int *flag, long long *counts) {
+    if (R.use_graphs < 0) {
+        const char *e = getenv("NB6_GRAPHS");
+        R.use_graphs = (e && atoi(e) == 0) ? 0 : 1;
+    }
+    if (flag && (*flag == 0 || *flag == 1)) {
+        if (*flag == 0) clear_graphs();
+        R.use_graphs = *flag;
+    }
+    if (counts) {
+        counts[0] = R.graph_builds;
+        counts[1] = R.graph_launches;
+        counts[2] = R.use_graphs;
+    }
 }
 
 void nb6_sync_() { NB6_CUDA_CHECK(cudaStreamSynchronize(nb6_stream())); nb6_check_dev_status(); }

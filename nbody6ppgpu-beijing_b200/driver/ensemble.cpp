@@ -1,0 +1,389 @@
+// ensemble.cpp -- block-step integration of an ensemble of independent star
+// clusters on one GPU, with each force kind issued once per block for all
+// clusters together.
+//
+// Each cluster keeps its own Henon units and its own block-step hierarchy:
+// the per-body steps are those of the single-cluster driver (hermite.h), and
+// a body's step sequence depends only on its own cluster, so every cluster
+// follows the trajectory it would follow alone.  What changes is how the
+// force calls are issued.  The bodies of all clusters share one address
+// space (cluster c holds addresses base[c]+1 .. base[c]+n[c]); at each global
+// block time (the earliest t0 + step over all bodies):
+//   * one irr_simd_firr_vec_ for the active bodies of every cluster (their
+//     neighbour lists only hold bodies of their own cluster);
+//   * when regular steps are due: the j set of the clusters involved made on
+//     the device from the irregular library's resident records
+//     (nb6_irr_predict_send_), and one nb6_regf_seg_ for all due bodies,
+//     segment = cluster.
+// With a backend lacking those two extension calls (the reference's CPU
+// libraries) or with batched = 0, the regular force falls back to one
+// host-predicted gpunb_send_ and chunked gpunb_regf_ calls per cluster, which
+// is what running each cluster alone does.
+//
+// Energies are computed per cluster (gpupot_ on the cluster's own bodies).
+#include "hermite.h"
+
+namespace {
+
+using namespace nb6drv;
+
+struct Ensemble : Bodies {
+    Backend B;
+    bool batched = true;
+    int ncl = 0;
+    std::vector<int> base, cnt, cl_of;
+    double time = 0;
+    std::vector<double> prop;  // learned dlog RS per row of the last regular_forces
+
+    int cluster_count(int c) const { return cnt[c]; }
+
+    void set_jp(int i) {
+        int a = i + 1;
+        double mm = m[i], tt = t0[i];
+        B.irr_set_jp(&a, &x0[3 * i], &v0[3 * i], &f[3 * i], &fdot[3 * i], &mm, &tt);
+    }
+
+    void set_list(int i) {
+        int a = i + 1;
+        B.irr_set_list(&a, row(i));
+    }
+
+    // Regular force and new lists (global 1-based, self removed) of the
+    // bodies in idx (ascending, so grouped by cluster) at `time`.
+    void regular_forces(const std::vector<int> &idx, std::vector<double> &freg, std::vector<double> &fdr,
+                        std::vector<int> &nlist) {
+        const double t_0 = wtime();
+        const size_t ni = idx.size();
+        freg.assign(3 * ni, 0.0);
+        fdr.assign(3 * ni, 0.0);
+        nlist.assign(ni * (size_t)LS, 0);
+        prop.assign(ni, 0.0);
+        // runs of idx per cluster
+        std::vector<int> run0, runc;
+        for (size_t q = 0; q < ni; ++q)
+            if (q == 0 || cl_of[idx[q]] != cl_of[idx[q - 1]]) {
+                run0.push_back((int)q);
+                runc.push_back(cl_of[idx[q]]);
+            }
+        run0.push_back((int)ni);
+        const int nrun = (int)runc.size();
+        if (batched && B.regf_seg && B.predict_send)
+            regular_batched(idx, run0, runc, nrun, freg, fdr, nlist);
+        else
+            for (int r = 0; r < nrun; ++r) regular_one_cluster(idx, run0[r], run0[r + 1], runc[r], freg, fdr, nlist);
+        st.wall_reg += wtime() - t_0;
+    }
+
+    // Copy one result row into the global list layout.
+    void take_row(int i, int c, const int *src, const double *acc, const double *jrk, size_t q,
+                  std::vector<double> &freg, std::vector<double> &fdr, std::vector<int> &nlist) {
+        for (int k = 0; k < 3; ++k) {
+            freg[3 * q + k] = acc[k];
+            fdr[3 * q + k] = jrk[k];
+        }
+        const int nb = src[0];
+        int *out = &nlist[q * (size_t)LS];
+        int l1 = 0;
+        const int self = i - base[c];
+        for (int l = 1; l <= nb; ++l) {
+            const int j = src[l];
+            if (j != self) out[1 + l1++] = base[c] + j + 1;
+        }
+        out[0] = l1;
+    }
+
+    void regular_batched(const std::vector<int> &idx, const std::vector<int> &run0,
+                         const std::vector<int> &runc, int nrun, std::vector<double> &freg,
+                         std::vector<double> &fdr, std::vector<int> &nlist) {
+        // the bodies corrected in this block must be on the device first
+        // (their t0 is the block time, so they predict to themselves)
+        std::vector<int> addr0(nrun), count(nrun), seg_j0(nrun + 1, 0);
+        for (int r = 0; r < nrun; ++r) {
+            addr0[r] = base[runc[r]] + 1;
+            count[r] = cnt[runc[r]];
+            seg_j0[r + 1] = seg_j0[r] + count[r];
+        }
+        double t = time;
+        int nseg = nrun;
+        B.predict_send(&t, &nseg, addr0.data(), count.data());
+        // pending rows: first all, then the overflowed ones after a shrink
+        std::vector<int> pend(idx.size());
+        for (size_t q = 0; q < idx.size(); ++q) pend[q] = (int)q;
+        std::vector<int> seg_of_q(idx.size());
+        for (int r = 0; r < nrun; ++r)
+            for (int q = run0[r]; q < run0[r + 1]; ++q) seg_of_q[q] = r;
+        while (!pend.empty()) {
+            const int np = (int)pend.size();
+            std::vector<int> iseg(np);
+            std::vector<double> h2(np), dtr(np), xi(3 * (size_t)np), vi(3 * (size_t)np), acc(3 * (size_t)np),
+                jrk(3 * (size_t)np), pot(np);
+            std::vector<int> lst((size_t)np * P.lmax);
+            for (int p = 0; p < np; ++p) {
+                const int q = pend[p], i = idx[q], c = cl_of[i];
+                iseg[p] = seg_of_q[q];
+                h2[p] = h2_of(i, 1.0 / cnt[c]);
+                dtr[p] = stepr[i];
+                pred_at(i, time, &xi[3 * (size_t)p], &vi[3 * (size_t)p]);
+            }
+            int nni = np, lmax = P.lmax, nnbmax = P.nnbmax, mf = P.m_flag;
+            B.regf_seg(&nni, iseg.data(), h2.data(), dtr.data(), (double(*)[3])xi.data(), (double(*)[3])vi.data(),
+                       (double(*)[3])acc.data(), (double(*)[3])jrk.data(), pot.data(), &lmax, &nnbmax, lst.data(),
+                       &mf, &nseg, seg_j0.data());
+            st.reg_calls++;
+            std::vector<double> pr(np, 0.0);
+            if (P.mlp_mode == 2) B.proposals(&nni, pr.data());
+            std::vector<int> again;
+            for (int p = 0; p < np; ++p) {
+                prop[pend[p]] = pr[p];
+                const int q = pend[p], i = idx[q], c = cl_of[i];
+                st.reg_pairs += cnt[c];
+                const int *src = &lst[(size_t)p * P.lmax];
+                if (src[0] < 0) {
+                    shrink_radius(i, src[0]);
+                    again.push_back(q);
+                    continue;
+                }
+                take_row(i, c, src, &acc[3 * (size_t)p], &jrk[3 * (size_t)p], (size_t)q, freg, fdr, nlist);
+            }
+            if (!again.empty()) st.overflow_retries++;
+            pend.swap(again);
+        }
+    }
+
+    // One cluster as the single-cluster driver does it: host prediction of
+    // its bodies, gpunb_send_, gpunb_regf_ in chunks with overflow retry.
+    void regular_one_cluster(const std::vector<int> &idx, int q0, int q1, int c, std::vector<double> &freg,
+                             std::vector<double> &fdr, std::vector<int> &nlist) {
+        const int nc = cnt[c], b = base[c];
+        std::vector<double> xp(3 * (size_t)nc), vp(3 * (size_t)nc);
+        for (int j = 0; j < nc; ++j) pred_at(b + j, time, &xp[3 * (size_t)j], &vp[3 * (size_t)j]);
+        int nn = nc;
+        B.gpunb_send(&nn, &m[b], (double(*)[3])xp.data(), (double(*)[3])vp.data());
+        const int C = P.chunk;
+        std::vector<double> h2(C + 4), dtr(C + 4), xi(3 * (C + 4)), vi(3 * (C + 4)), acc(3 * (C + 4)),
+            jrk(3 * (C + 4)), pot(C + 4);
+        std::vector<int> lst((size_t)(C + 4) * P.lmax);
+        for (int c0 = q0; c0 < q1; c0 += C) {
+            const int ni = std::min(C, q1 - c0);
+            for (;;) {
+                for (int q = 0; q < ni; ++q) {
+                    const int i = idx[c0 + q];
+                    h2[q] = h2_of(i, 1.0 / nc);
+                    dtr[q] = stepr[i];
+                    for (int k = 0; k < 3; ++k) {
+                        xi[3 * q + k] = xp[3 * (size_t)(i - b) + k];
+                        vi[3 * q + k] = vp[3 * (size_t)(i - b) + k];
+                    }
+                }
+                for (int q = ni; q < ni + 4 && q < C + 4; ++q) {  // AVX library reads 4 at a time
+                    h2[q] = 0;
+                    dtr[q] = 0;
+                    for (int k = 0; k < 3; ++k) xi[3 * q + k] = vi[3 * q + k] = 0;
+                }
+                int nni = ni, lmax = P.lmax, nnbmax = P.nnbmax, mf = P.m_flag;
+                B.gpunb_regf(&nni, h2.data(), dtr.data(), (double(*)[3])xi.data(), (double(*)[3])vi.data(),
+                             (double(*)[3])acc.data(), (double(*)[3])jrk.data(), pot.data(), &lmax, &nnbmax,
+                             lst.data(), &mf);
+                st.reg_calls++;
+                st.reg_pairs += (long long)ni * nc;
+                bool retry = false;
+                for (int q = 0; q < ni; ++q) {
+                    const int nb = lst[(size_t)q * P.lmax];
+                    if (nb < 0) {
+                        shrink_radius(idx[c0 + q], nb);
+                        retry = true;
+                    }
+                }
+                if (retry) {
+                    st.overflow_retries++;
+                    continue;
+                }
+                break;
+            }
+            if (P.mlp_mode == 2) {
+                int nq = ni;
+                B.proposals(&nq, &prop[c0]);
+            }
+            for (int q = 0; q < ni; ++q)
+                take_row(idx[c0 + q], c, &lst[(size_t)q * P.lmax], &acc[3 * q], &jrk[3 * q], (size_t)(c0 + q), freg,
+                         fdr, nlist);
+        }
+    }
+
+    bool init() {
+        alloc();
+        cl_of.assign(n, 0);
+        for (int c = 0; c < ncl; ++c)
+            for (int k = 0; k < cnt[c]; ++k) cl_of[base[c] + k] = c;
+        for (int i = 0; i < n; ++i) init_radius(i, &x0[3 * (size_t)i]);
+        int nb = n + 10, rank = 0;
+        B.gpunb_open(&nb, &rank);
+        int nmax = n, lmax = P.lmax;
+        B.irr_open(&nmax, &lmax, &rank);
+        time = 0.0;
+        // F = FDOT = 0 at t = 0: the records predict to themselves
+        for (int i = 0; i < n; ++i) set_jp(i);
+        std::vector<int> all(n);
+        for (int i = 0; i < n; ++i) all[i] = i;
+        std::vector<double> freg, fdr;
+        std::vector<int> nl;
+        regular_forces(all, freg, fdr, nl);
+        for (int i = 0; i < n; ++i) {
+            memcpy(row(i), &nl[(size_t)i * LS], sizeof(int) * LS);
+            set_list(i);
+        }
+        std::vector<int> addr(n);
+        for (int i = 0; i < n; ++i) addr[i] = i + 1;
+        std::vector<double> a(3 * (size_t)n), jd(3 * (size_t)n);
+        std::vector<int> nnbid(n);
+        double t = 0.0;
+        int nn = n;
+        B.irr_firr_vec(&t, &nn, addr.data(), (double(*)[3])a.data(), (double(*)[3])jd.data(), nnbid.data());
+        for (int i = 0; i < n; ++i) {
+            init_forces(i, &freg[3 * (size_t)i], &fdr[3 * (size_t)i], &a[3 * (size_t)i], &jd[3 * (size_t)i]);
+            set_jp(i);
+        }
+        return true;
+    }
+
+    // Kinetic and potential energy of cluster c at `time`.
+    void energy(int c, double &ekin, double &epot) {
+        const int nc = cnt[c], b = base[c];
+        std::vector<double> xp(3 * (size_t)nc), vp(3 * (size_t)nc), phi(nc + 8);
+        for (int j = 0; j < nc; ++j) pred(b + j, time, &xp[3 * (size_t)j], &vp[3 * (size_t)j]);
+        int rank = 0, istart = 1, ni = nc, nn = nc;
+        B.gpupot(&rank, &istart, &ni, &nn, &m[b], (double(*)[3])xp.data(), phi.data());
+        ekin = 0;
+        epot = 0;
+        for (int j = 0; j < nc; ++j) {
+            const double *v = &vp[3 * (size_t)j];
+            ekin += 0.5 * m[b + j] * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+            epot -= 0.5 * m[b + j] * phi[j];
+        }
+    }
+
+    void record(double *tout, double *eout, int &nout, int nout_max) {
+        if (nout >= nout_max) return;
+        tout[nout] = time;
+        for (int c = 0; c < ncl; ++c) {
+            double ek, ep;
+            energy(c, ek, ep);
+            double *e = eout + ((size_t)nout * ncl + c) * 3;
+            e[0] = ek;
+            e[1] = ep;
+            e[2] = ek + ep;
+        }
+        nout++;
+    }
+
+    void run(double *tout, double *eout, int nout_max) {
+        const double tw = wtime();
+        int nout = 0;
+        record(tout, eout, nout, nout_max);
+        double tnext_out = P.dt_out;
+        std::vector<int> active, reg, addr, nnbid;
+        std::vector<double> a, jd, freg, fdr;
+        std::vector<int> nl;
+        while (st.blocks < P.max_blocks) {
+            double tmin = 1e300;
+            for (int i = 0; i < n; ++i) tmin = std::min(tmin, t0[i] + step[i]);
+            if (tmin > P.tcrit + 1e-12) break;
+            time = tmin;
+            active.clear();
+            for (int i = 0; i < n; ++i)
+                if (t0[i] + step[i] == tmin) active.push_back(i);
+            st.blocks++;
+            const int na = (int)active.size();
+            addr.resize(na);
+            for (int q = 0; q < na; ++q) addr[q] = active[q] + 1;
+            a.assign(3 * (size_t)na, 0.0);
+            jd.assign(3 * (size_t)na, 0.0);
+            nnbid.assign(na, 0);
+            const double ti0 = wtime();
+            double t = time;
+            int nna = na;
+            B.irr_firr_vec(&t, &nna, addr.data(), (double(*)[3])a.data(), (double(*)[3])jd.data(), nnbid.data());
+            st.wall_irr += wtime() - ti0;
+            reg.clear();
+            for (int q = 0; q < na; ++q)
+                if (irr_correct(active[q], time, &a[3 * (size_t)q], &jd[3 * (size_t)q])) reg.push_back(active[q]);
+            if (!reg.empty()) {
+                // corrected states of this block to the device before the
+                // j set is predicted there
+                if (batched && B.predict_send)
+                    for (int q = 0; q < na; ++q) set_jp(active[q]);
+                regular_forces(reg, freg, fdr, nl);
+                snapshot(reg, time);
+                for (size_t q = 0; q < reg.size(); ++q) {
+                    const int i = reg[q];
+                    const int *row_new = &nl[q * (size_t)LS];
+                    const double rs_used = rs[i];
+                    if (P.mlp_mode == 1)
+                        learn_log(i, row_new[0], rs_used, h2_of(i, 1.0 / cnt[cl_of[i]]), &freg[3 * q], stepr[i]);
+                    reg_correct(i, time, row_new, &freg[3 * q], &fdr[3 * q]);
+                    if (P.mlp_mode == 2) learn_apply(i, row_new[0], rs_used, prop[q]);
+                    set_list(i);
+                }
+                release_snapshot(reg);
+            }
+            for (int q = 0; q < na; ++q) set_jp(active[q]);
+            if (time >= tnext_out - 1e-15) {
+                record(tout, eout, nout, nout_max);
+                tnext_out += P.dt_out;
+            }
+        }
+        st.t_end = time;
+        st.nout = nout;
+        st.wall_total = wtime() - tw;
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+// Integrate ncl independent clusters (counts[c] bodies each, stored back to
+// back in mass[], x[][3], v[][3], each in its own Henon units) to p->tcrit.
+// batched = 1 issues every force kind once per block for all clusters when
+// the backend has the batched calls; 0 issues the regular force per cluster.
+// x and v are overwritten with the final state predicted to the end time;
+// tout[k] and eout[k][c][3] = (kinetic, potential, total) of cluster c at
+// every p->dt_out.  Returns 0 on success.
+int nb6drive_ensemble(const char *reg_lib, const char *irr_lib, const char *pot_lib, int ncl,
+                      const int *counts, const double *mass, double *x, double *v,
+                      const nb6drive_params *p, int batched, double *tout, double *eout, int nout_max,
+                      nb6drive_stats *stats) {
+    Ensemble e;
+    e.P = *p;
+    e.ncl = ncl;
+    e.batched = batched != 0;
+    if (ncl <= 0) return 3;
+    e.base.assign(ncl, 0);
+    e.cnt.assign(counts, counts + ncl);
+    long long total = 0;
+    for (int c = 0; c < ncl; ++c) {
+        if (counts[c] < 2) return 3;
+        e.base[c] = (int)total;
+        total += counts[c];
+    }
+    if (total > (1LL << 30)) return 3;
+    e.n = (int)total;
+    if (!load_backend(e.B, reg_lib, irr_lib, pot_lib)) return 1;
+    if (e.P.mlp_mode == 2 && !e.B.proposals) {
+        fprintf(stderr, "nb6drive: mlp_mode 2 needs a backend with nb6_regf_proposals_\n");
+        return 4;
+    }
+    e.m.assign(mass, mass + e.n);
+    e.x0.assign(x, x + 3 * (size_t)e.n);
+    e.v0.assign(v, v + 3 * (size_t)e.n);
+    if (!e.init()) return 2;
+    e.run(tout, eout, nout_max);
+    for (int j = 0; j < e.n; ++j) e.pred(j, e.time, &x[3 * (size_t)j], &v[3 * (size_t)j]);
+    int rank = 0;
+    e.B.irr_close(&rank);
+    e.B.gpunb_close();
+    if (stats) *stats = e.st;
+    return 0;
+}
+
+}  // extern "C"

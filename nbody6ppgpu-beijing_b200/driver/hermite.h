@@ -1,0 +1,518 @@
+// hermite.h -- per-body pieces of the Hermite 4th-order block-step scheme
+// with the Ahmad-Cohen neighbour split, shared by the single-cluster driver
+// (blockstep.cpp) and the ensemble driver (ensemble.cpp).
+//
+// Restated from the reference's integrator (single stars only):
+//   irregular corrector + step   nbint_cor.f:113-173,215-236, tstep.f
+//   F, FDOT between regular steps intgrt.F:558-581
+//   regular corrector            regcor_gpu.F:131-196 (radius update),
+//                                :284-444 (neighbour gain/loss force moves),
+//                                :442-537 (corrector), :593-737 (new step)
+//   initial steps                fpoly0.F:55-59,100-206
+// Bodies keep the reference's Fortran names in lower case (X0, X0DOT, T0,
+// STEP, T0R, STEPR, FI, FIDOT, D2, D3, FR, FRDOT, D2R, D3R, F, FDOT, RS,
+// LIST); neighbour rows hold 1-based body addresses, self excluded.
+#pragma once
+
+#include <dlfcn.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+
+#include <algorithm>
+#include <vector>
+
+extern "C" {
+
+// Run parameters (names follow the reference's input namelist, input.F).
+struct nb6drive_params {
+    double eta_i, eta_r;   // ETAI, ETAR
+    double smax;           // SMAX, power of two
+    double dtmin;          // smallest allowed step (power of two)
+    double tcrit;          // end time
+    double dt_out;         // energy output interval (power of two, >= smax)
+    double rs0;            // initial neighbour radius scale (fpoly0.F:55)
+    int nnbopt, nnbmax, lmax, m_flag;
+    int chunk;             // i per gpunb_regf call (util_gpu.F: 1024)
+    long long max_blocks;  // safety bound on the number of block steps
+    // learned neighbour radius: 0 = Ahmad-Cohen only; 1 = Ahmad-Cohen and
+    // log (features, target) samples into samples[sample_cap][6]; 2 = the
+    // library's proposals, Ahmad-Cohen as fallback
+    int mlp_mode;
+    int mlp_pad;
+    float *samples;
+    long long sample_cap;
+};
+
+// Counters returned by the drivers.
+struct nb6drive_stats {
+    long long blocks, irr_steps, reg_steps, reg_calls, overflow_retries;
+    long long nb_sum;       // sum of neighbour counts over regular steps
+    long long reg_pairs;    // sum of ni * nj over regular-force calls
+    double wall_reg, wall_irr, wall_total;
+    double t_end;
+    int nout;
+    long long nsamples;      // samples logged (mlp_mode 1)
+    long long mlp_used;      // regular steps that took the learned radius (mlp_mode 2)
+    long long mlp_fallback;  // ... that fell back to the Ahmad-Cohen radius
+    double nb_absdev;        // sum over regular steps of |nnb - NNBOPT|
+};
+
+}  // extern "C"
+
+namespace nb6drv {
+
+typedef void (*fn_open)(int *, int *);
+typedef void (*fn_close)();
+typedef void (*fn_send)(int *, double *, double (*)[3], double (*)[3]);
+typedef void (*fn_regf)(int *, double *, double *, double (*)[3], double (*)[3], double (*)[3],
+                        double (*)[3], double *, int *, int *, int *, int *);
+typedef void (*fn_regf_seg)(int *, int *, double *, double *, double (*)[3], double (*)[3],
+                            double (*)[3], double (*)[3], double *, int *, int *, int *, int *, int *,
+                            int *);
+typedef void (*fn_pred_send)(double *, int *, int *, int *);
+typedef void (*fn_pot)(int *, int *, int *, int *, double *, double (*)[3], double *);
+typedef void (*fn_irr_open)(int *, int *, int *);
+typedef void (*fn_irr_close)(int *);
+typedef void (*fn_irr_set_jp)(int *, double *, double *, double *, double *, double *, double *);
+typedef void (*fn_irr_set_list)(int *, int *);
+typedef void (*fn_irr_firr)(double *, int *, int *, double (*)[3], double (*)[3], int *);
+typedef void (*fn_proposals)(int *, double *);
+
+struct Backend {
+    void *hreg = nullptr, *hirr = nullptr, *hpot = nullptr;
+    fn_open gpunb_open = nullptr;
+    fn_close gpunb_close = nullptr;
+    fn_send gpunb_send = nullptr;
+    fn_regf gpunb_regf = nullptr;
+    fn_pot gpupot = nullptr;
+    fn_irr_open irr_open = nullptr;
+    fn_irr_close irr_close = nullptr;
+    fn_irr_set_jp irr_set_jp = nullptr;
+    fn_irr_set_list irr_set_list = nullptr;
+    fn_irr_firr irr_firr_vec = nullptr;
+    // extensions of libnb6b200 (absent from the reference's libraries)
+    fn_regf_seg regf_seg = nullptr;
+    fn_pred_send predict_send = nullptr;
+    fn_proposals proposals = nullptr;
+};
+
+inline void *must_sym(void *h, const char *name) {
+    void *p = dlsym(h, name);
+    if (!p) fprintf(stderr, "nb6drive: missing symbol %s\n", name);
+    return p;
+}
+
+inline bool load_backend(Backend &b, const char *reg, const char *irr, const char *pot) {
+    b.hreg = dlopen(reg, RTLD_NOW | RTLD_LOCAL);
+    b.hirr = dlopen(irr, RTLD_NOW | RTLD_LOCAL);
+    b.hpot = dlopen(pot, RTLD_NOW | RTLD_LOCAL);
+    if (!b.hreg || !b.hirr || !b.hpot) {
+        fprintf(stderr, "nb6drive: dlopen failed: %s\n", dlerror());
+        return false;
+    }
+    b.gpunb_open = (fn_open)must_sym(b.hreg, "gpunb_open_");
+    b.gpunb_close = (fn_close)must_sym(b.hreg, "gpunb_close_");
+    b.gpunb_send = (fn_send)must_sym(b.hreg, "gpunb_send_");
+    b.gpunb_regf = (fn_regf)must_sym(b.hreg, "gpunb_regf_");
+    b.gpupot = (fn_pot)must_sym(b.hpot, "gpupot_");
+    b.irr_open = (fn_irr_open)must_sym(b.hirr, "irr_simd_open_");
+    b.irr_close = (fn_irr_close)must_sym(b.hirr, "irr_simd_close_");
+    b.irr_set_jp = (fn_irr_set_jp)must_sym(b.hirr, "irr_simd_set_jp_");
+    b.irr_set_list = (fn_irr_set_list)must_sym(b.hirr, "irr_simd_set_list_");
+    b.irr_firr_vec = (fn_irr_firr)must_sym(b.hirr, "irr_simd_firr_vec_");
+    // optional: batched calls of libnb6b200, only when reg and irr are the
+    // same library (the device j set comes from the irregular records)
+    if (b.hreg == b.hirr) {
+        b.regf_seg = (fn_regf_seg)dlsym(b.hreg, "nb6_regf_seg_");
+        b.predict_send = (fn_pred_send)dlsym(b.hreg, "nb6_irr_predict_send_");
+    }
+    b.proposals = (fn_proposals)dlsym(b.hreg, "nb6_regf_proposals_");
+    return b.gpunb_open && b.gpunb_close && b.gpunb_send && b.gpunb_regf && b.gpupot &&
+           b.irr_open && b.irr_close && b.irr_set_jp && b.irr_set_list && b.irr_firr_vec;
+}
+
+inline double wtime() {
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return ts.tv_sec + 1e-9 * ts.tv_nsec;
+}
+
+// STEP = sqrt(ETA (|F||F2| + |F1|^2) / (|F1||F3| + |F2|^2))   (tstep.f)
+inline double tstep(const double *f, const double *f1, const double *f2, const double *f3, double eta) {
+    double F2 = 0, F12 = 0, F22 = 0, F32 = 0;
+    for (int k = 0; k < 3; ++k) {
+        F2 += f[k] * f[k];
+        F12 += f1[k] * f1[k];
+        F22 += f2[k] * f2[k];
+        F32 += f3[k] * f3[k];
+    }
+    const double num = sqrt(F2 * F22) + F12;
+    const double den = sqrt(F12 * F32) + F22;
+    if (!(den > 0)) return 1e30;
+    return sqrt(eta * num / den);
+}
+
+// Largest power of two <= x, clamped to [lo, hi].
+inline double pow2_floor(double x, double lo, double hi) {
+    if (!(x > lo)) return lo;
+    double p = hi;
+    while (p > x && p > lo) p *= 0.5;
+    return std::max(p, lo);
+}
+
+// State of n bodies (one cluster or several back to back).
+struct Bodies {
+    int n = 0;
+    nb6drive_params P;
+    std::vector<double> m, x0, v0, t0, step, t0r, stepr, fi, fidot, d2, d3, fr, frdot, d2r, d3r, f,
+        fdot, rs;
+    std::vector<int> list;  // n x LS: [nnb, 1-based addresses ascending] (self excluded)
+    int LS = 0;             // row stride (lmax + 8 so the AVX library can over-read)
+    double tcr = 2.0 * sqrt(2.0);  // crossing time in Henon units
+    nb6drive_stats st{};
+
+    // State at the block time of the bodies being regular-corrected, taken
+    // before any of them is corrected: the neighbour gain/loss force moves of
+    // one body must see the others as predicted, not as corrected.
+    std::vector<unsigned char> snapped;
+    std::vector<double> xs, vs;
+
+    int *row(int i) { return &list[(size_t)i * LS]; }
+
+    void alloc() {
+        snapped.assign(n, 0);
+        xs.assign(3 * (size_t)n, 0.0);
+        vs.assign(3 * (size_t)n, 0.0);
+        LS = P.lmax + 8;
+        list.assign((size_t)n * LS, 0);
+        auto z3 = [&](std::vector<double> &v) { v.assign(3 * (size_t)n, 0.0); };
+        z3(fi), z3(fidot), z3(d2), z3(d3), z3(fr), z3(frdot), z3(d2r), z3(d3r), z3(f), z3(fdot);
+        t0.assign(n, 0.0);
+        t0r.assign(n, 0.0);
+        step.assign(n, P.smax);
+        stepr.assign(n, P.smax);
+        rs.assign(n, 0.0);
+    }
+
+    // Initial radius and regular step from the distance to the cluster
+    // centre (fpoly0.F:55-59); xc is the body's position relative to it.
+    void init_radius(int i, const double *xc) {
+        const double ri2 = xc[0] * xc[0] + xc[1] * xc[1] + xc[2] * xc[2];
+        rs[i] = P.rs0 * sqrt(1.0 + ri2);
+        stepr[i] = std::min(P.smax * sqrt(1.0 + ri2), P.smax);
+    }
+
+    // Hermite predictor of body j to time t (xbpredall.F:50-59).
+    void pred(int j, double t, double *x, double *v) const {
+        const double s = t - t0[j], s1 = 1.5 * s, s2 = 2.0 * s;
+        for (int k = 0; k < 3; ++k) {
+            const size_t q = 3 * (size_t)j + k;
+            x[k] = ((fdot[q] * s + f[q]) * s + v0[q]) * s + x0[q];
+            v[k] = (fdot[q] * s1 + f[q]) * s2 + v0[q];
+        }
+    }
+
+    void snapshot(const std::vector<int> &ids, double t) {
+        for (int i : ids) {
+            pred(i, t, &xs[3 * (size_t)i], &vs[3 * (size_t)i]);
+            snapped[i] = 1;
+        }
+    }
+    void release_snapshot(const std::vector<int> &ids) {
+        for (int i : ids) snapped[i] = 0;
+    }
+    // Body j at t: the snapshot if it holds one, else the predictor.
+    void pred_at(int j, double t, double *x, double *v) const {
+        if (snapped[j]) {
+            for (int k = 0; k < 3; ++k) {
+                x[k] = xs[3 * (size_t)j + k];
+                v[k] = vs[3 * (size_t)j + k];
+            }
+        } else {
+            pred(j, t, x, v);
+        }
+    }
+
+    // FP64 pair force and jerk of body j (at t) on (xi, vi).
+    void pair_force(const double *xi, const double *vi, int j, double t, double *a, double *jd) const {
+        double xj[3], vj[3];
+        pred_at(j, t, xj, vj);
+        const double dx = xj[0] - xi[0], dy = xj[1] - xi[1], dz = xj[2] - xi[2];
+        const double dvx = vj[0] - vi[0], dvy = vj[1] - vi[1], dvz = vj[2] - vi[2];
+        const double r2 = dx * dx + dy * dy + dz * dz;
+        const double dr2i = 1.0 / r2, dr3i = m[j] * dr2i * sqrt(dr2i);
+        const double drdp = 3.0 * (dx * dvx + dy * dvy + dz * dvz) * dr2i;
+        a[0] = dx * dr3i;
+        a[1] = dy * dr3i;
+        a[2] = dz * dr3i;
+        jd[0] = (dvx - dx * drdp) * dr3i;
+        jd[1] = (dvy - dy * drdp) * dr3i;
+        jd[2] = (dvz - dz * drdp) * dr3i;
+    }
+
+    // Split forces at t = 0 from the first regular and irregular evaluation,
+    // and the initial steps from |F|/|FDOT| (two-term form of the criterion).
+    void init_forces(int i, const double *freg, const double *fdr, const double *a, const double *jd) {
+        double ft[3], fdt[3];
+        for (int k = 0; k < 3; ++k) {
+            fr[3 * i + k] = freg[k];
+            frdot[3 * i + k] = fdr[k];
+            fi[3 * i + k] = a[k];
+            fidot[3 * i + k] = jd[k];
+            f[3 * i + k] = 0.5 * (fi[3 * i + k] + fr[3 * i + k]);
+            fdot[3 * i + k] = (fidot[3 * i + k] + frdot[3 * i + k]) / 6.0;
+            ft[k] = fi[3 * i + k] + fr[3 * i + k];
+            fdt[k] = fidot[3 * i + k] + frdot[3 * i + k];
+        }
+        double F = 0, FD = 0, FR = 0, FRD = 0;
+        for (int k = 0; k < 3; ++k) {
+            F += ft[k] * ft[k];
+            FD += fdt[k] * fdt[k];
+            FR += fr[3 * i + k] * fr[3 * i + k];
+            FRD += frdot[3 * i + k] * frdot[3 * i + k];
+        }
+        const double dti = FD > 0 ? 0.5 * P.eta_i * sqrt(F / FD) : P.smax;
+        const double dtr = FRD > 0 ? 0.5 * P.eta_r * sqrt(FR / FRD) : P.smax;
+        stepr[i] = pow2_floor(dtr, P.dtmin, P.smax);
+        step[i] = std::min(pow2_floor(dti, P.dtmin, P.smax), stepr[i]);
+    }
+
+    // Irregular corrector and new irregular step of body i at `time` from its
+    // new neighbour force a and jerk jd; returns true when its regular step
+    // is due too (otherwise F, FDOT are extrapolated, intgrt.F:570-578).
+    bool irr_correct(int i, double time, const double *a, const double *jd) {
+        const double s = time - t0[i], s1 = 1.5 * s, s2 = 2.0 * s;
+        double xi[3], vi[3];
+        for (int k = 0; k < 3; ++k) {
+            const size_t c = 3 * (size_t)i + k;
+            xi[k] = ((fdot[c] * s + f[c]) * s + v0[c]) * s + x0[c];
+            vi[k] = (fdot[c] * s1 + f[c]) * s2 + v0[c];
+        }
+        const double dt = s, dtsq = dt * dt, dt6 = 6.0 / (dt * dtsq), dt2 = 2.0 / dtsq;
+        const double dtsq12 = dtsq / 12.0, dt13 = dt / 3.0;
+        double ftot[3];
+        for (int k = 0; k < 3; ++k) {  // nbint_cor.f:130-150
+            const size_t c = 3 * (size_t)i + k;
+            const double df = fi[c] - a[k];
+            const double fid = fidot[c];
+            const double sum = fid + jd[k];
+            const double at3 = 2.0 * df + dt * sum;
+            const double bt2 = -3.0 * df - dt * (sum + fid);
+            x0[c] = xi[k] + (0.6 * at3 + bt2) * dtsq12;
+            v0[c] = vi[k] + (0.75 * at3 + bt2) * dt13;
+            fi[c] = a[k];
+            fidot[c] = jd[k];
+            ftot[k] = fi[c] + fr[c];
+            d2[c] = (3.0 * at3 + bt2) * dt2;
+            d3[c] = at3 * dt6;
+        }
+        // irregular step (nbint_cor.f:146,215-236)
+        double ttmp = tstep(ftot, &fidot[3 * i], &d2[3 * i], &d3[3 * i], P.eta_i);
+        const double dt0 = ttmp;
+        if (ttmp > 2.0 * step[i]) {
+            ttmp = (fmod(time, 2.0 * step[i]) == 0.0) ? std::min(2.0 * step[i], P.smax) : step[i];
+        } else if (ttmp < step[i]) {
+            ttmp = 0.5 * step[i];
+            if (ttmp > dt0) ttmp *= 0.5;
+        } else {
+            ttmp = step[i];
+        }
+        step[i] = std::max(ttmp, P.dtmin);
+        t0[i] = time;
+        st.irr_steps++;
+        if (t0r[i] + stepr[i] <= time) return true;
+        const double dtr = time - t0r[i];
+        for (int k = 0; k < 3; ++k) {
+            const size_t c = 3 * (size_t)i + k;
+            f[c] = 0.5 * (frdot[c] * dtr + fr[c] + fi[c]);
+            fdot[c] = (frdot[c] + fidot[c]) / 6.0;
+        }
+        // keep the irregular step inside the regular interval
+        while (t0[i] + step[i] > t0r[i] + stepr[i] && step[i] > P.dtmin) step[i] *= 0.5;
+        return false;
+    }
+
+    // Overflow handling of one regular-force row (util_gpu.F:69-100, NB_FLAG
+    // branch): shrink RS; the caller re-runs the force.
+    void shrink_radius(int i, int nb_neg) {
+        if (-nb_neg > P.nnbopt) rs[i] *= pow((double)P.nnbopt / (double)(-nb_neg), 0.333);
+        else rs[i] *= pow((double)P.nnbopt / (double)P.nnbmax, 0.4);
+    }
+
+    // Regular corrector of body i at `time`: Ahmad-Cohen radius update, force
+    // moves for neighbours gained and lost, Hermite corrector on the regular
+    // force, new regular step.  nlist is the new row (1-based, self removed),
+    // freg/fdr the new regular force and jerk.  (xi, vi) is i at `time`.
+    void reg_correct(int i, double time, const int *nlist, const double *freg, const double *fdr) {
+        const int nnb = nlist[0];
+        const int nnb0 = row(i)[0];
+        const double dtr = time - t0r[i];
+        double xi[3], vi[3];
+        pred_at(i, time, xi, vi);
+        const double ri2 = xi[0] * xi[0] + xi[1] * xi[1] + xi[2] * xi[2];
+        const double znbmin = 0.2 * P.nnbopt;
+        const double rsfac = std::max(25.0 / tcr, 0.0);
+        // Ahmad-Cohen radius update (regcor_gpu.F:131-196, NB_FLAG = 0 form)
+        if (nnb > 0) {
+            const double fac = 1.0 + 0.1 * (double)(P.nnbopt - nnb) / (double)nnb;
+            double a3 = nnb * fac;
+            const double nbave = std::min(P.nnbopt + 150, std::max(P.nnbmax - 50, (int)znbmin));
+            a3 = std::min(a3, 0.9 * nbave);
+            const int nbp = (int)a3;
+            a3 = std::max(a3, znbmin);
+            double a4 = a3 / nnb;
+            if ((a3 - nnb0) * (a3 - nnb) < 0.0) a4 = sqrt(a4);
+            const double a5 = std::min(rsfac * dtr, 0.25);
+            a4 -= 1.0;
+            a4 = a4 > a5 ? a5 : std::max(a4, -a5);
+            const double a3b = a4 / 3.0;
+            double a1 = 1.0 + a3b - a3b * a3b;
+            if (nnb < znbmin && nbp > znbmin && a1 < 1.0) a1 = 1.05;
+            if (fabs(a1 - 1.0) > 0.003) {
+                if (rs[i] * rs[i] > ri2 && rs[i] * rs[i] < 2.0 * ri2 && nnb > 5) a1 = sqrt(a1);
+                rs[i] *= a1;
+            }
+            const double ridot = xi[0] * vi[0] + xi[1] * vi[1] + xi[2] * vi[2];
+            if (nnb > nbave && ridot < 0.0) rs[i] *= 1.0 - (nnb - nbave) / (3.0 * nnb);
+        } else {
+            rs[i] *= 1.5;  // zero membership (fpoly0.F:140-160)
+        }
+        // neighbour gains and losses: move their force between the parts
+        // (regcor_gpu.F:284-444)
+        double dfirr[3] = {0, 0, 0}, dfd[3] = {0, 0, 0};
+        const int *old = row(i);
+        int a = 1, b = 1;
+        while (a <= nnb0 || b <= nnb) {
+            const int jo = a <= nnb0 ? old[a] : 0x7fffffff;
+            const int jn = b <= nnb ? nlist[b] : 0x7fffffff;
+            double fa[3], fj[3];
+            if (jo == jn) {
+                ++a;
+                ++b;
+            } else if (jo < jn) {  // lost
+                pair_force(xi, vi, jo - 1, time, fa, fj);
+                for (int k = 0; k < 3; ++k) {
+                    dfirr[k] -= fa[k];
+                    dfd[k] -= fj[k];
+                }
+                ++a;
+            } else {  // gained
+                pair_force(xi, vi, jn - 1, time, fa, fj);
+                for (int k = 0; k < 3; ++k) {
+                    dfirr[k] += fa[k];
+                    dfd[k] += fj[k];
+                }
+                ++b;
+            }
+        }
+        // regular corrector (regcor_gpu.F:442-537)
+        const double dtsq = dtr * dtr, dt6 = 6.0 / (dtr * dtsq), dt2 = 2.0 / dtsq;
+        const double dtsq12 = dtsq / 12.0, dtr13 = dtr / 3.0;
+        for (int k = 0; k < 3; ++k) {
+            const size_t c = 3 * (size_t)i + k;
+            const double dfr = fr[c] - freg[k] - dfirr[k];
+            const double fdr0 = fdr[k] + dfd[k];
+            const double frd = frdot[c];
+            const double sum = frd + fdr0;
+            const double at3 = 2.0 * dfr + dtr * sum;
+            const double bt2 = -3.0 * dfr - dtr * (sum + frd);
+            x0[c] += (0.6 * at3 + bt2) * dtsq12;
+            v0[c] += (0.75 * at3 + bt2) * dtr13;
+            fi[c] += dfirr[k];
+            fr[c] = freg[k];
+            fidot[c] += dfd[k];
+            frdot[c] = fdr[k];
+            d3r[c] = at3 * dt6;
+            d2r[c] = (3.0 * at3 + bt2) * dt2;
+        }
+        memcpy(row(i), nlist, sizeof(int) * LS);
+        st.nb_sum += nnb;
+        st.nb_absdev += fabs((double)(nnb - P.nnbopt));
+        // new regular step (regcor_gpu.F:593-737)
+        double ttmp = tstep(&fr[3 * i], &frdot[3 * i], &d2r[3 * i], &d3r[3 * i], P.eta_r);
+        const double dt0 = ttmp;
+        if (ttmp > 2.0 * stepr[i]) {
+            ttmp = (fmod(time, 2.0 * dtr) == 0.0) ? std::min(2.0 * dtr, P.smax) : stepr[i];
+        } else if (ttmp < dtr) {
+            ttmp = 0.5 * dtr;
+            if (ttmp > dt0) ttmp *= 0.5;
+        } else {
+            ttmp = stepr[i];
+        }
+        ttmp = std::max(std::min(ttmp, P.smax), P.dtmin);
+        stepr[i] = ttmp;
+        t0r[i] = time;
+        for (int k = 0; k < 3; ++k) {
+            const size_t c = 3 * (size_t)i + k;
+            f[c] = 0.5 * (fi[c] + fr[c]);
+            fdot[c] = (fidot[c] + frdot[c]) / 6.0;
+        }
+        if (step[i] > stepr[i]) step[i] = stepr[i];
+        st.reg_steps++;
+    }
+
+    // ---- learned neighbour radius ----------------------------------------
+    // Features of body i at a regular step, the same formula as the library's
+    // epilogue (mlp.cuh): log(1+nnb) with self counted, log RS,
+    // log(1+nnb) - 1.5 log h2, log|a_reg|, -log2 dtr.
+    static void features(double nnb_self, double h2, double a2, double dtr, float *f) {
+        const double ln = log(1.0 + fabs(nnb_self));
+        const double lh = log(h2 > 1e-300 ? h2 : 1e-300);
+        f[0] = (float)ln;
+        f[1] = (float)(0.5 * lh);
+        f[2] = (float)(ln - 1.5 * lh);
+        f[3] = (float)(0.5 * log(a2 > 1e-300 ? a2 : 1e-300));
+        f[4] = (float)(-log2(dtr > 1e-300 ? dtr : 1e-300));
+    }
+    std::vector<float> feat;            // [n][5] at the body's last regular step
+    std::vector<double> rs_feat;        // RS used at that step
+    std::vector<unsigned char> have_feat;
+
+    // Mode 1, before the corrector of body i: the sample of its previous
+    // regular step is completed with this step's outcome -- target
+    // log(RS* / RS_prev), RS* = RS_used (NNBOPT / nnb)^(1/3) -- and this
+    // step's features are kept for the next one.
+    void learn_log(int i, int nnb_noself, double rs_used, double h2_used, const double *freg,
+                   double dtr_used) {
+        if (feat.empty()) {
+            feat.assign(5 * (size_t)n, 0.f);
+            rs_feat.assign(n, 0.0);
+            have_feat.assign(n, 0);
+        }
+        if (have_feat[i] && nnb_noself > 0 && st.nsamples < P.sample_cap && P.samples) {
+            float *o = P.samples + 6 * (size_t)st.nsamples;
+            for (int k = 0; k < 5; ++k) o[k] = feat[5 * (size_t)i + k];
+            o[5] = (float)(log(rs_used / rs_feat[i]) + log((double)P.nnbopt / nnb_noself) / 3.0);
+            st.nsamples++;
+        }
+        const double a2 = freg[0] * freg[0] + freg[1] * freg[1] + freg[2] * freg[2];
+        features(nnb_noself + 1, h2_used, a2, dtr_used, &feat[5 * (size_t)i]);
+        rs_feat[i] = rs_used;
+        have_feat[i] = 1;
+    }
+
+    // Mode 2, after the corrector: take RS_used exp(dlog) when the count it
+    // implies (nnb ~ RS^3) stays inside [NNBOPT/2, NNBMAX]; otherwise keep the
+    // Ahmad-Cohen radius the corrector just set.
+    void learn_apply(int i, int nnb_noself, double rs_used, double dlog) {
+        const double r = rs_used * exp(dlog);
+        const double expect = nnb_noself * exp(3.0 * dlog);
+        if (nnb_noself > 0 && dlog == dlog && expect >= 0.5 * P.nnbopt && expect <= P.nnbmax) {
+            rs[i] = r;
+            st.mlp_used++;
+        } else {
+            st.mlp_fallback++;
+        }
+    }
+
+    // neighbour-sphere criterion h2 of body i for gpunb_regf (m_flag: per
+    // unit mass, util_gpu.F:45-52; bodym = mean mass of its cluster)
+    double h2_of(int i, double bodym) const {
+        return P.m_flag ? rs[i] * rs[i] / bodym : rs[i] * rs[i];
+    }
+};
+
+}  // namespace nb6drv

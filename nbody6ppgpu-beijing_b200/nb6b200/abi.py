@@ -66,7 +66,8 @@ class ForceLib:
         for fn in ("gpunb_open_", "gpunb_close_", "gpunb_send_", "gpunb_regf_",
                    "gpunb_profile_", "gpunb_devinit_", "gpupot_", "irr_simd_open_",
                    "irr_simd_close_", "irr_simd_set_jp_", "irr_simd_set_list_",
-                   "irr_simd_firr_vec_", "irr_simd_profile_"):
+                   "irr_simd_firr_vec_", "irr_simd_profile_", "nb6_regf_seg_",
+                   "nb6_irr_predict_send_"):
             if hasattr(lib, fn):
                 getattr(lib, fn).restype = None
 
@@ -111,6 +112,29 @@ class ForceLib:
         self.lib.gpunb_regf_(_ci(ni), _dp(h2p), _dp(dtrp), _dp(xip), _dp(vip), _dp(acc),
                              _dp(jrk), _dp(pot), _ci(lmax), _ci(nnbmax), _ip(lst), _ci(m_flag))
         return acc[:ni], jrk[:ni], pot[:ni], lst[:ni]
+
+    def regf_seg(self, h2, dtr, xi, vi, iseg, seg_j0, lmax: int, nnbmax: int, m_flag: int = 0):
+        """nb6_regf_seg_ (this package's extension; no reference counterpart):
+        gpunb_regf for an ensemble of clusters sent together.  Segment c is
+        j range [seg_j0[c], seg_j0[c+1]) of the last send; i-particle k
+        belongs to segment iseg[k] (non-decreasing).  List ids come back
+        relative to the segment's first j."""
+        h2 = _f64(h2)
+        ni = h2.shape[0]
+        iseg = np.ascontiguousarray(iseg, dtype=np.int32)
+        seg_j0 = np.ascontiguousarray(seg_j0, dtype=np.int32)
+        nseg = seg_j0.shape[0] - 1
+        dtr = _f64(dtr, (ni,))
+        xi = _f64(xi, (ni, 3))
+        vi = _f64(vi, (ni, 3))
+        acc = np.zeros((ni, 3))
+        jrk = np.zeros((ni, 3))
+        pot = np.zeros(ni)
+        lst = np.zeros((ni, lmax), dtype=np.int32)
+        self.lib.nb6_regf_seg_(_ci(ni), _ip(iseg), _dp(h2), _dp(dtr), _dp(xi), _dp(vi), _dp(acc),
+                               _dp(jrk), _dp(pot), _ci(lmax), _ci(nnbmax), _ip(lst), _ci(m_flag),
+                               _ci(nseg), _ip(seg_j0))
+        return acc, jrk, pot, lst
 
     # ----------------------------------------------------------------- gpupot
     def gpupot(self, m, x, istart: int = 1, ni: int | None = None, irank: int = 0,
@@ -157,6 +181,14 @@ class ForceLib:
         for k in range(n):
             fn(_ci(first + k), _dp(pos[k]), _dp(vel[k]), _dp(acc2[k]), _dp(jrk6[k]),
                C.byref(C.c_double(mass[k])), C.byref(C.c_double(time[k])))
+
+    def irr_predict_send(self, t: float, addr0, count) -> None:
+        """nb6_irr_predict_send_ (extension): the gpunb j set made on the
+        device from the resident irregular records predicted to t; segment s
+        is count[s] records from 1-based address addr0[s]."""
+        addr0 = np.ascontiguousarray(addr0, dtype=np.int32)
+        count = np.ascontiguousarray(count, dtype=np.int32)
+        self.lib.nb6_irr_predict_send_(_cd(t), _ci(addr0.shape[0]), _ip(addr0), _ip(count))
 
     def irr_set_list(self, addr: int, nblist) -> None:
         """nblist = [nnb, j1, ..., jnnb] with 1-based j (Fortran LIST(1,I)).

@@ -2,7 +2,10 @@
 
 ``run(backend, cluster, ...)`` integrates a cluster of single stars with the
 Hermite / Ahmad-Cohen block-step scheme of the reference (see
-``driver/blockstep.cpp``) on a force backend given as shared-object paths:
+``driver/blockstep.cpp``), and ``run_ensemble(backend, clusters, ...)`` an
+ensemble of independent clusters with every force kind issued once per block
+for all of them (``driver/ensemble.cpp``), on a force backend given as
+shared-object paths:
 
 * ``backend_paths("nb6b200")``  -- this package's libnb6b200.so for all three
   libraries;
@@ -26,7 +29,8 @@ class Params(C.Structure):
                 ("dtmin", C.c_double), ("tcrit", C.c_double), ("dt_out", C.c_double),
                 ("rs0", C.c_double), ("nnbopt", C.c_int), ("nnbmax", C.c_int),
                 ("lmax", C.c_int), ("m_flag", C.c_int), ("chunk", C.c_int),
-                ("max_blocks", C.c_longlong)]
+                ("max_blocks", C.c_longlong), ("mlp_mode", C.c_int), ("mlp_pad", C.c_int),
+                ("samples", C.POINTER(C.c_float)), ("sample_cap", C.c_longlong)]
 
 
 class Stats(C.Structure):
@@ -35,7 +39,9 @@ class Stats(C.Structure):
                 ("overflow_retries", C.c_longlong), ("nb_sum", C.c_longlong),
                 ("reg_pairs", C.c_longlong), ("wall_reg", C.c_double),
                 ("wall_irr", C.c_double), ("wall_total", C.c_double),
-                ("t_end", C.c_double), ("nout", C.c_int)]
+                ("t_end", C.c_double), ("nout", C.c_int), ("nsamples", C.c_longlong),
+                ("mlp_used", C.c_longlong), ("mlp_fallback", C.c_longlong),
+                ("nb_absdev", C.c_double)]
 
 
 @dataclass
@@ -47,6 +53,7 @@ class RunResult:
     x: np.ndarray
     v: np.ndarray
     stats: dict
+    samples: np.ndarray | None = None   # [nsamples, 6] (mlp_mode 1)
 
     @property
     def de_max(self) -> float:
@@ -64,6 +71,7 @@ def _lib():
             raise RuntimeError(f"{DRIVER_LIB} missing: run nbody6ppgpu-beijing_b200/build.py")
         _LIB = C.CDLL(DRIVER_LIB, mode=C.RTLD_LOCAL)
         _LIB.nb6drive_run.restype = C.c_int
+        _LIB.nb6drive_ensemble.restype = C.c_int
     return _LIB
 
 
@@ -74,15 +82,34 @@ def backend_paths(name: str = "nb6b200") -> dict:
     raise ValueError(name)
 
 
+def _mlp_fields(p: "Params", mlp_mode: int, sample_cap: int):
+    """Fill the learned-radius fields; returns the sample buffer (or None)."""
+    p.mlp_mode = mlp_mode
+    p.mlp_pad = 0
+    buf = None
+    if mlp_mode == 1 and sample_cap > 0:
+        buf = np.zeros((sample_cap, 6), dtype=np.float32)
+        p.samples = buf.ctypes.data_as(C.POINTER(C.c_float))
+        p.sample_cap = sample_cap
+    else:
+        p.samples = C.POINTER(C.c_float)()
+        p.sample_cap = 0
+    return buf
+
+
 def run(backend: dict, mass, pos, vel, *, tcrit=1.0, eta_i=0.02, eta_r=0.03, smax=0.125,
         dtmin=2.0 ** -24, dt_out=0.125, rs0=0.3, nnbopt=50, nnbmax=400, lmax=512, m_flag=0,
-        chunk=1024, max_blocks=10_000_000) -> RunResult:
+        chunk=1024, max_blocks=10_000_000, mlp_mode=0, sample_cap=0) -> RunResult:
+    """mlp_mode: 0 Ahmad-Cohen radii; 1 Ahmad-Cohen and log up to sample_cap
+    (features, target) samples into RunResult.samples; 2 the library's learned
+    proposals (nb6b200.mlp.enable(True) first), Ahmad-Cohen as fallback."""
     mass = np.ascontiguousarray(mass, dtype=np.float64)
     n = mass.shape[0]
     x = np.ascontiguousarray(pos, dtype=np.float64).reshape(n, 3).copy()
     v = np.ascontiguousarray(vel, dtype=np.float64).reshape(n, 3).copy()
     p = Params(eta_i, eta_r, smax, dtmin, tcrit, dt_out, rs0, nnbopt, nnbmax, lmax, m_flag,
                chunk, max_blocks)
+    buf = _mlp_fields(p, mlp_mode, sample_cap)
     nout_max = int(tcrit / dt_out) + 4
     eout = np.zeros((nout_max, 4))
     st = Stats()
@@ -95,4 +122,60 @@ def run(backend: dict, mass, pos, vel, *, tcrit=1.0, eta_i=0.02, eta_r=0.03, sma
         raise RuntimeError(f"nb6drive_run failed with code {rc}")
     k = st.nout
     stats = {f: getattr(st, f) for f, _ in Stats._fields_}
-    return RunResult(eout[:k, 0], eout[:k, 1], eout[:k, 2], eout[:k, 3], x, v, stats)
+    samples = buf[:st.nsamples].copy() if buf is not None else None
+    return RunResult(eout[:k, 0], eout[:k, 1], eout[:k, 2], eout[:k, 3], x, v, stats, samples)
+
+
+@dataclass
+class EnsembleResult:
+    times: np.ndarray      # [nout]
+    energy: np.ndarray     # [nout, ncl, 3]: kinetic, potential, total
+    x: list                # per cluster [n_c, 3]
+    v: list
+    stats: dict
+    samples: np.ndarray | None = None
+
+    @property
+    def de_max(self) -> np.ndarray:
+        """max_t |E_c(t) - E_c(0)| / |E_c(0)| per cluster."""
+        e = self.energy[:, :, 2]
+        return np.max(np.abs(e - e[0]), axis=0) / np.abs(e[0])
+
+
+def run_ensemble(backend: dict, clusters, *, batched=True, tcrit=1.0, eta_i=0.02, eta_r=0.03,
+                 smax=0.125, dtmin=2.0 ** -24, dt_out=0.125, rs0=0.3, nnbopt=50, nnbmax=400,
+                 lmax=512, m_flag=0, chunk=1024, max_blocks=100_000_000, mlp_mode=0,
+                 sample_cap=0) -> EnsembleResult:
+    """clusters: sequence of (mass, pos, vel) (or objects with .mass/.pos/.vel),
+    each in its own Henon units.  batched=False issues the regular force per
+    cluster (what running each alone does); the result is then identical to
+    ``run`` on each cluster with a deterministic backend."""
+    parts = [(c.mass, c.pos, c.vel) if hasattr(c, "mass") else c for c in clusters]
+    counts = np.array([len(p[0]) for p in parts], dtype=np.int32)
+    ncl = len(parts)
+    mass = np.ascontiguousarray(np.concatenate([p[0] for p in parts]), dtype=np.float64)
+    x = np.ascontiguousarray(np.concatenate([np.reshape(p[1], (-1, 3)) for p in parts]), dtype=np.float64)
+    v = np.ascontiguousarray(np.concatenate([np.reshape(p[2], (-1, 3)) for p in parts]), dtype=np.float64)
+    p = Params(eta_i, eta_r, smax, dtmin, tcrit, dt_out, rs0, nnbopt, nnbmax, lmax, m_flag,
+               chunk, max_blocks)
+    buf = _mlp_fields(p, mlp_mode, sample_cap)
+    nout_max = int(tcrit / dt_out) + 4
+    tout = np.zeros(nout_max)
+    eout = np.zeros((nout_max, ncl, 3))
+    st = Stats()
+    dp = C.POINTER(C.c_double)
+    rc = _lib().nb6drive_ensemble(backend["reg"].encode(), backend["irr"].encode(),
+                                  backend["pot"].encode(), C.c_int(ncl),
+                                  counts.ctypes.data_as(C.POINTER(C.c_int)), mass.ctypes.data_as(dp),
+                                  x.ctypes.data_as(dp), v.ctypes.data_as(dp), C.byref(p),
+                                  C.c_int(1 if batched else 0), tout.ctypes.data_as(dp),
+                                  eout.ctypes.data_as(dp), C.c_int(nout_max), C.byref(st))
+    if rc != 0:
+        raise RuntimeError(f"nb6drive_ensemble failed with code {rc}")
+    k = st.nout
+    stats = {f: getattr(st, f) for f, _ in Stats._fields_}
+    off = np.concatenate([[0], np.cumsum(counts)])
+    xs = [x[off[c]:off[c + 1]] for c in range(ncl)]
+    vs = [v[off[c]:off[c + 1]] for c in range(ncl)]
+    samples = buf[:st.nsamples].copy() if buf is not None else None
+    return EnsembleResult(tout[:k], eout[:k], xs, vs, stats, samples)

@@ -1,0 +1,28 @@
+"""What the trained network gains over the Ahmad-Cohen rule alone.
+
+Samples are logged from plain runs of two Plummer/Kroupa clusters, the model
+is trained on the GPU by the library's own kernels, and a third cluster
+(unseen seed) is integrated twice to the same time: with the plain rule and
+with the learned proposals (Ahmad-Cohen as fallback).  The learned run must
+keep the neighbour counts closer to NNBOPT, without more overflow
+re-evaluations and with an energy error of the same order."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_learned_radius_keeps_counts_closer_to_nnbopt(nb6):
+    from nb6b200 import ics, learn
+    train = [ics.plummer(4096, seed=300 + k, imf=True) for k in range(2)]
+    samples = learn.collect(train, tcrit=0.25)
+    assert len(samples) > 5000 and np.all(np.isfinite(samples))
+    hist = learn.fit(samples, epochs=15)
+    assert hist[-1] < 0.8 * hist[0], hist
+    res = learn.compare(ics.plummer(4096, seed=399, imf=True), tcrit=0.25)
+    p, q = res["plain"], res["learned"]
+    print(f"\nsamples {len(samples)}, loss {hist[0]:.3f} -> {hist[-1]:.3f}\nplain   {p}\nlearned {q}")
+    assert q["mlp_used"] > 0.5 * (q["mlp_used"] + q["mlp_fallback"])
+    assert q["nnb_absdev_mean"] < p["nnb_absdev_mean"]
+    assert q["overflow_retries"] <= p["overflow_retries"] + 2
+    assert q["dE"] < 3.0 * p["dE"] + 1e-6

