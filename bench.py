@@ -44,9 +44,10 @@ import numpy as np  # noqa: E402
 
 METRIC = "Regular force+jerk+nbr pair interactions/s at N=1M"
 FLOPS_PER_PAIR = 60          # gpunb.velocity.cu:895, reg.avx.cpp:343
-# DRAM bytes per regf_kernel launch (1024 i x 996,147 j), from the ncu capture
-# summarised in profiles/regf_kernel_king1m.md; None until captured.
-NCU_TRAFFIC_PER_LAUNCH = None
+# DRAM bytes (read + write) per launch of the headline force kernel,
+# regf_x2_kernel<1> with 1024 i x 996,147 j, from the ncu capture summarised
+# in profiles/regf_x2_kernel_king1m.md (56.09 MB read + 0.66 MB written).
+NCU_TRAFFIC_PER_LAUNCH = 56.09e6 + 0.658e6
 
 
 def parse():
@@ -63,6 +64,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-pot", action="store_true", help="skip the N^2 potential leg")
     ap.add_argument("--seed", type=int, default=20260)
     return ap.parse_args()
 
@@ -349,6 +351,28 @@ def main():
                "d2h_bytes_per_step": int(n * 64 + n * W * 4),
                "steps": e2e_steps, "timing": "wall clock around synchronous ABI calls"}
 
+    # the N^2 potential of the same cluster (GPUPOT, energy.F:33): kernel
+    # time on the library stream, 27 flops per pair (pot.avx.cpp:123-135);
+    # accuracy on a contiguous sample of 64 i against the FP64 oracle
+    pot = None
+    if not args.no_pot:
+        d_m = torch.tensor(m, dtype=torch.float64, device=dev)
+        outp = C.POINTER(C.c_double)()
+        for _ in range(2):
+            raw.nb6_pot_device_(C.byref(ci(1)), C.byref(ci(n)), C.byref(ci(n)),
+                                C.c_void_p(d_m.data_ptr()), C.c_void_p(d_x.data_ptr()), C.byref(outp))
+        pot_ms = float(raw.nb6_pot_last_kernel_ms_())
+        pot = {"pairs_per_s": float(n) * n / (pot_ms * 1e-3), "kernel_ms": pot_ms,
+               "flops_per_pair": 27,
+               "frac_fp32_peak": 27.0 * n * n / (pot_ms * 1e-3) / 1e12 / peak_tf}
+        del d_m
+        if rank == 0:
+            import oracle
+            i0 = int(np.random.default_rng(9).integers(1, n - 64))
+            po = oracle.pot(m, x, i0, 64)
+            pg_ = lib.gpupot(m, x, istart=i0, ni=64)
+            pot["rel_err_max_sample64"] = float(np.max(np.abs(pg_ / po - 1)))
+
     # accuracy against the FP64 oracle on a sample of i (rank 0)
     err = None
     cpu = None
@@ -384,7 +408,10 @@ def main():
     roof = {"bound": "fp32", "achieved": achieved, "peak": peak_tf, "unit": "TFLOP/s",
             "frac": achieved / peak_tf if peak_tf else None,
             "traffic": NCU_TRAFFIC_PER_LAUNCH,
-            "kernel": "regf_kernel", "kernel_ms_per_launch": kernel_ms,
+            "kernel": {11: "regf_x2_kernel<1>", 12: "regf_x2_kernel<2>", 13: "regf_x2_kernel<1,f64dx>",
+                       1: "regf_kernel<1>", 2: "regf_kernel<2>", 4: "regf_kernel<4>"}.get(
+                           geom[0], f"regf_jpar_kernel<{-geom[0]}>"),
+            "kernel_ms_per_launch": kernel_ms,
             "flops_per_launch": FLOPS_PER_PAIR * args.chunk * n,
             "algorithmic_bytes_per_launch": 48 * n + 64 * args.chunk,
             "peak_source": "measured: FFMA probe kernel in the library, same process "
@@ -408,6 +435,7 @@ def main():
             "gpu_launches": int(args.steps * len(chunks) * 2),
             "clocks": clk, "roofline": roof, "e2e": e2e, "cpu_baseline": cpu,
             "err_vs_fp64": err,
+            "gpupot": pot,
             "pct_fp32_peak": 100.0 * FLOPS_PER_PAIR * pairs_step / (ms * 1e-3) / 1e12 / peak_tf,
         }
         print(json.dumps(out), flush=True)

@@ -53,10 +53,10 @@ NB6_DEV void load_rec(const Rec *__restrict__ p, Rec &r) {
     r.m = g.x; r.t0 = g.y;
 }
 
+// out row k = (ax, ay, az, jx, jy, jz, nnbid, 0): one download per call.
 __global__ void __launch_bounds__(IRR_WARPS * 32)
     irr_kernel(int ni, const int *__restrict__ addr, double ti, const Rec *__restrict__ rec,
-               const int *__restrict__ lists, int ls, int nmax, double *__restrict__ out,
-               int *__restrict__ outid) {
+               const int *__restrict__ lists, int ls, int nmax, double *__restrict__ out) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int k = blockIdx.x * IRR_WARPS + warp;
     if (k >= ni) return;
@@ -113,31 +113,36 @@ __global__ void __launch_bounds__(IRR_WARPS * 32)
         }
     }
     if (lane == 0) {
-        double *o = out + (size_t)k * 6;
+        double *o = out + (size_t)k * 8;
         o[0] = ax;
         o[1] = ay;
         o[2] = az;
         o[3] = jx;
         o[4] = jy;
         o[5] = jz;
-        outid[k] = (nnb > 0 && jmin != 0x7fffffff) ? jmin + 1 : -1;
+        o[6] = (double)((nnb > 0 && jmin != 0x7fffffff) ? jmin + 1 : -1);
+        o[7] = 0.0;
     }
 }
 
-// Scatter staged records: slot s goes to particle saddr[s].
-__global__ void irr_scatter_jp(int ns, const int *__restrict__ saddr, const Rec *__restrict__ src,
-                               Rec *__restrict__ rec) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s < ns) rec[saddr[s]] = src[s];
-}
-
-// Scatter staged lists: entry e starts at off[e] in `stage` as [addr, nnb, ids].
-__global__ void irr_scatter_list(int ne, const int *__restrict__ off, const int *__restrict__ stage,
-                                 int *__restrict__ lists, int ls) {
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+// Scatter everything staged since the last flush, in one launch: blocks
+// [0, nbr) move record slot s to particle saddr[s] (one thread per record);
+// the remaining blocks move list entry e (one warp per entry), which starts
+// at off[e] in `words` as [addr, nnb, ids...].
+constexpr int SCATTER_NT = 256;
+__global__ void __launch_bounds__(SCATTER_NT)
+    irr_scatter(int njp, int nbr, const int *__restrict__ saddr, const Rec *__restrict__ src,
+                Rec *__restrict__ rec, int ne, const int *__restrict__ off, const int *__restrict__ words,
+                int *__restrict__ lists, int ls) {
+    if ((int)blockIdx.x < nbr) {
+        const int s = blockIdx.x * SCATTER_NT + threadIdx.x;
+        if (s < njp) rec[saddr[s]] = src[s];
+        return;
+    }
+    const int warp = ((blockIdx.x - nbr) * SCATTER_NT + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= ne) return;
-    const int *e = stage + off[warp];
+    const int *e = words + off[warp];
     const int a = e[0], nnb = e[1];
     int *row = lists + (size_t)a * ls;
     if (lane == 0) row[0] = nnb;
@@ -197,15 +202,16 @@ struct IrrState {
     DevBuf<Rec> rec;
     DevBuf<int> lists;
     DevBuf<Rec> dstage_rec;
-    DevBuf<int> dstage_addr, dstage_list, dstage_off, daddr, dnnbid;
+    DevBuf<int> dints;     // [jp addr | list offsets | active addr | list words]
     DevBuf<double> dout;
     DevBuf<int> dseg;      // predict-send segment tables
     HostBuf<int> hseg;
     HostBuf<Rec> hstage_rec;
-    HostBuf<int> hstage_addr, hstage_list, hstage_off, haddr, hnnbid;
+    HostBuf<int> hstage_addr, hstage_list, hints;
     HostBuf<double> hout;
     std::vector<int> jp_slot, list_slot;  // staged slot per particle, -1 if none
     std::vector<int> nnb_host;            // list lengths, for the profile counters
+    std::vector<int> flush_off;           // latest list entry per particle, per flush
     int njp = 0, nlist = 0;
     size_t list_words = 0;
     double time_grav = 0;
@@ -250,20 +256,14 @@ void irr_close_impl() {
     I.rec.release();
     I.lists.release();
     I.dstage_rec.release();
-    I.dstage_addr.release();
-    I.dstage_list.release();
-    I.dstage_off.release();
-    I.daddr.release();
-    I.dnnbid.release();
+    I.dints.release();
     I.dout.release();
     I.dseg.release();
     I.hseg.release();
     I.hstage_rec.release();
     I.hstage_addr.release();
     I.hstage_list.release();
-    I.hstage_off.release();
-    I.haddr.release();
-    I.hnnbid.release();
+    I.hints.release();
     I.hout.release();
     I.jp_slot.clear();
     I.list_slot.clear();
@@ -351,49 +351,69 @@ void irr_set_list_impl(int a, const int *nblist) {
     I.nlist++;
 }
 
-// Upload and scatter everything staged since the last flush.
-void irr_flush(cudaStream_t st) {
-    if (I.njp > 0) {
-        I.dstage_rec.reserve(I.njp);
-        I.dstage_addr.reserve(I.njp);
-        NB6_CUDA_CHECK(cudaMemcpyAsync(I.dstage_rec.ptr, I.hstage_rec.ptr, sizeof(Rec) * I.njp,
-                                       cudaMemcpyHostToDevice, st));
-        NB6_CUDA_CHECK(cudaMemcpyAsync(I.dstage_addr.ptr, I.hstage_addr.ptr, sizeof(int) * I.njp,
-                                       cudaMemcpyHostToDevice, st));
-        irr_scatter_jp<<<(I.njp + 255) / 256, 256, 0, st>>>(I.njp, I.dstage_addr.ptr, I.dstage_rec.ptr,
-                                                           I.rec.ptr);
-        NB6_CUDA_CHECK(cudaGetLastError());
-        for (int s = 0; s < I.njp; ++s) I.jp_slot[I.hstage_addr.ptr[s]] = -1;
-        I.njp = 0;
-    }
+// Small stagings are read by the kernels straight from pinned host memory
+// (mapped under unified addressing), which saves the copy launches that
+// dominate a block's irregular call; large ones (start-up, many actives)
+// go through one bulk DMA copy each.
+constexpr size_t ZERO_COPY_MAX = 1 << 20;
+size_t zero_copy_bytes() { return nb6_uva() ? ZERO_COPY_MAX : 0; }
+
+// Upload and scatter everything staged since the last flush, with the
+// active addresses of a force call (active may be null): the records and
+// all integers either read in place or copied once each, then one scatter
+// launch.  Returns a device-readable pointer to the active addresses.
+const int *irr_flush(cudaStream_t st, const int *active = nullptr, int ni = 0) {
+    // keep only the latest list entry per particle
+    int ne = 0;
+    std::vector<int> &offs = I.flush_off;
+    offs.clear();
     if (I.nlist > 0) {
-        // keep only the latest entry per particle
-        I.hstage_off.reserve(I.nlist);
-        int ne = 0;
         size_t w = 0;
         while (w < I.list_words) {
             const int a = I.hstage_list.ptr[w];
             const int nnb = I.hstage_list.ptr[w + 1];
             if (I.list_slot[a] == (int)w) {
-                I.hstage_off.ptr[ne++] = (int)w;
+                offs.push_back((int)w);
                 I.list_slot[a] = -1;
             }
             w += 2 + nnb;
         }
-        I.dstage_list.reserve(I.list_words);
-        I.dstage_off.reserve(ne);
-        NB6_CUDA_CHECK(cudaMemcpyAsync(I.dstage_list.ptr, I.hstage_list.ptr, sizeof(int) * I.list_words,
-                                       cudaMemcpyHostToDevice, st));
-        NB6_CUDA_CHECK(cudaMemcpyAsync(I.dstage_off.ptr, I.hstage_off.ptr, sizeof(int) * ne,
-                                       cudaMemcpyHostToDevice, st));
-        const int threads = 256;
-        const int blocks = (int)(((size_t)ne * 32 + threads - 1) / threads);
-        irr_scatter_list<<<blocks, threads, 0, st>>>(ne, I.dstage_off.ptr, I.dstage_list.ptr,
-                                                     I.lists.ptr, I.lmax);
-        NB6_CUDA_CHECK(cudaGetLastError());
-        I.nlist = 0;
-        I.list_words = 0;
+        ne = (int)offs.size();
     }
+    const int njp = I.njp;
+    const size_t nint = (size_t)njp + ne + ni + I.list_words;
+    if (nint == 0) return nullptr;
+    I.hints.reserve(nint);
+    I.dints.reserve(nint);
+    int *h = I.hints.ptr;
+    if (njp) memcpy(h, I.hstage_addr.ptr, sizeof(int) * njp);
+    if (ne) memcpy(h + njp, offs.data(), sizeof(int) * ne);
+    if (ni) memcpy(h + njp + ne, active, sizeof(int) * ni);
+    if (I.list_words) memcpy(h + njp + ne + ni, I.hstage_list.ptr, sizeof(int) * I.list_words);
+    const Rec *drec = I.hstage_rec.ptr;
+    if (njp && sizeof(Rec) * (size_t)njp > zero_copy_bytes()) {
+        I.dstage_rec.reserve(njp);
+        NB6_CUDA_CHECK(cudaMemcpyAsync(I.dstage_rec.ptr, I.hstage_rec.ptr, sizeof(Rec) * njp,
+                                       cudaMemcpyHostToDevice, st));
+        drec = I.dstage_rec.ptr;
+    }
+    const int *d = h;
+    if (sizeof(int) * nint > zero_copy_bytes()) {
+        NB6_CUDA_CHECK(cudaMemcpyAsync(I.dints.ptr, h, sizeof(int) * nint, cudaMemcpyHostToDevice, st));
+        d = I.dints.ptr;
+    }
+    const int nbr = (njp + SCATTER_NT - 1) / SCATTER_NT;
+    const int nbl = (int)(((size_t)ne * 32 + SCATTER_NT - 1) / SCATTER_NT);
+    if (nbr + nbl > 0) {
+        irr_scatter<<<nbr + nbl, SCATTER_NT, 0, st>>>(njp, nbr, d, drec, I.rec.ptr, ne, d + njp,
+                                                      d + njp + ne + ni, I.lists.ptr, I.lmax);
+        NB6_CUDA_CHECK(cudaGetLastError());
+    }
+    for (int q = 0; q < njp; ++q) I.jp_slot[I.hstage_addr.ptr[q]] = -1;
+    I.njp = 0;
+    I.nlist = 0;
+    I.list_words = 0;
+    return d + njp + ne;
 }
 
 void irr_firr_vec_impl(double ti, int ni, const int *addr, double (*acc)[3], double (*jrk)[3],
@@ -412,38 +432,38 @@ void irr_firr_vec_impl(double ti, int ni, const int *addr, double (*acc)[3], dou
     }
     const double t0 = nb6_wtime();
     cudaStream_t st = nb6_stream();
-    // the staged records must reach the device before we clear the staging,
-    // which the stream order guarantees (copies precede the next host write
-    // only after this call's synchronize below)
-    irr_flush(st);
-    I.haddr.reserve(ni);
-    I.daddr.reserve(ni);
-    I.dout.reserve((size_t)ni * 6);
-    I.dnnbid.reserve(ni);
-    I.hout.reserve((size_t)ni * 6);
-    I.hnnbid.reserve(ni);
-    memcpy(I.haddr.ptr, addr, sizeof(int) * ni);
-    NB6_CUDA_CHECK(cudaMemcpyAsync(I.daddr.ptr, I.haddr.ptr, sizeof(int) * ni, cudaMemcpyHostToDevice, st));
-    irr_kernel<<<(ni + IRR_WARPS - 1) / IRR_WARPS, IRR_WARPS * 32, 0, st>>>(
-        ni, I.daddr.ptr, ti, I.rec.ptr, I.lists.ptr, I.lmax, I.nmax, I.dout.ptr, I.dnnbid.ptr);
+    // the pinned staging is reused only after this call's synchronize, so
+    // the uploads enqueued here read it intact
+    const int *daddr = irr_flush(st, addr, ni);
+    I.hout.reserve((size_t)ni * 8);
+    // results go straight to pinned host memory when small, else through
+    // one device buffer and one copy
+    const bool direct = sizeof(double) * 8 * (size_t)ni <= zero_copy_bytes();
+    double *out = I.hout.ptr;
+    if (!direct) {
+        I.dout.reserve((size_t)ni * 8);
+        out = I.dout.ptr;
+    }
+    irr_kernel<<<(ni + IRR_WARPS - 1) / IRR_WARPS, IRR_WARPS * 32, 0, st>>>(ni, daddr, ti, I.rec.ptr, I.lists.ptr,
+                                                                       I.lmax, I.nmax, out);
     NB6_CUDA_CHECK(cudaGetLastError());
-    NB6_CUDA_CHECK(cudaMemcpyAsync(I.hout.ptr, I.dout.ptr, sizeof(double) * 6 * ni,
-                                   cudaMemcpyDeviceToHost, st));
-    NB6_CUDA_CHECK(cudaMemcpyAsync(I.hnnbid.ptr, I.dnnbid.ptr, sizeof(int) * ni, cudaMemcpyDeviceToHost, st));
+    if (!direct)
+        NB6_CUDA_CHECK(cudaMemcpyAsync(I.hout.ptr, I.dout.ptr, sizeof(double) * 8 * ni, cudaMemcpyDeviceToHost, st));
+    nb6_status_fetch(st);
     NB6_CUDA_CHECK(cudaStreamSynchronize(st));
     if (nb6_check_dev_status() != 0) return;
     unsigned long long inter = 0;
     for (int k = 0; k < ni; ++k) inter += (unsigned long long)I.nnb_host[addr[k] - 1];
     I.num_inter += inter;
     for (int k = 0; k < ni; ++k) {
-        const double *o = I.hout.ptr + (size_t)k * 6;
+        const double *o = I.hout.ptr + (size_t)k * 8;
         acc[k][0] = o[0];
         acc[k][1] = o[1];
         acc[k][2] = o[2];
         jrk[k][0] = o[3];
         jrk[k][1] = o[4];
         jrk[k][2] = o[5];
-        nnbid[k] = I.hnnbid.ptr[k];
+        nnbid[k] = (int)o[6];
     }
     I.time_grav += nb6_wtime() - t0;
     I.num_fcall++;

@@ -226,7 +226,9 @@ int nb6_device_id();               // device picked at devinit (GPU_LIST / NB_GP
 void nb6_devinit_once(int irank);
 cudaStream_t nb6_stream();         // the library's stream (non-blocking)
 int *nb6_dev_status();             // device status word (zeroed at init)
-int nb6_check_dev_status();        // sync-free read after a stream sync
+int nb6_check_dev_status();        // read (and clear) after a stream sync
+void nb6_status_fetch(cudaStream_t st);  // enqueue the status copy before that sync
+bool nb6_uva();                    // device reads/writes pinned host memory in place
 int nb6_num_sms();
 
 static inline double nb6_wtime() {

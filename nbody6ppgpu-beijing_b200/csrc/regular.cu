@@ -1829,6 +1829,7 @@ void gpunb_regf_(int *ni_, double *h2, double *dtr, double (*xi)[3], double (*vi
     R.houtf.reserve((size_t)ni * 8);
     R.houtl.reserve((size_t)ni * W);
     regf_submit(L, st);
+    nb6_status_fetch(st);
     NB6_CUDA_CHECK(cudaStreamSynchronize(st));
     NB6_CUDA_CHECK(cudaEventElapsedTime(&R.last_kernel_ms, R.ev0, R.ev1));
     const double wt = nb6_wtime();

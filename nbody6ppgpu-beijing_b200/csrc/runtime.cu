@@ -19,6 +19,9 @@ static int g_device = -1;
 static int g_num_sms = 0;
 static cudaStream_t g_stream = nullptr;
 static int *g_dev_status = nullptr;
+static int *g_status_host = nullptr;   // pinned copy, filled by nb6_status_fetch
+static bool g_status_fetched = false;
+static bool g_uva = false;
 static int g_host_status = 0;
 static int g_abort_on_error = 1;
 static bool g_abort_env_read = false;
@@ -67,6 +70,11 @@ void nb6_devinit_once(int irank) {
     NB6_CUDA_CHECK(cudaStreamCreateWithFlags(&g_stream, cudaStreamNonBlocking));
     NB6_CUDA_CHECK(cudaMalloc((void **)&g_dev_status, sizeof(int)));
     NB6_CUDA_CHECK(cudaMemset(g_dev_status, 0, sizeof(int)));
+    NB6_CUDA_CHECK(cudaMallocHost((void **)&g_status_host, sizeof(int)));
+    *g_status_host = 0;
+    int uva = 0;
+    NB6_CUDA_CHECK(cudaDeviceGetAttribute(&uva, cudaDevAttrUnifiedAddressing, dev));
+    g_uva = uva != 0;
     if (getenv("NB6_VERBOSE")) {
         cudaDeviceProp prop;
         cudaGetDeviceProperties(&prop, dev);
@@ -80,10 +88,25 @@ int nb6_num_sms() { return g_num_sms; }
 cudaStream_t nb6_stream() { return g_stream; }
 int *nb6_dev_status() { return g_dev_status; }
 
+bool nb6_uva() { return g_uva; }
+
+// Enqueue a copy of the device status word into pinned host memory; the
+// next nb6_check_dev_status after a sync of `st` reads that copy instead of
+// doing a synchronous copy of its own.
+void nb6_status_fetch(cudaStream_t st) {
+    NB6_CUDA_CHECK(cudaMemcpyAsync(g_status_host, g_dev_status, sizeof(int), cudaMemcpyDeviceToHost, st));
+    g_status_fetched = true;
+}
+
 // Read (and clear) the device status word; call after a stream sync.
 int nb6_check_dev_status() {
     int st = 0;
-    NB6_CUDA_CHECK(cudaMemcpy(&st, g_dev_status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (g_status_fetched) {
+        st = *(volatile int *)g_status_host;
+        g_status_fetched = false;
+    } else {
+        NB6_CUDA_CHECK(cudaMemcpy(&st, g_dev_status, sizeof(int), cudaMemcpyDeviceToHost));
+    }
     if (st != 0) {
         NB6_CUDA_CHECK(cudaMemset(g_dev_status, 0, sizeof(int)));
         fprintf(stderr, "libnb6b200: device reported status %d\n", st);

@@ -218,14 +218,11 @@ bool Sim::run(double *eout, int nout_max) {
     std::vector<int> active, reg, addr;
     std::vector<double> a, jd;
     std::vector<int> nnbid;
+    clock_reset();
     while (st.blocks < P.max_blocks) {
-        double tmin = 1e300;
-        for (int i = 0; i < n; ++i) tmin = std::min(tmin, t0[i] + step[i]);
+        const double tmin = clock_next(active);
         if (tmin > P.tcrit + 1e-12) break;
         time = tmin;
-        active.clear();
-        for (int i = 0; i < n; ++i)
-            if (t0[i] + step[i] == tmin) active.push_back(i);
         st.blocks++;
         // irregular force at the block time (intgrt.F:533) and corrector
         const int na = (int)active.size();
@@ -244,6 +241,7 @@ bool Sim::run(double *eout, int nout_max) {
             if (irr_correct(active[q], time, &a[3 * (size_t)q], &jd[3 * (size_t)q])) reg.push_back(active[q]);
         if (!reg.empty()) regular_step(reg);
         for (int q = 0; q < na; ++q) set_jp(active[q]);
+        clock_push(active);
         if (time >= tnext_out - 1e-15) {
             energy(ek, ep);
             if (nout < nout_max) {

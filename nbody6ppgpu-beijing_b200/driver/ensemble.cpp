@@ -34,6 +34,10 @@ struct Ensemble : Bodies {
     std::vector<int> base, cnt, cl_of;
     double time = 0;
     std::vector<double> prop;  // learned dlog RS per row of the last regular_forces
+    // per-call buffers of the batched regular force, kept across calls (the
+    // library writes every entry that is read back)
+    std::vector<int> b_iseg, b_lst;
+    std::vector<double> b_h2, b_dtr, b_xi, b_vi, b_acc, b_jrk, b_pot, b_prop;
 
     int cluster_count(int c) const { return cnt[c]; }
 
@@ -54,9 +58,9 @@ struct Ensemble : Bodies {
                         std::vector<int> &nlist) {
         const double t_0 = wtime();
         const size_t ni = idx.size();
-        freg.assign(3 * ni, 0.0);
-        fdr.assign(3 * ni, 0.0);
-        nlist.assign(ni * (size_t)LS, 0);
+        freg.resize(3 * ni);
+        fdr.resize(3 * ni);
+        nlist.resize(ni * (size_t)LS);  // take_row writes each row's ids and a zero pad
         prop.assign(ni, 0.0);
         // runs of idx per cluster
         std::vector<int> run0, runc;
@@ -90,6 +94,7 @@ struct Ensemble : Bodies {
             if (j != self) out[1 + l1++] = base[c] + j + 1;
         }
         out[0] = l1;
+        for (int k = l1 + 1; k < std::min(LS, l1 + 9); ++k) out[k] = 0;
     }
 
     void regular_batched(const std::vector<int> &idx, const std::vector<int> &run0,
@@ -114,10 +119,22 @@ struct Ensemble : Bodies {
             for (int q = run0[r]; q < run0[r + 1]; ++q) seg_of_q[q] = r;
         while (!pend.empty()) {
             const int np = (int)pend.size();
-            std::vector<int> iseg(np);
-            std::vector<double> h2(np), dtr(np), xi(3 * (size_t)np), vi(3 * (size_t)np), acc(3 * (size_t)np),
-                jrk(3 * (size_t)np), pot(np);
-            std::vector<int> lst((size_t)np * P.lmax);
+            auto grow = [](auto &v, size_t k) {
+                if (v.size() < k) v.resize(k);
+            };
+            grow(b_iseg, np);
+            grow(b_h2, np);
+            grow(b_dtr, np);
+            grow(b_xi, 3 * (size_t)np);
+            grow(b_vi, 3 * (size_t)np);
+            grow(b_acc, 3 * (size_t)np);
+            grow(b_jrk, 3 * (size_t)np);
+            grow(b_pot, np);
+            grow(b_prop, np);
+            grow(b_lst, (size_t)np * P.lmax);
+            int *iseg = b_iseg.data(), *lst = b_lst.data();
+            double *h2 = b_h2.data(), *dtr = b_dtr.data(), *xi = b_xi.data(), *vi = b_vi.data(),
+                   *acc = b_acc.data(), *jrk = b_jrk.data(), *pot = b_pot.data(), *pr = b_prop.data();
             for (int p = 0; p < np; ++p) {
                 const int q = pend[p], i = idx[q], c = cl_of[i];
                 iseg[p] = seg_of_q[q];
@@ -126,15 +143,13 @@ struct Ensemble : Bodies {
                 pred_at(i, time, &xi[3 * (size_t)p], &vi[3 * (size_t)p]);
             }
             int nni = np, lmax = P.lmax, nnbmax = P.nnbmax, mf = P.m_flag;
-            B.regf_seg(&nni, iseg.data(), h2.data(), dtr.data(), (double(*)[3])xi.data(), (double(*)[3])vi.data(),
-                       (double(*)[3])acc.data(), (double(*)[3])jrk.data(), pot.data(), &lmax, &nnbmax, lst.data(),
-                       &mf, &nseg, seg_j0.data());
+            B.regf_seg(&nni, iseg, h2, dtr, (double(*)[3])xi, (double(*)[3])vi, (double(*)[3])acc,
+                       (double(*)[3])jrk, pot, &lmax, &nnbmax, lst, &mf, &nseg, seg_j0.data());
             st.reg_calls++;
-            std::vector<double> pr(np, 0.0);
-            if (P.mlp_mode == 2) B.proposals(&nni, pr.data());
+            if (P.mlp_mode == 2) B.proposals(&nni, pr);
             std::vector<int> again;
             for (int p = 0; p < np; ++p) {
-                prop[pend[p]] = pr[p];
+                prop[pend[p]] = P.mlp_mode == 2 ? pr[p] : 0.0;
                 const int q = pend[p], i = idx[q], c = cl_of[i];
                 st.reg_pairs += cnt[c];
                 const int *src = &lst[(size_t)p * P.lmax];
@@ -143,7 +158,7 @@ struct Ensemble : Bodies {
                     again.push_back(q);
                     continue;
                 }
-                take_row(i, c, src, &acc[3 * (size_t)p], &jrk[3 * (size_t)p], (size_t)q, freg, fdr, nlist);
+                take_row(i, c, src, acc + 3 * (size_t)p, jrk + 3 * (size_t)p, (size_t)q, freg, fdr, nlist);
             }
             if (!again.empty()) st.overflow_retries++;
             pend.swap(again);
@@ -284,14 +299,14 @@ struct Ensemble : Bodies {
         std::vector<int> active, reg, addr, nnbid;
         std::vector<double> a, jd, freg, fdr;
         std::vector<int> nl;
+        clock_reset();
+        double t_clock = 0, t_icor = 0, t_rcor = 0, t_jp = 0;
         while (st.blocks < P.max_blocks) {
-            double tmin = 1e300;
-            for (int i = 0; i < n; ++i) tmin = std::min(tmin, t0[i] + step[i]);
+            double w0 = wtime();
+            const double tmin = clock_next(active);
+            t_clock += wtime() - w0;
             if (tmin > P.tcrit + 1e-12) break;
             time = tmin;
-            active.clear();
-            for (int i = 0; i < n; ++i)
-                if (t0[i] + step[i] == tmin) active.push_back(i);
             st.blocks++;
             const int na = (int)active.size();
             addr.resize(na);
@@ -305,14 +320,17 @@ struct Ensemble : Bodies {
             B.irr_firr_vec(&t, &nna, addr.data(), (double(*)[3])a.data(), (double(*)[3])jd.data(), nnbid.data());
             st.wall_irr += wtime() - ti0;
             reg.clear();
+            w0 = wtime();
             for (int q = 0; q < na; ++q)
                 if (irr_correct(active[q], time, &a[3 * (size_t)q], &jd[3 * (size_t)q])) reg.push_back(active[q]);
+            t_icor += wtime() - w0;
             if (!reg.empty()) {
                 // corrected states of this block to the device before the
                 // j set is predicted there
                 if (batched && B.predict_send)
                     for (int q = 0; q < na; ++q) set_jp(active[q]);
                 regular_forces(reg, freg, fdr, nl);
+                w0 = wtime();
                 snapshot(reg, time);
                 for (size_t q = 0; q < reg.size(); ++q) {
                     const int i = reg[q];
@@ -325,8 +343,14 @@ struct Ensemble : Bodies {
                     set_list(i);
                 }
                 release_snapshot(reg);
+                t_rcor += wtime() - w0;
             }
+            w0 = wtime();
             for (int q = 0; q < na; ++q) set_jp(active[q]);
+            t_jp += wtime() - w0;
+            w0 = wtime();
+            clock_push(active);
+            t_clock += wtime() - w0;
             if (time >= tnext_out - 1e-15) {
                 record(tout, eout, nout, nout_max);
                 tnext_out += P.dt_out;
@@ -335,6 +359,11 @@ struct Ensemble : Bodies {
         st.t_end = time;
         st.nout = nout;
         st.wall_total = wtime() - tw;
+        if (getenv("NB6_VERBOSE"))
+            fprintf(stderr,
+                    "# nb6 ensemble: wall %.3f s = irr calls %.3f + reg calls %.3f + irr corrector %.3f"
+                    " + reg corrector %.3f + set_jp %.3f + clock %.3f + other\n",
+                    st.wall_total, st.wall_irr, st.wall_reg, t_icor, t_rcor, t_jp, t_clock);
     }
 };
 

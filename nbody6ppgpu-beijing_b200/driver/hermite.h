@@ -22,6 +22,7 @@
 #include <time.h>
 
 #include <algorithm>
+#include <map>
 #include <vector>
 
 extern "C" {
@@ -428,7 +429,11 @@ struct Bodies {
             d3r[c] = at3 * dt6;
             d2r[c] = (3.0 * at3 + bt2) * dt2;
         }
-        memcpy(row(i), nlist, sizeof(int) * LS);
+        // the ids, plus zeros over the 8-id window a SIMD list reader may
+        // touch past nnb (irr.avx.cpp:468-489)
+        const int keep = std::min(LS, nnb + 1);
+        memcpy(row(i), nlist, sizeof(int) * keep);
+        for (int k = keep; k < std::min(LS, keep + 8); ++k) row(i)[k] = 0;
         st.nb_sum += nnb;
         st.nb_absdev += fabs((double)(nnb - P.nnbopt));
         // new regular step (regcor_gpu.F:593-737)
@@ -496,8 +501,13 @@ struct Bodies {
 
     // Mode 2, after the corrector: take RS_used exp(dlog) when the count it
     // implies (nnb ~ RS^3) stays inside [NNBOPT/2, NNBMAX]; otherwise keep the
-    // Ahmad-Cohen radius the corrector just set.
+    // Ahmad-Cohen radius the corrector just set.  The proposal is clamped to
+    // a factor 2 change of RS per regular step (a guard against noisy count
+    // estimates from few neighbours; the Ahmad-Cohen rule itself moves RS by
+    // at most 25% per step).
     void learn_apply(int i, int nnb_noself, double rs_used, double dlog) {
+        const double lim = 0.69314718055994531;  // log 2
+        dlog = dlog > lim ? lim : (dlog < -lim ? -lim : dlog);
         const double r = rs_used * exp(dlog);
         const double expect = nnb_noself * exp(3.0 * dlog);
         if (nnb_noself > 0 && dlog == dlog && expect >= 0.5 * P.nnbopt && expect <= P.nnbmax) {
@@ -506,6 +516,37 @@ struct Bodies {
         } else {
             st.mlp_fallback++;
         }
+    }
+
+    // ---- block clock ------------------------------------------------------
+    // Next block: every body with the smallest t0 + step (next_tlist.f picks
+    // the same set from its level lists).  A body's t0 + step only changes
+    // when it is active, so bodies wait in buckets keyed by their exact next
+    // time; block steps make only a few distinct keys (about one per step
+    // level), so a block costs O(k) map work for its k bodies instead of a
+    // scan of all n.
+    std::map<double, std::vector<int>> clock;
+
+    void clock_reset() {
+        clock.clear();
+        for (int i = 0; i < n; ++i) clock[t0[i] + step[i]].push_back(i);
+    }
+
+    // Pops the next block into `active` (ascending body order); returns its
+    // time, or a value above tcrit when there is none left.
+    double clock_next(std::vector<int> &active) {
+        active.clear();
+        if (clock.empty()) return 1e300;
+        auto it = clock.begin();
+        const double tmin = it->first;
+        active.swap(it->second);
+        clock.erase(it);
+        std::sort(active.begin(), active.end());
+        return tmin;
+    }
+
+    void clock_push(const std::vector<int> &ids) {
+        for (int i : ids) clock[t0[i] + step[i]].push_back(i);
     }
 
     // neighbour-sphere criterion h2 of body i for gpunb_regf (m_flag: per
