@@ -65,6 +65,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-pot", action="store_true", help="skip the N^2 potential leg")
+    ap.add_argument("--no-irr", action="store_true", help="skip the irregular-force leg")
     ap.add_argument("--seed", type=int, default=20260)
     return ap.parse_args()
 
@@ -178,6 +179,59 @@ def cpu_reference_rate(m, x, v, rs, dtr, args, seconds: float, max_calls: int | 
     lib.gpunb_close()
     threads = int(os.environ.get("OMP_NUM_THREADS", "1"))
     return pairs / t_used, threads, calls, t_used
+
+
+def irregular_leg(lib, m, x, v, h2, dtr, args, nsample: int = 65536):
+    """Irregular force + jerk + nearest neighbour over lists of ~NNBOPT,
+    this library vs the reference's irr.avx.cpp, same inputs."""
+    import oracle
+    from nb6b200.abi import ForceLib
+    n = m.shape[0]
+    ns = min(nsample, n)
+    lmax = args.lmax
+    rows = np.zeros((ns, lmax), dtype=np.int32)
+    for s in range(0, ns, args.chunk):
+        e = min(ns, s + args.chunk)
+        _, _, _, lst = lib.gpunb_regf(h2[s:e], dtr[s:e], x[s:e], v[s:e], lmax, args.nnbmax, args.m_flag)
+        for r in range(e - s):
+            k = int(lst[r, 0])
+            ids = lst[r, 1:1 + max(k, 0)]
+            ids = ids[ids != s + r][: lmax - 1] + 1       # 1-based, self removed
+            rows[s + r, 0] = len(ids)
+            rows[s + r, 1:1 + len(ids)] = ids
+    zeros = np.zeros((n, 3))
+    t0 = np.zeros(n)
+    addr = np.arange(1, ns + 1, dtype=np.int32)
+    pairs = float(rows[:, 0].sum())
+    out = {"sample_i": ns, "list_pairs": int(pairs), "nnb_mean": pairs / ns}
+
+    def run(flib, name, reps):
+        flib.irr_open(n, lmax, 0)
+        flib.irr_set_jp_all(x, v, zeros, zeros, m, t0)
+        for i in range(ns):
+            flib.irr_set_list(i + 1, rows[i])
+        flib.irr_firr_vec(0.0, addr)               # uploads the staged state
+        t = time.perf_counter()
+        for _ in range(reps):
+            res = flib.irr_firr_vec(0.0, addr)
+        dt = (time.perf_counter() - t) / reps
+        flib.irr_close(0)
+        return res, dt
+
+    ours, t_ours = run(lib, "libnb6b200", 5)
+    if not oracle.ref_available("irr"):
+        oracle.build(ref=True)
+    ref, t_ref = run(ForceLib(oracle.ref_lib("irr"), "ref-irr-avx"), "irr.avx", 2)
+    a_o, a_r = ours[0], ref[0]
+    rel = np.sqrt(((a_o - a_r) ** 2).sum(1) / np.maximum((a_r ** 2).sum(1), 1e-300))
+    out.update({"pairs_per_s": pairs / t_ours, "ms_per_call": 1e3 * t_ours,
+                "cpu_reference_pairs_per_s": pairs / t_ref,
+                "cpu_reference_threads": int(os.environ.get("OMP_NUM_THREADS", "1")),
+                "acc_rel_diff_vs_reference_max": float(rel.max()),
+                "nnbid_equal_fraction": float(np.mean(ours[2] == ref[2])),
+                "timing": "wall clock around the synchronous irr_simd_firr_vec_ call (state "
+                          "already uploaded)"})
+    return out
 
 
 def run_reference(args):
@@ -373,6 +427,15 @@ def main():
             pg_ = lib.gpupot(m, x, istart=i0, ni=64)
             pot["rel_err_max_sample64"] = float(np.max(np.abs(pg_ / po - 1)))
 
+    # the irregular path on the same cluster: neighbour lists of a sample
+    # of bodies from this library's regular call, every body's state in the
+    # irregular store, one irr_simd_firr_vec_ over the sample; 60 flops per
+    # list pair (irr.avx.cpp:411).  The reference's irr.avx.cpp runs the
+    # identical calls on the host cores.
+    irr = None
+    if not args.no_irr and rank == 0:
+        irr = irregular_leg(lib, m, x, v, h2, dtr, args)
+
     # accuracy against the FP64 oracle on a sample of i (rank 0)
     err = None
     cpu = None
@@ -436,6 +499,7 @@ def main():
             "clocks": clk, "roofline": roof, "e2e": e2e, "cpu_baseline": cpu,
             "err_vs_fp64": err,
             "gpupot": pot,
+            "irregular": irr,
             "pct_fp32_peak": 100.0 * FLOPS_PER_PAIR * pairs_step / (ms * 1e-3) / 1e12 / peak_tf,
         }
         print(json.dumps(out), flush=True)

@@ -58,72 +58,29 @@ struct Sim : Bodies {
         predict_all(time);
         int nn = n;
         B.gpunb_send(&nn, m.data(), (double(*)[3])xp.data(), (double(*)[3])vp.data());
-        const int C = P.chunk;
-        std::vector<double> h2(C + 4), dtr(C + 4), xi(3 * (C + 4)), vi(3 * (C + 4)), acc(3 * (C + 4)),
-            jrk(3 * (C + 4)), pot(C + 4);
-        std::vector<int> lst((size_t)(C + 4) * P.lmax);
         const double bodym = 1.0 / n;
         freg.assign(3 * idx.size(), 0.0);
         fdr.assign(3 * idx.size(), 0.0);
         nlist.assign(idx.size() * (size_t)LS, 0);
         prop.assign(idx.size(), 0.0);
-        for (size_t c0 = 0; c0 < idx.size(); c0 += C) {
-            const int ni = (int)std::min<size_t>(C, idx.size() - c0);
-            for (;;) {
-                for (int q = 0; q < ni; ++q) {
-                    const int i = idx[c0 + q];
-                    h2[q] = h2_of(i, bodym);
-                    dtr[q] = stepr[i];
-                    for (int k = 0; k < 3; ++k) {
-                        xi[3 * q + k] = xp[3 * (size_t)i + k];
-                        vi[3 * q + k] = vp[3 * (size_t)i + k];
-                    }
-                }
-                for (int q = ni; q < ni + 4 && q < C + 4; ++q) {  // AVX library reads 4 at a time
-                    h2[q] = 0;
-                    dtr[q] = 0;
-                    for (int k = 0; k < 3; ++k) xi[3 * q + k] = vi[3 * q + k] = 0;
-                }
-                int nni = ni, lmax = P.lmax, nnbmax = P.nnbmax, mf = P.m_flag;
-                B.gpunb_regf(&nni, h2.data(), dtr.data(), (double(*)[3])xi.data(), (double(*)[3])vi.data(),
-                             (double(*)[3])acc.data(), (double(*)[3])jrk.data(), pot.data(), &lmax,
-                             &nnbmax, lst.data(), &mf);
-                st.reg_calls++;
-                st.reg_pairs += (long long)ni * n;
-                bool retry = false;
-                for (int q = 0; q < ni; ++q) {
-                    const int nb = lst[(size_t)q * P.lmax];
-                    if (nb < 0) {
-                        shrink_radius(idx[c0 + q], nb);
-                        retry = true;
-                    }
-                }
-                if (retry) {
-                    st.overflow_retries++;
-                    continue;
-                }
-                break;
+        auto fill = [&](int i, double *xi, double *vi) {
+            for (int k = 0; k < 3; ++k) {
+                xi[k] = xp[3 * (size_t)i + k];
+                vi[k] = vp[3 * (size_t)i + k];
             }
-            if (P.mlp_mode == 2) {
-                int nq = ni;
-                B.proposals(&nq, &prop[c0]);
+        };
+        auto take = [&](int q, int i, const int *row, const double *acc, const double *jrk) {
+            for (int k = 0; k < 3; ++k) {
+                freg[3 * (size_t)q + k] = acc[k];
+                fdr[3 * (size_t)q + k] = jrk[k];
             }
-            for (int q = 0; q < ni; ++q) {
-                const int i = idx[c0 + q];
-                for (int k = 0; k < 3; ++k) {
-                    freg[3 * (c0 + q) + k] = acc[3 * q + k];
-                    fdr[3 * (c0 + q) + k] = jrk[3 * q + k];
-                }
-                const int nb = lst[(size_t)q * P.lmax];
-                int *out = &nlist[(c0 + q) * (size_t)LS];
-                int l1 = 0;
-                for (int l = 1; l <= nb; ++l) {
-                    const int j = lst[(size_t)q * P.lmax + l];
-                    if (j != i) out[1 + l1++] = j + 1;
-                }
-                out[0] = l1;
-            }
-        }
+            int *out = &nlist[(size_t)q * LS];
+            int l1 = 0;
+            for (int l = 1; l <= row[0]; ++l)
+                if (row[l] != i) out[1 + l1++] = row[l] + 1;
+            out[0] = l1;
+        };
+        regf_rows(B, idx, 0, (int)idx.size(), n, bodym, fill, take, prop);
         st.wall_reg += wtime() - t_0;
     }
 

@@ -60,7 +60,9 @@ struct Ensemble : Bodies {
         const size_t ni = idx.size();
         freg.resize(3 * ni);
         fdr.resize(3 * ni);
-        nlist.resize(ni * (size_t)LS);  // take_row writes each row's ids and a zero pad
+        // grow only (a shrink then grow would zero the whole buffer again);
+        // take_row writes each row's ids and a zero pad
+        if (nlist.size() < ni * (size_t)LS) nlist.resize(ni * (size_t)LS);
         prop.assign(ni, 0.0);
         // runs of idx per cluster
         std::vector<int> run0, runc;
@@ -71,10 +73,19 @@ struct Ensemble : Bodies {
             }
         run0.push_back((int)ni);
         const int nrun = (int)runc.size();
-        if (batched && B.regf_seg && B.predict_send)
+        if (batched && B.regf_seg && B.predict_send && nrun > 1) {
             regular_batched(idx, run0, runc, nrun, freg, fdr, nlist);
-        else
+        } else if (batched && B.predict_send && nrun == 1) {
+            // one cluster: its j set predicted on the device, then the
+            // reference-ABI calls (the packed tile kernel, tuned per N_active)
+            const int c = runc[0];
+            double t = time;
+            int nseg = 1, a0 = base[c] + 1, cntc = cnt[c];
+            B.predict_send(&t, &nseg, &a0, &cntc);
+            regular_one_cluster(idx, run0[0], run0[1], c, freg, fdr, nlist, true);
+        } else {
             for (int r = 0; r < nrun; ++r) regular_one_cluster(idx, run0[r], run0[r + 1], runc[r], freg, fdr, nlist);
+        }
         st.wall_reg += wtime() - t_0;
     }
 
@@ -167,62 +178,33 @@ struct Ensemble : Bodies {
 
     // One cluster as the single-cluster driver does it: host prediction of
     // its bodies, gpunb_send_, gpunb_regf_ in chunks with overflow retry.
+    // With sent = true the cluster's j set is already on the device and only
+    // the active bodies are predicted on the host.
     void regular_one_cluster(const std::vector<int> &idx, int q0, int q1, int c, std::vector<double> &freg,
-                             std::vector<double> &fdr, std::vector<int> &nlist) {
+                             std::vector<double> &fdr, std::vector<int> &nlist, bool sent = false) {
         const int nc = cnt[c], b = base[c];
-        std::vector<double> xp(3 * (size_t)nc), vp(3 * (size_t)nc);
-        for (int j = 0; j < nc; ++j) pred_at(b + j, time, &xp[3 * (size_t)j], &vp[3 * (size_t)j]);
-        int nn = nc;
-        B.gpunb_send(&nn, &m[b], (double(*)[3])xp.data(), (double(*)[3])vp.data());
-        const int C = P.chunk;
-        std::vector<double> h2(C + 4), dtr(C + 4), xi(3 * (C + 4)), vi(3 * (C + 4)), acc(3 * (C + 4)),
-            jrk(3 * (C + 4)), pot(C + 4);
-        std::vector<int> lst((size_t)(C + 4) * P.lmax);
-        for (int c0 = q0; c0 < q1; c0 += C) {
-            const int ni = std::min(C, q1 - c0);
-            for (;;) {
-                for (int q = 0; q < ni; ++q) {
-                    const int i = idx[c0 + q];
-                    h2[q] = h2_of(i, 1.0 / nc);
-                    dtr[q] = stepr[i];
-                    for (int k = 0; k < 3; ++k) {
-                        xi[3 * q + k] = xp[3 * (size_t)(i - b) + k];
-                        vi[3 * q + k] = vp[3 * (size_t)(i - b) + k];
-                    }
-                }
-                for (int q = ni; q < ni + 4 && q < C + 4; ++q) {  // AVX library reads 4 at a time
-                    h2[q] = 0;
-                    dtr[q] = 0;
-                    for (int k = 0; k < 3; ++k) xi[3 * q + k] = vi[3 * q + k] = 0;
-                }
-                int nni = ni, lmax = P.lmax, nnbmax = P.nnbmax, mf = P.m_flag;
-                B.gpunb_regf(&nni, h2.data(), dtr.data(), (double(*)[3])xi.data(), (double(*)[3])vi.data(),
-                             (double(*)[3])acc.data(), (double(*)[3])jrk.data(), pot.data(), &lmax, &nnbmax,
-                             lst.data(), &mf);
-                st.reg_calls++;
-                st.reg_pairs += (long long)ni * nc;
-                bool retry = false;
-                for (int q = 0; q < ni; ++q) {
-                    const int nb = lst[(size_t)q * P.lmax];
-                    if (nb < 0) {
-                        shrink_radius(idx[c0 + q], nb);
-                        retry = true;
-                    }
-                }
-                if (retry) {
-                    st.overflow_retries++;
-                    continue;
-                }
-                break;
-            }
-            if (P.mlp_mode == 2) {
-                int nq = ni;
-                B.proposals(&nq, &prop[c0]);
-            }
-            for (int q = 0; q < ni; ++q)
-                take_row(idx[c0 + q], c, &lst[(size_t)q * P.lmax], &acc[3 * q], &jrk[3 * q], (size_t)(c0 + q), freg,
-                         fdr, nlist);
+        std::vector<double> xp, vp;
+        if (!sent) {
+            xp.resize(3 * (size_t)nc);
+            vp.resize(3 * (size_t)nc);
+            for (int j = 0; j < nc; ++j) pred_at(b + j, time, &xp[3 * (size_t)j], &vp[3 * (size_t)j]);
+            int nn = nc;
+            B.gpunb_send(&nn, &m[b], (double(*)[3])xp.data(), (double(*)[3])vp.data());
         }
+        auto fill = [&](int i, double *xi, double *vi) {
+            if (sent) {
+                pred_at(i, time, xi, vi);
+                return;
+            }
+            for (int k = 0; k < 3; ++k) {
+                xi[k] = xp[3 * (size_t)(i - b) + k];
+                vi[k] = vp[3 * (size_t)(i - b) + k];
+            }
+        };
+        auto take = [&](int q, int i, const int *row, const double *acc, const double *jrk) {
+            take_row(i, c, row, acc, jrk, (size_t)q, freg, fdr, nlist);
+        };
+        regf_rows(B, idx, q0, q1, nc, 1.0 / nc, fill, take, prop);
     }
 
     bool init() {
@@ -244,7 +226,8 @@ struct Ensemble : Bodies {
         std::vector<int> nl;
         regular_forces(all, freg, fdr, nl);
         for (int i = 0; i < n; ++i) {
-            memcpy(row(i), &nl[(size_t)i * LS], sizeof(int) * LS);
+            const int *src = &nl[(size_t)i * LS];
+            memcpy(row(i), src, sizeof(int) * std::min(LS, src[0] + 1));  // rows start zeroed
             set_list(i);
         }
         std::vector<int> addr(n);
@@ -359,11 +342,15 @@ struct Ensemble : Bodies {
         st.t_end = time;
         st.nout = nout;
         st.wall_total = wtime() - tw;
-        if (getenv("NB6_VERBOSE"))
+        if (getenv("NB6_VERBOSE")) {
             fprintf(stderr,
                     "# nb6 ensemble: wall %.3f s = irr calls %.3f + reg calls %.3f + irr corrector %.3f"
                     " + reg corrector %.3f + set_jp %.3f + clock %.3f + other\n",
                     st.wall_total, st.wall_irr, st.wall_reg, t_icor, t_rcor, t_jp, t_clock);
+            int rank = 0;
+            if (B.reg_profile) B.reg_profile(&rank);
+            if (B.irr_profile) B.irr_profile(&rank);
+        }
     }
 };
 

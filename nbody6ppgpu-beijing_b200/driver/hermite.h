@@ -45,6 +45,9 @@ struct nb6drive_params {
     int mlp_pad;
     float *samples;
     long long sample_cap;
+    // optional initial neighbour radii (one per body); null = RS0 sqrt(1+r^2)
+    // (fpoly0.F:55), the reference's rule with RS0 from the input file
+    const double *rs_init;
 };
 
 // Counters returned by the drivers.
@@ -81,6 +84,7 @@ typedef void (*fn_irr_set_jp)(int *, double *, double *, double *, double *, dou
 typedef void (*fn_irr_set_list)(int *, int *);
 typedef void (*fn_irr_firr)(double *, int *, int *, double (*)[3], double (*)[3], int *);
 typedef void (*fn_proposals)(int *, double *);
+typedef void (*fn_profile)(int *);
 
 struct Backend {
     void *hreg = nullptr, *hirr = nullptr, *hpot = nullptr;
@@ -98,6 +102,7 @@ struct Backend {
     fn_regf_seg regf_seg = nullptr;
     fn_pred_send predict_send = nullptr;
     fn_proposals proposals = nullptr;
+    fn_profile reg_profile = nullptr, irr_profile = nullptr;  // the libraries' timing lines
 };
 
 inline void *must_sym(void *h, const char *name) {
@@ -131,6 +136,8 @@ inline bool load_backend(Backend &b, const char *reg, const char *irr, const cha
         b.predict_send = (fn_pred_send)dlsym(b.hreg, "nb6_irr_predict_send_");
     }
     b.proposals = (fn_proposals)dlsym(b.hreg, "nb6_regf_proposals_");
+    b.reg_profile = (fn_profile)dlsym(b.hreg, "gpunb_profile_");
+    b.irr_profile = (fn_profile)dlsym(b.hirr, "irr_simd_profile_");
     return b.gpunb_open && b.gpunb_close && b.gpunb_send && b.gpunb_regf && b.gpupot &&
            b.irr_open && b.irr_close && b.irr_set_jp && b.irr_set_list && b.irr_firr_vec;
 }
@@ -202,7 +209,7 @@ struct Bodies {
     // centre (fpoly0.F:55-59); xc is the body's position relative to it.
     void init_radius(int i, const double *xc) {
         const double ri2 = xc[0] * xc[0] + xc[1] * xc[1] + xc[2] * xc[2];
-        rs[i] = P.rs0 * sqrt(1.0 + ri2);
+        rs[i] = P.rs_init ? P.rs_init[i] : P.rs0 * sqrt(1.0 + ri2);
         stepr[i] = std::min(P.smax * sqrt(1.0 + ri2), P.smax);
     }
 
@@ -521,32 +528,122 @@ struct Bodies {
     // ---- block clock ------------------------------------------------------
     // Next block: every body with the smallest t0 + step (next_tlist.f picks
     // the same set from its level lists).  A body's t0 + step only changes
-    // when it is active, so bodies wait in buckets keyed by their exact next
-    // time; block steps make only a few distinct keys (about one per step
-    // level), so a block costs O(k) map work for its k bodies instead of a
-    // scan of all n.
-    std::map<double, std::vector<int>> clock;
+    // when it is active.  Bodies wait in buckets keyed by their exact next
+    // time: one bucket per step level (every body on a level shares its next
+    // time, since t0 is a multiple of the step), with a general map for any
+    // body whose time does not match its level's bucket.  A block costs O(k)
+    // for its k bodies instead of a scan of all n.
+    static constexpr int NLEV = 64;
+    std::vector<int> lev_ids[NLEV];
+    double lev_t[NLEV];
+    std::map<double, std::vector<int>> clock_other;
+
+    static int level_of(double step) {
+        int e = 0;
+        const double mant = frexp(step, &e);  // step = mant 2^e
+        if (mant != 0.5) return -1;
+        const int L = 1 - e;                  // step = 2^-L
+        return (L >= 0 && L < NLEV) ? L : -1;
+    }
+
+    void clock_add(int i) {
+        const double t = t0[i] + step[i];
+        const int L = level_of(step[i]);
+        if (L >= 0 && (lev_ids[L].empty() || lev_t[L] == t)) {
+            lev_t[L] = t;
+            lev_ids[L].push_back(i);
+        } else {
+            clock_other[t].push_back(i);
+        }
+    }
 
     void clock_reset() {
-        clock.clear();
-        for (int i = 0; i < n; ++i) clock[t0[i] + step[i]].push_back(i);
+        for (auto &v : lev_ids) v.clear();
+        clock_other.clear();
+        for (int i = 0; i < n; ++i) clock_add(i);
     }
 
     // Pops the next block into `active` (ascending body order); returns its
     // time, or a value above tcrit when there is none left.
     double clock_next(std::vector<int> &active) {
         active.clear();
-        if (clock.empty()) return 1e300;
-        auto it = clock.begin();
-        const double tmin = it->first;
-        active.swap(it->second);
-        clock.erase(it);
+        double tmin = 1e300;
+        for (int L = 0; L < NLEV; ++L)
+            if (!lev_ids[L].empty()) tmin = std::min(tmin, lev_t[L]);
+        if (!clock_other.empty()) tmin = std::min(tmin, clock_other.begin()->first);
+        if (tmin == 1e300) return tmin;
+        for (int L = 0; L < NLEV; ++L)
+            if (!lev_ids[L].empty() && lev_t[L] == tmin) {
+                active.insert(active.end(), lev_ids[L].begin(), lev_ids[L].end());
+                lev_ids[L].clear();
+            }
+        if (!clock_other.empty() && clock_other.begin()->first == tmin) {
+            auto it = clock_other.begin();
+            active.insert(active.end(), it->second.begin(), it->second.end());
+            clock_other.erase(it);
+        }
         std::sort(active.begin(), active.end());
         return tmin;
     }
 
     void clock_push(const std::vector<int> &ids) {
-        for (int i : ids) clock[t0[i] + step[i]].push_back(i);
+        for (int i : ids) clock_add(i);
+    }
+
+    // Regular force of bodies idx[q0..q1) through gpunb_regf_ in calls of at
+    // most P.chunk (util_gpu.F:33-60) against the nj bodies last sent.  A
+    // row that overflows gets the radius shrink of util_gpu.F:69-100 and is
+    // evaluated again; only those rows go into the next call (the others'
+    // results do not depend on which rows share a call).  fill(i, xi, vi)
+    // gives body i at the block time; take(q, i, row, acc, jrk) receives a
+    // finished row (row = [nnb, ids]); prop[q] gets the learned proposal in
+    // mlp_mode 2.
+    template <class Fill, class Take>
+    void regf_rows(const Backend &B, const std::vector<int> &idx, int q0, int q1, int nj, double bodym,
+                   Fill fill, Take take, std::vector<double> &prop) {
+        const int C = P.chunk;
+        std::vector<double> h2(C + 4), dtr(C + 4), xi(3 * (C + 4)), vi(3 * (C + 4)), acc(3 * (C + 4)),
+            jrk(3 * (C + 4)), pot(C + 4), pr(C + 4);
+        std::vector<int> lst((size_t)(C + 4) * P.lmax), rows, again;
+        for (int c0 = q0; c0 < q1; c0 += C) {
+            rows.clear();
+            for (int q = c0; q < std::min(q1, c0 + C); ++q) rows.push_back(q);
+            while (!rows.empty()) {
+                const int ni = (int)rows.size();
+                for (int p = 0; p < ni; ++p) {
+                    const int i = idx[rows[p]];
+                    h2[p] = h2_of(i, bodym);
+                    dtr[p] = stepr[i];
+                    fill(i, &xi[3 * (size_t)p], &vi[3 * (size_t)p]);
+                }
+                for (int p = ni; p < ni + 4; ++p) {  // a SIMD library reads 4 i at a time
+                    h2[p] = 0;
+                    dtr[p] = 0;
+                    for (int k = 0; k < 3; ++k) xi[3 * p + k] = vi[3 * p + k] = 0;
+                }
+                int nni = ni, lmax = P.lmax, nnbmax = P.nnbmax, mf = P.m_flag;
+                B.gpunb_regf(&nni, h2.data(), dtr.data(), (double(*)[3])xi.data(), (double(*)[3])vi.data(),
+                             (double(*)[3])acc.data(), (double(*)[3])jrk.data(), pot.data(), &lmax, &nnbmax,
+                             lst.data(), &mf);
+                st.reg_calls++;
+                st.reg_pairs += (long long)ni * nj;
+                if (P.mlp_mode == 2) B.proposals(&nni, pr.data());
+                again.clear();
+                for (int p = 0; p < ni; ++p) {
+                    const int q = rows[p], i = idx[q];
+                    const int *row = &lst[(size_t)p * P.lmax];
+                    if (row[0] < 0) {
+                        shrink_radius(i, row[0]);
+                        again.push_back(q);
+                        continue;
+                    }
+                    if (P.mlp_mode == 2) prop[q] = pr[p];
+                    take(q, i, row, &acc[3 * (size_t)p], &jrk[3 * (size_t)p]);
+                }
+                if (!again.empty()) st.overflow_retries++;
+                rows.swap(again);
+            }
+        }
     }
 
     // neighbour-sphere criterion h2 of body i for gpunb_regf (m_flag: per

@@ -30,7 +30,8 @@ class Params(C.Structure):
                 ("rs0", C.c_double), ("nnbopt", C.c_int), ("nnbmax", C.c_int),
                 ("lmax", C.c_int), ("m_flag", C.c_int), ("chunk", C.c_int),
                 ("max_blocks", C.c_longlong), ("mlp_mode", C.c_int), ("mlp_pad", C.c_int),
-                ("samples", C.POINTER(C.c_float)), ("sample_cap", C.c_longlong)]
+                ("samples", C.POINTER(C.c_float)), ("sample_cap", C.c_longlong),
+                ("rs_init", C.POINTER(C.c_double))]
 
 
 class Stats(C.Structure):
@@ -97,12 +98,23 @@ def _mlp_fields(p: "Params", mlp_mode: int, sample_cap: int):
     return buf
 
 
+def _rs_field(p: "Params", rs_init, n: int):
+    if rs_init is None:
+        p.rs_init = C.POINTER(C.c_double)()
+        return None
+    arr = np.ascontiguousarray(rs_init, dtype=np.float64)
+    assert arr.shape == (n,)
+    p.rs_init = arr.ctypes.data_as(C.POINTER(C.c_double))
+    return arr
+
+
 def run(backend: dict, mass, pos, vel, *, tcrit=1.0, eta_i=0.02, eta_r=0.03, smax=0.125,
         dtmin=2.0 ** -24, dt_out=0.125, rs0=0.3, nnbopt=50, nnbmax=400, lmax=512, m_flag=0,
-        chunk=1024, max_blocks=10_000_000, mlp_mode=0, sample_cap=0) -> RunResult:
+        chunk=1024, max_blocks=10_000_000, mlp_mode=0, sample_cap=0, rs_init=None) -> RunResult:
     """mlp_mode: 0 Ahmad-Cohen radii; 1 Ahmad-Cohen and log up to sample_cap
     (features, target) samples into RunResult.samples; 2 the library's learned
-    proposals (nb6b200.mlp.enable(True) first), Ahmad-Cohen as fallback."""
+    proposals (nb6b200.mlp.enable(True) first), Ahmad-Cohen as fallback.
+    rs_init: initial neighbour radii per body (default RS0 sqrt(1 + r^2))."""
     mass = np.ascontiguousarray(mass, dtype=np.float64)
     n = mass.shape[0]
     x = np.ascontiguousarray(pos, dtype=np.float64).reshape(n, 3).copy()
@@ -110,6 +122,7 @@ def run(backend: dict, mass, pos, vel, *, tcrit=1.0, eta_i=0.02, eta_r=0.03, sma
     p = Params(eta_i, eta_r, smax, dtmin, tcrit, dt_out, rs0, nnbopt, nnbmax, lmax, m_flag,
                chunk, max_blocks)
     buf = _mlp_fields(p, mlp_mode, sample_cap)
+    rs_arr = _rs_field(p, rs_init, n)
     nout_max = int(tcrit / dt_out) + 4
     eout = np.zeros((nout_max, 4))
     st = Stats()
@@ -145,11 +158,13 @@ class EnsembleResult:
 def run_ensemble(backend: dict, clusters, *, batched=True, tcrit=1.0, eta_i=0.02, eta_r=0.03,
                  smax=0.125, dtmin=2.0 ** -24, dt_out=0.125, rs0=0.3, nnbopt=50, nnbmax=400,
                  lmax=512, m_flag=0, chunk=1024, max_blocks=100_000_000, mlp_mode=0,
-                 sample_cap=0) -> EnsembleResult:
+                 sample_cap=0, rs_init=None, rs_from_clusters=False) -> EnsembleResult:
     """clusters: sequence of (mass, pos, vel) (or objects with .mass/.pos/.vel),
     each in its own Henon units.  batched=False issues the regular force per
     cluster (what running each alone does); the result is then identical to
-    ``run`` on each cluster with a deterministic backend."""
+    ``run`` on each cluster with a deterministic backend.  rs_init (all
+    bodies) or rs_from_clusters=True (each cluster's .rs) sets the initial
+    neighbour radii."""
     parts = [(c.mass, c.pos, c.vel) if hasattr(c, "mass") else c for c in clusters]
     counts = np.array([len(p[0]) for p in parts], dtype=np.int32)
     ncl = len(parts)
@@ -159,6 +174,9 @@ def run_ensemble(backend: dict, clusters, *, batched=True, tcrit=1.0, eta_i=0.02
     p = Params(eta_i, eta_r, smax, dtmin, tcrit, dt_out, rs0, nnbopt, nnbmax, lmax, m_flag,
                chunk, max_blocks)
     buf = _mlp_fields(p, mlp_mode, sample_cap)
+    if rs_init is None and all(hasattr(c, "rs") for c in clusters) and rs_from_clusters:
+        rs_init = np.concatenate([c.rs for c in clusters])
+    rs_arr = _rs_field(p, rs_init, len(mass))
     nout_max = int(tcrit / dt_out) + 4
     tout = np.zeros(nout_max)
     eout = np.zeros((nout_max, ncl, 3))

@@ -1,6 +1,6 @@
 """Batched ensemble vs each cluster alone (the plain method), same GPU.
 
-    python -m nb6b200.ensemble_bench --clusters 256 --tcrit 1.0 [--alone-sample 32]
+    python -m nb6b200.ensemble_bench --clusters 256 --tcrit 1.0 [--alone-sample 32] [--mlp]
 
 (run from ``nbody6ppgpu-beijing_b200/``).  The ensemble is the batched
 driver (one irregular and one segmented regular call per block for all
@@ -33,15 +33,28 @@ def main(argv=None):
     ap.add_argument("--clusters", type=int, default=256)
     ap.add_argument("--tcrit", type=float, default=1.0)
     ap.add_argument("--alone-sample", type=int, default=0, help="0 = all clusters alone")
-    ap.add_argument("--mlp", action="store_true", help="use the loaded learned-radius model")
+    ap.add_argument("--mlp", action="store_true",
+                    help="learned radii: train on samples from plain runs of 16 other clusters "
+                         "of the same distribution, then run the ensemble with the proposals")
     a = ap.parse_args(argv)
     ours = drive.backend_paths("nb6b200")
     cls = make_clusters(a.clusters)
     sizes = np.array([c.n for c in cls])
+    train = None
+    if a.mlp:
+        from . import learn, mlp
+        t = time.perf_counter()
+        samples = learn.collect(make_clusters(16, seed=77), a.tcrit)
+        hist = learn.fit(samples, epochs=15)
+        train = {"samples": int(len(samples)), "loss": [float(hist[0]), float(hist[-1])],
+                 "wall_s": time.perf_counter() - t}
+        mlp.enable(True)
     t = time.perf_counter()
     ens = drive.run_ensemble(ours, cls, batched=True, tcrit=a.tcrit, dt_out=min(a.tcrit, 0.25),
                              mlp_mode=2 if a.mlp else 0)
     wall_ens = time.perf_counter() - t
+    if a.mlp:
+        mlp.enable(False)
     order = np.argsort(sizes)
     pick = order if a.alone_sample <= 0 else order[np.linspace(0, len(cls) - 1, a.alone_sample).astype(int)]
     de_alone, wall_alone, reg_alone, irr_alone = {}, 0.0, 0.0, 0.0
@@ -69,10 +82,15 @@ def main(argv=None):
         "dE_ensemble_median": float(np.median(de_e)),
         "dE_ensemble_max": float(np.max(de_e)),
         "dE_ratio_ensemble_over_alone_median": float(np.median(ratio)),
+        "dE_ratio_p90": float(np.percentile(ratio, 90)),
         "dE_ratio_max": float(np.max(ratio)),
+        "dE_alone_at_max_ratio": float(list(de_alone.values())[int(np.argmax(ratio))]),
         "ensemble_stats": {k: ens.stats[k] for k in ("blocks", "irr_steps", "reg_steps", "reg_calls",
                                                       "overflow_retries", "wall_reg", "wall_irr")},
         "alone_force_call_wall_s": {"reg": reg_alone * scale, "irr": irr_alone * scale},
+        "learned_radius": None if train is None else {
+            "training": train, "used": ens.stats["mlp_used"], "fallback": ens.stats["mlp_fallback"],
+            "nnb_absdev_mean": ens.stats["nb_absdev"] / max(ens.stats["reg_steps"], 1)},
     }
     print(json.dumps(out))
 

@@ -2,7 +2,7 @@
 Ahmad-Cohen runs, train the model on the GPU, and compare a run that uses
 its proposals with a plain run.
 
-    python -m nb6b200.learn --n-train 131072 --n-eval 131072 --tcrit 0.25
+    python -m nb6b200.learn --n-train 131072 --n-eval 1048576 --tcrit 0.0078125
 
 (run from ``nbody6ppgpu-beijing_b200/``; prints one JSON line).  A sample is
 (features of a particle at one regular step, log(RS* / RS)) where RS* is the
@@ -19,15 +19,16 @@ import numpy as np
 from . import drive, ics, mlp
 
 
-def collect(clusters, tcrit, sample_cap=2_000_000, **kw) -> np.ndarray:
-    """Samples [k, 6] from plain runs (libnb6b200 backend) of the clusters."""
-    out = []
+def collect(clusters, tcrit, sample_cap=2_000_000, rs_ics=False, **kw) -> np.ndarray:
+    """Samples [k, 6] from plain (Ahmad-Cohen) runs of the clusters on
+    libnb6b200, one ensemble run for all of them.  rs_ics: start from the
+    clusters' own radii (distance to the NNBOPT-th neighbour) instead of the
+    RS0 rule."""
     ours = drive.backend_paths("nb6b200")
-    for cl in clusters:
-        r = drive.run(ours, cl.mass, cl.pos, cl.vel, tcrit=tcrit, mlp_mode=1,
-                      sample_cap=sample_cap, dt_out=max(tcrit, 0.125), **kw)
-        out.append(r.samples)
-    return np.concatenate(out)
+    r = drive.run_ensemble(ours, clusters, batched=True, tcrit=tcrit, mlp_mode=1,
+                           sample_cap=sample_cap, dt_out=min(tcrit, 0.125),
+                           rs_from_clusters=rs_ics, **kw)
+    return r.samples
 
 
 def fit(samples, epochs=15, batch=1024, lr=2e-3, seed=0) -> np.ndarray:
@@ -38,29 +39,44 @@ def fit(samples, epochs=15, batch=1024, lr=2e-3, seed=0) -> np.ndarray:
     return mlp.train(x, y, epochs=epochs, batch=batch, lr=lr, seed=seed)
 
 
-def compare(cl, tcrit, **kw) -> dict:
-    """Plain and learned runs of one cluster with the current model."""
+def _summary(stats, de, tcrit):
+    steps = max(stats["reg_steps"], 1)
+    return {"nnb_mean": stats["nb_sum"] / steps, "nnb_absdev_mean": stats["nb_absdev"] / steps,
+            "overflow_retries": stats["overflow_retries"], "reg_calls": stats["reg_calls"],
+            "reg_steps": stats["reg_steps"], "irr_steps": stats["irr_steps"],
+            "reg_irr_ratio": stats["reg_steps"] / max(stats["irr_steps"], 1),
+            "wall_s": stats["wall_total"], "wall_per_nbody_time": stats["wall_total"] / tcrit,
+            "dE": float(de), "mlp_used": stats["mlp_used"], "mlp_fallback": stats["mlp_fallback"]}
+
+
+def compare(cl, tcrit, plain_method=True, rs_ics=False, **kw) -> dict:
+    """One cluster three ways, with the current model for the learned arm:
+    the plain GPU method (single-cluster driver: host prediction, gpunb_send_
+    per regular block, Ahmad-Cohen radii); the batched driver (j set
+    predicted on the device) with Ahmad-Cohen radii; and the batched driver
+    with the learned radii."""
     ours = drive.backend_paths("nb6b200")
-    plain = drive.run(ours, cl.mass, cl.pos, cl.vel, tcrit=tcrit, mlp_mode=0,
-                      dt_out=max(tcrit, 0.125), **kw)
+    dt_out = min(tcrit, 0.125)          # at least one energy after the start
+    rs = cl.rs if rs_ics else None
+    out = {}
+    if plain_method:
+        r = drive.run(ours, cl.mass, cl.pos, cl.vel, tcrit=tcrit, mlp_mode=0, dt_out=dt_out,
+                      rs_init=rs, **kw)
+        out["plain"] = _summary(r.stats, r.de_max, tcrit)
+    r = drive.run_ensemble(ours, [cl], batched=True, tcrit=tcrit, mlp_mode=0, dt_out=dt_out,
+                           rs_init=rs, **kw)
+    out["batched"] = _summary(r.stats, r.de_max[0], tcrit)
     mlp.enable(True)
     try:
-        learned = drive.run(ours, cl.mass, cl.pos, cl.vel, tcrit=tcrit, mlp_mode=2,
-                            dt_out=max(tcrit, 0.125), **kw)
+        r = drive.run_ensemble(ours, [cl], batched=True, tcrit=tcrit, mlp_mode=2, dt_out=dt_out,
+                               rs_init=rs, **kw)
     finally:
         mlp.enable(False)
-
-    def summary(r):
-        s = r.stats
-        steps = max(s["reg_steps"], 1)
-        return {"nnb_mean": s["nb_sum"] / steps, "nnb_absdev_mean": s["nb_absdev"] / steps,
-                "overflow_retries": s["overflow_retries"], "reg_calls": s["reg_calls"],
-                "reg_steps": s["reg_steps"], "irr_steps": s["irr_steps"],
-                "reg_irr_ratio": s["reg_steps"] / max(s["irr_steps"], 1),
-                "wall_s": s["wall_total"], "wall_per_nbody_time": s["wall_total"] / tcrit,
-                "dE": r.de_max, "mlp_used": s["mlp_used"], "mlp_fallback": s["mlp_fallback"]}
-
-    return {"plain": summary(plain), "learned": summary(learned)}
+    out["learned"] = _summary(r.stats, r.de_max[0], tcrit)
+    base = out.get("plain", out["batched"])
+    out["speedup_learned_vs_" + ("plain" if plain_method else "batched")] = \
+        base["wall_s"] / out["learned"]["wall_s"]
+    return out
 
 
 def main(argv=None):
@@ -68,19 +84,30 @@ def main(argv=None):
     ap.add_argument("--n-train", type=int, default=16384)
     ap.add_argument("--n-eval", type=int, default=16384)
     ap.add_argument("--train-clusters", type=int, default=2)
-    ap.add_argument("--tcrit", type=float, default=0.25)
+    ap.add_argument("--tcrit", type=float, default=0.25, help="length of the evaluation runs")
+    ap.add_argument("--train-tcrit", type=float, default=None, help="length of the sampling runs")
     ap.add_argument("--epochs", type=int, default=15)
     ap.add_argument("--model", choices=["plummer", "king"], default="king")
+    ap.add_argument("--no-plain", action="store_true", help="skip the single-cluster plain arm")
+    ap.add_argument("--save", default=None, help="write the trained model (.npy)")
+    ap.add_argument("--rs-ics", action="store_true",
+                    help="initial radii from the clusters (NNBOPT-th neighbour) instead of RS0")
     a = ap.parse_args(argv)
-    make = (lambda n, s: ics.king(n, w0=6.0, seed=s, imf=True)) if a.model == "king" else \
-        (lambda n, s: ics.plummer(n, seed=s, imf=True))
+    if a.model == "king":
+        def make(n, s):
+            return ics.king(n, w0=6.0, seed=s, imf=True, binary_fraction=0.05)
+    else:
+        def make(n, s):
+            return ics.plummer(n, seed=s, imf=True)
     train_cls = [make(a.n_train, 100 + k) for k in range(a.train_clusters)]
-    samples = collect(train_cls, a.tcrit)
+    samples = collect(train_cls, a.train_tcrit or a.tcrit, rs_ics=a.rs_ics)
     hist = fit(samples, epochs=a.epochs)
-    res = compare(make(a.n_eval, 999), a.tcrit)
+    if a.save:
+        np.save(a.save, mlp.get_model())
+    res = compare(make(a.n_eval, 999), a.tcrit, plain_method=not a.no_plain, rs_ics=a.rs_ics)
     res.update({"n_train": a.n_train, "n_eval": a.n_eval, "samples": int(len(samples)),
                 "loss_first_epoch": float(hist[0]), "loss_last_epoch": float(hist[-1]),
-                "tcrit": a.tcrit, "model": a.model})
+                "tcrit": a.tcrit, "model": a.model, "rs_ics": a.rs_ics})
     print(json.dumps(res))
 
 

@@ -2,8 +2,9 @@
 
 Samples are logged from plain runs of two Plummer/Kroupa clusters, the model
 is trained on the GPU by the library's own kernels, and a third cluster
-(unseen seed) is integrated twice to the same time: with the plain rule and
-with the learned proposals (Ahmad-Cohen as fallback).  The learned run must
+(unseen seed) is integrated by the same driver twice to the same time: with
+the Ahmad-Cohen rule and with the learned proposals (Ahmad-Cohen as
+fallback).  The learned run must
 keep the neighbour counts closer to NNBOPT, with overflow re-evaluations
 still rare and an energy error of the same order."""
 import numpy as np
@@ -20,7 +21,7 @@ def test_learned_radius_keeps_counts_closer_to_nnbopt(nb6):
     hist = learn.fit(samples, epochs=15)
     assert hist[-1] < 0.8 * hist[0], hist
     res = learn.compare(ics.plummer(4096, seed=399, imf=True), tcrit=0.25)
-    p, q = res["plain"], res["learned"]
+    p, q = res["batched"], res["learned"]
     print(f"\nsamples {len(samples)}, loss {hist[0]:.3f} -> {hist[-1]:.3f}\nplain   {p}\nlearned {q}")
     assert q["mlp_used"] > 0.5 * (q["mlp_used"] + q["mlp_fallback"])
     assert q["nnb_absdev_mean"] < p["nnb_absdev_mean"]
