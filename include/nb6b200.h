@@ -139,6 +139,13 @@ void nb6_regf_autotune_(int *flag);
  * the environment for off), 0 = off (plain launches), other values leave it
  * unchanged.  counts[3] receives {graphs built, graph launches, on}. */
 void nb6_regf_graphs_(int *flag, long long *counts);
+/* After each send the j set is also kept in Morton (Z-curve) order with a
+ * bounding box per 128-body tile; the packed kernel skips the neighbour
+ * candidate test for tiles out of reach of a whole warp.  Neighbour ids stay
+ * the caller's.  Applied to j sets of at least NB6_JSORT_MIN bodies
+ * (default 32768).  flag 1 = on (default; NB6_JSORT=0 in the environment for
+ * off), 0 = off, other values query.  Returns the setting. */
+int nb6_regf_jsort_(int *flag);
 
 /* Segmented regular force for ensembles of independent clusters sent
  * together (one persistent launch for all of them).  Segment c is the j

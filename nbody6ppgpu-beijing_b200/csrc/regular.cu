@@ -26,6 +26,8 @@
 #include "nb6_common.cuh"
 #include "mlp.cuh"
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include <algorithm>
 #include <climits>
 #include <map>
@@ -82,6 +84,15 @@ struct RegArgs {
     int *__restrict__ nbbuf;     // [ni][lcap]
     int lcap;
     int *status;
+    // spatially ordered j set: slot k holds body perm[k]; tile t's bounding
+    // box is tbox[2t] = (centre xyz, max |v|), tbox[2t+1] = (half extent xyz,
+    // max m).  Null: j slots are the caller's order, no boxes.
+    const int *__restrict__ perm = nullptr;
+    const float4 *__restrict__ tbox = nullptr;
+    // packed kernel: thread slot s takes i-particle iperm[s] (the active set
+    // in the same spatial order, so a warp covers a compact region); null =
+    // slot order.  Every index into i data and outputs stays the caller's.
+    const int *__restrict__ iperm = nullptr;
 };
 
 struct IPart {
@@ -152,7 +163,8 @@ NB6_DEV bool reg_pair(const IPart &ip, const float4 &a, const float4 &b, const f
 // Operation order matches the FP64 rule of regint.f:41-65 with the strict
 // "<" of gpunb.velocity.cu:188,236; no FMA contraction.
 template <bool MFLAG>
-NB6_DEV void reg_exact(const RegArgs &a, int i, int j, Sums &s, int joff = 0) {
+NB6_DEV void reg_exact(const RegArgs &a, int i, int jslot, Sums &s, int joff = 0) {
+    const int j = a.perm ? a.perm[jslot] : jslot;  // the caller's index of the body in this slot
     const double xi0 = a.ix[3 * i], xi1 = a.ix[3 * i + 1], xi2 = a.ix[3 * i + 2];
     const double vi0 = a.iv[3 * i], vi1 = a.iv[3 * i + 1], vi2 = a.iv[3 * i + 2];
     const double h2 = a.ih2[i], dt = a.idtr[i];
@@ -414,6 +426,57 @@ NB6_DEV unsigned pair_x2(const IP2 &ip, float2 xh, float2 yh, float2 zh, float2 
     return (c0 ? 1u : 0u) | (c1 ? 2u : 0u);
 }
 
+// pair_x2 for a pair known not to be a neighbour candidate: the same
+// operations in the same order minus the candidate test, so its results are
+// bit-identical to pair_x2's for such a pair.
+template <bool MFLAG>
+NB6_DEV void pair_x2_far(const IP2 &ip, float2 xh, float2 yh, float2 zh, float2 m, float2 xl, float2 yl,
+                         float2 zl, float2 vx, float2 vy, float2 vz, S2 &s) {
+    const float2 dx = __fadd2_rn(__fadd2_rn(xh, ip.nxh), __fadd2_rn(xl, ip.nxl));
+    const float2 dy = __fadd2_rn(__fadd2_rn(yh, ip.nyh), __fadd2_rn(yl, ip.nyl));
+    const float2 dz = __fadd2_rn(__fadd2_rn(zh, ip.nzh), __fadd2_rn(zl, ip.nzl));
+    const float2 dvx = __fadd2_rn(vx, ip.nvx);
+    const float2 dvy = __fadd2_rn(vy, ip.nvy);
+    const float2 dvz = __fadd2_rn(vz, ip.nvz);
+    const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+    const float2 rv = __ffma2_rn(dz, dvz, __ffma2_rn(dy, dvy, __fmul2_rn(dx, dvx)));
+    float2 y0;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y0.x) : "f"(r2.x));
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y0.y) : "f"(r2.y));
+    const float2 ra = __fmul2_rn(r2, y0);
+    const float2 nb = __ffma2_rn(ra, y0, dup2(-3.0f));
+    const float2 ny = __fmul2_rn(y0, nb);
+    const float2 y2 = __fmul2_rn(ny, ny);
+    const float2 nmy = __fmul2_rn(m, ny);
+    const float2 nmy3 = __fmul2_rn(nmy, y2);
+    const float2 al = __fmul2_rn(__fmul2_rn(y2, dup2(-0.75f)), rv);
+    s.po = __fadd2_rn(s.po, nmy);
+    s.ax = __ffma2_rn(nmy3, dx, s.ax);
+    s.ay = __ffma2_rn(nmy3, dy, s.ay);
+    s.az = __ffma2_rn(nmy3, dz, s.az);
+    s.jx = __ffma2_rn(nmy3, __ffma2_rn(al, dx, dvx), s.jx);
+    s.jy = __ffma2_rn(nmy3, __ffma2_rn(al, dy, dvy), s.jy);
+    s.jz = __ffma2_rn(nmy3, __ffma2_rn(al, dz, dvz), s.jz);
+}
+
+// True when no body of tile box (bc, bh) can be a neighbour candidate of the
+// i-particle: the box is farther than sqrt(crit) + dtr (|v_i| + max |v_j|),
+// the farthest reach of min(r, |r + dtr dv|) < sqrt(crit) (triangle
+// inequality), with margins for the FP32 rounding of positions, box and test.
+template <bool MFLAG>
+NB6_DEV bool tile_far(const IP2 &ip, float vabs, float4 bc, float4 bh) {
+    const float xi = -ip.nxh.x, yi = -ip.nyh.x, zi = -ip.nzh.x;
+    const float ex = fmaxf(fabsf(xi - bc.x) - bh.x, 0.f);
+    const float ey = fmaxf(fabsf(yi - bc.y) - bh.y, 0.f);
+    const float ez = fmaxf(fabsf(zi - bc.z) - bh.z, 0.f);
+    const float d2 = ex * ex + ey * ey + ez * ez;
+    const float crit = MFLAG ? bh.w * ip.h2c.x : ip.h2c.x;
+    const float mag = fmaxf(fmaxf(fabsf(xi), fabsf(yi)), fabsf(zi)) +
+                      fmaxf(fmaxf(fabsf(bc.x) + bh.x, fabsf(bc.y) + bh.y), fabsf(bc.z) + bh.z);
+    const float reach = (sqrtf(crit) + ip.dt.x * (vabs + bc.w)) * 1.001f + mag * 1.0e-6f;
+    return d2 > reach * reach;
+}
+
 // Same pair math with the coordinate differences formed in FP64 and rounded
 // once to FP32 (DADD + F2F on the FP64 pipe instead of three FP32 adds per
 // component on the FMA pipe).  xi/yi/zi are the i position in FP64.
@@ -504,18 +567,26 @@ __global__ void __launch_bounds__(NT, X2_MINB / NI) regf_x2_kernel(const RegArgs
 
     const int tid = threadIdx.x, lane = tid & 31;
     const int slice = blockIdx.y;
-    const int t_begin = (int)(((long long)slice * a.ntile) / a.nslices);
-    const int t_end = (int)(((long long)(slice + 1) * a.ntile) / a.nslices);
-    const int nt = t_end - t_begin;
+    // Tiles of this slice: a contiguous range, or with a spatially ordered j
+    // set (a.tbox) every nslices-th tile, so that the tiles near a compact
+    // group of i-particles -- the ones with neighbour candidates -- are
+    // shared out among the slices instead of falling to one CTA.
+    const bool strided = a.tbox != nullptr;
+    const int t_begin = strided ? slice : (int)(((long long)slice * a.ntile) / a.nslices);
+    const int t_step = strided ? a.nslices : 1;
+    const int nt = strided ? (slice < a.ntile ? (a.ntile - slice + a.nslices - 1) / a.nslices : 0)
+                           : (int)(((long long)(slice + 1) * a.ntile) / a.nslices) - t_begin;
 
     IP2 ip[NI];
     S2 s[NI];
     Sums fx[NI];
     int ii[NI];
+    float vabs[NI];                 // |v_i|, for the tile reach test
     double xd[NI], yd[NI], zd[NI];  // FP64 i position (F64DX layout)
 #pragma unroll
     for (int k = 0; k < NI; ++k) {
-        const int i = blockIdx.x * (NT * NI) + k * NT + tid;
+        const int slot = blockIdx.x * (NT * NI) + k * NT + tid;
+        const int i = (a.iperm && slot < a.ni) ? a.iperm[slot] : slot;
         ii[k] = i;
         zero2(s[k]);
         zero(fx[k]);
@@ -550,6 +621,7 @@ __global__ void __launch_bounds__(NT, X2_MINB / NI) regf_x2_kernel(const RegArgs
         ip[k].nvz = dup2(-p.vz);
         ip[k].h2c = dup2(p.h2c);
         ip[k].dt = dup2(p.dt);
+        vabs[k] = sqrtf(p.vx * p.vx + p.vy * p.vy + p.vz * p.vz);
     }
 
     if (tid == 0) {
@@ -564,7 +636,7 @@ __global__ void __launch_bounds__(NT, X2_MINB / NI) regf_x2_kernel(const RegArgs
     int issued = 0;
     if (tid == 0) {
         for (int st = 0; st < NSTAGE && st < nt; ++st)
-            issue_tile_soa<F64DX>(a, sj[st], &bar[st], t_begin + st);
+            issue_tile_soa<F64DX>(a, sj[st], &bar[st], t_begin + st * t_step);
         issued = min(nt, NSTAGE);
     }
 
@@ -580,9 +652,56 @@ __global__ void __launch_bounds__(NT, X2_MINB / NI) regf_x2_kernel(const RegArgs
             return;
         }
         const float(*S)[JT] = sj[st];
-        const int jt0 = (t_begin + t) * JT;
+        const int tile = t_begin + t * t_step;
+        const int jt0 = tile * JT;
+        // whole warp out of reach of this tile: no candidates, short loop
+        bool far = false;
+        if constexpr (!F64DX && NI == 1) {  // (two i per thread: no registers left for it)
+            if (a.tbox) {
+                const float4 bc = __ldg(&a.tbox[2 * tile]);
+                const float4 bh = __ldg(&a.tbox[2 * tile + 1]);
+                bool f = true;
+#pragma unroll
+                for (int k = 0; k < NI; ++k) f = f && (ii[k] >= a.ni || tile_far<MFLAG>(ip[k], vabs[k], bc, bh));
+                far = __all_sync(0xffffffffu, f);
+            }
+        }
+        if constexpr (!F64DX && NI == 1) {
+          if (far) {
 #pragma unroll 1
-        for (int g = 0; g < JT / 32; ++g) {
+            for (int g = 0; g < JT / 32; ++g) {
+#pragma unroll
+                for (int u = 0; u < 32; u += 4) {
+                    const int q = g * 32 + u;
+                    const float4 XH = *reinterpret_cast<const float4 *>(&S[0][q]);
+                    const float4 YH = *reinterpret_cast<const float4 *>(&S[1][q]);
+                    const float4 ZH = *reinterpret_cast<const float4 *>(&S[2][q]);
+                    const float4 MM = *reinterpret_cast<const float4 *>(&S[3][q]);
+                    const float4 XL = *reinterpret_cast<const float4 *>(&S[4][q]);
+                    const float4 YL = *reinterpret_cast<const float4 *>(&S[5][q]);
+                    const float4 ZL = *reinterpret_cast<const float4 *>(&S[6][q]);
+                    const float4 VX = *reinterpret_cast<const float4 *>(&S[7][q]);
+                    const float4 VY = *reinterpret_cast<const float4 *>(&S[8][q]);
+                    const float4 VZ = *reinterpret_cast<const float4 *>(&S[9][q]);
+#pragma unroll
+                    for (int k = 0; k < NI; ++k) {
+                        pair_x2_far<MFLAG>(ip[k], make_float2(XH.x, XH.y), make_float2(YH.x, YH.y),
+                                           make_float2(ZH.x, ZH.y), make_float2(MM.x, MM.y),
+                                           make_float2(XL.x, XL.y), make_float2(YL.x, YL.y),
+                                           make_float2(ZL.x, ZL.y), make_float2(VX.x, VX.y),
+                                           make_float2(VY.x, VY.y), make_float2(VZ.x, VZ.y), s[k]);
+                        pair_x2_far<MFLAG>(ip[k], make_float2(XH.z, XH.w), make_float2(YH.z, YH.w),
+                                           make_float2(ZH.z, ZH.w), make_float2(MM.z, MM.w),
+                                           make_float2(XL.z, XL.w), make_float2(YL.z, YL.w),
+                                           make_float2(ZL.z, ZL.w), make_float2(VX.z, VX.w),
+                                           make_float2(VY.z, VY.w), make_float2(VZ.z, VZ.w), s[k]);
+                    }
+                }
+            }
+          }
+        }
+#pragma unroll 1
+        for (int g = 0; g < (far ? 0 : JT / 32); ++g) {
             unsigned cnt[NI];
 #pragma unroll
             for (int k = 0; k < NI; ++k) cnt[k] = 0u;
@@ -656,7 +775,7 @@ __global__ void __launch_bounds__(NT, X2_MINB / NI) regf_x2_kernel(const RegArgs
                     mbar_wait_timed(&bar[u % NSTAGE], (uint32_t)((u / NSTAGE) & 1), WAIT_NS / 8);
                 return;
             }
-            issue_tile_soa<F64DX>(a, sj[st], &bar[st], t_begin + t + NSTAGE);
+            issue_tile_soa<F64DX>(a, sj[st], &bar[st], t_begin + (t + NSTAGE) * t_step);
             issued = t + NSTAGE + 1;
         }
         // fold: positive partial = rare-path sums - packed (negated) lane sums
@@ -1099,6 +1218,19 @@ struct RegState {
     // segmented calls: work list and per-i partial slots, staged as ints
     HostBuf<int> hseg;
     DevBuf<int> dseg;
+    // spatially ordered copy of the j set (see jset_keys)
+    int use_jsort = -1;                // -1 = read NB6_JSORT on first use
+    long long jver = 0, sorted_ver = -1;
+    DevBuf<float4> posH_s, posL_s, vel_s, tbox;
+    DevBuf<float> comp_s;
+    DevBuf<double> compd_s;
+    DevBuf<int> perm, vals_in, iperm;
+    DevBuf<unsigned> keys_in, keys_out, ext;
+    DevBuf<unsigned char> sort_tmp;
+    // NB6_SELFCHECK=1: host copy of the last send, to re-derive sample rows
+    int selfcheck = -1;
+    std::vector<double> chk_m, chk_x, chk_v;
+    long long chk_rows = 0, chk_bad = 0;
 };
 RegState R;
 
@@ -1228,11 +1360,184 @@ bool any_nan(const double *p, size_t n) {
     return false;
 }
 
+// ----------------------------------------------------------------------------
+// Spatial order of the j set.  After every send the bodies are put in Morton
+// (Z-curve) order of their positions, so that the 128 bodies of a tile are
+// close together, and each tile gets a bounding box.  The packed kernel then
+// skips the neighbour-candidate arithmetic for every (warp, tile) whose box is
+// provably out of reach of all the warp's i-particles.  Slot k of the ordered
+// set holds the caller's body perm[k]; the exact FP64 path maps slots back, so
+// neighbour ids are the caller's.
+// ----------------------------------------------------------------------------
+NB6_DEV unsigned f2ord(float f) {
+    const unsigned u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+NB6_DEV float ord2f(unsigned u) { return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u); }
+
+// ext[0..2] = min x, y, z and ext[3..5] = max (order-preserving uints).
+__global__ void jset_extent(int nj, const double *__restrict__ jx, unsigned *__restrict__ ext) {
+    unsigned mn[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu}, mx[3] = {0u, 0u, 0u};
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nj; j += gridDim.x * blockDim.x)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const unsigned o = f2ord((float)jx[3 * (size_t)j + k]);
+            mn[k] = min(mn[k], o);
+            mx[k] = max(mx[k], o);
+        }
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+        for (int o = 16; o > 0; o >>= 1) {
+            mn[k] = min(mn[k], __shfl_xor_sync(0xffffffffu, mn[k], o));
+            mx[k] = max(mx[k], __shfl_xor_sync(0xffffffffu, mx[k], o));
+        }
+    if ((threadIdx.x & 31) == 0)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            atomicMin(&ext[k], mn[k]);
+            atomicMax(&ext[3 + k], mx[k]);
+        }
+}
+
+NB6_DEV unsigned spread10(unsigned v) {
+    v &= 1023u;
+    v = (v | (v << 16)) & 0x030000FFu;
+    v = (v | (v << 8)) & 0x0300F00Fu;
+    v = (v | (v << 4)) & 0x030C30C3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+
+// 30-bit Morton key of each body on a 1024^3 grid over the extent.
+__global__ void jset_keys(int nj, const double *__restrict__ jx, const unsigned *__restrict__ ext,
+                          unsigned *__restrict__ keys, int *__restrict__ vals) {
+    float lo[3], sc[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        lo[k] = ord2f(ext[k]);
+        const float w = ord2f(ext[3 + k]) - lo[k];
+        sc[k] = w > 0.f ? 1023.99f / w : 0.f;
+    }
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nj; j += gridDim.x * blockDim.x) {
+        unsigned key = 0;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const float q = ((float)jx[3 * (size_t)j + k] - lo[k]) * sc[k];
+            const unsigned c = q <= 0.f ? 0u : (q >= 1023.f ? 1023u : (unsigned)q);
+            key |= spread10(c) << k;
+        }
+        keys[j] = key;
+        vals[j] = j;
+    }
+}
+
+// Ordered copies of the float layouts (slot k <- body perm[k]; padding slots
+// k >= nj are copied in place).
+__global__ void jset_permute(int nj, JSetOut src, JSetOut dst, const int *__restrict__ perm) {
+    const size_t np = src.npad;
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < np; k += (size_t)gridDim.x * blockDim.x) {
+        const size_t o = k < (size_t)nj ? (size_t)perm[k] : k;
+        dst.posH[k] = src.posH[o];
+        dst.posL[k] = src.posL[o];
+        dst.vel[k] = src.vel[o];
+#pragma unroll
+        for (int c = 0; c < NB6_NCOMP; ++c) dst.comp[c * np + k] = src.comp[c * np + o];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) dst.compd[c * np + k] = src.compd[c * np + o];
+    }
+}
+
+// One warp per tile: bounding box of the hi positions of its real bodies
+// (centre rounded to nearest, half extent, speeds and masses rounded up).
+__global__ void jset_tile_boxes(int nj, int ntile, const float4 *__restrict__ posH, const float4 *__restrict__ vel,
+                                float4 *__restrict__ tbox) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (warp >= ntile) return;
+    double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300}, vm = 0.0, mm = 0.0;
+    for (int q = lane; q < JT; q += 32) {
+        const int k = warp * JT + q;
+        if (k >= nj) break;
+        const float4 p = posH[k], v = vel[k];
+        const double c[3] = {p.x, p.y, p.z};
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            mn[d] = fmin(mn[d], c[d]);
+            mx[d] = fmax(mx[d], c[d]);
+        }
+        vm = fmax(vm, sqrt((double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z));
+        mm = fmax(mm, (double)p.w);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            mn[d] = fmin(mn[d], __shfl_xor_sync(0xffffffffu, mn[d], o));
+            mx[d] = fmax(mx[d], __shfl_xor_sync(0xffffffffu, mx[d], o));
+        }
+        vm = fmax(vm, __shfl_xor_sync(0xffffffffu, vm, o));
+        mm = fmax(mm, __shfl_xor_sync(0xffffffffu, mm, o));
+    }
+    if (lane == 0) {
+        tbox[2 * warp] = make_float4(__double2float_rn(0.5 * (mn[0] + mx[0])), __double2float_rn(0.5 * (mn[1] + mx[1])),
+                                     __double2float_rn(0.5 * (mn[2] + mx[2])), __double2float_ru(vm));
+        tbox[2 * warp + 1] = make_float4(__double2float_ru(0.5 * (mx[0] - mn[0])), __double2float_ru(0.5 * (mx[1] - mn[1])),
+                                         __double2float_ru(0.5 * (mx[2] - mn[2])), __double2float_ru(mm));
+    }
+}
+
+// Spatial order of the active set of one call (ni <= ISORT_MAX): Morton keys
+// on the j set's grid, bitonic sort of (key, index) in one CTA.
+constexpr int ISORT_MAX = 4096;
+__global__ void __launch_bounds__(1024) iset_order(int ni, const double *__restrict__ ix,
+                                                   const unsigned *__restrict__ ext, int *__restrict__ iperm) {
+    __shared__ unsigned long long kv[ISORT_MAX];
+    float lo[3], sc[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        lo[k] = ord2f(ext[k]);
+        const float w = ord2f(ext[3 + k]) - lo[k];
+        sc[k] = w > 0.f ? 1023.99f / w : 0.f;
+    }
+    int P = 1;
+    while (P < ni) P <<= 1;
+    for (int s = threadIdx.x; s < P; s += blockDim.x) {
+        unsigned long long v = ~0ull;  // padding sorts last
+        if (s < ni) {
+            unsigned key = 0;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const float q = ((float)ix[3 * (size_t)s + k] - lo[k]) * sc[k];
+                const unsigned c = q <= 0.f ? 0u : (q >= 1023.f ? 1023u : (unsigned)q);
+                key |= spread10(c) << k;
+            }
+            v = ((unsigned long long)key << 32) | (unsigned)s;
+        }
+        kv[s] = v;
+    }
+    __syncthreads();
+    for (int kk = 2; kk <= P; kk <<= 1)
+        for (int jj = kk >> 1; jj > 0; jj >>= 1) {
+            for (int x = threadIdx.x; x < P; x += blockDim.x) {
+                const int y = x ^ jj;
+                if (y > x) {
+                    const unsigned long long p0 = kv[x], p1 = kv[y];
+                    if ((p0 > p1) == ((x & kk) == 0)) {
+                        kv[x] = p1;
+                        kv[y] = p0;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    for (int s = threadIdx.x; s < ni; s += blockDim.x) iperm[s] = (int)(kv[s] & 0xffffffffu);
+}
+
 }  // namespace
 
 // Make n bodies the current j set: tile count, padded length and buffers for
 // both float layouts plus the FP64 copies.
 static JSetOut size_j_buffers(int n) {
+    R.jver++;  // a producer is about to write a new j set
     R.nj = n;
     R.ntile = std::max(1, (n + JT - 1) / JT);
     R.npad = (size_t)R.ntile * JT;
@@ -1252,6 +1557,56 @@ static JSetOut size_j_buffers(int n) {
     o.compd = R.compd.ptr;
     o.npad = R.npad;
     return o;
+}
+
+// Build (once per j set) the spatially ordered copy used by the tile and
+// j-parallel kernels.  Stream-ordered after the producer's kernels.
+static bool ensure_sorted(cudaStream_t st) {
+    if (R.use_jsort < 0) {
+        const char *e = getenv("NB6_JSORT");
+        R.use_jsort = (e && atoi(e) == 0) ? 0 : 1;
+    }
+    // small sets: the j-parallel kernel serves them and tiles span the whole
+    // system, so the order would only cost the sort (NB6_JSORT_MIN overrides)
+    static const int jsort_min = [] {
+        const char *e = getenv("NB6_JSORT_MIN");
+        return e ? atoi(e) : 32768;
+    }();
+    if (!R.use_jsort || R.nj < 1 || R.nj < jsort_min) return false;
+    if (R.sorted_ver == R.jver) return true;
+    const int nj = R.nj;
+    const size_t np = R.npad;
+    R.posH_s.reserve(np);
+    R.posL_s.reserve(np);
+    R.vel_s.reserve(np);
+    R.comp_s.reserve((size_t)NB6_NCOMP * np);
+    R.compd_s.reserve((size_t)3 * np);
+    R.perm.reserve(nj);
+    R.vals_in.reserve(nj);
+    R.keys_in.reserve(nj);
+    R.keys_out.reserve(nj);
+    R.ext.reserve(6);
+    R.tbox.reserve((size_t)2 * R.ntile);
+    const unsigned init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
+    NB6_CUDA_CHECK(cudaMemcpyAsync(R.ext.ptr, init, sizeof(init), cudaMemcpyHostToDevice, st));
+    const int blocks = std::max(1, std::min((nj + 255) / 256, nb6_num_sms() * 8));
+    jset_extent<<<blocks, 256, 0, st>>>(nj, R.jx.ptr, R.ext.ptr);
+    jset_keys<<<blocks, 256, 0, st>>>(nj, R.jx.ptr, R.ext.ptr, R.keys_in.ptr, R.vals_in.ptr);
+    NB6_CUDA_CHECK(cudaGetLastError());
+    size_t tmp = 0;
+    NB6_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(nullptr, tmp, R.keys_in.ptr, R.keys_out.ptr, R.vals_in.ptr,
+                                                   R.perm.ptr, nj, 0, 30, st));
+    R.sort_tmp.reserve(tmp + 16);
+    NB6_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(R.sort_tmp.ptr, tmp, R.keys_in.ptr, R.keys_out.ptr,
+                                                   R.vals_in.ptr, R.perm.ptr, nj, 0, 30, st));
+    JSetOut src{R.posH.ptr, R.posL.ptr, R.vel.ptr, R.comp.ptr, R.compd.ptr, np};
+    JSetOut dst{R.posH_s.ptr, R.posL_s.ptr, R.vel_s.ptr, R.comp_s.ptr, R.compd_s.ptr, np};
+    const int pblocks = (int)std::min<size_t>((np + 255) / 256, (size_t)nb6_num_sms() * 8);
+    jset_permute<<<pblocks, 256, 0, st>>>(nj, src, dst, R.perm.ptr);
+    jset_tile_boxes<<<(R.ntile * 32 + 255) / 256, 256, 0, st>>>(nj, R.ntile, R.posH_s.ptr, R.vel_s.ptr, R.tbox.ptr);
+    NB6_CUDA_CHECK(cudaGetLastError());
+    R.sorted_ver = R.jver;
+    return true;
 }
 
 // ----------------------------------------------------------------------------
@@ -1355,12 +1710,33 @@ static void regf_prepare(int ni, const double *d_h2, const double *d_dtr, const 
     R.outf.reserve((size_t)ni * 8);
     R.outl.reserve((size_t)ni * W);
 
+    const bool sorted = ensure_sorted(st);
     RegArgs a;
-    a.posH = R.posH.ptr;
-    a.posL = R.posL.ptr;
-    a.vel = R.vel.ptr;
-    a.comp = R.comp.ptr;
-    a.compd = R.compd.ptr;
+    a.posH = sorted ? R.posH_s.ptr : R.posH.ptr;
+    a.posL = sorted ? R.posL_s.ptr : R.posL.ptr;
+    a.vel = sorted ? R.vel_s.ptr : R.vel.ptr;
+    a.comp = sorted ? R.comp_s.ptr : R.comp.ptr;
+    a.compd = sorted ? R.compd_s.ptr : R.compd.ptr;
+    a.perm = sorted ? R.perm.ptr : nullptr;
+    static const int far_path = [] {
+        const char *e = getenv("NB6_FARPATH");
+        return (e && atoi(e) == 0) ? 0 : 1;
+    }();
+    a.tbox = (sorted && far_path) ? R.tbox.ptr : nullptr;
+    static const int i_order = [] {
+        const char *e = getenv("NB6_IORDER");
+        return (e && atoi(e) == 0) ? 0 : 1;
+    }();
+    if (i_order && a.tbox && ni > NT && ni <= ISORT_MAX) {
+        R.iperm.reserve(ni);
+        // the order reads this call's i positions: a host call's staging
+        // must be on the device first (the submission copies it again)
+        if (L.hin)
+            NB6_CUDA_CHECK(cudaMemcpyAsync(R.iin.ptr, L.hin, L.in_bytes, cudaMemcpyHostToDevice, st));
+        iset_order<<<1, 1024, 0, st>>>(ni, d_x, R.ext.ptr, R.iperm.ptr);
+        NB6_CUDA_CHECK(cudaGetLastError());
+        a.iperm = R.iperm.ptr;
+    }
     a.npad = R.npad;
     a.jm = R.jm.ptr;
     a.jx = R.jx.ptr;
@@ -1689,6 +2065,15 @@ void gpunb_send_(int *nj, double *mj, double (*xj)[3], double (*vj)[3]) {
     }
     R.time_send -= nb6_wtime();
     R.isend++;
+    if (R.selfcheck < 0) {
+        const char *e = getenv("NB6_SELFCHECK");
+        R.selfcheck = (e && atoi(e) != 0) ? 1 : 0;
+    }
+    if (R.selfcheck) {
+        R.chk_m.assign(mj, mj + n);
+        R.chk_x.assign(&xj[0][0], &xj[0][0] + 3 * (size_t)n);
+        R.chk_v.assign(&vj[0][0], &vj[0][0] + 3 * (size_t)n);
+    }
     cudaStream_t st = nb6_stream();
     const JSetOut o = size_j_buffers(n);
     if (n > 0) {
@@ -1746,6 +2131,71 @@ static void unpack_results(int ni, int W, int lmax, double (*acc)[3], double (*j
         const int nnb = src[0];
         dst[0] = nnb;
         if (nnb > 0) memcpy(dst + 1, src + 1, sizeof(int) * nnb);
+    }
+}
+
+// Diagnostic (NB6_SELFCHECK=1, off by default): re-derive sample rows of a
+// finished gpunb_regf_ call on the host in FP64 with the rule of
+// regint.f:41-65 (strict "<") and report rows whose neighbour list differs or
+// whose force/jerk/potential is off by more than 1e-5 relative.
+static void selfcheck_rows(int ni, const double *h2, const double *dtr, const double (*xi)[3],
+                           const double (*vi)[3], const double (*acc)[3], const double (*jrk)[3],
+                           const double *pot, const int *list, int lmax, int nnbmax, int mflag) {
+    const int nj = (int)R.chk_m.size();
+    if (nj != R.nj) return;
+    const int cap = std::max(0, std::min(nnbmax, lmax - 1));
+    int rows[4] = {0, ni / 3, (2 * ni) / 3, ni - 1};
+    for (int r : rows) {
+        if (r < 0 || r >= ni) continue;
+        double a[3] = {0, 0, 0}, jk[3] = {0, 0, 0}, po = 0;
+        std::vector<int> ids;
+        for (int j = 0; j < nj; ++j) {
+            double d[3], dv[3], r2 = 0, r2p = 0, rv = 0;
+            for (int k = 0; k < 3; ++k) {
+                d[k] = R.chk_x[3 * (size_t)j + k] - xi[r][k];
+                dv[k] = R.chk_v[3 * (size_t)j + k] - vi[r][k];
+            }
+            r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+            const double p0 = d[0] + dtr[r] * dv[0], p1 = d[1] + dtr[r] * dv[1], p2 = d[2] + dtr[r] * dv[2];
+            r2p = p0 * p0 + p1 * p1 + p2 * p2;
+            const double crit = mflag ? R.chk_m[j] * h2[r] : h2[r];
+            if ((r2 < r2p ? r2 : r2p) < crit) {
+                ids.push_back(j);
+                continue;
+            }
+            rv = d[0] * dv[0] + d[1] * dv[1] + d[2] * dv[2];
+            const double ri2 = 1.0 / r2, ri = sqrt(ri2), mr = R.chk_m[j] * ri, mr3 = mr * ri2;
+            const double al = -3.0 * rv * ri2;
+            po += mr;
+            for (int k = 0; k < 3; ++k) {
+                a[k] += mr3 * d[k];
+                jk[k] += mr3 * (dv[k] + al * d[k]);
+            }
+        }
+        R.chk_rows++;
+        const int *row = list + (size_t)r * lmax;
+        const int nnb = (int)ids.size();
+        bool bad = (nnb > cap) ? (row[0] != -nnb) : (row[0] != nnb);
+        if (!bad && nnb <= cap)
+            for (int k = 0; k < nnb; ++k) bad = bad || row[1 + k] != ids[k];
+        double ea = 0, ej = 0, na = 0, nj2 = 0;
+        for (int k = 0; k < 3; ++k) {
+            ea += (acc[r][k] - a[k]) * (acc[r][k] - a[k]);
+            na += a[k] * a[k];
+            ej += (jrk[r][k] - jk[k]) * (jrk[r][k] - jk[k]);
+            nj2 += jk[k] * jk[k];
+        }
+        const double era = sqrt(ea / (na > 0 ? na : 1)), erj = sqrt(ej / (nj2 > 0 ? nj2 : 1));
+        const double erp = fabs(pot[r] - po) / (po > 0 ? po : 1);
+        if (nnb <= cap && (era > 1e-5 || erj > 1e-4 || erp > 1e-5)) bad = true;
+        if (bad) {
+            R.chk_bad++;
+            fprintf(stderr,
+                    "# nb6 selfcheck: call ni=%d nj=%d variant %d grid (%d,%d) row %d: nnb %d (fp64 %d), acc err %.2e,"
+                    " jrk err %.2e, pot err %.2e\n",
+                    ni, nj, R.last_geometry[0], R.last_geometry[1], R.last_geometry[2], r, row[0], nnb, era, erj,
+                    erp);
+        }
     }
 }
 
@@ -1853,6 +2303,8 @@ void gpunb_regf_(int *ni_, double *h2, double *dtr, double (*xi)[3], double (*vi
 
     unpack_results(ni, W, lmax, acc, jrk, pot, list);
     R.time_reduce += nb6_wtime();
+    if (R.selfcheck > 0)
+        selfcheck_rows(ni, h2, dtr, xi, vi, acc, jrk, pot, list, lmax, nnbmax, *m_flag);
 }
 
 // Segmented regular force: gpunb_regf_ for an ensemble of independent
@@ -2126,6 +2578,21 @@ void nb6_regf_autotune_(int *flag) {
         return;
     }
     R.autotune = *flag ? 1 : 0;
+}
+
+// Spatial ordering of the j set for the tile kernels: 1 on (default;
+// NB6_JSORT=0 in the environment for off), 0 off, other values query.
+// Returns the setting.
+int nb6_regf_jsort_(int *flag) {
+    if (R.use_jsort < 0) {
+        const char *e = getenv("NB6_JSORT");
+        R.use_jsort = (e && atoi(e) == 0) ? 0 : 1;
+    }
+    if (flag && (*flag == 0 || *flag == 1)) {
+        R.use_jsort = *flag;
+        R.sorted_ver = -1;  // rebuild on the next call if turned on
+    }
+    return R.use_jsort;
 }
 
 // Learned radius proposals of the last gpunb_regf_ / nb6_regf_seg_ call:

@@ -271,3 +271,25 @@ def test_regular_graph_replay_matches_plain_launches(nb6, orc):
             ol = orc.regf(inp["mj"], inp["xj"], inp["vj"], inp["h2"], inp["dtr"], inp["xi"],
                           inp["vi"], inp["lmax"], inp["nnbmax"], inp["m_flag"])[3]
             np.testing.assert_array_equal(b[3][:, 0], ol[:, 0])
+
+
+def test_regular_spatial_order_matches_caller_order(nb6, orc):
+    """With the j set in Morton order (the default) the results are those of
+    the caller's order: identical neighbour lists (ids are the caller's) and
+    forces within the parity tolerances against the FP64 oracle, for the
+    packed kernel (with its far-tile path) and the j-parallel kernel, with
+    and without m_flag."""
+    import ctypes as C
+    from nb6b200 import ics
+    raw = nb6.lib
+    raw.nb6_regf_jsort_.restype = C.c_int
+    cl = ics.king(40000, w0=6.0, seed=5, imf=True, binary_fraction=0.05)   # above the order's minimum
+    try:
+        for flag in (1, 0):
+            assert raw.nb6_regf_jsort_(C.byref(C.c_int(flag))) == flag
+            for ni, m_flag in ((4096, 0), (4096, 1), (7, 0)):
+                isel = np.sort(np.random.default_rng(ni + m_flag).choice(cl.n, ni, replace=False))
+                inp = _inputs(cl, isel, 512, 400, m_flag)
+                check_vs_oracle(orc, inp, run_gpu(nb6, **inp))
+    finally:
+        raw.nb6_regf_jsort_(C.byref(C.c_int(1)))
