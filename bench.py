@@ -399,10 +399,15 @@ def main():
             t = torch.tensor([e2e_s], device=dev)
             pg.all_reduce(t, op=pg.ReduceOp.MAX)
             e2e_s = float(t.item())
-        W = min(args.nnbmax, args.lmax - 1) + 1
+        # bytes moved per step: the j set (m, x, v) and the i data up; the
+        # force rows (8 doubles) and each list row's count + ids down (the
+        # library writes only the used part of a row into pinned memory);
+        # the ids are counted from the neighbour lists of the last call
+        nnb_last = np.abs(lst[: chunks[-1][1] - chunks[-1][0], 0]).astype(float)
+        ids_per_i = float(nnb_last.mean()) + 1.0
         e2e = {"value": world * pairs_step / e2e_s, "unit": "pairs/s",
                "h2d_bytes_per_step": int(n * (8 + 24 + 24) + n * 64),
-               "d2h_bytes_per_step": int(n * 64 + n * W * 4),
+               "d2h_bytes_per_step": int(n * 64 + n * ids_per_i * 4),
                "steps": e2e_steps, "timing": "wall clock around synchronous ABI calls"}
 
     # the N^2 potential of the same cluster (GPUPOT, energy.F:33): kernel
