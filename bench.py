@@ -45,9 +45,10 @@ import numpy as np  # noqa: E402
 METRIC = "Regular force+jerk+nbr pair interactions/s at N=1M"
 FLOPS_PER_PAIR = 60          # gpunb.velocity.cu:895, reg.avx.cpp:343
 # DRAM bytes (read + write) per launch of the headline force kernel,
-# regf_x2_kernel<1> with 1024 i x 996,147 j, from the ncu capture summarised
-# in profiles/regf_x2_kernel_king1m.md (56.09 MB read + 0.66 MB written).
-NCU_TRAFFIC_PER_LAUNCH = 56.09e6 + 0.658e6
+# regf_x2_kernel<1> with 1024 i x 996,147 j over the Morton-ordered j set,
+# from the ncu capture summarised in profiles/regf_x2_kernel_king1m.md
+# (57.61 MB read + 0.73 MB written).
+NCU_TRAFFIC_PER_LAUNCH = 57.61e6 + 0.734e6
 
 
 def parse():
