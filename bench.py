@@ -182,6 +182,16 @@ def cpu_reference_rate(m, x, v, rs, dtr, args, seconds: float, max_calls: int | 
     return pairs / t_used, threads, calls, t_used
 
 
+def hbm_peak():
+    """Measured HBM copy bandwidth (GB/s) of this pool's B200s, else the
+    earlier fallback measurement."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured (MEASURED_PEAKS.json)"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
 def irregular_leg(lib, m, x, v, h2, dtr, args, nsample: int = 65536):
     """Irregular force + jerk + nearest neighbour over lists of ~NNBOPT,
     this library vs the reference's irr.avx.cpp, same inputs."""
@@ -220,11 +230,21 @@ def irregular_leg(lib, m, x, v, h2, dtr, args, nsample: int = 65536):
         return res, dt
 
     ours, t_ours = run(lib, "libnb6b200", 5)
+    k_ms = float(lib.lib.nb6_irr_last_kernel_ms_()) if hasattr(lib.lib, "nb6_irr_last_kernel_ms_") else None
     if not oracle.ref_available("irr"):
         oracle.build(ref=True)
     ref, t_ref = run(ForceLib(oracle.ref_lib("irr"), "ref-irr-avx"), "irr.avx", 2)
     a_o, a_r = ours[0], ref[0]
     rel = np.sqrt(((a_o - a_r) ** 2).sum(1) / np.maximum((a_r ** 2).sum(1), 1e-300))
+    if k_ms:
+        # 128-byte FP64 record + 4-byte id per list pair (HBM-bound gathers)
+        out["kernel_ms"] = k_ms
+        out["kernel_pairs_per_s"] = pairs / (k_ms * 1e-3)
+        out["kernel_gbs_algorithmic"] = 132.0 * pairs / (k_ms * 1e-3) / 1e9
+        hbm, src = hbm_peak()
+        out["kernel_frac_hbm"] = out["kernel_gbs_algorithmic"] / hbm
+        out["hbm_peak_gbs"] = hbm
+        out["hbm_peak_source"] = src
     out.update({"pairs_per_s": pairs / t_ours, "ms_per_call": 1e3 * t_ours,
                 "cpu_reference_pairs_per_s": pairs / t_ref,
                 "cpu_reference_threads": int(os.environ.get("OMP_NUM_THREADS", "1")),
@@ -501,7 +521,9 @@ def main():
                        "nnbopt": 50, "nnbmax": args.nnbmax, "lmax": args.lmax,
                        "m_flag": args.m_flag, "parallelism": f"replicas x{world}",
                        "l2": "flushed (256 MiB write) between timed steps"},
-            "gpu_launches": int(args.steps * len(chunks) * 2),
+            # per call: force kernel + finalize, plus the active-set order
+            # when the j set is spatially ordered (>= 32768 bodies)
+            "gpu_launches": int(args.steps * len(chunks) * (3 if n >= 32768 else 2)),
             "clocks": clk, "roofline": roof, "e2e": e2e, "cpu_baseline": cpu,
             "err_vs_fp64": err,
             "gpupot": pot,

@@ -164,6 +164,8 @@ void nb6_regf_seg_(int *ni, int *iseg, double *h2, double *dtr, double (*xi)[3],
  * Replaces XBPREDALL + GPUNB_SEND (intgrt.F:866-882) without host
  * prediction or j upload.  Needs gpunb_open_ and irr_simd_open_. */
 void nb6_irr_predict_send_(double *t, int *nseg, int *addr0, int *count);
+/* Device time (ms) of the force kernel of the last irr_simd_firr_vec_. */
+float nb6_irr_last_kernel_ms_(void);
 
 /* Learned neighbour radius (no reference counterpart; its fallback is the
  * reference's Ahmad-Cohen rule, regcor_gpu.F:131-196).  A 5-64-64-1 SiLU

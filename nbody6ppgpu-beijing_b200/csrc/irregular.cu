@@ -216,6 +216,7 @@ struct IrrState {
     size_t list_words = 0;
     double time_grav = 0;
     unsigned long long num_inter = 0, num_fcall = 0, num_steps = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // irr_kernel of the last call
 };
 IrrState I;
 
@@ -444,9 +445,15 @@ void irr_firr_vec_impl(double ti, int ni, const int *addr, double (*acc)[3], dou
         I.dout.reserve((size_t)ni * 8);
         out = I.dout.ptr;
     }
+    if (!I.ev0) {
+        NB6_CUDA_CHECK(cudaEventCreate(&I.ev0));
+        NB6_CUDA_CHECK(cudaEventCreate(&I.ev1));
+    }
+    NB6_CUDA_CHECK(cudaEventRecord(I.ev0, st));
     irr_kernel<<<(ni + IRR_WARPS - 1) / IRR_WARPS, IRR_WARPS * 32, 0, st>>>(ni, daddr, ti, I.rec.ptr, I.lists.ptr,
                                                                        I.lmax, I.nmax, out);
     NB6_CUDA_CHECK(cudaGetLastError());
+    NB6_CUDA_CHECK(cudaEventRecord(I.ev1, st));
     if (!direct)
         NB6_CUDA_CHECK(cudaMemcpyAsync(I.hout.ptr, I.dout.ptr, sizeof(double) * 8 * ni, cudaMemcpyDeviceToHost, st));
     nb6_status_fetch(st);
@@ -549,6 +556,16 @@ void gpuirr_set_jp_(int *addr, double pos[3], double vel[3], double acc2[3], dou
     irr_set_jp_impl(*addr - 1, pos, vel, acc2, jrk6, *mass, *time);
 }
 void gpuirr_set_list_(int *addr, int *nblist) { irr_set_list_impl(*addr - 1, nblist); }
+
+// Extension (no reference counterpart): device time (ms) of the force
+// kernel of the last irr_simd_firr_vec_ call.
+float nb6_irr_last_kernel_ms_() {
+    if (!I.ev1) return 0.f;
+    float ms = 0.f;
+    NB6_CUDA_CHECK(cudaEventSynchronize(I.ev1));
+    NB6_CUDA_CHECK(cudaEventElapsedTime(&ms, I.ev0, I.ev1));
+    return ms;
+}
 
 // Extension (no reference counterpart): make the regular-force j set (what
 // gpunb_send_ sends) from the resident irregular records, predicted to *t on

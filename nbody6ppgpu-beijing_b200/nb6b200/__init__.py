@@ -27,7 +27,7 @@ ABI_SYMBOLS = (
     "nb6_set_abort_on_error_", "nb6_last_status_", "nb6_device_",
     "nb6_regf_device_", "nb6_regf_outputs_", "nb6_regf_last_kernel_ms_", "nb6_regf_tune_",
     "nb6_regf_last_geometry_", "nb6_regf_autotune_", "nb6_regf_graphs_", "nb6_regf_jsort_", "nb6_regf_seg_",
-    "nb6_irr_predict_send_", "nb6_regf_proposals_",
+    "nb6_irr_predict_send_", "nb6_irr_last_kernel_ms_", "nb6_regf_proposals_",
     "nb6_mlp_size_", "nb6_mlp_init_", "nb6_mlp_set_", "nb6_mlp_get_", "nb6_mlp_grad_",
     "nb6_mlp_train_", "nb6_mlp_predict_", "nb6_mlp_enable_",
     "nb6_sync_", "nb6_stream_",
@@ -65,6 +65,8 @@ def load_cdll() -> C.CDLL:
             _LIB.nb6_fp32_peak_probe_.restype = C.c_double
         if hasattr(_LIB, "nb6_predict_last_kernel_ms_"):
             _LIB.nb6_predict_last_kernel_ms_.restype = C.c_float
+        if hasattr(_LIB, "nb6_irr_last_kernel_ms_"):
+            _LIB.nb6_irr_last_kernel_ms_.restype = C.c_float
     return _LIB
 
 
