@@ -167,6 +167,24 @@ void nb6_irr_predict_send_(double *t, int *nseg, int *addr0, int *count);
 /* Device time (ms) of the force kernel of the last irr_simd_firr_vec_. */
 float nb6_irr_last_kernel_ms_(void);
 
+/* Irregular corrector on the device (the Hermite state stays resident; the
+ * host's NBINT_COR work of nbint_cor.f:113-173,215-236 and intgrt.F:533-581
+ * per active body).  After irr_simd_open_: nb6_hermite_open_ allocates the
+ * per-body state; nb6_hermite_set_ stages a body's FI, FIDOT, FR, FRDOT,
+ * STEP, T0R, STEPR (1-based address) like irr_simd_set_jp_ stages its
+ * record.  nb6_irr_correct_ computes the neighbour force of the active
+ * bodies at *time, applies the corrector, chooses the new irregular step,
+ * tests whether the regular step is due and otherwise extrapolates F and
+ * FDOT -- updating the device state -- and returns per body out[k][24] =
+ * x0[3], v0[3], fi[3], fidot[3], F[3], FDOT[3], step, regular-due (0/1),
+ * nnbid, 0, 0, 0.  Each operation is rounded separately in the order of the
+ * driver's host corrector, so both give the same bits.  No reference
+ * counterpart: the reference corrects on the host. */
+void nb6_hermite_open_(double *eta_i, double *smax, double *dtmin);
+void nb6_hermite_set_(int *addr, double fi[3], double fidot[3], double fr[3], double frdot[3],
+                      double *step, double *t0r, double *stepr);
+void nb6_irr_correct_(double *time, int *ni, int *addr, double *out);
+
 /* Learned neighbour radius (no reference counterpart; its fallback is the
  * reference's Ahmad-Cohen rule, regcor_gpu.F:131-196).  A 5-64-64-1 SiLU
  * network, bf16 parameters, FP32 sums, proposing dlog = log(RS_next / RS)

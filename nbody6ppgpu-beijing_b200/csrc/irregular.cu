@@ -53,14 +53,10 @@ NB6_DEV void load_rec(const Rec *__restrict__ p, Rec &r) {
     r.m = g.x; r.t0 = g.y;
 }
 
-// out row k = (ax, ay, az, jx, jy, jz, nnbid, 0): one download per call.
-__global__ void __launch_bounds__(IRR_WARPS * 32)
-    irr_kernel(int ni, const int *__restrict__ addr, double ti, const Rec *__restrict__ rec,
-               const int *__restrict__ lists, int ls, int nmax, double *__restrict__ out) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int k = blockIdx.x * IRR_WARPS + warp;
-    if (k >= ni) return;
-    const int i = addr[k] - 1;
+// One warp, one active particle i: neighbour force, jerk and nearest
+// neighbour (1-based, -1 for an empty list), reduced into every lane.
+NB6_DEV void irr_force_warp(int i, int lane, double ti, const Rec *__restrict__ rec,
+                            const int *__restrict__ lists, int ls, int nmax, double *a, double *jd, int &nnbid) {
     Rec ri;
     load_rec(rec + i, ri);
     double xi[3], vi[3];
@@ -97,12 +93,12 @@ __global__ void __launch_bounds__(IRR_WARPS * 32)
         jy += mr3 * (dvy + al * dyd);
         jz += mr3 * (dvz + al * dzd);
     }
-    ax = warp_sum_d(ax);
-    ay = warp_sum_d(ay);
-    az = warp_sum_d(az);
-    jx = warp_sum_d(jx);
-    jy = warp_sum_d(jy);
-    jz = warp_sum_d(jz);
+    a[0] = warp_sum_d(ax);
+    a[1] = warp_sum_d(ay);
+    a[2] = warp_sum_d(az);
+    jd[0] = warp_sum_d(jx);
+    jd[1] = warp_sum_d(jy);
+    jd[2] = warp_sum_d(jz);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         const double r2 = __shfl_xor_sync(0xffffffffu, rmin, o);
@@ -112,17 +108,155 @@ __global__ void __launch_bounds__(IRR_WARPS * 32)
             jmin = j2;
         }
     }
+    nnbid = (nnb > 0 && jmin != 0x7fffffff) ? jmin + 1 : -1;
+}
+
+// out row k = (ax, ay, az, jx, jy, jz, nnbid, 0): one download per call.
+__global__ void __launch_bounds__(IRR_WARPS * 32)
+    irr_kernel(int ni, const int *__restrict__ addr, double ti, const Rec *__restrict__ rec,
+               const int *__restrict__ lists, int ls, int nmax, double *__restrict__ out) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int k = blockIdx.x * IRR_WARPS + warp;
+    if (k >= ni) return;
+    double a[3], jd[3];
+    int id;
+    irr_force_warp(addr[k] - 1, lane, ti, rec, lists, ls, nmax, a, jd, id);
     if (lane == 0) {
         double *o = out + (size_t)k * 8;
-        o[0] = ax;
-        o[1] = ay;
-        o[2] = az;
-        o[3] = jx;
-        o[4] = jy;
-        o[5] = jz;
-        o[6] = (double)((nnb > 0 && jmin != 0x7fffffff) ? jmin + 1 : -1);
+        o[0] = a[0];
+        o[1] = a[1];
+        o[2] = a[2];
+        o[3] = jd[0];
+        o[4] = jd[1];
+        o[5] = jd[2];
+        o[6] = (double)id;
         o[7] = 0.0;
     }
+}
+
+// ----------------------------------------------------------------------------
+// Device-resident irregular corrector (nb6_irr_correct_).  Beside each 128-byte
+// record the device keeps an Aux record with the rest of a body's Hermite
+// state; irr_kernel computes the neighbour force of each active body, then
+// irr_apply_corrector applies the irregular corrector and the new irregular step of
+// nbint_cor.f:113-173,215-236 (tstep.f), the regular-due test and the F/FDOT
+// extrapolation of intgrt.F:570-578.  Every operation is rounded separately
+// in the order of the host restatement (driver/hermite.h, Bodies::irr_correct),
+// so device and host give the same bits.
+// ----------------------------------------------------------------------------
+struct Aux {  // 16 doubles
+    double fi[3], fid[3], fr[3], frd[3], step, t0r, stepr, pad;
+};
+
+struct HermiteParams {
+    double eta_i, smax, dtmin;
+};
+
+NB6_DEV double dadd(double a, double b) { return __dadd_rn(a, b); }
+NB6_DEV double dmul(double a, double b) { return __dmul_rn(a, b); }
+NB6_DEV double dsub(double a, double b) { return __dsub_rn(a, b); }
+NB6_DEV double ddiv(double a, double b) { return __ddiv_rn(a, b); }
+
+// tstep.f: sqrt(eta (|F||F2| + |F1|^2) / (|F1||F3| + |F2|^2))
+NB6_DEV double tstep_dev(const double *f, const double *f1, const double *f2, const double *f3, double eta) {
+    double F2 = 0, F12 = 0, F22 = 0, F32 = 0;
+    for (int k = 0; k < 3; ++k) {
+        F2 = dadd(F2, dmul(f[k], f[k]));
+        F12 = dadd(F12, dmul(f1[k], f1[k]));
+        F22 = dadd(F22, dmul(f2[k], f2[k]));
+        F32 = dadd(F32, dmul(f3[k], f3[k]));
+    }
+    const double num = dadd(__dsqrt_rn(dmul(F2, F22)), F12);
+    const double den = dadd(__dsqrt_rn(dmul(F12, F32)), F22);
+    if (!(den > 0)) return 1e30;
+    return __dsqrt_rn(ddiv(dmul(eta, num), den));
+}
+
+// Second launch of a corrector call, one thread per active body: the forces
+// of every active body come from irr_kernel first (all neighbours seen as
+// predicted from their old state, as on the host), then each body is
+// corrected.  out row k (24 doubles): x0[3], v0[3], fi[3], fidot[3], F[3],
+// FDOT[3], step, regular-due flag, nnbid, 0, 0, 0.
+__global__ void irr_apply_corrector(int ni, const int *__restrict__ addr, double time,
+                                    const double *__restrict__ force, Rec *__restrict__ rec,
+                                    Aux *__restrict__ aux, HermiteParams hp, double *__restrict__ out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= ni) return;
+    const int i = addr[k] - 1;
+    const double *fk = force + (size_t)k * 8;
+    const double a[3] = {fk[0], fk[1], fk[2]}, jd[3] = {fk[3], fk[4], fk[5]};
+    const int id = (int)fk[6];
+    Rec r = rec[i];
+    Aux x = aux[i];
+    const double s = dsub(time, r.t0), s1 = dmul(1.5, s), s2 = dmul(2.0, s);
+    double xi[3], vi[3];
+    for (int c = 0; c < 3; ++c) {
+        xi[c] = dadd(dmul(dadd(dmul(dadd(dmul(r.fd[c], s), r.f[c]), s), r.v[c]), s), r.x[c]);
+        vi[c] = dadd(dmul(dadd(dmul(r.fd[c], s1), r.f[c]), s2), r.v[c]);
+    }
+    const double dt = s, dtsq = dmul(dt, dt), dt6 = ddiv(6.0, dmul(dt, dtsq)), dt2 = ddiv(2.0, dtsq);
+    const double dtsq12 = ddiv(dtsq, 12.0), dt13 = ddiv(dt, 3.0);
+    double ftot[3], d2[3], d3[3];
+    for (int c = 0; c < 3; ++c) {  // nbint_cor.f:130-150
+        const double df = dsub(x.fi[c], a[c]);
+        const double fid = x.fid[c];
+        const double sum = dadd(fid, jd[c]);
+        const double at3 = dadd(dmul(2.0, df), dmul(dt, sum));
+        const double bt2 = dsub(dmul(-3.0, df), dmul(dt, dadd(sum, fid)));
+        r.x[c] = dadd(xi[c], dmul(dadd(dmul(0.6, at3), bt2), dtsq12));
+        r.v[c] = dadd(vi[c], dmul(dadd(dmul(0.75, at3), bt2), dt13));
+        x.fi[c] = a[c];
+        x.fid[c] = jd[c];
+        ftot[c] = dadd(x.fi[c], x.fr[c]);
+        d2[c] = dmul(dadd(dmul(3.0, at3), bt2), dt2);
+        d3[c] = dmul(at3, dt6);
+    }
+    // irregular step (nbint_cor.f:146,215-236)
+    double ttmp = tstep_dev(ftot, x.fid, d2, d3, hp.eta_i);
+    const double dt0 = ttmp;
+    if (ttmp > dmul(2.0, x.step)) {
+        const double two = dmul(2.0, x.step);
+        ttmp = (fmod(time, two) == 0.0) ? (hp.smax < two ? hp.smax : two) : x.step;
+    } else if (ttmp < x.step) {
+        ttmp = dmul(0.5, x.step);
+        if (ttmp > dt0) ttmp = dmul(ttmp, 0.5);
+    } else {
+        ttmp = x.step;
+    }
+    x.step = ttmp < hp.dtmin ? hp.dtmin : ttmp;
+    r.t0 = time;
+    const bool regdue = dadd(x.t0r, x.stepr) <= time;
+    if (!regdue) {
+        const double dtr = dsub(time, x.t0r);
+        for (int c = 0; c < 3; ++c) {
+            r.f[c] = dmul(0.5, dadd(dadd(dmul(x.frd[c], dtr), x.fr[c]), x.fi[c]));
+            r.fd[c] = ddiv(dadd(x.frd[c], x.fid[c]), 6.0);
+        }
+        // keep the irregular step inside the regular interval
+        while (dadd(r.t0, x.step) > dadd(x.t0r, x.stepr) && x.step > hp.dtmin) x.step = dmul(x.step, 0.5);
+    }
+    rec[i] = r;
+    aux[i] = x;
+    double *o = out + (size_t)k * 24;
+    for (int c = 0; c < 3; ++c) {
+        o[c] = r.x[c];
+        o[3 + c] = r.v[c];
+        o[6 + c] = x.fi[c];
+        o[9 + c] = x.fid[c];
+        o[12 + c] = r.f[c];
+        o[15 + c] = r.fd[c];
+    }
+    o[18] = x.step;
+    o[19] = regdue ? 1.0 : 0.0;
+    o[20] = (double)id;
+    o[21] = o[22] = o[23] = 0.0;
+}
+
+// Scatter staged Aux records: slot s goes to particle saddr[s].
+__global__ void irr_scatter_aux(int n, const int *__restrict__ saddr, const Aux *__restrict__ src,
+                                Aux *__restrict__ aux) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < n) aux[saddr[s]] = src[s];
 }
 
 // Scatter everything staged since the last flush, in one launch: blocks
@@ -217,6 +351,15 @@ struct IrrState {
     double time_grav = 0;
     unsigned long long num_inter = 0, num_fcall = 0, num_steps = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // irr_kernel of the last call
+    // device-resident corrector state (nb6_hermite_open_)
+    bool hermite = false;
+    HermiteParams hp{};
+    DevBuf<Aux> aux, dstage_aux;
+    DevBuf<int> dstage_aux_addr;
+    HostBuf<Aux> hstage_aux;
+    HostBuf<int> hstage_aux_addr;
+    std::vector<int> aux_slot;
+    int naux = 0;
 };
 IrrState I;
 
@@ -261,6 +404,14 @@ void irr_close_impl() {
     I.dout.release();
     I.dseg.release();
     I.hseg.release();
+    I.aux.release();
+    I.dstage_aux.release();
+    I.dstage_aux_addr.release();
+    I.hstage_aux.release();
+    I.hstage_aux_addr.release();
+    I.aux_slot.clear();
+    I.naux = 0;
+    I.hermite = false;
     I.hstage_rec.release();
     I.hstage_addr.release();
     I.hstage_list.release();
@@ -364,6 +515,19 @@ size_t zero_copy_bytes() { return nb6_uva() ? ZERO_COPY_MAX : 0; }
 // all integers either read in place or copied once each, then one scatter
 // launch.  Returns a device-readable pointer to the active addresses.
 const int *irr_flush(cudaStream_t st, const int *active = nullptr, int ni = 0) {
+    if (I.naux > 0) {
+        I.dstage_aux.reserve(I.naux);
+        I.dstage_aux_addr.reserve(I.naux);
+        NB6_CUDA_CHECK(cudaMemcpyAsync(I.dstage_aux.ptr, I.hstage_aux.ptr, sizeof(Aux) * I.naux,
+                                       cudaMemcpyHostToDevice, st));
+        NB6_CUDA_CHECK(cudaMemcpyAsync(I.dstage_aux_addr.ptr, I.hstage_aux_addr.ptr, sizeof(int) * I.naux,
+                                       cudaMemcpyHostToDevice, st));
+        irr_scatter_aux<<<(I.naux + 255) / 256, 256, 0, st>>>(I.naux, I.dstage_aux_addr.ptr, I.dstage_aux.ptr,
+                                                             I.aux.ptr);
+        NB6_CUDA_CHECK(cudaGetLastError());
+        for (int q = 0; q < I.naux; ++q) I.aux_slot[I.hstage_aux_addr.ptr[q]] = -1;
+        I.naux = 0;
+    }
     // keep only the latest list entry per particle
     int ne = 0;
     std::vector<int> &offs = I.flush_off;
@@ -477,6 +641,113 @@ void irr_firr_vec_impl(double ti, int ni, const int *addr, double (*acc)[3], dou
     I.num_steps += ni;
 }
 
+void hermite_open_impl(double eta_i, double smax, double dtmin) {
+    if (!I.open) {
+        nb6_fatal(NB6_ERR_NOT_OPEN);
+        return;
+    }
+    I.aux.reserve((size_t)I.nmax + 1);
+    NB6_CUDA_CHECK(cudaMemsetAsync(I.aux.ptr, 0, sizeof(Aux) * ((size_t)I.nmax + 1), nb6_stream()));
+    I.aux_slot.assign(I.nmax, -1);
+    I.naux = 0;
+    I.hp.eta_i = eta_i;
+    I.hp.smax = smax;
+    I.hp.dtmin = dtmin;
+    I.hermite = true;
+}
+
+void hermite_set_impl(int a, const double *fi, const double *fid, const double *fr, const double *frd,
+                      double step, double t0r, double stepr) {
+    if (!I.hermite) {
+        nb6_fatal(NB6_ERR_NOT_OPEN);
+        return;
+    }
+    if (a < 0 || a >= I.nmax) {
+        fprintf(stderr, "nb6_hermite_set: address %d outside [1, %d]\n", a + 1, I.nmax);
+        nb6_fatal(NB6_ERR_BAD_ARG);
+        return;
+    }
+    int slot = I.aux_slot[a];
+    if (slot < 0) {
+        slot = I.naux++;
+        I.aux_slot[a] = slot;
+        if ((size_t)I.naux > I.hstage_aux.cap) {
+            HostBuf<Aux> na;
+            HostBuf<int> nd;
+            na.reserve((size_t)I.naux * 2);
+            nd.reserve((size_t)I.naux * 2);
+            if (I.naux > 1) {
+                memcpy(na.ptr, I.hstage_aux.ptr, sizeof(Aux) * (I.naux - 1));
+                memcpy(nd.ptr, I.hstage_aux_addr.ptr, sizeof(int) * (I.naux - 1));
+            }
+            I.hstage_aux.release();
+            I.hstage_aux_addr.release();
+            I.hstage_aux = na;
+            I.hstage_aux_addr = nd;
+        }
+        I.hstage_aux_addr.ptr[slot] = a;
+    }
+    Aux &x = I.hstage_aux.ptr[slot];
+    for (int k = 0; k < 3; ++k) {
+        x.fi[k] = fi[k];
+        x.fid[k] = fid[k];
+        x.fr[k] = fr[k];
+        x.frd[k] = frd[k];
+    }
+    x.step = step;
+    x.t0r = t0r;
+    x.stepr = stepr;
+    x.pad = 0.0;
+}
+
+void irr_correct_impl(double time, int ni, const int *addr, double *out) {
+    if (!I.open || !I.hermite) {
+        nb6_fatal(NB6_ERR_NOT_OPEN);
+        return;
+    }
+    if (ni <= 0) return;
+    for (int k = 0; k < ni; ++k) {
+        if (addr[k] < 1 || addr[k] > I.nmax) {
+            fprintf(stderr, "nb6_irr_correct: address %d outside [1, %d]\n", addr[k], I.nmax);
+            nb6_fatal(NB6_ERR_BAD_ARG);
+            return;
+        }
+    }
+    const double t0 = nb6_wtime();
+    cudaStream_t st = nb6_stream();
+    const int *daddr = irr_flush(st, addr, ni);
+    const size_t rowd = 24;
+    I.hout.reserve((size_t)ni * rowd);
+    const bool direct = sizeof(double) * rowd * (size_t)ni <= zero_copy_bytes();
+    // forces of all active bodies into a device buffer, then the corrector
+    I.dout.reserve((size_t)ni * (8 + (direct ? 0 : rowd)));
+    double *force = I.dout.ptr;
+    double *o = direct ? I.hout.ptr : I.dout.ptr + (size_t)ni * 8;
+    if (!I.ev0) {
+        NB6_CUDA_CHECK(cudaEventCreate(&I.ev0));
+        NB6_CUDA_CHECK(cudaEventCreate(&I.ev1));
+    }
+    NB6_CUDA_CHECK(cudaEventRecord(I.ev0, st));
+    irr_kernel<<<(ni + IRR_WARPS - 1) / IRR_WARPS, IRR_WARPS * 32, 0, st>>>(ni, daddr, time, I.rec.ptr, I.lists.ptr,
+                                                                       I.lmax, I.nmax, force);
+    NB6_CUDA_CHECK(cudaGetLastError());
+    NB6_CUDA_CHECK(cudaEventRecord(I.ev1, st));
+    irr_apply_corrector<<<(ni + 127) / 128, 128, 0, st>>>(ni, daddr, time, force, I.rec.ptr, I.aux.ptr, I.hp, o);
+    NB6_CUDA_CHECK(cudaGetLastError());
+    if (!direct)
+        NB6_CUDA_CHECK(cudaMemcpyAsync(I.hout.ptr, o, sizeof(double) * rowd * ni, cudaMemcpyDeviceToHost, st));
+    nb6_status_fetch(st);
+    NB6_CUDA_CHECK(cudaStreamSynchronize(st));
+    if (nb6_check_dev_status() != 0) return;
+    memcpy(out, I.hout.ptr, sizeof(double) * rowd * ni);
+    unsigned long long inter = 0;
+    for (int k = 0; k < ni; ++k) inter += (unsigned long long)I.nnb_host[addr[k] - 1];
+    I.num_inter += inter;
+    I.time_grav += nb6_wtime() - t0;
+    I.num_fcall++;
+    I.num_steps += ni;
+}
+
 // The regular-force j set from the resident records: segments of
 // consecutive addresses, predicted to t on the device (see irr_predict_pack).
 void irr_predict_send_impl(double t, int nseg, const int *addr0, const int *count) {
@@ -556,6 +827,24 @@ void gpuirr_set_jp_(int *addr, double pos[3], double vel[3], double acc2[3], dou
     irr_set_jp_impl(*addr - 1, pos, vel, acc2, jrk6, *mass, *time);
 }
 void gpuirr_set_list_(int *addr, int *nblist) { irr_set_list_impl(*addr - 1, nblist); }
+
+// Extensions (no reference counterpart): the irregular corrector on the
+// device (the host's NBINT_COR / intgrt.F:533-581 work for each active body).
+// nb6_hermite_open_ allocates the per-body corrector state beside the records
+// (after irr_simd_open_); nb6_hermite_set_ stages a body's FI, FIDOT, FR,
+// FRDOT (irregular and regular force and derivative), STEP, T0R, STEPR, the
+// way irr_simd_set_jp_ stages its position record.  nb6_irr_correct_ then
+// does, for the active bodies at *time: neighbour force, Hermite corrector,
+// new irregular step, the regular-due test and, when no regular step is due,
+// the F/FDOT extrapolation -- updating the device state and returning per body
+// out[k][24] = x0[3], v0[3], fi[3], fidot[3], F[3], FDOT[3], step,
+// regular-due (0/1), nnbid, 0, 0, 0.
+void nb6_hermite_open_(double *eta_i, double *smax, double *dtmin) { hermite_open_impl(*eta_i, *smax, *dtmin); }
+void nb6_hermite_set_(int *addr, double fi[3], double fidot[3], double fr[3], double frdot[3], double *step,
+                      double *t0r, double *stepr) {
+    hermite_set_impl(*addr - 1, fi, fidot, fr, frdot, *step, *t0r, *stepr);
+}
+void nb6_irr_correct_(double *time, int *ni, int *addr, double *out) { irr_correct_impl(*time, *ni, addr, out); }
 
 // Extension (no reference counterpart): device time (ms) of the force
 // kernel of the last irr_simd_firr_vec_ call.

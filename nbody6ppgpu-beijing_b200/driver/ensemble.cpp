@@ -34,6 +34,7 @@ struct Ensemble : Bodies {
     std::vector<int> base, cnt, cl_of;
     double time = 0;
     std::vector<double> prop;  // learned dlog RS per row of the last regular_forces
+    std::vector<double> crow;  // device corrector rows of the last block
     // per-call buffers of the batched regular force, kept across calls (the
     // library writes every entry that is read back)
     std::vector<int> b_iseg, b_lst;
@@ -50,6 +51,16 @@ struct Ensemble : Bodies {
     void set_list(int i) {
         int a = i + 1;
         B.irr_set_list(&a, row(i));
+    }
+
+    // irregular corrector on the device (batched mode, backend permitting)
+    bool dev_corr() const { return batched && P.dev_corrector && B.irr_correct && B.hermite_set && B.hermite_open; }
+
+    void set_hermite(int i) {
+        int a = i + 1;
+        double s = step[i], tr = t0r[i], sr = stepr[i];
+        B.hermite_set(&a, &fi[3 * (size_t)i], &fidot[3 * (size_t)i], &fr[3 * (size_t)i], &frdot[3 * (size_t)i], &s,
+                      &tr, &sr);
     }
 
     // Regular force and new lists (global 1-based, self removed) of the
@@ -241,6 +252,11 @@ struct Ensemble : Bodies {
             init_forces(i, &freg[3 * (size_t)i], &fdr[3 * (size_t)i], &a[3 * (size_t)i], &jd[3 * (size_t)i]);
             set_jp(i);
         }
+        if (dev_corr()) {
+            double eta = P.eta_i, smax = P.smax, dtmin = P.dtmin;
+            B.hermite_open(&eta, &smax, &dtmin);
+            for (int i = 0; i < n; ++i) set_hermite(i);
+        }
         return true;
     }
 
@@ -300,17 +316,47 @@ struct Ensemble : Bodies {
             const double ti0 = wtime();
             double t = time;
             int nna = na;
-            B.irr_firr_vec(&t, &nna, addr.data(), (double(*)[3])a.data(), (double(*)[3])jd.data(), nnbid.data());
-            st.wall_irr += wtime() - ti0;
+            const bool dc = dev_corr();
             reg.clear();
-            w0 = wtime();
-            for (int q = 0; q < na; ++q)
-                if (irr_correct(active[q], time, &a[3 * (size_t)q], &jd[3 * (size_t)q])) reg.push_back(active[q]);
-            t_icor += wtime() - w0;
+            if (dc) {
+                // force + corrector + new step on the device; take back the
+                // corrected state so the host copy stays exact
+                crow.resize(24 * (size_t)na);
+                B.irr_correct(&t, &nna, addr.data(), crow.data());
+                st.wall_irr += wtime() - ti0;
+                w0 = wtime();
+                for (int q = 0; q < na; ++q) {
+                    const int i = active[q];
+                    const double *o = &crow[24 * (size_t)q];
+                    for (int c = 0; c < 3; ++c) {
+                        const size_t k = 3 * (size_t)i + c;
+                        x0[k] = o[c];
+                        v0[k] = o[3 + c];
+                        fi[k] = o[6 + c];
+                        fidot[k] = o[9 + c];
+                        f[k] = o[12 + c];
+                        fdot[k] = o[15 + c];
+                    }
+                    step[i] = o[18];
+                    t0[i] = time;
+                    st.irr_steps++;
+                    if (o[19] != 0.0) reg.push_back(i);
+                }
+                t_icor += wtime() - w0;
+            } else {
+                B.irr_firr_vec(&t, &nna, addr.data(), (double(*)[3])a.data(), (double(*)[3])jd.data(),
+                               nnbid.data());
+                st.wall_irr += wtime() - ti0;
+                w0 = wtime();
+                for (int q = 0; q < na; ++q)
+                    if (irr_correct(active[q], time, &a[3 * (size_t)q], &jd[3 * (size_t)q])) reg.push_back(active[q]);
+                t_icor += wtime() - w0;
+            }
             if (!reg.empty()) {
                 // corrected states of this block to the device before the
-                // j set is predicted there
-                if (batched && B.predict_send)
+                // j set is predicted there (already there when the device
+                // ran the corrector)
+                if (batched && B.predict_send && !dc)
                     for (int q = 0; q < na; ++q) set_jp(active[q]);
                 regular_forces(reg, freg, fdr, nl);
                 w0 = wtime();
@@ -329,7 +375,15 @@ struct Ensemble : Bodies {
                 t_rcor += wtime() - w0;
             }
             w0 = wtime();
-            for (int q = 0; q < na; ++q) set_jp(active[q]);
+            if (dc) {
+                // only the regular corrector changed state on the host
+                for (int i : reg) {
+                    set_jp(i);
+                    set_hermite(i);
+                }
+            } else {
+                for (int q = 0; q < na; ++q) set_jp(active[q]);
+            }
             t_jp += wtime() - w0;
             w0 = wtime();
             clock_push(active);

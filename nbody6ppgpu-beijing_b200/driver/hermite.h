@@ -48,6 +48,10 @@ struct nb6drive_params {
     // optional initial neighbour radii (one per body); null = RS0 sqrt(1+r^2)
     // (fpoly0.F:55), the reference's rule with RS0 from the input file
     const double *rs_init;
+    // ensemble driver, batched mode: 1 = irregular corrector on the device
+    // (nb6_irr_correct_) when the backend has it, 0 = on the host
+    int dev_corrector;
+    int pad2;
 };
 
 // Counters returned by the drivers.
@@ -85,6 +89,9 @@ typedef void (*fn_irr_set_list)(int *, int *);
 typedef void (*fn_irr_firr)(double *, int *, int *, double (*)[3], double (*)[3], int *);
 typedef void (*fn_proposals)(int *, double *);
 typedef void (*fn_profile)(int *);
+typedef void (*fn_hermite_open)(double *, double *, double *);
+typedef void (*fn_hermite_set)(int *, double *, double *, double *, double *, double *, double *, double *);
+typedef void (*fn_irr_correct)(double *, int *, int *, double *);
 
 struct Backend {
     void *hreg = nullptr, *hirr = nullptr, *hpot = nullptr;
@@ -103,6 +110,9 @@ struct Backend {
     fn_pred_send predict_send = nullptr;
     fn_proposals proposals = nullptr;
     fn_profile reg_profile = nullptr, irr_profile = nullptr;  // the libraries' timing lines
+    fn_hermite_open hermite_open = nullptr;                    // device irregular corrector
+    fn_hermite_set hermite_set = nullptr;
+    fn_irr_correct irr_correct = nullptr;
 };
 
 inline void *must_sym(void *h, const char *name) {
@@ -138,6 +148,9 @@ inline bool load_backend(Backend &b, const char *reg, const char *irr, const cha
     b.proposals = (fn_proposals)dlsym(b.hreg, "nb6_regf_proposals_");
     b.reg_profile = (fn_profile)dlsym(b.hreg, "gpunb_profile_");
     b.irr_profile = (fn_profile)dlsym(b.hirr, "irr_simd_profile_");
+    b.hermite_open = (fn_hermite_open)dlsym(b.hirr, "nb6_hermite_open_");
+    b.hermite_set = (fn_hermite_set)dlsym(b.hirr, "nb6_hermite_set_");
+    b.irr_correct = (fn_irr_correct)dlsym(b.hirr, "nb6_irr_correct_");
     return b.gpunb_open && b.gpunb_close && b.gpunb_send && b.gpunb_regf && b.gpupot &&
            b.irr_open && b.irr_close && b.irr_set_jp && b.irr_set_list && b.irr_firr_vec;
 }

@@ -63,3 +63,20 @@ def test_ensemble_batched_energy_matches_alone(nb6):
     # the same initial energies (same bodies, FP64-accurate potentials)
     e0 = np.array([drive.run(ours, cl.mass, cl.pos, cl.vel, tcrit=0.0).etot[0] for cl in cls])
     np.testing.assert_allclose(ens.energy[0, :, 2], e0, rtol=1e-12)
+
+
+def test_device_corrector_equals_host_corrector_bit_for_bit(nb6):
+    """The batched ensemble with the irregular corrector on the device
+    (nb6_irr_correct_) follows exactly the trajectory of the same run with
+    the corrector on the host: same final state and energies, bit for bit."""
+    from nb6b200 import drive
+    ours = drive.backend_paths("nb6b200")
+    cls = _clusters(4, 80)
+    dev = drive.run_ensemble(ours, cls, batched=True, dev_corrector=True, tcrit=0.5, dt_out=0.125)
+    host = drive.run_ensemble(ours, cls, batched=True, dev_corrector=False, tcrit=0.5, dt_out=0.125)
+    assert dev.stats["irr_steps"] == host.stats["irr_steps"] > 0
+    assert dev.stats["reg_steps"] == host.stats["reg_steps"]
+    for c in range(len(cls)):
+        np.testing.assert_array_equal(dev.x[c], host.x[c])
+        np.testing.assert_array_equal(dev.v[c], host.v[c])
+    np.testing.assert_array_equal(dev.energy, host.energy)
