@@ -1,5 +1,5 @@
 """The same block-step driver on libnb6b200 (GPU) and on the reference's own
-CPU libraries.  Config 1: Plummer N = 1024, equal masses, Henon units,
+CPU libraries.  Plummer N = 1024, equal masses, Henon units,
 integrated to T = 1; energy drift over 10 N-body times compared with the
 reference's under the identical driver (contract: within 10%; a smaller drift
 passes)."""

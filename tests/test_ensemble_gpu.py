@@ -1,4 +1,4 @@
-"""Ensemble of independent clusters on libnb6b200 (config 4's method at small
+"""Ensemble of independent clusters on libnb6b200 (the 256-cluster method at small
 size): every force kind issued once per block for all clusters
 (nb6_irr_predict_send_ + nb6_regf_seg_ + one irr_simd_firr_vec_), against
 each cluster integrated alone with the plain method on the same GPU."""

@@ -1,4 +1,4 @@
-"""Config 2: Plummer N = 65,536 with a Kroupa IMF, the active set of each
+"""Plummer N = 65,536 with a Kroupa IMF: the active set of each
 power-of-two timestep level (a block at a time that is a multiple of 2^-l
 activates every body whose regular step is at most 2^-l).  Levels are drawn
 so that each holds about half the bodies of the one above, so N_active runs

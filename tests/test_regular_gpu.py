@@ -185,7 +185,7 @@ def test_regular_i_not_in_j_set(nb6, orc):
 
 
 def test_regular_mid_size_kroupa(nb6, orc):
-    """N = 65,536 Plummer + Kroupa (config 2's model), 1024 active."""
+    """N = 65,536 Plummer + Kroupa IMF, 1024 active."""
     from nb6b200 import ics
     cl = ics.plummer(65536, seed=2026, imf=True)
     isel = np.sort(np.random.default_rng(0).choice(cl.n, 1024, replace=False))
