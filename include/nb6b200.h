@@ -171,7 +171,7 @@ float nb6_irr_last_kernel_ms_(void);
  * host's NBINT_COR work of nbint_cor.f:113-173,215-236 and intgrt.F:533-581
  * per active body).  After irr_simd_open_: nb6_hermite_open_ allocates the
  * per-body state; nb6_hermite_set_ stages a body's FI, FIDOT, FR, FRDOT,
- * STEP, T0R, STEPR (1-based address) like irr_simd_set_jp_ stages its
+ * STEP, T0R, STEPR, RS (1-based address) like irr_simd_set_jp_ stages its
  * record.  nb6_irr_correct_ computes the neighbour force of the active
  * bodies at *time, applies the corrector, chooses the new irregular step,
  * tests whether the regular step is due and otherwise extrapolates F and
@@ -182,8 +182,36 @@ float nb6_irr_last_kernel_ms_(void);
  * counterpart: the reference corrects on the host. */
 void nb6_hermite_open_(double *eta_i, double *smax, double *dtmin);
 void nb6_hermite_set_(int *addr, double fi[3], double fidot[3], double fr[3], double frdot[3],
-                      double *step, double *t0r, double *stepr);
+                      double *step, double *t0r, double *stepr, double *rs);
 void nb6_irr_correct_(double *time, int *ni, int *addr, double *out);
+
+/* Regular force plus regular corrector on the device (the host's REGCOR_GPU
+ * work of regcor_gpu.F:131-196 radius update, :284-444 neighbour gain/loss
+ * force moves, :442-537 corrector, :593-737 new regular step), after
+ * nb6_irr_predict_send_ has put the j set of the segments on the device and
+ * the irregular corrector of the block has run.  addr[ni] are the bodies
+ * (1-based, grouped by segment iseg[k]); segment c is j range
+ * [seg_j0[c], seg_j0[c+1]) holding the bodies from address seg_a0[c] on.
+ * h2, dtr, xi, vi, lmax, nnbmax, m_flag as for nb6_regf_seg_; rs[k] is the
+ * radius h2[k] was formed from; prm = {ETAR, SMAX, DTMIN, 25 / TCR, NNBOPT,
+ * learned-radius mode (0, or 2 to take the network's proposal as in the
+ * driver)}.  Each body whose list fits gets its
+ * radius, neighbour list, Hermite state and regular step updated on the
+ * device; out[k][32] = x0[3], v0[3], fi[3], fidot[3], fr[3], frdot[3],
+ * F[3], FDOT[3], step, stepr, rs, nnb, overflow (-nnb, else 0),
+ * learned-radius outcome (0 none, 1 taken, 2 fallback), 0, 0.  An
+ * overflowed body is left as it was, for the caller to shrink its radius
+ * and call again with it on the same j set (util_gpu.F:69-100).
+ * Operations are rounded as in the driver's host corrector: the same bits
+ * with the learned radius off. */
+void nb6_regf_correct_(double *time, int *ni, int *addr, int *iseg, int *nseg, int *seg_j0, int *seg_a0,
+                       double *h2, double *dtr, double *rs, double (*xi)[3], double (*vi)[3], int *lmax,
+                       int *nnbmax, int *m_flag, double *prm, double *out);
+/* The device-resident state of bodies *a0 .. *a0 + *n - 1 (1-based), for a
+ * host that lets the device correctors keep it (energy output, the end of
+ * a run): rows of 32 doubles x0[3], v0[3], F[3], FDOT[3], fi[3], fidot[3],
+ * fr[3], frdot[3], t0, step, t0r, stepr, rs, mass, 0, 0. */
+void nb6_hermite_get_(int *a0, int *n, double *out);
 
 /* Learned neighbour radius (no reference counterpart; its fallback is the
  * reference's Ahmad-Cohen rule, regcor_gpu.F:131-196).  A 5-64-64-1 SiLU

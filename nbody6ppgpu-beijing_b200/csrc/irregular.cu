@@ -145,7 +145,7 @@ __global__ void __launch_bounds__(IRR_WARPS * 32)
 // so device and host give the same bits.
 // ----------------------------------------------------------------------------
 struct Aux {  // 16 doubles
-    double fi[3], fid[3], fr[3], frd[3], step, t0r, stepr, pad;
+    double fi[3], fid[3], fr[3], frd[3], step, t0r, stepr, rs;
 };
 
 struct HermiteParams {
@@ -250,6 +250,258 @@ __global__ void irr_apply_corrector(int ni, const int *__restrict__ addr, double
     o[19] = regdue ? 1.0 : 0.0;
     o[20] = (double)id;
     o[21] = o[22] = o[23] = 0.0;
+}
+
+// ----------------------------------------------------------------------------
+// Device-resident regular corrector (nb6_regf_correct_): the host's
+// Bodies::reg_correct (regcor_gpu.F:131-196 radius update, :284-444
+// neighbour gain/loss force moves, :442-537 corrector, :593-737 new regular
+// step) for every body of a segmented regular-force call whose list did not
+// overflow, one thread per body, every operation rounded as on the host.
+// Neighbours are taken from the predicted j set of the call (the state of
+// every body at the block time before any regular correction -- the host's
+// snapshot), the old list from the resident list rows, the new one from the
+// call's output rows.
+// ----------------------------------------------------------------------------
+struct RegCorrParams {
+    double eta_r, smax, dtmin, rsfac;
+    int nnbopt, nnbmax, cap, mlp_mode;
+};
+
+// host Bodies::pair_force: FP64 force and jerk of j (at xj, vj, mass mj) on i
+NB6_DEV void pair_force_dev(const double *xi, const double *vi, const double *xj, const double *vj, double mj,
+                            double *a, double *jd) {
+    const double dx = dsub(xj[0], xi[0]), dy = dsub(xj[1], xi[1]), dz = dsub(xj[2], xi[2]);
+    const double dvx = dsub(vj[0], vi[0]), dvy = dsub(vj[1], vi[1]), dvz = dsub(vj[2], vi[2]);
+    const double r2 = dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz));
+    const double dr2i = ddiv(1.0, r2), dr3i = dmul(dmul(mj, dr2i), __dsqrt_rn(dr2i));
+    const double drdp = dmul(dmul(3.0, dadd(dadd(dmul(dx, dvx), dmul(dy, dvy)), dmul(dz, dvz))), dr2i);
+    a[0] = dmul(dx, dr3i);
+    a[1] = dmul(dy, dr3i);
+    a[2] = dmul(dz, dr3i);
+    jd[0] = dmul(dsub(dvx, dmul(dx, drdp)), dr3i);
+    jd[1] = dmul(dsub(dvy, dmul(dy, drdp)), dr3i);
+    jd[2] = dmul(dsub(dvz, dmul(dz, drdp)), dr3i);
+}
+
+// out row k (32 doubles): x0[3], v0[3], fi[3], fidot[3], fr[3], frdot[3],
+// F[3], FDOT[3], step, stepr, rs, nnb (self removed), overflow (-nnb of an
+// overflowed row, else 0), learned-radius outcome (0 off, 1 taken, 2
+// fallback), 0, 0.
+__global__ void reg_corrector_kernel(int ni, const int *__restrict__ addr, const int *__restrict__ iseg,
+                                     const int *__restrict__ seg_j0, const int *__restrict__ seg_a0, double time,
+                                     RegDeviceOut ro, Rec *__restrict__ rec, Aux *__restrict__ aux,
+                                     int *__restrict__ lists, int ls, const double *__restrict__ rs_in,
+                                     RegCorrParams p, double *__restrict__ out, int *status) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= ni) return;
+    const int i = addr[k] - 1, sg = iseg[k];
+    const double *of = ro.outf + (size_t)k * 8;
+    const int *ol = ro.outl + (size_t)k * ro.W;
+    double *o = out + (size_t)k * 32;
+    for (int c = 0; c < 32; ++c) o[c] = 0.0;
+    const int raw = ol[0];
+    if (raw < 0 || raw > p.cap) {  // overflow: the host shrinks RS and asks again
+        o[28] = (double)(raw < 0 ? raw : -raw);
+        return;
+    }
+    const int base = seg_a0[sg], jb = seg_j0[sg], nj = seg_j0[sg + 1] - jb;
+    Rec r = rec[i];
+    Aux x = aux[i];
+    int *orow = lists + (size_t)i * ls;
+    const int nnb0 = min(max(orow[0], 0), ls - 1);
+    int self_in = 0;  // i itself is in the call's list when it belongs to the segment
+    for (int l = 1; l <= raw; ++l)
+        if (base + ol[l] == i) self_in = 1;
+    const int nnb = raw - self_in;
+    const double dtr = dsub(time, x.t0r);
+    const double xi[3] = {r.x[0], r.x[1], r.x[2]}, vi[3] = {r.v[0], r.v[1], r.v[2]};
+    const double ri2 = dadd(dadd(dmul(xi[0], xi[0]), dmul(xi[1], xi[1])), dmul(xi[2], xi[2]));
+    const double znbmin = dmul(0.2, (double)p.nnbopt);
+    double rs = rs_in[k];  // the radius the call's h2 was formed from
+    const double rs_used = rs;
+    // Ahmad-Cohen radius update (regcor_gpu.F:131-196, NB_FLAG = 0 form)
+    if (nnb > 0) {
+        const double fac = dadd(1.0, ddiv(dmul(0.1, (double)(p.nnbopt - nnb)), (double)nnb));
+        double a3 = dmul((double)nnb, fac);
+        const int zi = (int)znbmin;
+        const int nbave_i = min(p.nnbopt + 150, max(p.nnbmax - 50, zi));
+        const double nbave = (double)nbave_i;
+        const double cap9 = dmul(0.9, nbave);
+        a3 = (cap9 < a3) ? cap9 : a3;
+        const int nbp = (int)a3;
+        a3 = (a3 < znbmin) ? znbmin : a3;
+        double a4 = ddiv(a3, (double)nnb);
+        if (dmul(dsub(a3, (double)nnb0), dsub(a3, (double)nnb)) < 0.0) a4 = __dsqrt_rn(a4);
+        const double rd = dmul(p.rsfac, dtr);
+        const double a5 = (0.25 < rd) ? 0.25 : rd;
+        a4 = dsub(a4, 1.0);
+        const double na5 = -a5;
+        a4 = a4 > a5 ? a5 : ((a4 < na5) ? na5 : a4);
+        const double a3b = ddiv(a4, 3.0);
+        double a1 = dsub(dadd(1.0, a3b), dmul(a3b, a3b));
+        if (nnb < znbmin && nbp > znbmin && a1 < 1.0) a1 = 1.05;
+        if (fabs(dsub(a1, 1.0)) > 0.003) {
+            const double rs2 = dmul(rs, rs);
+            if (rs2 > ri2 && rs2 < dmul(2.0, ri2) && nnb > 5) a1 = __dsqrt_rn(a1);
+            rs = dmul(rs, a1);
+        }
+        const double ridot = dadd(dadd(dmul(xi[0], vi[0]), dmul(xi[1], vi[1])), dmul(xi[2], vi[2]));
+        if ((double)nnb > nbave && ridot < 0.0)
+            rs = dmul(rs, dsub(1.0, ddiv((double)nnb - nbave, dmul(3.0, (double)nnb))));
+    } else {
+        rs = dmul(rs, 1.5);  // zero membership (fpoly0.F:140-160)
+    }
+    // neighbour gains and losses (regcor_gpu.F:284-444); ids are 0-based
+    // global addresses, the new list's are relative to the segment
+    double dfirr[3] = {0, 0, 0}, dfd[3] = {0, 0, 0};
+    int a = 1, b = 1;
+    auto next_new = [&](int &bb) {  // skip self in the new list
+        while (bb <= raw && base + ol[bb] == i) ++bb;
+    };
+    next_new(b);
+    while (a <= nnb0 || b <= raw) {
+        const int jo = a <= nnb0 ? orow[a] : 0x7fffffff;
+        const int jn = b <= raw ? base + ol[b] : 0x7fffffff;
+        if (jo == jn) {
+            ++a;
+            ++b;
+            next_new(b);
+            continue;
+        }
+        const int j = jo < jn ? jo : jn;
+        if (j < base || j - base >= nj) {  // a neighbour outside the body's segment
+            set_status(status, NB6_ERR_BAD_ARG);
+            return;
+        }
+        const size_t q = (size_t)(jb + (j - base));
+        const double xj[3] = {ro.jx[3 * q], ro.jx[3 * q + 1], ro.jx[3 * q + 2]};
+        const double vj[3] = {ro.jv[3 * q], ro.jv[3 * q + 1], ro.jv[3 * q + 2]};
+        double fa[3], fj[3];
+        pair_force_dev(xi, vi, xj, vj, ro.jm[q], fa, fj);
+        if (jo < jn) {  // lost
+            for (int c = 0; c < 3; ++c) {
+                dfirr[c] = dsub(dfirr[c], fa[c]);
+                dfd[c] = dsub(dfd[c], fj[c]);
+            }
+            ++a;
+        } else {  // gained
+            for (int c = 0; c < 3; ++c) {
+                dfirr[c] = dadd(dfirr[c], fa[c]);
+                dfd[c] = dadd(dfd[c], fj[c]);
+            }
+            ++b;
+            next_new(b);
+        }
+    }
+    // regular corrector (regcor_gpu.F:442-537)
+    const double dtsq = dmul(dtr, dtr), dt6 = ddiv(6.0, dmul(dtr, dtsq)), dt2 = ddiv(2.0, dtsq);
+    const double dtsq12 = ddiv(dtsq, 12.0), dtr13 = ddiv(dtr, 3.0);
+    double d2r[3], d3r[3];
+    for (int c = 0; c < 3; ++c) {
+        const double dfr = dsub(dsub(x.fr[c], of[c]), dfirr[c]);
+        const double fdr0 = dadd(of[3 + c], dfd[c]);
+        const double frd = x.frd[c];
+        const double sum = dadd(frd, fdr0);
+        const double at3 = dadd(dmul(2.0, dfr), dmul(dtr, sum));
+        const double bt2 = dsub(dmul(-3.0, dfr), dmul(dtr, dadd(sum, frd)));
+        r.x[c] = dadd(r.x[c], dmul(dadd(dmul(0.6, at3), bt2), dtsq12));
+        r.v[c] = dadd(r.v[c], dmul(dadd(dmul(0.75, at3), bt2), dtr13));
+        x.fi[c] = dadd(x.fi[c], dfirr[c]);
+        x.fr[c] = of[c];
+        x.fid[c] = dadd(x.fid[c], dfd[c]);
+        x.frd[c] = of[3 + c];
+        d3r[c] = dmul(at3, dt6);
+        d2r[c] = dmul(dadd(dmul(3.0, at3), bt2), dt2);
+    }
+    // the new list into the resident rows (after the merge has read the old)
+    int w = 1;
+    for (int l = 1; l <= raw; ++l)
+        if (base + ol[l] != i) orow[w++] = base + ol[l];
+    orow[0] = nnb;
+    // new regular step (regcor_gpu.F:593-737)
+    double ttmp = tstep_dev(x.fr, x.frd, d2r, d3r, p.eta_r);
+    const double dt0 = ttmp;
+    if (ttmp > dmul(2.0, x.stepr)) {
+        const double two = dmul(2.0, dtr);
+        ttmp = (fmod(time, two) == 0.0) ? (p.smax < two ? p.smax : two) : x.stepr;
+    } else if (ttmp < dtr) {
+        ttmp = dmul(0.5, dtr);
+        if (ttmp > dt0) ttmp = dmul(ttmp, 0.5);
+    } else {
+        ttmp = x.stepr;
+    }
+    ttmp = (p.smax < ttmp) ? p.smax : ttmp;
+    ttmp = (ttmp < p.dtmin) ? p.dtmin : ttmp;
+    x.stepr = ttmp;
+    x.t0r = time;
+    for (int c = 0; c < 3; ++c) {
+        r.f[c] = dmul(0.5, dadd(x.fi[c], x.fr[c]));
+        r.fd[c] = ddiv(dadd(x.fid[c], x.frd[c]), 6.0);
+    }
+    if (x.step > x.stepr) x.step = x.stepr;
+    // learned radius (Bodies::learn_apply): take RS_used exp(dlog) when the
+    // count it implies stays in [NNBOPT/2, NNBMAX]
+    double outcome = 0.0;
+    if (p.mlp_mode == 2) {
+        const double lim = 0.69314718055994531;
+        double dl = of[7];
+        dl = dl > lim ? lim : (dl < -lim ? -lim : dl);
+        const double expect = dmul((double)nnb, exp(dmul(3.0, dl)));
+        if (nnb > 0 && dl == dl && expect >= dmul(0.5, (double)p.nnbopt) && expect <= (double)p.nnbmax) {
+            rs = dmul(rs_used, exp(dl));
+            outcome = 1.0;
+        } else {
+            outcome = 2.0;
+        }
+    }
+    x.rs = rs;
+    rec[i] = r;
+    aux[i] = x;
+    for (int c = 0; c < 3; ++c) {
+        o[c] = r.x[c];
+        o[3 + c] = r.v[c];
+        o[6 + c] = x.fi[c];
+        o[9 + c] = x.fid[c];
+        o[12 + c] = x.fr[c];
+        o[15 + c] = x.frd[c];
+        o[18 + c] = r.f[c];
+        o[21 + c] = r.fd[c];
+    }
+    o[24] = x.step;
+    o[25] = x.stepr;
+    o[26] = rs;
+    o[27] = (double)nnb;
+    o[29] = outcome;
+}
+
+// The resident Hermite state of addresses a0 .. a0+n-1 (0-based), one row
+// of 32 doubles each: x0[3], v0[3], F[3], FDOT[3], fi[3], fidot[3], fr[3],
+// frdot[3], t0, step, t0r, stepr, rs, m, 0, 0.
+__global__ void hermite_gather(int a0, int n, const Rec *__restrict__ rec, const Aux *__restrict__ aux,
+                               double *__restrict__ out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const Rec r = rec[a0 + k];
+    const Aux x = aux[a0 + k];
+    double *o = out + (size_t)k * 32;
+    for (int c = 0; c < 3; ++c) {
+        o[c] = r.x[c];
+        o[3 + c] = r.v[c];
+        o[6 + c] = r.f[c];
+        o[9 + c] = r.fd[c];
+        o[12 + c] = x.fi[c];
+        o[15 + c] = x.fid[c];
+        o[18 + c] = x.fr[c];
+        o[21 + c] = x.frd[c];
+    }
+    o[24] = r.t0;
+    o[25] = x.step;
+    o[26] = x.t0r;
+    o[27] = x.stepr;
+    o[28] = x.rs;
+    o[29] = r.m;
+    o[30] = o[31] = 0.0;
 }
 
 // Scatter staged Aux records: slot s goes to particle saddr[s].
@@ -657,7 +909,7 @@ void hermite_open_impl(double eta_i, double smax, double dtmin) {
 }
 
 void hermite_set_impl(int a, const double *fi, const double *fid, const double *fr, const double *frd,
-                      double step, double t0r, double stepr) {
+                      double step, double t0r, double stepr, double rs) {
     if (!I.hermite) {
         nb6_fatal(NB6_ERR_NOT_OPEN);
         return;
@@ -697,7 +949,7 @@ void hermite_set_impl(int a, const double *fi, const double *fid, const double *
     x.step = step;
     x.t0r = t0r;
     x.stepr = stepr;
-    x.pad = 0.0;
+    x.rs = rs;
 }
 
 void irr_correct_impl(double time, int ni, const int *addr, double *out) {
@@ -746,6 +998,93 @@ void irr_correct_impl(double time, int ni, const int *addr, double *out) {
     I.time_grav += nb6_wtime() - t0;
     I.num_fcall++;
     I.num_steps += ni;
+}
+
+void hermite_get_impl(int a0, int n, double *out) {
+    if (!I.open || !I.hermite) {
+        nb6_fatal(NB6_ERR_NOT_OPEN);
+        return;
+    }
+    if (n <= 0) return;
+    if (a0 < 1 || (long long)a0 - 1 + n > I.nmax) {
+        fprintf(stderr, "nb6_hermite_get: range outside [1, %d]\n", I.nmax);
+        nb6_fatal(NB6_ERR_BAD_ARG);
+        return;
+    }
+    cudaStream_t st = nb6_stream();
+    irr_flush(st);
+    I.dout.reserve((size_t)n * 32);
+    hermite_gather<<<(n + 127) / 128, 128, 0, st>>>(a0 - 1, n, I.rec.ptr, I.aux.ptr, I.dout.ptr);
+    NB6_CUDA_CHECK(cudaGetLastError());
+    NB6_CUDA_CHECK(cudaMemcpyAsync(out, I.dout.ptr, sizeof(double) * 32 * (size_t)n, cudaMemcpyDeviceToHost, st));
+    NB6_CUDA_CHECK(cudaStreamSynchronize(st));
+}
+
+void regf_correct_impl(double time, int ni, const int *addr, int *iseg, int nseg, int *seg_j0, const int *seg_a0,
+                       double *h2, double *dtr, const double *rs, double (*xi)[3], double (*vi)[3], int lmax,
+                       int nnbmax, int mflag, const double *prm, double *out) {
+    if (!I.open || !I.hermite) {
+        nb6_fatal(NB6_ERR_NOT_OPEN);
+        return;
+    }
+    if (ni <= 0) return;
+    bool bad = lmax > I.lmax || nseg <= 0;
+    for (int k = 0; k < ni && !bad; ++k) bad = addr[k] < 1 || addr[k] > I.nmax;
+    for (int c = 0; c < nseg && !bad; ++c) bad = seg_a0[c] < 1 || seg_a0[c] > I.nmax;
+    if (bad) {
+        fprintf(stderr, "nb6_regf_correct: bad address, segment or lmax (> %d)\n", I.lmax);
+        nb6_fatal(NB6_ERR_BAD_ARG);
+        return;
+    }
+    const double t0 = nb6_wtime();
+    cudaStream_t st = nb6_stream();
+    irr_flush(st);  // state staged by the host first
+    RegDeviceOut ro;
+    if (!regular_seg_on_device(ni, iseg, h2, dtr, xi, vi, lmax, nnbmax, mflag, nseg, seg_j0, &ro)) return;
+    // [addr | iseg | seg_j0 (nseg+1) | seg_a0 - 1 (nseg) | pad | rs (ni doubles)]
+    const size_t nint = 2 * (size_t)ni + 2 * (size_t)nseg + 1, nint2 = (nint + 1) & ~(size_t)1;
+    I.hseg.reserve(nint2 + 2 * (size_t)ni);
+    I.dseg.reserve(nint2 + 2 * (size_t)ni);
+    int *h = I.hseg.ptr;
+    memcpy(h + nint2, rs, sizeof(double) * ni);
+    memcpy(h, addr, sizeof(int) * ni);
+    memcpy(h + ni, iseg, sizeof(int) * ni);
+    memcpy(h + 2 * (size_t)ni, seg_j0, sizeof(int) * (nseg + 1));
+    for (int c = 0; c < nseg; ++c) h[2 * (size_t)ni + nseg + 1 + c] = seg_a0[c] - 1;
+    NB6_CUDA_CHECK(cudaMemcpyAsync(I.dseg.ptr, h, sizeof(int) * (nint2 + 2 * (size_t)ni), cudaMemcpyHostToDevice,
+                                   st));
+    const int *d = I.dseg.ptr;
+    const double *drs = reinterpret_cast<const double *>(I.dseg.ptr + nint2);
+    RegCorrParams p;
+    p.eta_r = prm[0];
+    p.smax = prm[1];
+    p.dtmin = prm[2];
+    p.rsfac = prm[3];
+    p.nnbopt = (int)prm[4];
+    p.nnbmax = nnbmax;
+    p.cap = std::max(0, std::min(nnbmax, lmax - 1));
+    p.mlp_mode = (int)prm[5];
+    const size_t rowd = 32;
+    I.hout.reserve((size_t)ni * rowd);
+    const bool direct = sizeof(double) * rowd * (size_t)ni <= zero_copy_bytes();
+    double *o = I.hout.ptr;
+    if (!direct) {
+        I.dout.reserve((size_t)ni * rowd);
+        o = I.dout.ptr;
+    }
+    reg_corrector_kernel<<<(ni + 127) / 128, 128, 0, st>>>(ni, d, d + ni, d + 2 * (size_t)ni,
+                                                         d + 2 * (size_t)ni + nseg + 1, time, ro, I.rec.ptr, I.aux.ptr,
+                                                         I.lists.ptr, I.lmax, drs, p, o, nb6_dev_status());
+    NB6_CUDA_CHECK(cudaGetLastError());
+    if (!direct)
+        NB6_CUDA_CHECK(cudaMemcpyAsync(I.hout.ptr, o, sizeof(double) * rowd * ni, cudaMemcpyDeviceToHost, st));
+    nb6_status_fetch(st);
+    NB6_CUDA_CHECK(cudaStreamSynchronize(st));
+    if (nb6_check_dev_status() != 0) return;
+    memcpy(out, I.hout.ptr, sizeof(double) * rowd * ni);
+    for (int k = 0; k < ni; ++k)
+        if (out[rowd * k + 28] == 0.0) I.nnb_host[addr[k] - 1] = (int)out[rowd * k + 27];
+    I.time_grav += nb6_wtime() - t0;
 }
 
 // The regular-force j set from the resident records: segments of
@@ -841,10 +1180,37 @@ void gpuirr_set_list_(int *addr, int *nblist) { irr_set_list_impl(*addr - 1, nbl
 // regular-due (0/1), nnbid, 0, 0, 0.
 void nb6_hermite_open_(double *eta_i, double *smax, double *dtmin) { hermite_open_impl(*eta_i, *smax, *dtmin); }
 void nb6_hermite_set_(int *addr, double fi[3], double fidot[3], double fr[3], double frdot[3], double *step,
-                      double *t0r, double *stepr) {
-    hermite_set_impl(*addr - 1, fi, fidot, fr, frdot, *step, *t0r, *stepr);
+                      double *t0r, double *stepr, double *rs) {
+    hermite_set_impl(*addr - 1, fi, fidot, fr, frdot, *step, *t0r, *stepr, *rs);
 }
 void nb6_irr_correct_(double *time, int *ni, int *addr, double *out) { irr_correct_impl(*time, *ni, addr, out); }
+
+// The resident state of bodies a0 .. a0+n-1 (1-based), rows of 32
+// doubles: x0[3], v0[3], F[3], FDOT[3], fi[3], fidot[3], fr[3], frdot[3],
+// t0, step, t0r, stepr, rs, mass, 0, 0.
+void nb6_hermite_get_(int *a0, int *n, double *out) { hermite_get_impl(*a0, *n, out); }
+
+// Regular force plus the regular corrector on the device for the bodies
+// addr[ni] (1-based, grouped by segment iseg[k]; segment c is the j range
+// [seg_j0[c], seg_j0[c+1]) of the current j set and holds the bodies from
+// address seg_a0[c] on, as nb6_irr_predict_send_ lays them out).  h2, dtr,
+// xi, vi, lmax, nnbmax, m_flag as for nb6_regf_seg_.  prm = {ETAR, SMAX,
+// DTMIN, 25 / TCR, NNBOPT, learned-radius mode (0 or 2)}; rs[k] is the
+// radius body k's h2 was formed from (the device copy is replaced by the
+// corrector's result).  For every body
+// whose list fits: the Ahmad-Cohen radius update, the neighbour gain/loss
+// force moves, the corrector, the new regular step and, in mode 2, the
+// learned proposal -- updating the resident state and neighbour list --
+// with out[k][32] = x0[3], v0[3], fi[3], fidot[3], fr[3], frdot[3], F[3],
+// FDOT[3], step, stepr, rs, nnb, overflow (-nnb, else 0), learned outcome,
+// 0, 0.  Overflowed bodies are left untouched for the caller's radius
+// shrink and retry with the smaller rs (util_gpu.F:69-100).
+void nb6_regf_correct_(double *time, int *ni, int *addr, int *iseg, int *nseg, int *seg_j0, int *seg_a0,
+                       double *h2, double *dtr, double *rs, double (*xi)[3], double (*vi)[3], int *lmax,
+                       int *nnbmax, int *m_flag, double *prm, double *out) {
+    regf_correct_impl(*time, *ni, addr, iseg, *nseg, seg_j0, seg_a0, h2, dtr, rs, xi, vi, *lmax, *nnbmax, *m_flag,
+                      prm, out);
+}
 
 // Extension (no reference counterpart): device time (ms) of the force
 // kernel of the last irr_simd_firr_vec_ call.

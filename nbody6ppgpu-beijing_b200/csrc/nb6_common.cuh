@@ -219,6 +219,19 @@ NB6_DEV void set_status(int *status, int code) { atomicCAS(status, 0, code); }
         }                                                                          \
     } while (0)
 
+// Results of a segmented regular-force call left on the device for a
+// following kernel (see regular_seg_on_device): outf [ni][8] = (acc, jrk,
+// pot, proposal), outl [ni][W] = [nnb, ids relative to the segment], and the
+// predicted FP64 j set (m, x, v) the call used.
+struct RegDeviceOut {
+    const double *outf;
+    const int *outl;
+    int W;
+    const double *jm, *jx, *jv;
+};
+bool regular_seg_on_device(int ni, int *iseg, double *h2, double *dtr, double (*xi)[3], double (*vi)[3], int lmax,
+                           int nnbmax, int mflag, int nseg, int *seg_j0, RegDeviceOut *out);
+
 extern "C" int nb6_last_status_();
 void nb6_fatal(int code);          // records status and aborts unless disabled
 void nb6_set_host_status(int code); // records status without aborting

@@ -2204,6 +2204,10 @@ static void selfcheck_rows(int ni, const double *h2, const double *dtr, const do
     }
 }
 
+// Set while regular_seg_on_device runs nb6_regf_seg_: results stay in the
+// device buffers and nothing is synchronised or unpacked.
+static bool g_seg_keep_device = false;
+
 template <bool MF> static const void *seg_kernel_of(int ib) {
     switch (ib) {
         case 1: return (const void *)regf_seg_kernel<1, MF>;
@@ -2488,11 +2492,17 @@ void nb6_regf_seg_(int *ni_, int *iseg, double *h2, double *dtr, double (*xi)[3]
     if (smem > 48 * 1024)
         NB6_CUDA_CHECK(cudaFuncSetAttribute(regf_finalize_seg, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)smem));
-    const bool direct = nb6_uva();  // finalize writes the pinned host staging in place
+    // finalize writes the pinned host staging in place, unless a device
+    // kernel consumes the results (regular_seg_on_device)
+    const bool direct = nb6_uva() && !g_seg_keep_device;
     regf_finalize_seg<<<(ni + FIN_WARPS - 1) / FIN_WARPS, FIN_WARPS * 32, smem, st>>>(
         R.part.ptr, d_pinfo, ni, R.nbcnt.ptr, R.nbbuf.ptr, a.lcap, cap, W, pmax,
         direct ? R.houtf.ptr : R.outf.ptr, direct ? R.houtl.ptr : R.outl.ptr, mlp);
     NB6_CUDA_CHECK(cudaGetLastError());
+    if (g_seg_keep_device) {
+        R.time_grav += nb6_wtime();
+        return;
+    }
     if (!direct) {
         NB6_CUDA_CHECK(cudaMemcpyAsync(R.houtf.ptr, R.outf.ptr, sizeof(double) * 8 * ni, cudaMemcpyDeviceToHost,
                                        st));
@@ -2512,6 +2522,28 @@ void nb6_regf_seg_(int *ni_, int *iseg, double *h2, double *dtr, double (*xi)[3]
     unpack_results(ni, W, lmax, acc, jrk, pot, list);
     R.time_reduce += nb6_wtime();
 }
+
+}  // extern "C"
+
+// Segmented regular force for a following device kernel: everything is
+// enqueued on the library stream, the results stay in the device output
+// buffers (described in *out); the caller synchronises.
+bool regular_seg_on_device(int ni, int *iseg, double *h2, double *dtr, double (*xi)[3], double (*vi)[3], int lmax,
+                           int nnbmax, int mflag, int nseg, int *seg_j0, RegDeviceOut *out) {
+    int n = ni, lm = lmax, nm = nnbmax, mf = mflag, ns = nseg;
+    g_seg_keep_device = true;
+    nb6_regf_seg_(&n, iseg, h2, dtr, xi, vi, nullptr, nullptr, nullptr, &lm, &nm, nullptr, &mf, &ns, seg_j0);
+    g_seg_keep_device = false;
+    out->outf = R.outf.ptr;
+    out->outl = R.outl.ptr;
+    out->W = std::max(0, std::min(nnbmax, lmax - 1)) + 1;
+    out->jm = R.jm.ptr;
+    out->jx = R.jx.ptr;
+    out->jv = R.jv.ptr;
+    return nb6_last_status_() == 0;
+}
+
+extern "C" {
 
 void gpunb_profile_(int *irank) {
     if (R.icall) {

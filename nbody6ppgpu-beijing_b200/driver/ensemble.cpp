@@ -35,6 +35,7 @@ struct Ensemble : Bodies {
     double time = 0;
     std::vector<double> prop;  // learned dlog RS per row of the last regular_forces
     std::vector<double> crow;  // device corrector rows of the last block
+    std::vector<double> rrow;  // device regular corrector rows of the last call
     // per-call buffers of the batched regular force, kept across calls (the
     // library writes every entry that is read back)
     std::vector<int> b_iseg, b_lst;
@@ -56,11 +57,136 @@ struct Ensemble : Bodies {
     // irregular corrector on the device (batched mode, backend permitting)
     bool dev_corr() const { return batched && P.dev_corrector && B.irr_correct && B.hermite_set && B.hermite_open; }
 
+    // regular corrector on the device too (needs the irregular one there)
+    bool dev_reg() const {
+        return dev_corr() && P.dev_corrector >= 2 && B.regf_correct && B.hermite_get && B.predict_send &&
+               P.mlp_mode != 1;
+    }
+
+    // With both correctors on the device the host keeps only what the block
+    // clock and the force calls need (t0, step, t0r, stepr, rs, and x0, v0
+    // of the bodies due a regular step); the rest is read back here for
+    // energies and at the end.
+    void pull_state() {
+        const int chunk = 1 << 16;
+        std::vector<double> rowbuf(32 * (size_t)std::min(n, chunk));
+        for (int a = 0; a < n; a += chunk) {
+            int a0 = a + 1, k = std::min(chunk, n - a);
+            B.hermite_get(&a0, &k, rowbuf.data());
+            for (int q = 0; q < k; ++q) {
+                const int i = a + q;
+                const double *o = &rowbuf[32 * (size_t)q];
+                for (int c = 0; c < 3; ++c) {
+                    const size_t j = 3 * (size_t)i + c;
+                    x0[j] = o[c];
+                    v0[j] = o[3 + c];
+                    f[j] = o[6 + c];
+                    fdot[j] = o[9 + c];
+                    fi[j] = o[12 + c];
+                    fidot[j] = o[15 + c];
+                    fr[j] = o[18 + c];
+                    frdot[j] = o[21 + c];
+                }
+                t0[i] = o[24];
+                step[i] = o[25];
+                t0r[i] = o[26];
+                stepr[i] = o[27];
+                rs[i] = o[28];
+            }
+        }
+    }
+
     void set_hermite(int i) {
         int a = i + 1;
-        double s = step[i], tr = t0r[i], sr = stepr[i];
+        double s = step[i], tr = t0r[i], sr = stepr[i], r = rs[i];
         B.hermite_set(&a, &fi[3 * (size_t)i], &fidot[3 * (size_t)i], &fr[3 * (size_t)i], &frdot[3 * (size_t)i], &s,
-                      &tr, &sr);
+                      &tr, &sr, &r);
+    }
+
+    // Regular force and regular corrector of the bodies in idx (ascending)
+    // on the device, one nb6_regf_correct_ per pass: the j set of the
+    // clusters involved is predicted once (every body as it stands before
+    // any regular correction of this block, as the host snapshot has it);
+    // rows that overflowed come back untouched, get a smaller radius here
+    // and go again.  The host keeps the new steps and radii of the rows.
+    void regular_on_device(const std::vector<int> &idx) {
+        const double t_0 = wtime();
+        const size_t ni = idx.size();
+        std::vector<int> runc, seg_of_q(ni);
+        for (size_t q = 0; q < ni; ++q) {
+            if (q == 0 || cl_of[idx[q]] != cl_of[idx[q - 1]]) runc.push_back(cl_of[idx[q]]);
+            seg_of_q[q] = (int)runc.size() - 1;
+        }
+        int nseg = (int)runc.size();
+        std::vector<int> addr0(nseg), count(nseg), seg_j0(nseg + 1, 0);
+        for (int r = 0; r < nseg; ++r) {
+            addr0[r] = base[runc[r]] + 1;
+            count[r] = cnt[runc[r]];
+            seg_j0[r + 1] = seg_j0[r] + count[r];
+        }
+        double t = time;
+        B.predict_send(&t, &nseg, addr0.data(), count.data());
+        double prm[6] = {P.eta_r, P.smax, P.dtmin, std::max(25.0 / tcr, 0.0), (double)P.nnbopt,
+                         (double)P.mlp_mode};
+        std::vector<int> pend(ni);
+        for (size_t q = 0; q < ni; ++q) pend[q] = (int)q;
+        std::vector<int> addr;
+        std::vector<double> rsv;
+        while (!pend.empty()) {
+            const int np = (int)pend.size();
+            auto grow = [](auto &v, size_t k) {
+                if (v.size() < k) v.resize(k);
+            };
+            grow(b_iseg, np);
+            grow(b_h2, np);
+            grow(b_dtr, np);
+            grow(b_xi, 3 * (size_t)np);
+            grow(b_vi, 3 * (size_t)np);
+            rrow.resize(32 * (size_t)np);
+            addr.resize(np);
+            rsv.resize(np);
+            for (int p = 0; p < np; ++p) {
+                const int q = pend[p], i = idx[q];
+                addr[p] = i + 1;
+                b_iseg[p] = seg_of_q[q];
+                b_h2[p] = h2_of(i, 1.0 / cnt[cl_of[i]]);
+                b_dtr[p] = stepr[i];
+                rsv[p] = rs[i];
+                for (int c = 0; c < 3; ++c) {  // t0 = time: the body is at x0, v0
+                    b_xi[3 * (size_t)p + c] = x0[3 * (size_t)i + c];
+                    b_vi[3 * (size_t)p + c] = v0[3 * (size_t)i + c];
+                }
+            }
+            int nni = np, lmax = P.lmax, nnbmax = P.nnbmax, mf = P.m_flag;
+            B.regf_correct(&t, &nni, addr.data(), b_iseg.data(), &nseg, seg_j0.data(), addr0.data(), b_h2.data(),
+                           b_dtr.data(), rsv.data(), (double(*)[3])b_xi.data(), (double(*)[3])b_vi.data(), &lmax,
+                           &nnbmax, &mf, prm, rrow.data());
+            st.reg_calls++;
+            std::vector<int> again;
+            for (int p = 0; p < np; ++p) {
+                const int q = pend[p], i = idx[q];
+                st.reg_pairs += cnt[cl_of[i]];
+                const double *o = &rrow[32 * (size_t)p];
+                if (o[28] != 0.0) {
+                    shrink_radius(i, (int)o[28]);
+                    again.push_back(q);
+                    continue;
+                }
+                step[i] = o[24];
+                stepr[i] = o[25];
+                rs[i] = o[26];
+                t0r[i] = time;
+                const int nnb = (int)o[27];
+                st.nb_sum += nnb;
+                st.nb_absdev += fabs((double)(nnb - P.nnbopt));
+                st.reg_steps++;
+                if (o[29] == 1.0) st.mlp_used++;
+                if (o[29] == 2.0) st.mlp_fallback++;
+            }
+            if (!again.empty()) st.overflow_retries++;
+            pend.swap(again);
+        }
+        st.wall_reg += wtime() - t_0;
     }
 
     // Regular force and new lists (global 1-based, self removed) of the
@@ -84,7 +210,7 @@ struct Ensemble : Bodies {
             }
         run0.push_back((int)ni);
         const int nrun = (int)runc.size();
-        if (batched && B.regf_seg && B.predict_send && nrun > 1) {
+        if (batched && B.regf_seg && B.predict_send && (nrun > 1 || P.seg_single)) {
             regular_batched(idx, run0, runc, nrun, freg, fdr, nlist);
         } else if (batched && B.predict_send && nrun == 1) {
             // one cluster: its j set predicted on the device, then the
@@ -316,16 +442,32 @@ struct Ensemble : Bodies {
             const double ti0 = wtime();
             double t = time;
             int nna = na;
-            const bool dc = dev_corr();
+            const bool dc = dev_corr(), dr = dc && dev_reg();
             reg.clear();
             if (dc) {
-                // force + corrector + new step on the device; take back the
-                // corrected state so the host copy stays exact
+                // force + corrector + new step on the device; the host
+                // takes back the corrected state (with the regular corrector
+                // on the device too: the step, and x0, v0 of the bodies due
+                // a regular step, which the regular call takes as its i)
                 crow.resize(24 * (size_t)na);
                 B.irr_correct(&t, &nna, addr.data(), crow.data());
                 st.wall_irr += wtime() - ti0;
                 w0 = wtime();
-                for (int q = 0; q < na; ++q) {
+                for (int q = 0; q < na && dr; ++q) {
+                    const int i = active[q];
+                    const double *o = &crow[24 * (size_t)q];
+                    step[i] = o[18];
+                    t0[i] = time;
+                    st.irr_steps++;
+                    if (o[19] != 0.0) {
+                        reg.push_back(i);
+                        for (int c = 0; c < 3; ++c) {
+                            x0[3 * (size_t)i + c] = o[c];
+                            v0[3 * (size_t)i + c] = o[3 + c];
+                        }
+                    }
+                }
+                for (int q = 0; q < na && !dr; ++q) {
                     const int i = active[q];
                     const double *o = &crow[24 * (size_t)q];
                     for (int c = 0; c < 3; ++c) {
@@ -352,7 +494,9 @@ struct Ensemble : Bodies {
                     if (irr_correct(active[q], time, &a[3 * (size_t)q], &jd[3 * (size_t)q])) reg.push_back(active[q]);
                 t_icor += wtime() - w0;
             }
-            if (!reg.empty()) {
+            if (!reg.empty() && dr) {
+                regular_on_device(reg);
+            } else if (!reg.empty()) {
                 // corrected states of this block to the device before the
                 // j set is predicted there (already there when the device
                 // ran the corrector)
@@ -375,7 +519,9 @@ struct Ensemble : Bodies {
                 t_rcor += wtime() - w0;
             }
             w0 = wtime();
-            if (dc) {
+            if (dr) {
+                // nothing changed on the host alone
+            } else if (dc) {
                 // only the regular corrector changed state on the host
                 for (int i : reg) {
                     set_jp(i);
@@ -389,10 +535,12 @@ struct Ensemble : Bodies {
             clock_push(active);
             t_clock += wtime() - w0;
             if (time >= tnext_out - 1e-15) {
+                if (dr) pull_state();
                 record(tout, eout, nout, nout_max);
                 tnext_out += P.dt_out;
             }
         }
+        if (dev_corr() && dev_reg()) pull_state();
         st.t_end = time;
         st.nout = nout;
         st.wall_total = wtime() - tw;

@@ -48,10 +48,15 @@ struct nb6drive_params {
     // optional initial neighbour radii (one per body); null = RS0 sqrt(1+r^2)
     // (fpoly0.F:55), the reference's rule with RS0 from the input file
     const double *rs_init;
-    // ensemble driver, batched mode: 1 = irregular corrector on the device
-    // (nb6_irr_correct_) when the backend has it, 0 = on the host
+    // ensemble driver, batched mode: 0 = correctors on the host; 1 =
+    // irregular corrector on the device (nb6_irr_correct_) when the backend
+    // has it; 2 = the regular corrector there too (nb6_regf_correct_; the
+    // host one under mlp_mode 1, which logs samples on the host)
     int dev_corrector;
-    int pad2;
+    // ensemble driver, batched mode: 1 = a block whose regular bodies all
+    // belong to one cluster also takes the segmented call (nb6_regf_seg_,
+    // as the device regular corrector does); 0 = gpunb_regf_ for it
+    int seg_single;
 };
 
 // Counters returned by the drivers.
@@ -90,8 +95,12 @@ typedef void (*fn_irr_firr)(double *, int *, int *, double (*)[3], double (*)[3]
 typedef void (*fn_proposals)(int *, double *);
 typedef void (*fn_profile)(int *);
 typedef void (*fn_hermite_open)(double *, double *, double *);
-typedef void (*fn_hermite_set)(int *, double *, double *, double *, double *, double *, double *, double *);
+typedef void (*fn_hermite_set)(int *, double *, double *, double *, double *, double *, double *, double *,
+                               double *);
 typedef void (*fn_irr_correct)(double *, int *, int *, double *);
+typedef void (*fn_regf_correct)(double *, int *, int *, int *, int *, int *, int *, double *, double *, double *,
+                                double (*)[3], double (*)[3], int *, int *, int *, double *, double *);
+typedef void (*fn_hermite_get)(int *, int *, double *);
 
 struct Backend {
     void *hreg = nullptr, *hirr = nullptr, *hpot = nullptr;
@@ -113,6 +122,8 @@ struct Backend {
     fn_hermite_open hermite_open = nullptr;                    // device irregular corrector
     fn_hermite_set hermite_set = nullptr;
     fn_irr_correct irr_correct = nullptr;
+    fn_regf_correct regf_correct = nullptr;                    // device regular corrector
+    fn_hermite_get hermite_get = nullptr;
 };
 
 inline void *must_sym(void *h, const char *name) {
@@ -151,6 +162,8 @@ inline bool load_backend(Backend &b, const char *reg, const char *irr, const cha
     b.hermite_open = (fn_hermite_open)dlsym(b.hirr, "nb6_hermite_open_");
     b.hermite_set = (fn_hermite_set)dlsym(b.hirr, "nb6_hermite_set_");
     b.irr_correct = (fn_irr_correct)dlsym(b.hirr, "nb6_irr_correct_");
+    b.regf_correct = (fn_regf_correct)dlsym(b.hirr, "nb6_regf_correct_");
+    b.hermite_get = (fn_hermite_get)dlsym(b.hirr, "nb6_hermite_get_");
     return b.gpunb_open && b.gpunb_close && b.gpunb_send && b.gpunb_regf && b.gpupot &&
            b.irr_open && b.irr_close && b.irr_set_jp && b.irr_set_list && b.irr_firr_vec;
 }

@@ -32,7 +32,7 @@ class Params(C.Structure):
                 ("max_blocks", C.c_longlong), ("mlp_mode", C.c_int), ("mlp_pad", C.c_int),
                 ("samples", C.POINTER(C.c_float)), ("sample_cap", C.c_longlong),
                 ("rs_init", C.POINTER(C.c_double)), ("dev_corrector", C.c_int),
-                ("pad2", C.c_int)]
+                ("seg_single", C.c_int)]
 
 
 class Stats(C.Structure):
@@ -160,15 +160,20 @@ def run_ensemble(backend: dict, clusters, *, batched=True, tcrit=1.0, eta_i=0.02
                  smax=0.125, dtmin=2.0 ** -24, dt_out=0.125, rs0=0.3, nnbopt=50, nnbmax=400,
                  lmax=512, m_flag=0, chunk=1024, max_blocks=100_000_000, mlp_mode=0,
                  sample_cap=0, rs_init=None, rs_from_clusters=False,
-                 dev_corrector=True) -> EnsembleResult:
+                 dev_corrector=True, seg_single=False) -> EnsembleResult:
     """clusters: sequence of (mass, pos, vel) (or objects with .mass/.pos/.vel),
     each in its own Henon units.  batched=False issues the regular force per
     cluster (what running each alone does); the result is then identical to
     ``run`` on each cluster with a deterministic backend.  rs_init (all
     bodies) or rs_from_clusters=True (each cluster's .rs) sets the initial
-    neighbour radii.  dev_corrector (batched mode): the irregular corrector
-    runs on the device (nb6_irr_correct_); the result is the same bit for
-    bit."""
+    neighbour radii.  dev_corrector (batched mode): 1 (True) runs the
+    irregular corrector on the device (nb6_irr_correct_), 2 the regular
+    corrector there too (nb6_regf_correct_); the result is the same bit for
+    bit (with mlp_mode 2 up to the last bit of exp on the device) when
+    seg_single is set: blocks whose regular bodies are all in one cluster
+    then take the segmented call too, as the device regular corrector
+    always does (otherwise they take gpunb_regf_, whose sums round
+    differently)."""
     parts = [(c.mass, c.pos, c.vel) if hasattr(c, "mass") else c for c in clusters]
     counts = np.array([len(p[0]) for p in parts], dtype=np.int32)
     ncl = len(parts)
@@ -178,7 +183,8 @@ def run_ensemble(backend: dict, clusters, *, batched=True, tcrit=1.0, eta_i=0.02
     p = Params(eta_i, eta_r, smax, dtmin, tcrit, dt_out, rs0, nnbopt, nnbmax, lmax, m_flag,
                chunk, max_blocks)
     buf = _mlp_fields(p, mlp_mode, sample_cap)
-    p.dev_corrector = 1 if dev_corrector else 0
+    p.dev_corrector = int(dev_corrector)
+    p.seg_single = 1 if seg_single else 0
     if rs_init is None and all(hasattr(c, "rs") for c in clusters) and rs_from_clusters:
         rs_init = np.concatenate([c.rs for c in clusters])
     rs_arr = _rs_field(p, rs_init, len(mass))

@@ -1,10 +1,12 @@
 """Batched ensemble vs each cluster alone (the plain method), same GPU.
 
     python -m nb6b200.ensemble_bench --clusters 256 --tcrit 1.0 [--alone-sample 32] [--mlp]
+        [--dev-corrector 2]
 
 (run from ``nbody6ppgpu-beijing_b200/``).  The ensemble is the batched
 driver (one irregular and one segmented regular call per block for all
-clusters); "alone" integrates each cluster with the single-cluster driver
+clusters; --dev-corrector 1 runs the irregular corrector on the device, 2
+both correctors); "alone" integrates each cluster with the single-cluster driver
 and the reference ABI calls.  With --alone-sample k only k clusters, spread
 over the size range, are run alone and their wall time is scaled by the
 ensemble's total pair count over theirs (stated in the output).  Prints one
@@ -36,6 +38,7 @@ def main(argv=None):
     ap.add_argument("--mlp", action="store_true",
                     help="learned radii: train on samples from plain runs of 16 other clusters "
                          "of the same distribution, then run the ensemble with the proposals")
+    ap.add_argument("--dev-corrector", type=int, default=2, choices=(0, 1, 2))
     a = ap.parse_args(argv)
     ours = drive.backend_paths("nb6b200")
     cls = make_clusters(a.clusters)
@@ -51,12 +54,15 @@ def main(argv=None):
         mlp.enable(True)
     t = time.perf_counter()
     ens = drive.run_ensemble(ours, cls, batched=True, tcrit=a.tcrit, dt_out=min(a.tcrit, 0.25),
-                             mlp_mode=2 if a.mlp else 0)
+                             mlp_mode=2 if a.mlp else 0, dev_corrector=a.dev_corrector)
     wall_ens = time.perf_counter() - t
     if a.mlp:
         mlp.enable(False)
     order = np.argsort(sizes)
     pick = order if a.alone_sample <= 0 else order[np.linspace(0, len(cls) - 1, a.alone_sample).astype(int)]
+    worst = int(np.argmax(ens.de_max))  # always compared alone as well
+    if worst not in set(int(c) for c in pick):
+        pick = np.append(pick, worst)
     de_alone, wall_alone, reg_alone, irr_alone = {}, 0.0, 0.0, 0.0
     for c in pick:
         cl = cls[c]
@@ -73,6 +79,7 @@ def main(argv=None):
     out = {
         "workload": f"{a.clusters} Plummer clusters, Kroupa IMF, N log-uniform 512-8192, total {int(sizes.sum())}",
         "tcrit": a.tcrit,
+        "dev_corrector": a.dev_corrector,
         "ensemble_wall_s": wall_ens,
         "alone_wall_s": wall_alone_all,
         "alone_clusters_run": int(len(pick)),
@@ -81,6 +88,9 @@ def main(argv=None):
         "speedup": wall_alone_all / wall_ens,
         "dE_ensemble_median": float(np.median(de_e)),
         "dE_ensemble_max": float(np.max(de_e)),
+        "dE_ensemble_p99": float(np.percentile(de_e, 99)),
+        "worst_cluster": {"n": int(sizes[worst]), "dE_ensemble": float(de_e[worst]),
+                          "dE_alone": float(de_alone[worst])},
         "dE_ratio_ensemble_over_alone_median": float(np.median(ratio)),
         "dE_ratio_p90": float(np.percentile(ratio, 90)),
         "dE_ratio_max": float(np.max(ratio)),

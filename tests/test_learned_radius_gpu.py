@@ -29,3 +29,17 @@ def test_learned_radius_keeps_counts_closer_to_nnbopt(nb6):
     # ~35-39k regular steps before the factor-2 clamp)
     assert q["overflow_retries"] <= 3 * p["overflow_retries"] + 10
     assert q["dE"] < 3.0 * p["dE"] + 1e-6
+    # the same proposals taken by the device regular corrector: an ensemble
+    # of three clusters with the corrector on the device and on the host
+    # (identical but for the last bit of exp on either side)
+    from nb6b200 import drive
+    ours = drive.backend_paths("nb6b200")
+    cls = [ics.plummer(1024, seed=400 + k, imf=True) for k in range(3)]
+    dev = drive.run_ensemble(ours, cls, mlp_mode=2, dev_corrector=2, tcrit=0.25)
+    host = drive.run_ensemble(ours, cls, mlp_mode=2, dev_corrector=1, seg_single=True, tcrit=0.25)
+    print(f"device corrector {dev.stats}\nhost corrector {host.stats}")
+    for key in ("reg_steps", "mlp_used", "mlp_fallback", "nb_sum"):
+        assert abs(dev.stats[key] - host.stats[key]) <= 0.02 * host.stats[key] + 5, key
+    assert dev.stats["mlp_used"] > 0.5 * dev.stats["reg_steps"]
+    assert np.all(dev.de_max < 3.0 * host.de_max + 1e-6)
+
