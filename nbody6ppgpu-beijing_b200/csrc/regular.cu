@@ -1669,7 +1669,13 @@ static void regf_prepare(int ni, const double *d_h2, const double *d_dtr, const 
         R.autotune = (e && atoi(e) == 0) ? 0 : 1;
     }
     int variant = default_variant(ni);
-    const TuneKey key{ilog2(std::max(ni, 1)), ilog2(std::max(R.nj, 1)), mf ? 1 : 0};
+    // calls above TUNE_NI rows share one bucket, tuned on their first
+    // TUNE_NI rows: the choice no longer changes with ni there, and trials on
+    // every row of a very large call would cost seconds
+    constexpr int TUNE_NI = 8192;
+    static_assert(ISORT_MAX <= TUNE_NI, "an ordered call must be tuned on all its rows");
+    const int nt = std::min(ni, TUNE_NI);
+    const TuneKey key{ilog2(std::max(nt, 1)), ilog2(std::max(R.nj, 1)), mf ? 1 : 0};
     bool tune_now = false;
     if (R.forced_ni_per_thread != 0) {
         variant = R.forced_ni_per_thread;
@@ -1696,12 +1702,11 @@ static void regf_prepare(int ni, const double *d_h2, const double *d_dtr, const 
         if (ncand == 0) tune_now = false;
     }
     Plan plan = make_plan(variant, ni, R.nj, R.ntile, mf, R.forced_slices);
-    size_t max_slices = plan.nslices;
+    size_t part_need = (size_t)plan.nslices * ni_pad;
     if (tune_now)
         for (int c = 0; c < ncand; ++c)
-            max_slices = std::max<size_t>(max_slices,
-                                          make_plan(cands[c], ni, R.nj, R.ntile, mf, 0).nslices);
-    R.part.reserve(max_slices * ni_pad * 4);
+            part_need = std::max<size_t>(part_need, (size_t)make_plan(cands[c], nt, R.nj, R.ntile, mf, 0).nslices * nt);
+    R.part.reserve(part_need * 4);
     const int *cnt_before = R.nbcnt.ptr;
     const size_t cnt_cap_before = R.nbcnt.cap;
     R.nbcnt.reserve(ni);
@@ -1710,7 +1715,9 @@ static void regf_prepare(int ni, const double *d_h2, const double *d_dtr, const 
     R.outf.reserve((size_t)ni * 8);
     R.outl.reserve((size_t)ni * W);
 
-    const bool sorted = ensure_sorted(st);
+    // the spatial order serves the packed tile kernels (far tiles); a call
+    // that runs the j-parallel kernel does not wait for it
+    const bool sorted = (tune_now || variant > 0) && ensure_sorted(st);
     RegArgs a;
     a.posH = sorted ? R.posH_s.ptr : R.posH.ptr;
     a.posL = sorted ? R.posL_s.ptr : R.posL.ptr;
@@ -1775,12 +1782,13 @@ static void regf_prepare(int ni, const double *d_h2, const double *d_dtr, const 
         int bestv = variant;
         for (int c = -1; c < ncand; ++c) {
             const int v = cands[c < 0 ? 0 : c];
-            Plan p = make_plan(v, ni, R.nj, R.ntile, mf, 0);
+            Plan p = make_plan(v, nt, R.nj, R.ntile, mf, 0);
             RegArgs t = a;
             t.nslices = p.nslices;
+            t.ni = t.ni_pad = nt;
             float vbest = 1e30f;
             for (int rep = 0; rep < (c < 0 ? 1 : 3); ++rep) {
-                NB6_CUDA_CHECK(cudaMemsetAsync(R.nbcnt.ptr, 0, sizeof(int) * ni, st));
+                NB6_CUDA_CHECK(cudaMemsetAsync(R.nbcnt.ptr, 0, sizeof(int) * nt, st));
                 NB6_CUDA_CHECK(cudaEventRecord(R.tev0, st));
                 if (mf) launch_plan<true>(p, t, st);
                 else launch_plan<false>(p, t, st);
@@ -1804,6 +1812,19 @@ static void regf_prepare(int ni, const double *d_h2, const double *d_dtr, const 
         if (getenv("NB6_VERBOSE"))
             fprintf(stderr, "# nb6 autotune: ni~2^%d nj~2^%d mflag %d -> variant %d (%.3f ms)\n",
                     key.li, key.lj, key.mf, bestv, best);
+    }
+    if (plan.variant < 0 && a.perm) {
+        // the j-parallel kernel takes the j set in its sent order, whether
+        // or not this call's trials needed the spatial order: the same
+        // variant always sums in the same order
+        a.posH = R.posH.ptr;
+        a.posL = R.posL.ptr;
+        a.vel = R.vel.ptr;
+        a.comp = R.comp.ptr;
+        a.compd = R.compd.ptr;
+        a.perm = nullptr;
+        a.tbox = nullptr;
+        a.iperm = nullptr;
     }
     R.last_geometry[0] = plan.variant;
     R.last_geometry[1] = plan.igrid;
@@ -2364,6 +2385,47 @@ void nb6_regf_seg_(int *ni_, int *iseg, double *h2, double *dtr, double (*xi)[3]
     memcpy(h + ni, dtr, sizeof(double) * ni);
     memcpy(h + 2 * (size_t)ni, xi, sizeof(double) * 3 * ni);
     memcpy(h + 5 * (size_t)ni, vi, sizeof(double) * 3 * ni);
+
+    // One segment spanning a large j set (one big cluster): the tuned tile
+    // kernels of gpunb_regf_ (packed pair math, spatial order, far tiles)
+    // beat the segmented kernel's j-parallel loop there; the results are the
+    // same rows (ids relative to the segment = to the first j sent).
+    static const int seg_tile_min = [] {
+        const char *e = getenv("NB6_SEG_TILE_MIN");
+        return e ? atoi(e) : 32768;
+    }();
+    if (nseg == 1 && seg_j0[0] == 0 && seg_j0[1] == R.nj && R.nj >= seg_tile_min) {
+        R.time_out += nb6_wtime() - t_start;
+        R.time_grav -= nb6_wtime();
+        R.numInter += (long long)ni * R.nj;
+        NB6_CUDA_CHECK(cudaMemcpyAsync(R.iin.ptr, h, sizeof(double) * nin, cudaMemcpyHostToDevice, st));
+        const double *d = R.iin.ptr;
+        int Wt = W;
+        regf_device(ni, d, d + ni, d + 2 * (size_t)ni, d + 5 * (size_t)ni, lmax, nnbmax, *m_flag, st, Wt);
+        if (g_seg_keep_device) {
+            R.time_grav += nb6_wtime();
+            return;
+        }
+        R.houtf.reserve((size_t)ni * 8);
+        R.houtl.reserve((size_t)ni * W);
+        NB6_CUDA_CHECK(cudaMemcpyAsync(R.houtf.ptr, R.outf.ptr, sizeof(double) * 8 * ni, cudaMemcpyDeviceToHost,
+                                       st));
+        NB6_CUDA_CHECK(cudaMemcpyAsync(R.houtl.ptr, R.outl.ptr, sizeof(int) * (size_t)W * ni,
+                                       cudaMemcpyDeviceToHost, st));
+        nb6_status_fetch(st);
+        NB6_CUDA_CHECK(cudaStreamSynchronize(st));
+        NB6_CUDA_CHECK(cudaEventElapsedTime(&R.last_kernel_ms, R.ev0, R.ev1));
+        const double wt2 = nb6_wtime();
+        R.time_grav += wt2;
+        R.time_reduce -= wt2;
+        if (nb6_check_dev_status() != 0) {
+            R.nbcnt_dirty = true;
+            return;
+        }
+        unpack_results(ni, W, lmax, acc, jrk, pot, list);
+        R.time_reduce += nb6_wtime();
+        return;
+    }
 
     // runs of active particles per segment, and the CTA i-group size
     std::vector<int> run_k0, run_c;

@@ -36,6 +36,7 @@ struct Ensemble : Bodies {
     std::vector<double> prop;  // learned dlog RS per row of the last regular_forces
     std::vector<double> crow;  // device corrector rows of the last block
     std::vector<double> rrow;  // device regular corrector rows of the last call
+    double t_pred = 0;         // wall time in nb6_irr_predict_send_ (device regular corrector)
     // per-call buffers of the batched regular force, kept across calls (the
     // library writes every entry that is read back)
     std::vector<int> b_iseg, b_lst;
@@ -125,7 +126,9 @@ struct Ensemble : Bodies {
             seg_j0[r + 1] = seg_j0[r] + count[r];
         }
         double t = time;
+        const double tp = wtime();
         B.predict_send(&t, &nseg, addr0.data(), count.data());
+        t_pred += wtime() - tp;
         double prm[6] = {P.eta_r, P.smax, P.dtmin, std::max(25.0 / tcr, 0.0), (double)P.nnbopt,
                          (double)P.mlp_mode};
         std::vector<int> pend(ni);
@@ -547,8 +550,8 @@ struct Ensemble : Bodies {
         if (getenv("NB6_VERBOSE")) {
             fprintf(stderr,
                     "# nb6 ensemble: wall %.3f s = irr calls %.3f + reg calls %.3f + irr corrector %.3f"
-                    " + reg corrector %.3f + set_jp %.3f + clock %.3f + other\n",
-                    st.wall_total, st.wall_irr, st.wall_reg, t_icor, t_rcor, t_jp, t_clock);
+                    " + reg corrector %.3f + set_jp %.3f + clock %.3f + other (j-set prediction %.3f of reg calls)\n",
+                    st.wall_total, st.wall_irr, st.wall_reg, t_icor, t_rcor, t_jp, t_clock, t_pred);
             int rank = 0;
             if (B.reg_profile) B.reg_profile(&rank);
             if (B.irr_profile) B.irr_profile(&rank);

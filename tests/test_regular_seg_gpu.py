@@ -176,3 +176,27 @@ def test_predict_send_from_irregular_records_equals_host_send(nb6):
     for a, b in zip(dev, host):
         np.testing.assert_array_equal(a, b)
     assert (host[3][:, 0] > 0).all()
+
+
+def test_seg_single_large_segment_takes_the_tile_kernels(nb6, orc):
+    """One segment spanning a j set of 40,000 bodies (one big cluster) runs
+    on the tuned tile kernels of gpunb_regf_: the rows equal gpunb_regf_'s
+    bit for bit, and the oracle's lists and forces within the usual bounds."""
+    import ctypes as C
+    from nb6b200 import ics
+    cl = ics.plummer(40000, seed=4242, imf=True)
+    rng = np.random.default_rng(3)
+    a = np.sort(rng.choice(cl.n, 700, replace=False))
+    h2, dtr, xi, vi = cl.h2(0)[a], cl.dtr[a], cl.pos[a], cl.vel[a]
+    nb6.gpunb_open(cl.n + 10, 0)
+    try:
+        nb6.gpunb_send(cl.mass, cl.pos, cl.vel)
+        seg = nb6.regf_seg(h2, dtr, xi, vi, np.zeros(len(a), np.int32), [0, cl.n], 512, 400, 0)
+        plain = nb6.gpunb_regf(h2, dtr, xi, vi, 512, 400, 0)
+    finally:
+        nb6.gpunb_close()
+    for s, p in zip(seg, plain):
+        np.testing.assert_array_equal(s, p)
+    sub = np.sort(rng.choice(len(a), 64, replace=False))
+    ref = orc.regf(cl.mass, cl.pos, cl.vel, h2[sub], dtr[sub], xi[sub], vi[sub], 512, 400, 0)
+    _check(tuple(o[sub] for o in seg), ref)
