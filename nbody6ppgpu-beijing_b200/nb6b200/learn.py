@@ -49,12 +49,14 @@ def _summary(stats, de, tcrit):
             "dE": float(de), "mlp_used": stats["mlp_used"], "mlp_fallback": stats["mlp_fallback"]}
 
 
-def compare(cl, tcrit, plain_method=True, rs_ics=False, **kw) -> dict:
+def compare(cl, tcrit, plain_method=True, rs_ics=False, dev_corrector=2, **kw) -> dict:
     """One cluster three ways, with the current model for the learned arm:
     the plain GPU method (single-cluster driver: host prediction, gpunb_send_
-    per regular block, Ahmad-Cohen radii); the batched driver (j set
-    predicted on the device) with Ahmad-Cohen radii; and the batched driver
-    with the learned radii."""
+    per regular block, host correctors, Ahmad-Cohen radii); the batched
+    driver (j set predicted on the device; with dev_corrector = 2 both
+    correctors on the device too) with Ahmad-Cohen radii; and the batched
+    driver with the learned radii.  Wall times are the drivers' own (block
+    loop and energies, not the start-up)."""
     ours = drive.backend_paths("nb6b200")
     dt_out = min(tcrit, 0.125)          # at least one energy after the start
     rs = cl.rs if rs_ics else None
@@ -64,18 +66,20 @@ def compare(cl, tcrit, plain_method=True, rs_ics=False, **kw) -> dict:
                       rs_init=rs, **kw)
         out["plain"] = _summary(r.stats, r.de_max, tcrit)
     r = drive.run_ensemble(ours, [cl], batched=True, tcrit=tcrit, mlp_mode=0, dt_out=dt_out,
-                           rs_init=rs, **kw)
+                           rs_init=rs, dev_corrector=dev_corrector, **kw)
     out["batched"] = _summary(r.stats, r.de_max[0], tcrit)
     mlp.enable(True)
     try:
         r = drive.run_ensemble(ours, [cl], batched=True, tcrit=tcrit, mlp_mode=2, dt_out=dt_out,
-                               rs_init=rs, **kw)
+                               rs_init=rs, dev_corrector=dev_corrector, **kw)
     finally:
         mlp.enable(False)
     out["learned"] = _summary(r.stats, r.de_max[0], tcrit)
     base = out.get("plain", out["batched"])
-    out["speedup_learned_vs_" + ("plain" if plain_method else "batched")] = \
-        base["wall_s"] / out["learned"]["wall_s"]
+    key = "plain" if plain_method else "batched"
+    out["speedup_learned_vs_" + key] = base["wall_s"] / out["learned"]["wall_s"]
+    out["speedup_batched_vs_" + key] = base["wall_s"] / out["batched"]["wall_s"]
+    out["dev_corrector"] = dev_corrector
     return out
 
 
