@@ -207,6 +207,24 @@ void nb6_irr_correct_(double *time, int *ni, int *addr, double *out);
 void nb6_regf_correct_(double *time, int *ni, int *addr, int *iseg, int *nseg, int *seg_j0, int *seg_a0,
                        double *h2, double *dtr, double *rs, double (*xi)[3], double (*vi)[3], int *lmax,
                        int *nnbmax, int *m_flag, double *prm, double *out);
+/* KS c.m. corrections of the irregular force (cmfirr_cor.f:13-130,
+ * cmfirr_ucor.f:14-116, called from nbint_cor.f:37-65; no reference
+ * counterpart in the force libraries: the reference applies them on the
+ * host after irr_simd_firr_vec_).  Replaces the table of perturbed KS
+ * pairs; *npair = 0 clears it.  Pair p: c.m. body cm[p] (1-based address),
+ * component positions xk[p][2][3] and velocities vk[p][2][3] at the time of
+ * the coming irregular calls (the host's KS resolution), masses mk[p][2],
+ * perturbers of the first component plist[pofs[p] .. pofs[p+1]) (1-based,
+ * pofs[0] = 0).  While a table is set, irr_simd_firr_vec_ and
+ * nb6_irr_correct_ return FIRR and FD with the corrections included: for a
+ * neighbour that is a perturbed pair, its two components replace its
+ * point mass; for the c.m. of a perturbed pair, the perturbation of its
+ * components by each perturber (resolved too when it is a perturbed pair)
+ * minus that perturber's c.m. force is added; an empty neighbour list gets
+ * none.  The caller then skips CMFIRR_COR and CMFIRR_UCOR.  The chain terms
+ * (KCPERT_COR, CHFIRR, FCHAIN) stay on the host. */
+void nb6_ks_set_(int *npair, int *cm, double *xk, double *vk, double *mk, int *pofs, int *plist);
+
 /* The device-resident state of bodies *a0 .. *a0 + *n - 1 (1-based), for a
  * host that lets the device correctors keep it (energy output, the end of
  * a run): rows of 32 doubles x0[3], v0[3], F[3], FDOT[3], fi[3], fidot[3],

@@ -53,16 +53,60 @@ NB6_DEV void load_rec(const Rec *__restrict__ p, Rec &r) {
     r.m = g.x; r.t0 = g.y;
 }
 
+// Perturbed KS pairs whose components the irregular force resolves
+// (nb6_ks_set_): slot[a] = pair p of c.m. body a (0-based) or -1; pair p
+// has component positions xk[6p..6p+5] and velocities vk[6p..] at the
+// block time (first component, then second), masses mk[2p], mk[2p+1], and
+// perturbers plist[pofs[p] .. pofs[p+1]) (0-based).  slot == nullptr: no
+// table, no corrections.
+struct KsArgs {
+    const int *slot;
+    const double *xk, *vk, *mk;
+    const int *pofs, *plist;
+};
+
+// Force and jerk on (xi, vi) from a point mass m at (xj, vj), operation
+// order of cmfirr_cor.f:47-93.
+NB6_DEV void cm_pair(const double *xi, const double *vi, const double *xj, const double *vj, double m, double *f,
+                     double *fd) {
+    double dx[3], dv[3], dr2 = 0.0, drdv = 0.0;
+#pragma unroll
+    for (int l = 0; l < 3; ++l) {
+        dx[l] = xj[l] - xi[l];
+        dv[l] = vj[l] - vi[l];
+        dr2 += dx[l] * dx[l];
+        drdv += dx[l] * dv[l];
+    }
+    const double dr2i = 1.0 / dr2;
+    const double dr3i = m * dr2i * sqrt(dr2i);
+    drdv = 3.0 * drdv * dr2i;
+#pragma unroll
+    for (int l = 0; l < 3; ++l) {
+        f[l] = dx[l] * dr3i;
+        fd[l] = (dv[l] - dx[l] * drdv) * dr3i;
+    }
+}
+
 // One warp, one active particle i: neighbour force, jerk and nearest
 // neighbour (1-based, -1 for an empty list), reduced into every lane.
+// With a KS pair table the force includes the c.m. corrections NBINT_COR
+// adds on the host (nbint_cor.f:37-65): for a neighbour that is a
+// perturbed pair, the sum over its two components replaces its point-mass
+// term (cmfirr_ucor.f:14-116); for i itself the c.m. of a perturbed pair,
+// the perturbation terms over its perturber list are added instead
+// (cmfirr_cor.f:13-130).  An empty list gets no corrections.
+template <bool KS>
 NB6_DEV void irr_force_warp(int i, int lane, double ti, const Rec *__restrict__ rec,
-                            const int *__restrict__ lists, int ls, int nmax, double *a, double *jd, int &nnbid) {
+                            const int *__restrict__ lists, int ls, int nmax, const KsArgs &ks, double *a,
+                            double *jd, int &nnbid) {
     Rec ri;
     load_rec(rec + i, ri);
     double xi[3], vi[3];
     predict(ri, ti, xi, vi);
     const int *row = lists + (size_t)i * ls;
     const int nnb = row[0];
+    const int pi = KS ? ks.slot[i] : -1;
+    const bool resolve = KS && pi < 0;  // components of perturbed neighbours
     double ax = 0, ay = 0, az = 0, jx = 0, jy = 0, jz = 0;
     double rmin = 1.0e300;
     int jmin = 0x7fffffff;
@@ -79,6 +123,21 @@ NB6_DEV void irr_force_warp(int i, int lane, double ti, const Rec *__restrict__ 
             rmin = r2d;
             jmin = j;
         }
+        const int q = resolve ? ks.slot[j] : -1;
+        if (q >= 0) {
+            double f[3], fd[3];
+            for (int c = 0; c < 2; ++c) {
+                cm_pair(xi, vi, ks.xk + 6 * (size_t)q + 3 * c, ks.vk + 6 * (size_t)q + 3 * c, ks.mk[2 * q + c], f,
+                        fd);
+                ax += f[0];
+                ay += f[1];
+                az += f[2];
+                jx += fd[0];
+                jy += fd[1];
+                jz += fd[2];
+            }
+            continue;
+        }
         // The list walk is bound by the record gathers, not by arithmetic,
         // so the pair math stays in FP64 (nbint.F:143-158).
         const double dvx = vj[0] - vi[0], dvy = vj[1] - vi[1], dvz = vj[2] - vi[2];
@@ -92,6 +151,39 @@ NB6_DEV void irr_force_warp(int i, int lane, double ti, const Rec *__restrict__ 
         jx += mr3 * (dvx + al * dxd);
         jy += mr3 * (dvy + al * dyd);
         jz += mr3 * (dvz + al * dzd);
+    }
+    if (KS && pi >= 0 && nnb > 0) {
+        // i is the c.m. of a perturbed pair: perturbation of its components
+        // by each perturber (itself resolved when it is a perturbed pair)
+        // minus the perturber's c.m. force on the c.m.
+        const double *x1 = ks.xk + 6 * (size_t)pi, *x2 = x1 + 3;
+        const double *v1 = ks.vk + 6 * (size_t)pi, *v2 = v1 + 3;
+        const double m1 = ks.mk[2 * pi], m2 = ks.mk[2 * pi + 1], mi = ri.m;
+        for (int l = ks.pofs[pi] + lane; l < ks.pofs[pi + 1]; l += 32) {
+            const int j = ks.plist[l];
+            if (j < 0 || j >= nmax) continue;   // ids are checked at set time
+            Rec rj;
+            load_rec(rec + j, rj);
+            double xj[3], vj[3], fcm[3], fcmd[3];
+            predict(rj, ti, xj, vj);
+            cm_pair(xi, vi, xj, vj, rj.m, fcm, fcmd);
+            const int q = ks.slot[j];
+            for (int c = 0; c < (q >= 0 ? 2 : 1); ++c) {
+                const double *xs = q >= 0 ? ks.xk + 6 * (size_t)q + 3 * c : xj;
+                const double *vs = q >= 0 ? ks.vk + 6 * (size_t)q + 3 * c : vj;
+                const double ms = q >= 0 ? ks.mk[2 * q + c] : rj.m;
+                double f1[3], fd1[3], f2[3], fd2[3];
+                cm_pair(x1, v1, xs, vs, ms, f1, fd1);
+                cm_pair(x2, v2, xs, vs, ms, f2, fd2);
+                const double s = c == 0 ? 1.0 : 0.0;  // the c.m. term once
+                ax += (m1 * f1[0] + m2 * f2[0]) / mi - s * fcm[0];
+                ay += (m1 * f1[1] + m2 * f2[1]) / mi - s * fcm[1];
+                az += (m1 * f1[2] + m2 * f2[2]) / mi - s * fcm[2];
+                jx += (m1 * fd1[0] + m2 * fd2[0]) / mi - s * fcmd[0];
+                jy += (m1 * fd1[1] + m2 * fd2[1]) / mi - s * fcmd[1];
+                jz += (m1 * fd1[2] + m2 * fd2[2]) / mi - s * fcmd[2];
+            }
+        }
     }
     a[0] = warp_sum_d(ax);
     a[1] = warp_sum_d(ay);
@@ -112,15 +204,18 @@ NB6_DEV void irr_force_warp(int i, int lane, double ti, const Rec *__restrict__ 
 }
 
 // out row k = (ax, ay, az, jx, jy, jz, nnbid, 0): one download per call.
+// KS: with the pair table (a separate instance: the corrections double the
+// registers of the plain walk).
+template <bool KS>
 __global__ void __launch_bounds__(IRR_WARPS * 32)
     irr_kernel(int ni, const int *__restrict__ addr, double ti, const Rec *__restrict__ rec,
-               const int *__restrict__ lists, int ls, int nmax, double *__restrict__ out) {
+               const int *__restrict__ lists, int ls, int nmax, KsArgs ks, double *__restrict__ out) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int k = blockIdx.x * IRR_WARPS + warp;
     if (k >= ni) return;
     double a[3], jd[3];
     int id;
-    irr_force_warp(addr[k] - 1, lane, ti, rec, lists, ls, nmax, a, jd, id);
+    irr_force_warp<KS>(addr[k] - 1, lane, ti, rec, lists, ls, nmax, ks, a, jd, id);
     if (lane == 0) {
         double *o = out + (size_t)k * 8;
         o[0] = a[0];
@@ -612,8 +707,41 @@ struct IrrState {
     HostBuf<int> hstage_aux_addr;
     std::vector<int> aux_slot;
     int naux = 0;
+    // perturbed KS pairs (nb6_ks_set_): slot table over addresses, pair
+    // data [xk 6P | vk 6P | mk 2P], ints [pofs P+1 | plist]
+    DevBuf<int> ks_slot, ks_int;
+    DevBuf<double> ks_dbl;
+    HostBuf<int> ks_hint;
+    HostBuf<double> ks_hdbl;
+    int ks_npair = 0;
 };
 IrrState I;
+
+// the current pair table for the force kernels (none: slot == nullptr)
+KsArgs ks_args() {
+    KsArgs k{};
+    if (I.ks_npair <= 0) return k;
+    const size_t P = (size_t)I.ks_npair;
+    k.slot = I.ks_slot.ptr;
+    k.xk = I.ks_dbl.ptr;
+    k.vk = I.ks_dbl.ptr + 6 * P;
+    k.mk = I.ks_dbl.ptr + 12 * P;
+    k.pofs = I.ks_int.ptr;
+    k.plist = I.ks_int.ptr + P + 1;
+    return k;
+}
+
+void launch_irr_kernel(int ni, const int *daddr, double ti, double *out, cudaStream_t st) {
+    const KsArgs ks = ks_args();
+    const dim3 grid((ni + IRR_WARPS - 1) / IRR_WARPS), block(IRR_WARPS * 32);
+    if (ks.slot) irr_kernel<true><<<grid, block, 0, st>>>(ni, daddr, ti, I.rec.ptr, I.lists.ptr, I.lmax, I.nmax, ks, out);
+    else irr_kernel<false><<<grid, block, 0, st>>>(ni, daddr, ti, I.rec.ptr, I.lists.ptr, I.lmax, I.nmax, ks, out);
+}
+
+__global__ void ks_scatter_slots(int npair, const int *__restrict__ cm, int *__restrict__ slot) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < npair) slot[cm[p]] = p;
+}
 
 void irr_open_impl(int nmax, int lmax, int rank) {
     nb6_devinit_once(rank);
@@ -664,6 +792,12 @@ void irr_close_impl() {
     I.aux_slot.clear();
     I.naux = 0;
     I.hermite = false;
+    I.ks_slot.release();
+    I.ks_int.release();
+    I.ks_dbl.release();
+    I.ks_hint.release();
+    I.ks_hdbl.release();
+    I.ks_npair = 0;
     I.hstage_rec.release();
     I.hstage_addr.release();
     I.hstage_list.release();
@@ -866,8 +1000,7 @@ void irr_firr_vec_impl(double ti, int ni, const int *addr, double (*acc)[3], dou
         NB6_CUDA_CHECK(cudaEventCreate(&I.ev1));
     }
     NB6_CUDA_CHECK(cudaEventRecord(I.ev0, st));
-    irr_kernel<<<(ni + IRR_WARPS - 1) / IRR_WARPS, IRR_WARPS * 32, 0, st>>>(ni, daddr, ti, I.rec.ptr, I.lists.ptr,
-                                                                       I.lmax, I.nmax, out);
+    launch_irr_kernel(ni, daddr, ti, out, st);
     NB6_CUDA_CHECK(cudaGetLastError());
     NB6_CUDA_CHECK(cudaEventRecord(I.ev1, st));
     if (!direct)
@@ -980,8 +1113,7 @@ void irr_correct_impl(double time, int ni, const int *addr, double *out) {
         NB6_CUDA_CHECK(cudaEventCreate(&I.ev1));
     }
     NB6_CUDA_CHECK(cudaEventRecord(I.ev0, st));
-    irr_kernel<<<(ni + IRR_WARPS - 1) / IRR_WARPS, IRR_WARPS * 32, 0, st>>>(ni, daddr, time, I.rec.ptr, I.lists.ptr,
-                                                                       I.lmax, I.nmax, force);
+    launch_irr_kernel(ni, daddr, time, force, st);
     NB6_CUDA_CHECK(cudaGetLastError());
     NB6_CUDA_CHECK(cudaEventRecord(I.ev1, st));
     irr_apply_corrector<<<(ni + 127) / 128, 128, 0, st>>>(ni, daddr, time, force, I.rec.ptr, I.aux.ptr, I.hp, o);
@@ -998,6 +1130,65 @@ void irr_correct_impl(double time, int ni, const int *addr, double *out) {
     I.time_grav += nb6_wtime() - t0;
     I.num_fcall++;
     I.num_steps += ni;
+}
+
+void ks_set_impl(int npair, const int *cm, const double *xk, const double *vk, const double *mk, const int *pofs,
+                 const int *plist) {
+    if (!I.open) {
+        nb6_fatal(NB6_ERR_NOT_OPEN);
+        return;
+    }
+    if (npair < 0) {
+        nb6_fatal(NB6_ERR_BAD_ARG);
+        return;
+    }
+    cudaStream_t st = nb6_stream();
+    if (npair == 0) {  // no perturbed pairs: the forces go uncorrected
+        I.ks_npair = 0;
+        return;
+    }
+    bool bad = pofs[0] != 0;
+    std::vector<char> seen(I.nmax, 0);
+    for (int p = 0; p < npair && !bad; ++p) {
+        bad = cm[p] < 1 || cm[p] > I.nmax || seen[cm[p] - 1] || pofs[p + 1] < pofs[p];
+        if (!bad) seen[cm[p] - 1] = 1;
+    }
+    const int nl = bad ? 0 : pofs[npair];
+    for (int l = 0; l < nl && !bad; ++l) bad = plist[l] < 1 || plist[l] > I.nmax;
+    if (bad) {
+        fprintf(stderr, "nb6_ks_set: pair address, perturber id or list offsets outside [1, %d]\n", I.nmax);
+        nb6_fatal(NB6_ERR_BAD_ARG);
+        return;
+    }
+    for (size_t k = 0; k < 6 * (size_t)npair; ++k)
+        if (xk[k] != xk[k] || vk[k] != vk[k]) {
+            fprintf(stderr, "nb6_ks_set: NaN in a pair's components\n");
+            nb6_fatal(NB6_ERR_NAN_INPUT);
+            return;
+        }
+    const size_t P = (size_t)npair;
+    const size_t nd = 14 * P, ni = P + (P + 1) + (size_t)nl;
+    I.ks_hdbl.reserve(nd);
+    I.ks_hint.reserve(ni);
+    I.ks_dbl.reserve(nd);
+    I.ks_int.reserve(ni);
+    I.ks_slot.reserve(I.nmax);
+    memcpy(I.ks_hdbl.ptr, xk, sizeof(double) * 6 * P);
+    memcpy(I.ks_hdbl.ptr + 6 * P, vk, sizeof(double) * 6 * P);
+    memcpy(I.ks_hdbl.ptr + 12 * P, mk, sizeof(double) * 2 * P);
+    // ints on the device: [pofs | plist - 1 | cm - 1]
+    int *h = I.ks_hint.ptr;
+    memcpy(h, pofs, sizeof(int) * (P + 1));
+    for (int l = 0; l < nl; ++l) h[P + 1 + l] = plist[l] - 1;
+    for (size_t p = 0; p < P; ++p) h[P + 1 + nl + p] = cm[p] - 1;
+    NB6_CUDA_CHECK(cudaMemcpyAsync(I.ks_dbl.ptr, I.ks_hdbl.ptr, sizeof(double) * nd, cudaMemcpyHostToDevice, st));
+    NB6_CUDA_CHECK(cudaMemcpyAsync(I.ks_int.ptr, h, sizeof(int) * ni, cudaMemcpyHostToDevice, st));
+    NB6_CUDA_CHECK(cudaMemsetAsync(I.ks_slot.ptr, 0xff, sizeof(int) * (size_t)I.nmax, st));
+    ks_scatter_slots<<<(npair + 255) / 256, 256, 0, st>>>(npair, I.ks_int.ptr + P + 1 + nl, I.ks_slot.ptr);
+    NB6_CUDA_CHECK(cudaGetLastError());
+    // the pinned staging is rewritten by the next call
+    NB6_CUDA_CHECK(cudaStreamSynchronize(st));
+    I.ks_npair = npair;
 }
 
 void hermite_get_impl(int a0, int n, double *out) {
@@ -1184,6 +1375,21 @@ void nb6_hermite_set_(int *addr, double fi[3], double fidot[3], double fr[3], do
     hermite_set_impl(*addr - 1, fi, fidot, fr, frdot, *step, *t0r, *stepr, *rs);
 }
 void nb6_irr_correct_(double *time, int *ni, int *addr, double *out) { irr_correct_impl(*time, *ni, addr, out); }
+
+// KS pairs whose components the irregular force resolves, replacing the
+// table of the previous call (npair = 0 clears it).  Pair p: the c.m. body
+// cm[p] (1-based address), its components' positions xk[p][2][3] and
+// velocities vk[p][2][3] at the time of the coming irregular calls, their
+// masses mk[p][2], and the perturber list (LIST(2..,I1) of the first
+// component) plist[pofs[p] .. pofs[p+1]) (1-based, pofs[0] = 0).  Every
+// following irr_simd_firr_vec_ / nb6_irr_correct_ returns FIRR and FD with
+// the corrections NBINT_COR adds on the host (cmfirr_cor.f,
+// cmfirr_ucor.f; nbint_cor.f:37-65), so a caller skips its own CMFIRR_COR
+// and CMFIRR_UCOR.  Only perturbed pairs are listed: an unperturbed pair
+// acts as its c.m. point mass, as in the reference.
+void nb6_ks_set_(int *npair, int *cm, double *xk, double *vk, double *mk, int *pofs, int *plist) {
+    ks_set_impl(*npair, cm, xk, vk, mk, pofs, plist);
+}
 
 // The resident state of bodies a0 .. a0+n-1 (1-based), rows of 32
 // doubles: x0[3], v0[3], F[3], FDOT[3], fi[3], fidot[3], fr[3], frdot[3],

@@ -201,6 +201,25 @@ class ForceLib:
         padded[: row.shape[0]] = row[: padded.shape[0]]
         self.lib.irr_simd_set_list_(_ci(addr), _ip(padded))
 
+    def ks_set(self, cm, xk, vk, mk, pofs, plist) -> None:
+        """nb6_ks_set_ (extension): the perturbed KS pairs whose components
+        the irregular force resolves from now on.  cm: 1-based c.m.
+        addresses (npair); xk, vk: (npair, 2, 3) component positions and
+        velocities at the coming irregular calls' time; mk: (npair, 2);
+        pofs (npair + 1, pofs[0] = 0) and plist (1-based) the perturber
+        lists.  An empty cm clears the table."""
+        cm = np.ascontiguousarray(cm, dtype=np.int32).reshape(-1)
+        npair = cm.shape[0]
+        xk = _f64(np.reshape(xk, (-1, 6)) if npair else np.zeros((1, 6)))
+        vk = _f64(np.reshape(vk, (-1, 6)) if npair else np.zeros((1, 6)))
+        mk = _f64(np.reshape(mk, (-1, 2)) if npair else np.zeros((1, 2)))
+        pofs = np.ascontiguousarray(pofs if npair else [0], dtype=np.int32)
+        plist = np.ascontiguousarray(plist, dtype=np.int32).reshape(-1)
+        if plist.size == 0:
+            plist = np.zeros(1, dtype=np.int32)
+        cmp = cm if npair else np.zeros(1, dtype=np.int32)
+        self.lib.nb6_ks_set_(_ci(npair), _ip(cmp), _dp(xk), _dp(vk), _dp(mk), _ip(pofs), _ip(plist))
+
     def irr_firr_vec(self, ti: float, addr) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
         addr = np.ascontiguousarray(addr, dtype=np.int32)
         ni = addr.shape[0]

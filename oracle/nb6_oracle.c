@@ -158,3 +158,93 @@ void orc_firr(double ti, int ni, const int *addr, int nmax,
         nnbid[k] = imin;
     }
 }
+
+/* Force and jerk on a body at (xi, vi) from a point mass m at (xj, vj), in
+ * the operation order of cmfirr_cor.f:47-93 / cmfirr_ucor.f:58-104. */
+static void cm_pair(const double *xi, const double *vi, const double *xj,
+                    const double *vj, double m, double *f, double *fd)
+{
+    double dx[3], dv[3], dr2 = 0.0, drdv = 0.0;
+    for (int l = 0; l < 3; l++) {
+        dx[l] = xj[l] - xi[l];
+        dv[l] = vj[l] - vi[l];
+        dr2 += dx[l] * dx[l];
+        drdv += dx[l] * dv[l];
+    }
+    const double dr2i = 1.0 / dr2;
+    const double dr3i = m * dr2i * sqrt(dr2i);
+    drdv = 3.0 * drdv * dr2i;
+    for (int l = 0; l < 3; l++) {
+        f[l] = dx[l] * dr3i;
+        fd[l] = (dv[l] - dx[l] * drdv) * dr3i;
+    }
+}
+
+void orc_ks_cmcorr(double ti, int ni, const int *addr, const double *x0,
+                   const double *v0, const double *acc2, const double *jrk6,
+                   const double *mass, const double *t0, const int *lists,
+                   int lmax, const int *slot, const double *xk,
+                   const double *vk, const double *mk, const int *pofs,
+                   const int *plist, double *acc, double *jrk)
+{
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int k = 0; k < ni; k++) {
+        const int i = addr[k] - 1;
+        const int *row = lists + (long)i * lmax;
+        if (row[0] == 0) continue;  /* nbint_cor.f:37-49: no corrections */
+        double xi[3], vi[3];
+        pred1(ti - t0[i], x0 + 3 * i, v0 + 3 * i, acc2 + 3 * i, jrk6 + 3 * i, xi, vi);
+        double cf[3] = {0, 0, 0}, cd[3] = {0, 0, 0};
+        const int p = slot[i];
+        if (p >= 0) {
+            /* cmfirr_cor.f: perturbed pair i, corrections over the
+             * perturbers of its first component */
+            const double *x1 = xk + 6 * p, *x2 = xk + 6 * p + 3;
+            const double *v1 = vk + 6 * p, *v2 = vk + 6 * p + 3;
+            const double m1 = mk[2 * p], m2 = mk[2 * p + 1], mi = mass[i];
+            for (int l = pofs[p]; l < pofs[p + 1]; l++) {
+                const int j = plist[l] - 1;
+                double xj[3], vj[3], fcm[3], fcmd[3];
+                pred1(ti - t0[j], x0 + 3 * j, v0 + 3 * j, acc2 + 3 * j, jrk6 + 3 * j, xj, vj);
+                cm_pair(xi, vi, xj, vj, mass[j], fcm, fcmd);
+                const int q = slot[j];
+                const int nk = q >= 0 ? 2 : 1;   /* resolve a perturbed pair j */
+                for (int c = 0; c < nk; c++) {
+                    const double *xkk = q >= 0 ? xk + 6 * q + 3 * c : xj;
+                    const double *vkk = q >= 0 ? vk + 6 * q + 3 * c : vj;
+                    const double mkk = q >= 0 ? mk[2 * q + c] : mass[j];
+                    double fp1[3], fpd1[3], fp2[3], fpd2[3];
+                    cm_pair(x1, v1, xkk, vkk, mkk, fp1, fpd1);
+                    cm_pair(x2, v2, xkk, vkk, mkk, fp2, fpd2);
+                    for (int d = 0; d < 3; d++) {
+                        /* the c.m. term enters once, with the first component */
+                        const double sc = c == 0 ? fcm[d] : 0.0, sd = c == 0 ? fcmd[d] : 0.0;
+                        cf[d] += (m1 * fp1[d] + m2 * fp2[d]) / mi - sc;
+                        cd[d] += (m1 * fpd1[d] + m2 * fpd2[d]) / mi - sd;
+                    }
+                }
+            }
+        } else {
+            /* cmfirr_ucor.f: neighbours that are perturbed pairs summed over
+             * their components */
+            for (int l = 1; l <= row[0]; l++) {
+                const int j = row[l] - 1;
+                const int q = slot[j];
+                if (q < 0) continue;
+                double xj[3], vj[3], fcm[3], fcmd[3], fp1[3], fpd1[3], fp2[3], fpd2[3];
+                pred1(ti - t0[j], x0 + 3 * j, v0 + 3 * j, acc2 + 3 * j, jrk6 + 3 * j, xj, vj);
+                cm_pair(xi, vi, xj, vj, mass[j], fcm, fcmd);
+                cm_pair(xi, vi, xk + 6 * q, vk + 6 * q, mk[2 * q], fp1, fpd1);
+                cm_pair(xi, vi, xk + 6 * q + 3, vk + 6 * q + 3, mk[2 * q + 1], fp2, fpd2);
+                for (int d = 0; d < 3; d++) {
+                    cf[d] += fp1[d] + fp2[d] - fcm[d];
+                    cd[d] += fpd1[d] + fpd2[d] - fcmd[d];
+                }
+            }
+        }
+        for (int d = 0; d < 3; d++) {
+            acc[3 * k + d] += cf[d];
+            jrk[3 * k + d] += cd[d];
+        }
+    }
+}

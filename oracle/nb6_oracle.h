@@ -60,6 +60,24 @@ void orc_firr(double ti, int ni, const int *addr, int nmax,
               const int *lists, int lmax,
               double *acc, double *jrk, int *nnbid);
 
+/* KS c.m. corrections of the irregular force, added into acc/jrk of the
+ * active bodies addr[ni] (1-based) as NBINT_COR adds them to FIRR and FD
+ * (nbint_cor.f:37-65): none for an empty neighbour list; for the c.m. of a
+ * perturbed pair, cmfirr_cor.f:13-130 over the pair's perturber list (each
+ * perturber that is itself a perturbed pair resolved into its components);
+ * for any other body, cmfirr_ucor.f:14-116 over the neighbours that are
+ * perturbed pairs.  slot[a-1] = pair p >= 0 when body a is the c.m. of
+ * perturbed pair p, else -1; pair p: components' positions xk[p][2][3] and
+ * velocities vk[p][2][3] at ti, masses mk[p][2], perturbers
+ * plist[pofs[p] .. pofs[p+1]) (1-based).  Bodies are predicted to ti as in
+ * orc_firr.  (The chain terms KCPERT_COR / CHFIRR are not restated.) */
+void orc_ks_cmcorr(double ti, int ni, const int *addr, const double *x0,
+                   const double *v0, const double *acc2, const double *jrk6,
+                   const double *mass, const double *t0, const int *lists,
+                   int lmax, const int *slot, const double *xk,
+                   const double *vk, const double *mk, const int *pofs,
+                   const int *plist, double *acc, double *jrk);
+
 #ifdef __cplusplus
 }
 #endif

@@ -128,3 +128,34 @@ def firr(ti, addr, x0, v0, acc2, jrk6, mass, t0, lists):
                     int(lmax), acc.ctypes.data_as(_d), jrk.ctypes.data_as(_d),
                     nnbid.ctypes.data_as(_i))
     return acc, jrk, nnbid
+
+
+def ks_cmcorr(ti, addr, x0, v0, acc2, jrk6, mass, t0, lists, slot, xk, vk, mk, pofs, plist, acc, jrk):
+    """acc, jrk of the active bodies addr (1-based) plus the KS c.m.
+    corrections of cmfirr_cor.f / cmfirr_ucor.f (returned as new arrays).
+    slot[a-1] = perturbed pair of c.m. body a or -1; xk, vk (npair, 2, 3),
+    mk (npair, 2); pofs (npair+1), plist 1-based perturbers."""
+    x0, v0, acc2, jrk6, mass, t0 = map(_f, (x0, v0, acc2, jrk6, mass, t0))
+    lists = np.ascontiguousarray(lists, dtype=np.int32)
+    addr = np.ascontiguousarray(addr, dtype=np.int32)
+    slot = np.ascontiguousarray(slot, dtype=np.int32)
+    xk = np.ascontiguousarray(xk, dtype=np.float64).reshape(-1, 6)
+    vk = np.ascontiguousarray(vk, dtype=np.float64).reshape(-1, 6)
+    mk = np.ascontiguousarray(mk, dtype=np.float64).reshape(-1, 2)
+    pofs = np.ascontiguousarray(pofs, dtype=np.int32)
+    plist = np.ascontiguousarray(plist, dtype=np.int32)
+    if plist.size == 0:
+        plist = np.zeros(1, dtype=np.int32)
+    if xk.size == 0:
+        xk, vk, mk = np.zeros((1, 6)), np.zeros((1, 6)), np.zeros((1, 2))
+    acc = np.array(acc, dtype=np.float64, order="C")
+    jrk = np.array(jrk, dtype=np.float64, order="C")
+    lmax = lists.shape[1]
+    fp64().orc_ks_cmcorr(C.c_double(float(ti)), int(addr.shape[0]), addr.ctypes.data_as(_i),
+                         x0.ctypes.data_as(_d), v0.ctypes.data_as(_d), acc2.ctypes.data_as(_d),
+                         jrk6.ctypes.data_as(_d), mass.ctypes.data_as(_d), t0.ctypes.data_as(_d),
+                         lists.ctypes.data_as(_i), int(lmax), slot.ctypes.data_as(_i),
+                         xk.ctypes.data_as(_d), vk.ctypes.data_as(_d), mk.ctypes.data_as(_d),
+                         pofs.ctypes.data_as(_i), plist.ctypes.data_as(_i),
+                         acc.ctypes.data_as(_d), jrk.ctypes.data_as(_d))
+    return acc, jrk
