@@ -462,13 +462,14 @@ def main():
     if not args.no_irr and rank == 0:
         irr = irregular_leg(lib, m, x, v, h2, dtr, args)
 
-    # accuracy against the FP64 oracle on a sample of i (rank 0)
+    # accuracy against the FP64 oracle on one call of the timed shape (a
+    # chunk of i, so the same tuned kernel and its far-tile path run; rank 0)
     err = None
     cpu = None
     if rank == 0:
         import oracle
         rng = np.random.default_rng(5)
-        isel = np.sort(rng.choice(n, 64, replace=False))
+        isel = np.sort(rng.choice(n, min(args.chunk, n), replace=False))
         a_g, j_g, p_g, l_g = lib.gpunb_regf(h2[isel], dtr[isel], x[isel], v[isel], args.lmax,
                                             args.nnbmax, args.m_flag)
         a_o, j_o, p_o, l_o = oracle.regf(m, x, v, h2[isel], dtr[isel], x[isel], v[isel],

@@ -93,6 +93,9 @@ struct RegArgs {
     // in the same spatial order, so a warp covers a compact region); null =
     // slot order.  Every index into i data and outputs stays the caller's.
     const int *__restrict__ iperm = nullptr;
+    // ordered j set only: positions relative to their tile's box centre,
+    // fl32(x - c), component-major (3 x npad) -- the far-tile operands
+    const float *__restrict__ comprel = nullptr;
 };
 
 struct IPart {
@@ -428,13 +431,52 @@ NB6_DEV unsigned pair_x2(const IP2 &ip, float2 xh, float2 yh, float2 zh, float2 
 
 // pair_x2 for a pair known not to be a neighbour candidate: the same
 // operations in the same order minus the candidate test, so its results are
-// bit-identical to pair_x2's for such a pair.
+// bit-identical to pair_x2's for such a pair.  (Kept for reference and for
+// a j set without relative coordinates; the far tiles of an ordered set
+// take pair_x2_rel.)
 template <bool MFLAG>
 NB6_DEV void pair_x2_far(const IP2 &ip, float2 xh, float2 yh, float2 zh, float2 m, float2 xl, float2 yl,
                          float2 zl, float2 vx, float2 vy, float2 vz, S2 &s) {
     const float2 dx = __fadd2_rn(__fadd2_rn(xh, ip.nxh), __fadd2_rn(xl, ip.nxl));
     const float2 dy = __fadd2_rn(__fadd2_rn(yh, ip.nyh), __fadd2_rn(yl, ip.nyl));
     const float2 dz = __fadd2_rn(__fadd2_rn(zh, ip.nzh), __fadd2_rn(zl, ip.nzl));
+    const float2 dvx = __fadd2_rn(vx, ip.nvx);
+    const float2 dvy = __fadd2_rn(vy, ip.nvy);
+    const float2 dvz = __fadd2_rn(vz, ip.nvz);
+    const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+    const float2 rv = __ffma2_rn(dz, dvz, __ffma2_rn(dy, dvy, __fmul2_rn(dx, dvx)));
+    float2 y0;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y0.x) : "f"(r2.x));
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y0.y) : "f"(r2.y));
+    const float2 ra = __fmul2_rn(r2, y0);
+    const float2 nb = __ffma2_rn(ra, y0, dup2(-3.0f));
+    const float2 ny = __fmul2_rn(y0, nb);
+    const float2 y2 = __fmul2_rn(ny, ny);
+    const float2 nmy = __fmul2_rn(m, ny);
+    const float2 nmy3 = __fmul2_rn(nmy, y2);
+    const float2 al = __fmul2_rn(__fmul2_rn(y2, dup2(-0.75f)), rv);
+    s.po = __fadd2_rn(s.po, nmy);
+    s.ax = __ffma2_rn(nmy3, dx, s.ax);
+    s.ay = __ffma2_rn(nmy3, dy, s.ay);
+    s.az = __ffma2_rn(nmy3, dz, s.az);
+    s.jx = __ffma2_rn(nmy3, __ffma2_rn(al, dx, dvx), s.jx);
+    s.jy = __ffma2_rn(nmy3, __ffma2_rn(al, dy, dvy), s.jy);
+    s.jz = __ffma2_rn(nmy3, __ffma2_rn(al, dz, dvz), s.jz);
+}
+
+// Far pair from tile-relative coordinates: xr = fl32(x_j - c) (stored with
+// the ordered j set) and nxr = -fl32(x_i - c) (formed per tile in FP64), c
+// the tile's box centre, so each difference is one FP32 add instead of
+// three.  With the tile at least one half extent h away from i, the
+// three roundings (of x_j - c, x_i - c and their difference) stay within
+// u (|x_j - c| + |x_i - c| + r) <= u (2h + 2r) <= 4u r of the separation r
+// (u = 2^-24): four FP32 ulps of an FP64-formed difference at most.
+template <bool MFLAG>
+NB6_DEV void pair_x2_rel(const IP2 &ip, float2 nxr, float2 nyr, float2 nzr, float2 xr, float2 yr, float2 zr,
+                         float2 m, float2 vx, float2 vy, float2 vz, S2 &s) {
+    const float2 dx = __fadd2_rn(xr, nxr);
+    const float2 dy = __fadd2_rn(yr, nyr);
+    const float2 dz = __fadd2_rn(zr, nzr);
     const float2 dvx = __fadd2_rn(vx, ip.nvx);
     const float2 dvy = __fadd2_rn(vy, ip.nvy);
     const float2 dvz = __fadd2_rn(vz, ip.nvz);
@@ -474,7 +516,9 @@ NB6_DEV bool tile_far(const IP2 &ip, float vabs, float4 bc, float4 bh) {
     const float mag = fmaxf(fmaxf(fabsf(xi), fabsf(yi)), fabsf(zi)) +
                       fmaxf(fmaxf(fabsf(bc.x) + bh.x, fabsf(bc.y) + bh.y), fabsf(bc.z) + bh.z);
     const float reach = (sqrtf(crit) + ip.dt.x * (vabs + bc.w)) * 1.001f + mag * 1.0e-6f;
-    return d2 > reach * reach;
+    // and, for the relative coordinates, at least one half extent away
+    const float hmax = fmaxf(fmaxf(bh.x, bh.y), bh.z);
+    return d2 > reach * reach && d2 > hmax * hmax;
 }
 
 // Same pair math with the coordinate differences formed in FP64 and rounded
@@ -540,7 +584,9 @@ NB6_DEV Sums reg_flush_mask(const RegArgs &a, int i, unsigned mask, int jbase, S
 template <bool F64DX>
 NB6_DEV void issue_tile_soa(const RegArgs &a, float (*stage)[JT], uint64_t *bar, int tile) {
     const size_t off = (size_t)tile * JT;
-    mbar_arrive_expect_tx(bar, (uint32_t)(NB6_NCOMP * JT * sizeof(float)));
+    // rows 10..12: the tile-relative positions of an ordered j set
+    const bool rel = !F64DX && a.comprel != nullptr;
+    mbar_arrive_expect_tx(bar, (uint32_t)((NB6_NCOMP + (rel ? 3 : 0)) * JT * sizeof(float)));
     if constexpr (F64DX) {
 #pragma unroll
         for (int c = 0; c < 3; ++c)
@@ -553,12 +599,17 @@ NB6_DEV void issue_tile_soa(const RegArgs &a, float (*stage)[JT], uint64_t *bar,
 #pragma unroll
         for (int c = 0; c < NB6_NCOMP; ++c)
             bulk_g2s(stage[c], a.comp + (size_t)c * a.npad + off, JT * sizeof(float), bar);
+        if (rel) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+                bulk_g2s(stage[NB6_NCOMP + c], a.comprel + (size_t)c * a.npad + off, JT * sizeof(float), bar);
+        }
     }
 }
 
 template <int NI, bool MFLAG, bool F64DX = false>
 __global__ void __launch_bounds__(NT, X2_MINB / NI) regf_x2_kernel(const RegArgs a) {
-    __shared__ __align__(128) float sj[NSTAGE][NB6_NCOMP][JT];
+    __shared__ __align__(128) float sj[NSTAGE][NB6_NCOMP + 3][JT];
     __shared__ __align__(8) uint64_t bar[NSTAGE];
     __shared__ __align__(8) uint64_t ebar[NSTAGE];
     // double-single accumulators, touched once per tile: kept in shared
@@ -656,14 +707,23 @@ __global__ void __launch_bounds__(NT, X2_MINB / NI) regf_x2_kernel(const RegArgs
         const int jt0 = tile * JT;
         // whole warp out of reach of this tile: no candidates, short loop
         bool far = false;
+        float2 nxr[NI], nyr[NI], nzr[NI];  // -fl32(x_i - c) of this tile (far path)
         if constexpr (!F64DX && NI == 1) {  // (two i per thread: no registers left for it)
-            if (a.tbox) {
+            if (a.comprel) {
                 const float4 bc = __ldg(&a.tbox[2 * tile]);
                 const float4 bh = __ldg(&a.tbox[2 * tile + 1]);
                 bool f = true;
 #pragma unroll
                 for (int k = 0; k < NI; ++k) f = f && (ii[k] >= a.ni || tile_far<MFLAG>(ip[k], vabs[k], bc, bh));
                 far = __all_sync(0xffffffffu, f);
+                if (far) {
+#pragma unroll
+                    for (int k = 0; k < NI; ++k) {
+                        nxr[k] = dup2(-__double2float_rn(xd[k] - (double)bc.x));
+                        nyr[k] = dup2(-__double2float_rn(yd[k] - (double)bc.y));
+                        nzr[k] = dup2(-__double2float_rn(zd[k] - (double)bc.z));
+                    }
+                }
             }
         }
         if constexpr (!F64DX && NI == 1) {
@@ -673,27 +733,22 @@ __global__ void __launch_bounds__(NT, X2_MINB / NI) regf_x2_kernel(const RegArgs
 #pragma unroll
                 for (int u = 0; u < 32; u += 4) {
                     const int q = g * 32 + u;
-                    const float4 XH = *reinterpret_cast<const float4 *>(&S[0][q]);
-                    const float4 YH = *reinterpret_cast<const float4 *>(&S[1][q]);
-                    const float4 ZH = *reinterpret_cast<const float4 *>(&S[2][q]);
                     const float4 MM = *reinterpret_cast<const float4 *>(&S[3][q]);
-                    const float4 XL = *reinterpret_cast<const float4 *>(&S[4][q]);
-                    const float4 YL = *reinterpret_cast<const float4 *>(&S[5][q]);
-                    const float4 ZL = *reinterpret_cast<const float4 *>(&S[6][q]);
                     const float4 VX = *reinterpret_cast<const float4 *>(&S[7][q]);
                     const float4 VY = *reinterpret_cast<const float4 *>(&S[8][q]);
                     const float4 VZ = *reinterpret_cast<const float4 *>(&S[9][q]);
+                    const float4 XR = *reinterpret_cast<const float4 *>(&S[NB6_NCOMP][q]);
+                    const float4 YR = *reinterpret_cast<const float4 *>(&S[NB6_NCOMP + 1][q]);
+                    const float4 ZR = *reinterpret_cast<const float4 *>(&S[NB6_NCOMP + 2][q]);
 #pragma unroll
                     for (int k = 0; k < NI; ++k) {
-                        pair_x2_far<MFLAG>(ip[k], make_float2(XH.x, XH.y), make_float2(YH.x, YH.y),
-                                           make_float2(ZH.x, ZH.y), make_float2(MM.x, MM.y),
-                                           make_float2(XL.x, XL.y), make_float2(YL.x, YL.y),
-                                           make_float2(ZL.x, ZL.y), make_float2(VX.x, VX.y),
+                        pair_x2_rel<MFLAG>(ip[k], nxr[k], nyr[k], nzr[k], make_float2(XR.x, XR.y),
+                                           make_float2(YR.x, YR.y), make_float2(ZR.x, ZR.y),
+                                           make_float2(MM.x, MM.y), make_float2(VX.x, VX.y),
                                            make_float2(VY.x, VY.y), make_float2(VZ.x, VZ.y), s[k]);
-                        pair_x2_far<MFLAG>(ip[k], make_float2(XH.z, XH.w), make_float2(YH.z, YH.w),
-                                           make_float2(ZH.z, ZH.w), make_float2(MM.z, MM.w),
-                                           make_float2(XL.z, XL.w), make_float2(YL.z, YL.w),
-                                           make_float2(ZL.z, ZL.w), make_float2(VX.z, VX.w),
+                        pair_x2_rel<MFLAG>(ip[k], nxr[k], nyr[k], nzr[k], make_float2(XR.z, XR.w),
+                                           make_float2(YR.z, YR.w), make_float2(ZR.z, ZR.w),
+                                           make_float2(MM.z, MM.w), make_float2(VX.z, VX.w),
                                            make_float2(VY.z, VY.w), make_float2(VZ.z, VZ.w), s[k]);
                     }
                 }
@@ -1222,7 +1277,7 @@ struct RegState {
     int use_jsort = -1;                // -1 = read NB6_JSORT on first use
     long long jver = 0, sorted_ver = -1;
     DevBuf<float4> posH_s, posL_s, vel_s, tbox;
-    DevBuf<float> comp_s;
+    DevBuf<float> comp_s, comprel;  // ordered layout; tile-relative positions (3 x npad)
     DevBuf<double> compd_s;
     DevBuf<int> perm, vals_in, iperm;
     DevBuf<unsigned> keys_in, keys_out, ext;
@@ -1485,6 +1540,21 @@ __global__ void jset_tile_boxes(int nj, int ntile, const float4 *__restrict__ po
     }
 }
 
+// Tile-relative positions of the ordered j set: xr = fl32(x - c) with c the
+// box centre of the body's tile (an FP32 number, so x - c is formed exactly
+// in FP64 up to one rounding).  Padding slots keep their far-away marker.
+__global__ void jset_rel(int npad, int ntile, const double *__restrict__ compd, const float4 *__restrict__ tbox,
+                         float *__restrict__ comprel) {
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < (size_t)npad;
+         q += (size_t)gridDim.x * blockDim.x) {
+        const int t = (int)(q / JT);
+        const float4 c = t < ntile ? tbox[2 * t] : make_float4(0.f, 0.f, 0.f, 0.f);
+        comprel[q] = __double2float_rn(compd[q] - (double)c.x);
+        comprel[(size_t)npad + q] = __double2float_rn(compd[(size_t)npad + q] - (double)c.y);
+        comprel[2 * (size_t)npad + q] = __double2float_rn(compd[2 * (size_t)npad + q] - (double)c.z);
+    }
+}
+
 // Spatial order of the active set of one call (ni <= ISORT_MAX): Morton keys
 // on the j set's grid, bitonic sort of (key, index) in one CTA.
 constexpr int ISORT_MAX = 4096;
@@ -1604,6 +1674,8 @@ static bool ensure_sorted(cudaStream_t st) {
     const int pblocks = (int)std::min<size_t>((np + 255) / 256, (size_t)nb6_num_sms() * 8);
     jset_permute<<<pblocks, 256, 0, st>>>(nj, src, dst, R.perm.ptr);
     jset_tile_boxes<<<(R.ntile * 32 + 255) / 256, 256, 0, st>>>(nj, R.ntile, R.posH_s.ptr, R.vel_s.ptr, R.tbox.ptr);
+    R.comprel.reserve((size_t)3 * np);
+    jset_rel<<<pblocks, 256, 0, st>>>((int)np, R.ntile, R.compd_s.ptr, R.tbox.ptr, R.comprel.ptr);
     NB6_CUDA_CHECK(cudaGetLastError());
     R.sorted_ver = R.jver;
     return true;
@@ -1730,6 +1802,7 @@ static void regf_prepare(int ni, const double *d_h2, const double *d_dtr, const 
         return (e && atoi(e) == 0) ? 0 : 1;
     }();
     a.tbox = (sorted && far_path) ? R.tbox.ptr : nullptr;
+    a.comprel = (sorted && far_path) ? R.comprel.ptr : nullptr;
     static const int i_order = [] {
         const char *e = getenv("NB6_IORDER");
         return (e && atoi(e) == 0) ? 0 : 1;
@@ -1825,6 +1898,7 @@ static void regf_prepare(int ni, const double *d_h2, const double *d_dtr, const 
         a.perm = nullptr;
         a.tbox = nullptr;
         a.iperm = nullptr;
+        a.comprel = nullptr;
     }
     R.last_geometry[0] = plan.variant;
     R.last_geometry[1] = plan.igrid;
