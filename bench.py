@@ -45,10 +45,10 @@ import numpy as np  # noqa: E402
 METRIC = "Regular force+jerk+nbr pair interactions/s at N=1M"
 FLOPS_PER_PAIR = 60          # gpunb.velocity.cu:895, reg.avx.cpp:343
 # DRAM bytes (read + write) per launch of the headline force kernel,
-# regf_x2_kernel<1> with 1024 i x 996,147 j over the Morton-ordered j set,
-# from the ncu capture summarised in profiles/regf_x2_kernel_king1m.md
-# (57.61 MB read + 0.73 MB written).
-NCU_TRAFFIC_PER_LAUNCH = 57.61e6 + 0.734e6
+# regf_x2_kernel<1> with 1024 i x 996,147 j over the Morton-ordered j set
+# (tile-relative far operands included), from one ncu capture of that
+# launch: dram__bytes_read.sum 69.58 MB + dram__bytes_write.sum 2.22 MB.
+NCU_TRAFFIC_PER_LAUNCH = 69.58e6 + 2.22e6
 
 
 def parse():
