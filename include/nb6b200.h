@@ -225,6 +225,25 @@ void nb6_regf_correct_(double *time, int *ni, int *addr, int *iseg, int *nseg, i
  * (KCPERT_COR, CHFIRR, FCHAIN) stay on the host. */
 void nb6_ks_set_(int *npair, int *cm, double *xk, double *vk, double *mk, int *pofs, int *plist);
 
+/* Device block clock (no reference counterpart; next_tlist.f and the block
+ * loop of intgrt.F run on the host there).  After nb6_hermite_open_ and the
+ * state of every body: runs blocks of irregular steps on the device, each
+ * block the bodies with the earliest T0 + STEP (bit for bit the host's
+ * choice) corrected as by nb6_irr_correct_, until a block has bodies due a
+ * regular step (*reason = 1: that block's irregular part is done), the next
+ * block time passes *tlimit (*reason = 2: not started) or *max_blocks
+ * blocks ran (*reason = 0).  *nblocks, *nirr: blocks and irregular steps of
+ * the call; *tblock, *nact: time and active count of the last block.
+ * nb6_blocks_regular_ then gives that block's regular-due bodies (ascending
+ * 1-based addresses, their corrected x0[3], v0[3] in xv[k][6]) for
+ * nb6_irr_predict_send_ + nb6_regf_correct_; nb6_blocks_active_ its whole
+ * active set (in no particular order) with the 24-double corrector rows of
+ * nb6_irr_correct_. */
+void nb6_blocks_run_(double *tlimit, int *max_blocks, int *reason, long long *nblocks, long long *nirr,
+                     double *tblock, int *nact);
+void nb6_blocks_regular_(int *nreg, int *addr, double *xv);
+void nb6_blocks_active_(int *nact, int *addr, double *rows);
+
 /* The device-resident state of bodies *a0 .. *a0 + *n - 1 (1-based), for a
  * host that lets the device correctors keep it (energy output, the end of
  * a run): rows of 32 doubles x0[3], v0[3], F[3], FDOT[3], fi[3], fidot[3],

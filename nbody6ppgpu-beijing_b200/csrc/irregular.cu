@@ -272,13 +272,12 @@ NB6_DEV double tstep_dev(const double *f, const double *f1, const double *f2, co
 // predicted from their old state, as on the host), then each body is
 // corrected.  out row k (24 doubles): x0[3], v0[3], fi[3], fidot[3], F[3],
 // FDOT[3], step, regular-due flag, nnbid, 0, 0, 0.
-__global__ void irr_apply_corrector(int ni, const int *__restrict__ addr, double time,
-                                    const double *__restrict__ force, Rec *__restrict__ rec,
-                                    Aux *__restrict__ aux, HermiteParams hp, double *__restrict__ out) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= ni) return;
-    const int i = addr[k] - 1;
-    const double *fk = force + (size_t)k * 8;
+// The corrector of body i (0-based) at `time` from its force row fk, out row
+// o (24 doubles); tn[i] = t0 + step, the body's next block time, is kept for
+// the device block clock.  Returns the regular-due flag.
+NB6_DEV bool correct_irr_body(int i, double time, const double *__restrict__ fk, Rec *__restrict__ rec,
+                              Aux *__restrict__ aux, const HermiteParams &hp, double *__restrict__ o,
+                              double *__restrict__ tn) {
     const double a[3] = {fk[0], fk[1], fk[2]}, jd[3] = {fk[3], fk[4], fk[5]};
     const int id = (int)fk[6];
     Rec r = rec[i];
@@ -332,7 +331,7 @@ __global__ void irr_apply_corrector(int ni, const int *__restrict__ addr, double
     }
     rec[i] = r;
     aux[i] = x;
-    double *o = out + (size_t)k * 24;
+    tn[i] = dadd(r.t0, x.step);
     for (int c = 0; c < 3; ++c) {
         o[c] = r.x[c];
         o[3 + c] = r.v[c];
@@ -345,6 +344,16 @@ __global__ void irr_apply_corrector(int ni, const int *__restrict__ addr, double
     o[19] = regdue ? 1.0 : 0.0;
     o[20] = (double)id;
     o[21] = o[22] = o[23] = 0.0;
+    return regdue;
+}
+
+__global__ void irr_apply_corrector(int ni, const int *__restrict__ addr, double time,
+                                    const double *__restrict__ force, Rec *__restrict__ rec,
+                                    Aux *__restrict__ aux, HermiteParams hp, double *__restrict__ out,
+                                    double *__restrict__ tn) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= ni) return;
+    correct_irr_body(addr[k] - 1, time, force + (size_t)k * 8, rec, aux, hp, out + (size_t)k * 24, tn);
 }
 
 // ----------------------------------------------------------------------------
@@ -387,7 +396,8 @@ __global__ void reg_corrector_kernel(int ni, const int *__restrict__ addr, const
                                      const int *__restrict__ seg_j0, const int *__restrict__ seg_a0, double time,
                                      RegDeviceOut ro, Rec *__restrict__ rec, Aux *__restrict__ aux,
                                      int *__restrict__ lists, int ls, const double *__restrict__ rs_in,
-                                     RegCorrParams p, double *__restrict__ out, int *status) {
+                                     RegCorrParams p, double *__restrict__ out, int *status,
+                                     double *__restrict__ tn) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= ni) return;
     const int i = addr[k] - 1, sg = iseg[k];
@@ -553,6 +563,7 @@ __global__ void reg_corrector_kernel(int ni, const int *__restrict__ addr, const
     x.rs = rs;
     rec[i] = r;
     aux[i] = x;
+    tn[i] = dadd(r.t0, x.step);
     for (int c = 0; c < 3; ++c) {
         o[c] = r.x[c];
         o[3 + c] = r.v[c];
@@ -568,6 +579,149 @@ __global__ void reg_corrector_kernel(int ni, const int *__restrict__ addr, const
     o[26] = rs;
     o[27] = (double)nnb;
     o[29] = outcome;
+}
+
+// ----------------------------------------------------------------------------
+// Device block clock (nb6_blocks_run_): blocks of irregular steps run back to
+// back on the device, each as four launches of one CUDA graph --
+//   blk_min      the block time, min over all bodies of tn = t0 + step;
+//   blk_collect  the active set {i : tn_i == block time} (next_tlist.f picks
+//                the same set from its level lists), or a stop when the
+//                block time passes the caller's limit;
+//   blk_irr      the neighbour force of every active body (irr_force_warp);
+//   blk_corr     the irregular corrector of every active body (the same
+//                correct_irr_body as nb6_irr_correct_), then, in the last CTA
+//                to finish, the block's bookkeeping and a stop when a body is
+//                due a regular step (the host runs the regular part).
+// A stopped control block turns every later launch into an early return, so
+// the host enqueues many blocks and synchronises once.  No kernel waits on
+// another: the ordering is the stream's, the last-CTA test is one atomic.
+// ----------------------------------------------------------------------------
+struct BlockCtl {
+    unsigned long long tmin_bits[2];  // per parity: min tn as the bits of a non-negative double
+    int nact[2];                      // per parity: active count
+    int parity;
+    int stop;                         // 0 run; 1 a regular-due block's irregular part is done; 2 block time > tlimit
+    int regdue;                       // the running block has a regular-due body
+    unsigned cta_done;                // blk_corr CTAs finished (last-CTA test)
+    long long blocks, irr_steps;      // since the last reset by the host
+    double tlimit, tblock;            // run limit; time of the last block done
+    int last_nact;
+    int nreg;                         // regular-due bodies of the running block (breg, bregxv)
+};
+
+constexpr int BLK_NT = 256;
+
+__global__ void __launch_bounds__(BLK_NT) blk_min(int n, const double *__restrict__ tn, BlockCtl *c) {
+    if (c->stop) return;
+    const int p = c->parity;
+    unsigned long long m = ~0ull;
+    for (size_t i = blockIdx.x * (size_t)BLK_NT + threadIdx.x; i < (size_t)n; i += (size_t)gridDim.x * BLK_NT)
+        m = min(m, (unsigned long long)__double_as_longlong(tn[i]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = min(m, __shfl_xor_sync(0xffffffffu, m, o));
+    __shared__ unsigned long long wm[BLK_NT / 32];
+    if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < BLK_NT / 32; ++w) m = min(m, wm[w]);
+        atomicMin(&c->tmin_bits[p], m);
+    }
+}
+
+__global__ void __launch_bounds__(BLK_NT) blk_collect(int n, const double *__restrict__ tn, BlockCtl *c,
+                                                      int *__restrict__ act) {
+    if (c->stop) return;
+    const int p = c->parity;
+    const double t = __longlong_as_double((long long)c->tmin_bits[p]);
+    if (t > c->tlimit) {  // every thread reads the same t: all return
+        if (blockIdx.x == 0 && threadIdx.x == 0) c->stop = 2;
+        return;
+    }
+    const int lane = threadIdx.x & 31;
+    for (size_t i0 = blockIdx.x * (size_t)BLK_NT; i0 < (size_t)n; i0 += (size_t)gridDim.x * BLK_NT) {
+        const size_t i = i0 + threadIdx.x;
+        const bool on = i < (size_t)n && tn[i] == t;
+        const unsigned b = __ballot_sync(0xffffffffu, on);
+        if (b) {
+            int base = 0;
+            if (lane == 0) base = atomicAdd(&c->nact[p], __popc(b));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (on) act[base + __popc(b & ((1u << lane) - 1u))] = (int)i;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {  // the next block's accumulators; this block's list
+        c->tmin_bits[p ^ 1] = ~0ull;
+        c->nact[p ^ 1] = 0;
+        c->nreg = 0;
+    }
+}
+
+template <bool KS>
+__global__ void __launch_bounds__(IRR_WARPS * 32)
+    blk_irr(const BlockCtl *c, const int *__restrict__ act, const Rec *__restrict__ rec,
+            const int *__restrict__ lists, int ls, int nmax, KsArgs ks, double *__restrict__ out) {
+    if (c->stop) return;
+    const int p = c->parity, na = c->nact[p];
+    const double t = __longlong_as_double((long long)c->tmin_bits[p]);
+    const int lane = threadIdx.x & 31;
+    for (int k = blockIdx.x * IRR_WARPS + (threadIdx.x >> 5); k < na; k += gridDim.x * IRR_WARPS) {
+        double a[3], jd[3];
+        int id;
+        irr_force_warp<KS>(act[k], lane, t, rec, lists, ls, nmax, ks, a, jd, id);
+        if (lane == 0) {
+            double *o = out + (size_t)k * 8;
+            o[0] = a[0];
+            o[1] = a[1];
+            o[2] = a[2];
+            o[3] = jd[0];
+            o[4] = jd[1];
+            o[5] = jd[2];
+            o[6] = (double)id;
+            o[7] = 0.0;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(BLK_NT)
+    blk_corr(BlockCtl *c, const int *__restrict__ act, const double *__restrict__ force, Rec *__restrict__ rec,
+             Aux *__restrict__ aux, HermiteParams hp, double *__restrict__ rows, double *__restrict__ tn,
+             int *__restrict__ reg, double *__restrict__ regxv) {
+    if (c->stop) return;
+    const int p = c->parity, na = c->nact[p];
+    const double t = __longlong_as_double((long long)c->tmin_bits[p]);
+    bool due = false;
+    for (int k = blockIdx.x * BLK_NT + threadIdx.x; k < na; k += gridDim.x * BLK_NT) {
+        double *o = rows + (size_t)k * 24;
+        if (correct_irr_body(act[k], t, force + (size_t)k * 8, rec, aux, hp, o, tn)) {
+            due = true;
+            const int q = atomicAdd(&c->nreg, 1);  // (q < na <= nmax)
+            reg[q] = act[k];
+            for (int d = 0; d < 6; ++d) regxv[6 * (size_t)q + d] = o[d];  // x0, v0
+        }
+    }
+    if (__syncthreads_or(due) && threadIdx.x == 0) atomicOr(&c->regdue, 1);
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&c->cta_done, 1u) == gridDim.x - 1) {  // last CTA: the block is done
+            __threadfence();
+            c->cta_done = 0;
+            c->blocks += 1;
+            c->irr_steps += na;
+            c->tblock = t;
+            c->last_nact = na;
+            c->parity = p ^ 1;
+            if (atomicExch(&c->regdue, 0)) c->stop = 1;
+        }
+    }
+}
+
+// tn = t0 + step of every body (after host staging)
+__global__ void blk_clock_sync(int n, const Rec *__restrict__ rec, const Aux *__restrict__ aux,
+                               double *__restrict__ tn) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < (size_t)n;
+         i += (size_t)gridDim.x * blockDim.x)
+        tn[i] = dadd(rec[i].t0, aux[i].step);
 }
 
 // The resident Hermite state of addresses a0 .. a0+n-1 (0-based), one row
@@ -714,6 +868,21 @@ struct IrrState {
     HostBuf<int> ks_hint;
     HostBuf<double> ks_hdbl;
     int ks_npair = 0;
+    // device block clock (nb6_blocks_run_): tn[i] = t0 + step of every
+    // body, kept by the correctors; recomputed after host staging
+    DevBuf<double> tn;
+    bool clock_dirty = true;
+    DevBuf<int> bact;                 // active set of the running block
+    DevBuf<double> bforce, brows;     // its force rows [nmax][8], corrector rows [nmax][24]
+    DevBuf<BlockCtl> bctl;
+    HostBuf<BlockCtl> hctl;
+    cudaGraphExec_t bgraph = nullptr;
+    const void *bgraph_key[8] = {};   // buffers and pair-table flag the graph was made with
+    int blk_batch = 16;               // graph launches per synchronisation
+    DevBuf<int> breg;                 // regular-due bodies of the running block
+    DevBuf<double> bregxv;            // their x0, v0
+    long long rc_calls = 0;           // nb6_regf_correct_ calls and their host-side phases
+    double rc_t[4] = {0, 0, 0, 0};
 };
 IrrState I;
 
@@ -785,6 +954,18 @@ void irr_close_impl() {
     I.dseg.release();
     I.hseg.release();
     I.aux.release();
+    I.tn.release();
+    I.clock_dirty = true;
+    if (I.bgraph) cudaGraphExecDestroy(I.bgraph);
+    I.bgraph = nullptr;
+    memset(I.bgraph_key, 0, sizeof(I.bgraph_key));
+    I.bact.release();
+    I.breg.release();
+    I.bregxv.release();
+    I.bforce.release();
+    I.brows.release();
+    I.bctl.release();
+    I.hctl.release();
     I.dstage_aux.release();
     I.dstage_aux_addr.release();
     I.hstage_aux.release();
@@ -913,6 +1094,7 @@ const int *irr_flush(cudaStream_t st, const int *active = nullptr, int ni = 0) {
         NB6_CUDA_CHECK(cudaGetLastError());
         for (int q = 0; q < I.naux; ++q) I.aux_slot[I.hstage_aux_addr.ptr[q]] = -1;
         I.naux = 0;
+        I.clock_dirty = true;
     }
     // keep only the latest list entry per particle
     int ne = 0;
@@ -961,6 +1143,7 @@ const int *irr_flush(cudaStream_t st, const int *active = nullptr, int ni = 0) {
         NB6_CUDA_CHECK(cudaGetLastError());
     }
     for (int q = 0; q < njp; ++q) I.jp_slot[I.hstage_addr.ptr[q]] = -1;
+    if (njp) I.clock_dirty = true;
     I.njp = 0;
     I.nlist = 0;
     I.list_words = 0;
@@ -1033,6 +1216,8 @@ void hermite_open_impl(double eta_i, double smax, double dtmin) {
     }
     I.aux.reserve((size_t)I.nmax + 1);
     NB6_CUDA_CHECK(cudaMemsetAsync(I.aux.ptr, 0, sizeof(Aux) * ((size_t)I.nmax + 1), nb6_stream()));
+    I.tn.reserve((size_t)I.nmax + 1);
+    I.clock_dirty = true;
     I.aux_slot.assign(I.nmax, -1);
     I.naux = 0;
     I.hp.eta_i = eta_i;
@@ -1116,7 +1301,8 @@ void irr_correct_impl(double time, int ni, const int *addr, double *out) {
     launch_irr_kernel(ni, daddr, time, force, st);
     NB6_CUDA_CHECK(cudaGetLastError());
     NB6_CUDA_CHECK(cudaEventRecord(I.ev1, st));
-    irr_apply_corrector<<<(ni + 127) / 128, 128, 0, st>>>(ni, daddr, time, force, I.rec.ptr, I.aux.ptr, I.hp, o);
+    irr_apply_corrector<<<(ni + 127) / 128, 128, 0, st>>>(ni, daddr, time, force, I.rec.ptr, I.aux.ptr, I.hp, o,
+                                                          I.tn.ptr);
     NB6_CUDA_CHECK(cudaGetLastError());
     if (!direct)
         NB6_CUDA_CHECK(cudaMemcpyAsync(I.hout.ptr, o, sizeof(double) * rowd * ni, cudaMemcpyDeviceToHost, st));
@@ -1191,6 +1377,145 @@ void ks_set_impl(int npair, const int *cm, const double *xk, const double *vk, c
     I.ks_npair = npair;
 }
 
+// Capture the four launches of one block as a graph (rebuilt when a buffer
+// moved or the pair table came or went).
+bool blocks_graph(cudaStream_t st) {
+    const KsArgs ks = ks_args();
+    const void *key[8] = {I.bact.ptr, I.bforce.ptr, I.brows.ptr, I.bctl.ptr, I.tn.ptr, I.breg.ptr, I.bregxv.ptr,
+                          ks.slot ? (const void *)I.ks_slot.ptr : nullptr};
+    // (a pair table's layout depends on its size: with one set, capture anew)
+    if (I.bgraph && memcmp(key, I.bgraph_key, sizeof(key)) == 0 && !ks.slot) return true;
+    if (I.bgraph) {
+        cudaGraphExecDestroy(I.bgraph);
+        I.bgraph = nullptr;
+    }
+    const int sms = nb6_num_sms();
+    cudaGraph_t g = nullptr;
+    if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return false;
+    blk_min<<<sms * 4, BLK_NT, 0, st>>>(I.nmax, I.tn.ptr, I.bctl.ptr);
+    blk_collect<<<sms * 4, BLK_NT, 0, st>>>(I.nmax, I.tn.ptr, I.bctl.ptr, I.bact.ptr);
+    if (ks.slot)
+        blk_irr<true><<<sms * 12, IRR_WARPS * 32, 0, st>>>(I.bctl.ptr, I.bact.ptr, I.rec.ptr, I.lists.ptr, I.lmax,
+                                                           I.nmax, ks, I.bforce.ptr);
+    else
+        blk_irr<false><<<sms * 12, IRR_WARPS * 32, 0, st>>>(I.bctl.ptr, I.bact.ptr, I.rec.ptr, I.lists.ptr, I.lmax,
+                                                            I.nmax, ks, I.bforce.ptr);
+    blk_corr<<<sms * 2, BLK_NT, 0, st>>>(I.bctl.ptr, I.bact.ptr, I.bforce.ptr, I.rec.ptr, I.aux.ptr, I.hp,
+                                          I.brows.ptr, I.tn.ptr, I.breg.ptr, I.bregxv.ptr);
+    if (cudaStreamEndCapture(st, &g) != cudaSuccess || !g) return false;
+    const bool ok = cudaGraphInstantiate(&I.bgraph, g, 0) == cudaSuccess;
+    cudaGraphDestroy(g);
+    if (!ok) {
+        I.bgraph = nullptr;
+        return false;
+    }
+    memcpy(I.bgraph_key, key, sizeof(key));
+    return true;
+}
+
+void blocks_run_impl(double tlimit, int max_blocks, int *reason, long long *nblocks, long long *nirr,
+                     double *tblock, int *nact) {
+    *reason = 0;
+    *nblocks = *nirr = 0;
+    *nact = 0;
+    if (!I.open || !I.hermite) {
+        nb6_fatal(NB6_ERR_NOT_OPEN);
+        return;
+    }
+    if (max_blocks < 1 || tlimit != tlimit) {
+        nb6_fatal(NB6_ERR_BAD_ARG);
+        return;
+    }
+    const double t0 = nb6_wtime();
+    cudaStream_t st = nb6_stream();
+    irr_flush(st);
+    I.bact.reserve((size_t)I.nmax);
+    I.bforce.reserve((size_t)I.nmax * 8);
+    I.brows.reserve((size_t)I.nmax * 24);
+    I.breg.reserve((size_t)I.nmax);
+    I.bregxv.reserve((size_t)I.nmax * 6);
+    I.bctl.reserve(1);
+    I.hctl.reserve(1);
+    if (I.clock_dirty) {
+        blk_clock_sync<<<nb6_num_sms() * 8, 256, 0, st>>>(I.nmax, I.rec.ptr, I.aux.ptr, I.tn.ptr);
+        NB6_CUDA_CHECK(cudaGetLastError());
+        I.clock_dirty = false;
+    }
+    BlockCtl &h = *I.hctl.ptr;
+    memset(&h, 0, sizeof(h));
+    h.tmin_bits[0] = h.tmin_bits[1] = ~0ull;
+    h.tlimit = tlimit;
+    NB6_CUDA_CHECK(cudaMemcpyAsync(I.bctl.ptr, &h, sizeof(BlockCtl), cudaMemcpyHostToDevice, st));
+    if (!blocks_graph(st)) {
+        fprintf(stderr, "nb6_blocks_run: the block graph could not be built\n");
+        nb6_fatal(NB6_ERR_CUDA);
+        return;
+    }
+    long long done = 0;
+    int batch = I.blk_batch;
+    for (;;) {
+        const int k = (int)std::min<long long>(batch, (long long)max_blocks - done);
+        for (int b = 0; b < k; ++b) NB6_CUDA_CHECK(cudaGraphLaunch(I.bgraph, st));
+        NB6_CUDA_CHECK(cudaMemcpyAsync(&h, I.bctl.ptr, sizeof(BlockCtl), cudaMemcpyDeviceToHost, st));
+        nb6_status_fetch(st);
+        NB6_CUDA_CHECK(cudaStreamSynchronize(st));
+        if (nb6_check_dev_status() != 0) return;
+        done = h.blocks;
+        if (h.stop || done >= max_blocks) break;
+        batch = std::min(batch * 2, 256);
+    }
+    // next run's first batch: about twice this run's length
+    I.blk_batch = (int)std::max<long long>(2, std::min<long long>(128, 2 * done));
+    *reason = h.stop;
+    *nblocks = h.blocks;
+    *nirr = h.irr_steps;
+    *tblock = h.tblock;
+    *nact = h.last_nact;
+    I.time_grav += nb6_wtime() - t0;
+    I.num_fcall += (unsigned long long)h.blocks;
+    I.num_steps += (unsigned long long)h.irr_steps;
+}
+
+void blocks_active_impl(int *nact, int *addr, double *rows) {
+    if (!I.open || !I.hermite || !I.hctl.ptr) {
+        nb6_fatal(NB6_ERR_NOT_OPEN);
+        return;
+    }
+    const int na = I.hctl.ptr->last_nact;
+    *nact = na;
+    if (na <= 0) return;
+    cudaStream_t st = nb6_stream();
+    NB6_CUDA_CHECK(cudaMemcpyAsync(addr, I.bact.ptr, sizeof(int) * na, cudaMemcpyDeviceToHost, st));
+    NB6_CUDA_CHECK(cudaMemcpyAsync(rows, I.brows.ptr, sizeof(double) * 24 * (size_t)na, cudaMemcpyDeviceToHost, st));
+    NB6_CUDA_CHECK(cudaStreamSynchronize(st));
+    for (int k = 0; k < na; ++k) addr[k] += 1;
+}
+
+void blocks_regular_impl(int *nreg, int *addr, double *xv) {
+    if (!I.open || !I.hermite || !I.hctl.ptr) {
+        nb6_fatal(NB6_ERR_NOT_OPEN);
+        return;
+    }
+    const int nr = I.hctl.ptr->nreg;
+    *nreg = nr;
+    if (nr <= 0) return;
+    cudaStream_t st = nb6_stream();
+    std::vector<int> a(nr);
+    std::vector<double> x(6 * (size_t)nr);
+    NB6_CUDA_CHECK(cudaMemcpyAsync(a.data(), I.breg.ptr, sizeof(int) * nr, cudaMemcpyDeviceToHost, st));
+    NB6_CUDA_CHECK(cudaMemcpyAsync(x.data(), I.bregxv.ptr, sizeof(double) * 6 * (size_t)nr, cudaMemcpyDeviceToHost,
+                                   st));
+    NB6_CUDA_CHECK(cudaStreamSynchronize(st));
+    // ascending addresses (the device appends in no particular order)
+    std::vector<int> ord(nr);
+    for (int k = 0; k < nr; ++k) ord[k] = k;
+    std::sort(ord.begin(), ord.end(), [&](int u, int v) { return a[u] < a[v]; });
+    for (int k = 0; k < nr; ++k) {
+        addr[k] = a[ord[k]] + 1;
+        memcpy(xv + 6 * (size_t)k, &x[6 * (size_t)ord[k]], sizeof(double) * 6);
+    }
+}
+
 void hermite_get_impl(int a0, int n, double *out) {
     if (!I.open || !I.hermite) {
         nb6_fatal(NB6_ERR_NOT_OPEN);
@@ -1232,6 +1557,7 @@ void regf_correct_impl(double time, int ni, const int *addr, int *iseg, int nseg
     irr_flush(st);  // state staged by the host first
     RegDeviceOut ro;
     if (!regular_seg_on_device(ni, iseg, h2, dtr, xi, vi, lmax, nnbmax, mflag, nseg, seg_j0, &ro)) return;
+    const double t1 = nb6_wtime();
     // [addr | iseg | seg_j0 (nseg+1) | seg_a0 - 1 (nseg) | pad | rs (ni doubles)]
     const size_t nint = 2 * (size_t)ni + 2 * (size_t)nseg + 1, nint2 = (nint + 1) & ~(size_t)1;
     I.hseg.reserve(nint2 + 2 * (size_t)ni);
@@ -1265,17 +1591,26 @@ void regf_correct_impl(double time, int ni, const int *addr, int *iseg, int nseg
     }
     reg_corrector_kernel<<<(ni + 127) / 128, 128, 0, st>>>(ni, d, d + ni, d + 2 * (size_t)ni,
                                                          d + 2 * (size_t)ni + nseg + 1, time, ro, I.rec.ptr, I.aux.ptr,
-                                                         I.lists.ptr, I.lmax, drs, p, o, nb6_dev_status());
+                                                         I.lists.ptr, I.lmax, drs, p, o, nb6_dev_status(),
+                                                         I.tn.ptr);
     NB6_CUDA_CHECK(cudaGetLastError());
     if (!direct)
         NB6_CUDA_CHECK(cudaMemcpyAsync(I.hout.ptr, o, sizeof(double) * rowd * ni, cudaMemcpyDeviceToHost, st));
     nb6_status_fetch(st);
+    const double t2 = nb6_wtime();
     NB6_CUDA_CHECK(cudaStreamSynchronize(st));
+    const double t3 = nb6_wtime();
     if (nb6_check_dev_status() != 0) return;
     memcpy(out, I.hout.ptr, sizeof(double) * rowd * ni);
     for (int k = 0; k < ni; ++k)
         if (out[rowd * k + 28] == 0.0) I.nnb_host[addr[k] - 1] = (int)out[rowd * k + 27];
-    I.time_grav += nb6_wtime() - t0;
+    const double t4 = nb6_wtime();
+    I.time_grav += t4 - t0;
+    I.rc_calls++;
+    I.rc_t[0] += t1 - t0;  // regular force enqueued (host preparation)
+    I.rc_t[1] += t2 - t1;  // corrector enqueued
+    I.rc_t[2] += t3 - t2;  // waiting for the device
+    I.rc_t[3] += t4 - t3;  // results out
 }
 
 // The regular-force j set from the resident records: segments of
@@ -1321,6 +1656,12 @@ void irr_predict_send_impl(double t, int nseg, const int *addr0, const int *coun
 }
 
 void irr_profile_impl(int rank) {
+    if (I.open && I.rc_calls && getenv("NB6_VERBOSE"))
+        fprintf(stderr,
+                "[R.%d GPU Reg.C ] Ncall: %lld prepare+force %.3f s, corrector %.3f s, wait %.3f s, out %.3f s\n",
+                rank, I.rc_calls, I.rc_t[0], I.rc_t[1], I.rc_t[2], I.rc_t[3]);
+    I.rc_calls = 0;
+    I.rc_t[0] = I.rc_t[1] = I.rc_t[2] = I.rc_t[3] = 0;
     if (I.open && I.num_fcall) {
         const double gf = I.time_grav > 0 ? 60.0 * (double)I.num_inter * 1e-9 / I.time_grav : 0.0;
         fprintf(stderr, "[R.%d GPU Irr.F ] Ncall: %llu <NI>: %d grav: %f s, %f Gflops, %f usec\n", rank,
@@ -1390,6 +1731,32 @@ void nb6_irr_correct_(double *time, int *ni, int *addr, double *out) { irr_corre
 void nb6_ks_set_(int *npair, int *cm, double *xk, double *vk, double *mk, int *pofs, int *plist) {
     ks_set_impl(*npair, cm, xk, vk, mk, pofs, plist);
 }
+
+// Device block clock: run blocks of irregular steps on the device (each
+// block: the earliest t0 + STEP over all bodies, its active set, the
+// neighbour force and the irregular corrector, as nb6_irr_correct_ does
+// for a host-chosen set) until a block has a body due a regular step (its
+// irregular part done: *reason = 1, the host runs the regular part with
+// nb6_blocks_active_ and nb6_regf_correct_), the next block time passes
+// *tlimit (*reason = 2, that block not started) or *max_blocks blocks ran
+// (*reason = 0).  *nblocks and *nirr count the blocks and irregular steps
+// of this call, *tblock is the last block's time, *nact its active count.
+// The host's block clock is not needed meanwhile (next_tlist.f's choice is
+// made on the device, bit for bit the same).
+void nb6_blocks_run_(double *tlimit, int *max_blocks, int *reason, long long *nblocks, long long *nirr,
+                     double *tblock, int *nact) {
+    blocks_run_impl(*tlimit, *max_blocks, reason, nblocks, nirr, tblock, nact);
+}
+
+// The last block of nb6_blocks_run_: its active bodies (1-based, in no
+// particular order) and their corrector rows out[k][24] as nb6_irr_correct_
+// returns them.
+void nb6_blocks_active_(int *nact, int *addr, double *rows) { blocks_active_impl(nact, addr, rows); }
+
+// The bodies of the last block of nb6_blocks_run_ that are due a regular
+// step (*reason = 1): *nreg of them, ascending 1-based addresses, with
+// their corrected x0[3], v0[3] (xv[k][6]) -- the i of nb6_regf_correct_.
+void nb6_blocks_regular_(int *nreg, int *addr, double *xv) { blocks_regular_impl(nreg, addr, xv); }
 
 // The resident state of bodies a0 .. a0+n-1 (1-based), rows of 32
 // doubles: x0[3], v0[3], F[3], FDOT[3], fi[3], fidot[3], fr[3], frdot[3],

@@ -419,7 +419,81 @@ struct Ensemble : Bodies {
         nout++;
     }
 
+    // block clock on the device too
+    bool dev_clock() const { return dev_reg() && P.dev_corrector >= 3 && B.blocks_run && B.blocks_regular; }
+
+    // The block loop with the device's block clock: runs of irregular blocks
+    // on the device (nb6_blocks_run_) until a block has bodies due a regular
+    // step or the next output time is reached; the host runs those regular
+    // steps (regular_on_device) and the energy output.  Same arithmetic and
+    // order as run()'s host clock, so the same trajectory.
+    void run_device_clock(double *tout, double *eout, int nout_max) {
+        const double tw = wtime();
+        int nout = 0;
+        record(tout, eout, nout, nout_max);
+        double tnext_out = P.dt_out;
+        std::vector<int> act, reg;
+        std::vector<double> rows;
+        double t_reg = 0;
+        for (;;) {
+            double tlimit = std::min(tnext_out, P.tcrit);
+            const long long left = P.max_blocks - st.blocks;
+            if (left <= 0) break;
+            int maxb = (int)std::min<long long>(left, 1 << 30), reason = 0, nact = 0;
+            long long nb = 0, nirr = 0;
+            double tb = time;
+            const double ti0 = wtime();
+            B.blocks_run(&tlimit, &maxb, &reason, &nb, &nirr, &tb, &nact);
+            st.wall_irr += wtime() - ti0;
+            st.blocks += nb;
+            st.irr_steps += nirr;
+            if (nb > 0) time = tb;
+            if (reason == 1) {
+                // the block's bodies due a regular step, ascending, with
+                // their corrected x0, v0 (the i of the regular call)
+                const double w0 = wtime();
+                act.resize(std::max(nact, 1));
+                rows.resize(6 * (size_t)std::max(nact, 1));
+                int nr = 0;
+                B.blocks_regular(&nr, act.data(), rows.data());
+                reg.resize(nr);
+                for (int q = 0; q < nr; ++q) {
+                    const int i = act[q] - 1;
+                    reg[q] = i;
+                    for (int c = 0; c < 3; ++c) {
+                        x0[3 * (size_t)i + c] = rows[6 * (size_t)q + c];
+                        v0[3 * (size_t)i + c] = rows[6 * (size_t)q + 3 + c];
+                    }
+                }
+                regular_on_device(reg);
+                t_reg += wtime() - w0;
+            }
+            if (time >= tnext_out - 1e-15) {
+                pull_state();
+                record(tout, eout, nout, nout_max);
+                tnext_out += P.dt_out;
+            }
+            if (reason == 0) break;                           // block budget spent
+            if (reason == 2 && tlimit >= P.tcrit) break;      // next block beyond the end
+        }
+        pull_state();
+        st.t_end = time;
+        st.nout = nout;
+        st.wall_total = wtime() - tw;
+        if (getenv("NB6_VERBOSE")) {
+            fprintf(stderr, "# nb6 ensemble (device clock): wall %.3f s = block runs %.3f + regular part %.3f + other\n",
+                    st.wall_total, st.wall_irr, t_reg);
+            int rank = 0;
+            if (B.reg_profile) B.reg_profile(&rank);
+            if (B.irr_profile) B.irr_profile(&rank);
+        }
+    }
+
     void run(double *tout, double *eout, int nout_max) {
+        if (dev_clock()) {
+            run_device_clock(tout, eout, nout_max);
+            return;
+        }
         const double tw = wtime();
         int nout = 0;
         record(tout, eout, nout, nout_max);

@@ -51,7 +51,9 @@ struct nb6drive_params {
     // ensemble driver, batched mode: 0 = correctors on the host; 1 =
     // irregular corrector on the device (nb6_irr_correct_) when the backend
     // has it; 2 = the regular corrector there too (nb6_regf_correct_; the
-    // host one under mlp_mode 1, which logs samples on the host)
+    // host one under mlp_mode 1, which logs samples on the host); 3 = the
+    // block clock too (nb6_blocks_run_: runs of irregular blocks on the
+    // device, the host only for regular steps and output)
     int dev_corrector;
     // ensemble driver, batched mode: 1 = a block whose regular bodies all
     // belong to one cluster also takes the segmented call (nb6_regf_seg_,
@@ -101,6 +103,9 @@ typedef void (*fn_irr_correct)(double *, int *, int *, double *);
 typedef void (*fn_regf_correct)(double *, int *, int *, int *, int *, int *, int *, double *, double *, double *,
                                 double (*)[3], double (*)[3], int *, int *, int *, double *, double *);
 typedef void (*fn_hermite_get)(int *, int *, double *);
+typedef void (*fn_blocks_run)(double *, int *, int *, long long *, long long *, double *, int *);
+typedef void (*fn_blocks_active)(int *, int *, double *);
+typedef void (*fn_blocks_regular)(int *, int *, double *);
 
 struct Backend {
     void *hreg = nullptr, *hirr = nullptr, *hpot = nullptr;
@@ -124,6 +129,9 @@ struct Backend {
     fn_irr_correct irr_correct = nullptr;
     fn_regf_correct regf_correct = nullptr;                    // device regular corrector
     fn_hermite_get hermite_get = nullptr;
+    fn_blocks_run blocks_run = nullptr;                        // device block clock
+    fn_blocks_active blocks_active = nullptr;
+    fn_blocks_regular blocks_regular = nullptr;
 };
 
 inline void *must_sym(void *h, const char *name) {
@@ -164,6 +172,9 @@ inline bool load_backend(Backend &b, const char *reg, const char *irr, const cha
     b.irr_correct = (fn_irr_correct)dlsym(b.hirr, "nb6_irr_correct_");
     b.regf_correct = (fn_regf_correct)dlsym(b.hirr, "nb6_regf_correct_");
     b.hermite_get = (fn_hermite_get)dlsym(b.hirr, "nb6_hermite_get_");
+    b.blocks_run = (fn_blocks_run)dlsym(b.hirr, "nb6_blocks_run_");
+    b.blocks_active = (fn_blocks_active)dlsym(b.hirr, "nb6_blocks_active_");
+    b.blocks_regular = (fn_blocks_regular)dlsym(b.hirr, "nb6_blocks_regular_");
     return b.gpunb_open && b.gpunb_close && b.gpunb_send && b.gpunb_regf && b.gpupot &&
            b.irr_open && b.irr_close && b.irr_set_jp && b.irr_set_list && b.irr_firr_vec;
 }

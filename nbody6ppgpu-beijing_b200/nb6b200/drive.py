@@ -168,7 +168,9 @@ def run_ensemble(backend: dict, clusters, *, batched=True, tcrit=1.0, eta_i=0.02
     bodies) or rs_from_clusters=True (each cluster's .rs) sets the initial
     neighbour radii.  dev_corrector (batched mode): 1 (True) runs the
     irregular corrector on the device (nb6_irr_correct_), 2 the regular
-    corrector there too (nb6_regf_correct_); the result is the same bit for
+    corrector there too (nb6_regf_correct_), 3 the block clock too
+    (nb6_blocks_run_: runs of irregular blocks without the host); the
+    result is the same bit for
     bit (with mlp_mode 2 up to the last bit of exp on the device) when
     seg_single is set: blocks whose regular bodies are all in one cluster
     then take the segmented call too, as the device regular corrector

@@ -1,12 +1,12 @@
 """Batched ensemble vs each cluster alone (the plain method), same GPU.
 
     python -m nb6b200.ensemble_bench --clusters 256 --tcrit 1.0 [--alone-sample 32] [--mlp]
-        [--dev-corrector 2]
+        [--dev-corrector 3]
 
 (run from ``nbody6ppgpu-beijing_b200/``).  The ensemble is the batched
 driver (one irregular and one segmented regular call per block for all
 clusters; --dev-corrector 1 runs the irregular corrector on the device, 2
-both correctors); "alone" integrates each cluster with the single-cluster driver
+both correctors, 3 the block clock too); "alone" integrates each cluster with the single-cluster driver
 and the reference ABI calls.  With --alone-sample k only k clusters, spread
 over the size range, are run alone and their wall time is scaled by the
 ensemble's total pair count over theirs (stated in the output).  Prints one
@@ -38,7 +38,7 @@ def main(argv=None):
     ap.add_argument("--mlp", action="store_true",
                     help="learned radii: train on samples from plain runs of 16 other clusters "
                          "of the same distribution, then run the ensemble with the proposals")
-    ap.add_argument("--dev-corrector", type=int, default=2, choices=(0, 1, 2))
+    ap.add_argument("--dev-corrector", type=int, default=3, choices=(0, 1, 2, 3))
     a = ap.parse_args(argv)
     ours = drive.backend_paths("nb6b200")
     cls = make_clusters(a.clusters)

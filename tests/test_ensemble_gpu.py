@@ -84,9 +84,10 @@ def test_device_corrector_equals_host_corrector_bit_for_bit(nb6):
 
 @pytest.mark.parametrize("small_lists", [False, True])
 def test_device_regular_corrector_equals_host_corrector_bit_for_bit(nb6, small_lists):
-    """Both correctors on the device (nb6_irr_correct_ + nb6_regf_correct_)
-    against both on the host (the same segmented regular-force call for
-    every block): same steps, neighbour counts, final state and
+    """Both correctors on the device (nb6_irr_correct_ + nb6_regf_correct_),
+    and both plus the block clock (nb6_blocks_run_), against both on the
+    host (the same segmented regular-force call for every block): same
+    blocks, steps, neighbour counts, final state and
     energies, bit for bit.  With small_lists the neighbour lists overflow
     (NNBMAX 24) so the shrink-and-retry path runs too."""
     from nb6b200 import drive
@@ -97,13 +98,17 @@ def test_device_regular_corrector_equals_host_corrector_bit_for_bit(nb6, small_l
         kw.update(nnbopt=12, nnbmax=24, lmax=32, tcrit=0.25)
     dev = drive.run_ensemble(ours, cls, dev_corrector=2, **kw)
     host = drive.run_ensemble(ours, cls, dev_corrector=0, seg_single=True, **kw)
-    for key in ("irr_steps", "reg_steps", "reg_calls", "overflow_retries", "nb_sum"):
-        assert dev.stats[key] == host.stats[key], key
-    assert dev.stats["reg_steps"] > 0
-    if small_lists:
-        assert host.stats["overflow_retries"] > 0
-    for c in range(len(cls)):
-        np.testing.assert_array_equal(dev.x[c], host.x[c])
-        np.testing.assert_array_equal(dev.v[c], host.v[c])
-    np.testing.assert_array_equal(dev.energy, host.energy)
+    # and with the block clock on the device as well (nb6_blocks_run_)
+    clk = drive.run_ensemble(ours, cls, dev_corrector=3, **kw)
+    for run in (dev, clk):
+        for key in ("blocks", "irr_steps", "reg_steps", "reg_calls", "overflow_retries", "nb_sum"):
+            assert run.stats[key] == host.stats[key], key
+        assert run.stats["reg_steps"] > 0
+        if small_lists:
+            assert host.stats["overflow_retries"] > 0
+        for c in range(len(cls)):
+            np.testing.assert_array_equal(run.x[c], host.x[c])
+            np.testing.assert_array_equal(run.v[c], host.v[c])
+        np.testing.assert_array_equal(run.energy, host.energy)
+        np.testing.assert_array_equal(run.times, host.times)
 
