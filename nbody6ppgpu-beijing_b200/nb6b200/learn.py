@@ -49,12 +49,13 @@ def _summary(stats, de, tcrit):
             "dE": float(de), "mlp_used": stats["mlp_used"], "mlp_fallback": stats["mlp_fallback"]}
 
 
-def compare(cl, tcrit, plain_method=True, rs_ics=False, dev_corrector=2, **kw) -> dict:
+def compare(cl, tcrit, plain_method=True, rs_ics=False, dev_corrector=3, **kw) -> dict:
     """One cluster three ways, with the current model for the learned arm:
     the plain GPU method (single-cluster driver: host prediction, gpunb_send_
     per regular block, host correctors, Ahmad-Cohen radii); the batched
     driver (j set predicted on the device; with dev_corrector = 2 both
-    correctors on the device too) with Ahmad-Cohen radii; and the batched
+    correctors on the device too, with 3 the block clock as well) with
+    Ahmad-Cohen radii; and the batched
     driver with the learned radii.  Wall times are the drivers' own (block
     loop and energies, not the start-up)."""
     ours = drive.backend_paths("nb6b200")
