@@ -275,7 +275,7 @@ def _radii_steps(pos, mass, rho_of_r, sig_of_r, nnbopt, smax):
     dist, _ = cKDTree(pos).query(pos, k=[k], workers=-1)
     rs = dist[:, 0] * (1.0 + 1e-9)
     sig = np.maximum(sig_of_r(r), 1e-6)
-    t = 0.25 * rs / sig
+    t = np.maximum(0.25 * rs / sig, 1e-300)   # (coincident bodies: rs = 0)
     k = np.ceil(np.log2(np.maximum(smax / t, 1.0)))
     dtr = smax / 2.0 ** k
     return rs, dtr
