@@ -431,9 +431,11 @@ def main():
                "d2h_bytes_per_step": int(n * 64 + n * ids_per_i * 4),
                "steps": e2e_steps, "timing": "wall clock around synchronous ABI calls"}
 
-    # the N^2 potential of the same cluster (GPUPOT, energy.F:33): kernel
-    # time on the library stream, 27 flops per pair (pot.avx.cpp:123-135);
-    # accuracy on a contiguous sample of 64 i against the FP64 oracle
+    # the N^2 potential of the same cluster (GPUPOT, energy.F:33): device
+    # time on the library stream of the whole call after the upload (the
+    # spatial order, the kernel and the sums), 27 flops per pair
+    # (pot.avx.cpp:123-135); accuracy of that call's result on a contiguous
+    # sample of 64 i against the FP64 oracle
     pot = None
     if not args.no_pot:
         d_m = torch.tensor(m, dtype=torch.float64, device=dev)
@@ -444,14 +446,16 @@ def main():
         pot_ms = float(raw.nb6_pot_last_kernel_ms_())
         pot = {"pairs_per_s": float(n) * n / (pot_ms * 1e-3), "kernel_ms": pot_ms,
                "flops_per_pair": 27,
-               "frac_fp32_peak": 27.0 * n * n / (pot_ms * 1e-3) / 1e12 / peak_tf}
-        del d_m
+               "frac_fp32_peak": 27.0 * n * n / (pot_ms * 1e-3) / 1e12 / peak_tf,
+               "note": "27 flops per pair is the reference's count (hi/lo differences); "
+                       "the ordered far loop issues 11 FP32 lane operations per pair"}
         if rank == 0:
             import oracle
             i0 = int(np.random.default_rng(9).integers(1, n - 64))
             po = oracle.pot(m, x, i0, 64)
-            pg_ = lib.gpupot(m, x, istart=i0, ni=64)
+            pg_ = lib.gpupot(m, x)[i0 - 1:i0 - 1 + 64]   # the whole-set call, as timed
             pot["rel_err_max_sample64"] = float(np.max(np.abs(pg_ / po - 1)))
+        del d_m
 
     # the irregular path on the same cluster: neighbour lists of a sample
     # of bodies from this library's regular call, every body's state in the

@@ -195,6 +195,25 @@ NB6_DEV bool mbar_wait_timed(uint64_t *bar, uint32_t parity, uint64_t budget_ns)
     }
 }
 
+// Order-preserving map of a float to an unsigned (for atomicMin/Max of
+// positions) and back.
+NB6_DEV unsigned f2ord(float f) {
+    const unsigned u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+NB6_DEV float ord2f(unsigned u) { return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u); }
+
+// The 10 low bits of v spread to every third bit (one axis of a 30-bit
+// Morton key).
+NB6_DEV unsigned spread10(unsigned v) {
+    v &= 1023u;
+    v = (v | (v << 16)) & 0x030000FFu;
+    v = (v | (v << 8)) & 0x0300F00Fu;
+    v = (v | (v << 4)) & 0x030C30C3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+
 // Warp-level inclusive max/sum helpers used by the finalize kernels.
 NB6_DEV double warp_sum_d(double v) {
 #pragma unroll

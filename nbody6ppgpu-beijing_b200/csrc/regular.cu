@@ -1424,11 +1424,6 @@ bool any_nan(const double *p, size_t n) {
 // set holds the caller's body perm[k]; the exact FP64 path maps slots back, so
 // neighbour ids are the caller's.
 // ----------------------------------------------------------------------------
-NB6_DEV unsigned f2ord(float f) {
-    const unsigned u = __float_as_uint(f);
-    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
-}
-NB6_DEV float ord2f(unsigned u) { return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u); }
 
 // ext[0..2] = min x, y, z and ext[3..5] = max (order-preserving uints).
 __global__ void jset_extent(int nj, const double *__restrict__ jx, unsigned *__restrict__ ext) {
@@ -1454,14 +1449,6 @@ __global__ void jset_extent(int nj, const double *__restrict__ jx, unsigned *__r
         }
 }
 
-NB6_DEV unsigned spread10(unsigned v) {
-    v &= 1023u;
-    v = (v | (v << 16)) & 0x030000FFu;
-    v = (v | (v << 8)) & 0x0300F00Fu;
-    v = (v | (v << 4)) & 0x030C30C3u;
-    v = (v | (v << 2)) & 0x09249249u;
-    return v;
-}
 
 // 30-bit Morton key of each body on a 1024^3 grid over the extent.
 __global__ void jset_keys(int nj, const double *__restrict__ jx, const unsigned *__restrict__ ext,

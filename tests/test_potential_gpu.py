@@ -59,3 +59,22 @@ def test_potential_energy_plummer(nb6):
     p = nb6.gpupot(cl.mass, cl.pos)
     w = -0.5 * float((cl.mass * p).sum())
     assert abs(w + 0.5) < 0.03
+
+
+def test_potential_ordered_path_stress(nb6, orc):
+    """A whole-set call above 32,768 bodies takes the Morton-ordered path
+    (packed far loop on tile-relative coordinates): every body's potential
+    within the tolerance of the FP64 oracle, with escapers far out, close
+    and coincident pairs, results in the caller's order."""
+    from nb6b200 import ics
+    cl = ics.king(40000, w0=6.0, seed=11, imf=True, binary_fraction=0.05)
+    x = cl.pos.copy()
+    rng = np.random.default_rng(2)
+    k = rng.choice(len(x), len(x) // 100, replace=False)
+    x[k] *= 50.0                                            # escapers
+    k = rng.choice(len(x), len(x) // 20, replace=False)
+    x[k[1:]] = x[k[:-1]] + rng.normal(size=(len(k) - 1, 3)) * 1e-5   # close pairs
+    x[7] = x[8]                                             # a coincident pair
+    p = nb6.gpupot(cl.mass, x)
+    po = orc.pot(cl.mass, x)
+    assert rel_err_vec(p, po).max() <= TOL
