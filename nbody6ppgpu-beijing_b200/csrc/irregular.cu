@@ -17,6 +17,8 @@
 // smallest index on ties (irr.avx.cpp:320-323 packs (r2, idx) the same way).
 #include "nb6_common.cuh"
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include <algorithm>
 #include <climits>
 #include <string.h>
@@ -881,6 +883,9 @@ struct IrrState {
     int blk_batch = 16;               // graph launches per synchronisation
     DevBuf<int> breg;                 // regular-due bodies of the running block
     DevBuf<double> bregxv;            // their x0, v0
+    DevBuf<int> bsort;                // [sorted addresses | slots in | slots out], 3 x nmax
+    DevBuf<double> bsortxv;           // x0, v0 in address order
+    DevBuf<char> bsort_tmp;
     long long rc_calls = 0;           // nb6_regf_correct_ calls and their host-side phases
     double rc_t[4] = {0, 0, 0, 0};
 };
@@ -962,6 +967,9 @@ void irr_close_impl() {
     I.bact.release();
     I.breg.release();
     I.bregxv.release();
+    I.bsort.release();
+    I.bsortxv.release();
+    I.bsort_tmp.release();
     I.bforce.release();
     I.brows.release();
     I.bctl.release();
@@ -1491,6 +1499,21 @@ void blocks_active_impl(int *nact, int *addr, double *rows) {
     for (int k = 0; k < na; ++k) addr[k] += 1;
 }
 
+__global__ void iota_kernel(int n, int *v) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) v[k] = k;
+}
+
+// The due list in address order: 1-based addresses and the x0, v0 rows
+// permuted to match.
+__global__ void due_gather(int n, int *__restrict__ addr, const int *__restrict__ slot,
+                           const double *__restrict__ xv, double *__restrict__ out) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        addr[k] += 1;
+        const double *src = xv + 6 * (size_t)slot[k];
+        for (int d = 0; d < 6; ++d) out[6 * (size_t)k + d] = src[d];
+    }
+}
+
 void blocks_regular_impl(int *nreg, int *addr, double *xv) {
     if (!I.open || !I.hermite || !I.hctl.ptr) {
         nb6_fatal(NB6_ERR_NOT_OPEN);
@@ -1500,20 +1523,26 @@ void blocks_regular_impl(int *nreg, int *addr, double *xv) {
     *nreg = nr;
     if (nr <= 0) return;
     cudaStream_t st = nb6_stream();
-    std::vector<int> a(nr);
-    std::vector<double> x(6 * (size_t)nr);
-    NB6_CUDA_CHECK(cudaMemcpyAsync(a.data(), I.breg.ptr, sizeof(int) * nr, cudaMemcpyDeviceToHost, st));
-    NB6_CUDA_CHECK(cudaMemcpyAsync(x.data(), I.bregxv.ptr, sizeof(double) * 6 * (size_t)nr, cudaMemcpyDeviceToHost,
-                                   st));
+    // ascending addresses (the device appends in no particular order): a
+    // radix sort of (address, slot) on the device
+    I.bsort.reserve(3 * (size_t)nr);
+    I.bsortxv.reserve(6 * (size_t)nr);
+    int *keys_out = I.bsort.ptr, *vals_in = I.bsort.ptr + nr, *vals_out = I.bsort.ptr + 2 * (size_t)nr;
+    const int g = std::min((nr + 255) / 256, nb6_num_sms() * 4);
+    iota_kernel<<<g, 256, 0, st>>>(nr, vals_in);
+    int bits = 1;
+    while (bits < 31 && (1 << bits) < I.nmax) ++bits;
+    size_t tmp = 0;
+    NB6_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(nullptr, tmp, I.breg.ptr, keys_out, vals_in, vals_out, nr, 0, bits,
+                                                   st));
+    I.bsort_tmp.reserve(tmp + 16);
+    NB6_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(I.bsort_tmp.ptr, tmp, I.breg.ptr, keys_out, vals_in, vals_out, nr,
+                                                   0, bits, st));
+    due_gather<<<g, 256, 0, st>>>(nr, keys_out, vals_out, I.bregxv.ptr, I.bsortxv.ptr);
+    NB6_CUDA_CHECK(cudaGetLastError());
+    NB6_CUDA_CHECK(cudaMemcpyAsync(addr, keys_out, sizeof(int) * nr, cudaMemcpyDeviceToHost, st));
+    NB6_CUDA_CHECK(cudaMemcpyAsync(xv, I.bsortxv.ptr, sizeof(double) * 6 * (size_t)nr, cudaMemcpyDeviceToHost, st));
     NB6_CUDA_CHECK(cudaStreamSynchronize(st));
-    // ascending addresses (the device appends in no particular order)
-    std::vector<int> ord(nr);
-    for (int k = 0; k < nr; ++k) ord[k] = k;
-    std::sort(ord.begin(), ord.end(), [&](int u, int v) { return a[u] < a[v]; });
-    for (int k = 0; k < nr; ++k) {
-        addr[k] = a[ord[k]] + 1;
-        memcpy(xv + 6 * (size_t)k, &x[6 * (size_t)ord[k]], sizeof(double) * 6);
-    }
 }
 
 void hermite_get_impl(int a0, int n, double *out) {

@@ -37,6 +37,9 @@ struct Ensemble : Bodies {
     std::vector<double> crow;  // device corrector rows of the last block
     std::vector<double> rrow;  // device regular corrector rows of the last call
     double t_pred = 0;         // wall time in nb6_irr_predict_send_ (device regular corrector)
+    double t_rcall = 0;        // ... in nb6_regf_correct_
+    double t_out = 0;          // ... in energy output (state read-back + energies)
+    double t_breg = 0;         // ... in nb6_blocks_regular_
     // per-call buffers of the batched regular force, kept across calls (the
     // library writes every entry that is read back)
     std::vector<int> b_iseg, b_lst;
@@ -161,9 +164,11 @@ struct Ensemble : Bodies {
                 }
             }
             int nni = np, lmax = P.lmax, nnbmax = P.nnbmax, mf = P.m_flag;
+            const double tc = wtime();
             B.regf_correct(&t, &nni, addr.data(), b_iseg.data(), &nseg, seg_j0.data(), addr0.data(), b_h2.data(),
                            b_dtr.data(), rsv.data(), (double(*)[3])b_xi.data(), (double(*)[3])b_vi.data(), &lmax,
                            &nnbmax, &mf, prm, rrow.data());
+            t_rcall += wtime() - tc;
             st.reg_calls++;
             std::vector<int> again;
             for (int p = 0; p < np; ++p) {
@@ -455,7 +460,9 @@ struct Ensemble : Bodies {
                 act.resize(std::max(nact, 1));
                 rows.resize(6 * (size_t)std::max(nact, 1));
                 int nr = 0;
+                const double tq = wtime();
                 B.blocks_regular(&nr, act.data(), rows.data());
+                t_breg += wtime() - tq;
                 reg.resize(nr);
                 for (int q = 0; q < nr; ++q) {
                     const int i = act[q] - 1;
@@ -469,9 +476,11 @@ struct Ensemble : Bodies {
                 t_reg += wtime() - w0;
             }
             if (time >= tnext_out - 1e-15) {
+                const double to = wtime();
                 pull_state();
                 record(tout, eout, nout, nout_max);
                 tnext_out += P.dt_out;
+                t_out += wtime() - to;
             }
             if (reason == 0) break;                           // block budget spent
             if (reason == 2 && tlimit >= P.tcrit) break;      // next block beyond the end
@@ -481,8 +490,10 @@ struct Ensemble : Bodies {
         st.nout = nout;
         st.wall_total = wtime() - tw;
         if (getenv("NB6_VERBOSE")) {
-            fprintf(stderr, "# nb6 ensemble (device clock): wall %.3f s = block runs %.3f + regular part %.3f + other\n",
-                    st.wall_total, st.wall_irr, t_reg);
+            fprintf(stderr,
+                    "# nb6 ensemble (device clock): wall %.3f s = block runs %.3f + regular part %.3f (j-set "
+                    "prediction %.3f, regular calls %.3f, due list %.3f) + output %.3f + other\n",
+                    st.wall_total, st.wall_irr, t_reg, t_pred, t_rcall, t_breg, t_out);
             int rank = 0;
             if (B.reg_profile) B.reg_profile(&rank);
             if (B.irr_profile) B.irr_profile(&rank);
