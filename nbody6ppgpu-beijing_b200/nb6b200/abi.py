@@ -201,6 +201,63 @@ class ForceLib:
         padded[: row.shape[0]] = row[: padded.shape[0]]
         self.lib.irr_simd_set_list_(_ci(addr), _ip(padded))
 
+    # ------------------------------------------ device correctors and clock
+    def hermite_open(self, eta_i: float, smax: float, dtmin: float) -> None:
+        """nb6_hermite_open_ (extension): the per-body Hermite state on the
+        device, after irr_open."""
+        self.lib.nb6_hermite_open_(_cd(eta_i), _cd(smax), _cd(dtmin))
+
+    def hermite_set_all(self, fi, fidot, fr, frdot, step, t0r, stepr, rs, first: int = 1) -> None:
+        """nb6_hermite_set_ for bodies first, first+1, ... (1-based)."""
+        fi, fidot, fr, frdot = _f64(fi), _f64(fidot), _f64(fr), _f64(frdot)
+        step, t0r, stepr, rs = _f64(step), _f64(t0r), _f64(stepr), _f64(rs)
+        fn = self.lib.nb6_hermite_set_
+        for k in range(fi.shape[0]):
+            fn(_ci(first + k), _dp(fi[k]), _dp(fidot[k]), _dp(fr[k]), _dp(frdot[k]),
+               C.byref(C.c_double(step[k])), C.byref(C.c_double(t0r[k])),
+               C.byref(C.c_double(stepr[k])), C.byref(C.c_double(rs[k])))
+
+    def hermite_get(self, a0: int, n: int) -> np.ndarray:
+        """nb6_hermite_get_: rows (n, 32) of the resident state."""
+        out = np.zeros((max(n, 1), 32))
+        self.lib.nb6_hermite_get_(_ci(a0), _ci(n), _dp(out))
+        return out[:n]
+
+    def irr_correct(self, time: float, addr) -> np.ndarray:
+        """nb6_irr_correct_: corrector rows (ni, 24) of the bodies addr."""
+        addr = np.ascontiguousarray(addr, dtype=np.int32)
+        out = np.zeros((max(addr.shape[0], 1), 24))
+        self.lib.nb6_irr_correct_(_cd(time), _ci(addr.shape[0]), _ip(addr), _dp(out))
+        return out[:addr.shape[0]]
+
+    def blocks_run(self, tlimit: float, max_blocks: int) -> dict:
+        """nb6_blocks_run_: blocks of irregular steps on the device."""
+        reason, nact = C.c_int(0), C.c_int(0)
+        nb, nirr = C.c_longlong(0), C.c_longlong(0)
+        tb = C.c_double(0.0)
+        self.lib.nb6_blocks_run_(_cd(tlimit), _ci(max_blocks), C.byref(reason), C.byref(nb), C.byref(nirr),
+                                 C.byref(tb), C.byref(nact))
+        return {"reason": reason.value, "blocks": nb.value, "irr_steps": nirr.value, "tblock": tb.value,
+                "nact": nact.value}
+
+    def blocks_active(self, nmax: int) -> tuple[np.ndarray, np.ndarray]:
+        """nb6_blocks_active_: the last block's active bodies (1-based) and
+        corrector rows."""
+        addr = np.zeros(max(nmax, 1), dtype=np.int32)
+        rows = np.zeros((max(nmax, 1), 24))
+        na = C.c_int(0)
+        self.lib.nb6_blocks_active_(C.byref(na), _ip(addr), _dp(rows))
+        return addr[:na.value], rows[:na.value]
+
+    def blocks_regular(self, nmax: int) -> tuple[np.ndarray, np.ndarray]:
+        """nb6_blocks_regular_: the last block's regular-due bodies
+        (ascending, 1-based) with x0, v0."""
+        addr = np.zeros(max(nmax, 1), dtype=np.int32)
+        xv = np.zeros((max(nmax, 1), 6))
+        nr = C.c_int(0)
+        self.lib.nb6_blocks_regular_(C.byref(nr), _ip(addr), _dp(xv))
+        return addr[:nr.value], xv[:nr.value]
+
     def ks_set(self, cm, xk, vk, mk, pofs, plist) -> None:
         """nb6_ks_set_ (extension): the perturbed KS pairs whose components
         the irregular force resolves from now on.  cm: 1-based c.m.

@@ -1,0 +1,103 @@
+"""The device block clock (nb6_blocks_run_) and the device correctors'
+state calls, at the C ABI: the block it picks is the host's choice (the
+bodies with the smallest T0 + STEP), its corrector rows equal
+nb6_irr_correct_'s for that set bit for bit, the due list is the rows'
+regular-due flags in ascending order, and the stop reasons follow
+tlimit and max_blocks."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _state(seed, n=3000, lmax=128):
+    """A Plummer cluster at t0 = 0 with random power-of-two steps, lists
+    from the FP64 oracle's regular call, forces from a random draw."""
+    from nb6b200 import ics
+    cl = ics.plummer(n, seed=seed, imf=True)
+    rng = np.random.default_rng(seed)
+    f = rng.normal(size=(n, 3)) * 0.05
+    fd = rng.normal(size=(n, 3)) * 0.01
+    step = 2.0 ** -rng.integers(6, 10, n).astype(float)
+    stepr = np.maximum(step, 2.0 ** -rng.integers(4, 7, n).astype(float))
+    stepr[::3] = step[::3]         # a third of the bodies due a regular step with their first
+    t0 = np.zeros(n)
+    d = np.linalg.norm(cl.pos[:, None, :] - cl.pos[None, :200, :], axis=2)
+    lists = np.zeros((n, lmax), dtype=np.int32)
+    for i in range(n):
+        nb = np.nonzero((d[i] < 0.3) & (np.arange(200) != i))[0][: lmax - 9] + 1
+        lists[i, 0] = len(nb)
+        lists[i, 1:1 + len(nb)] = nb
+    fi = rng.normal(size=(n, 3)) * 0.1
+    fid = rng.normal(size=(n, 3)) * 0.01
+    fr = rng.normal(size=(n, 3)) * 0.1
+    frd = rng.normal(size=(n, 3)) * 0.01
+    return dict(cl=cl, f=f, fd=fd, t0=t0, step=step, stepr=stepr, lists=lists, fi=fi, fid=fid, fr=fr, frd=frd,
+                lmax=lmax)
+
+
+def _open(nb6, S):
+    cl = S["cl"]
+    n = cl.n
+    nb6.irr_open(n, S["lmax"], 0)
+    nb6.irr_set_jp_all(cl.pos, cl.vel, S["f"], S["fd"], cl.mass, S["t0"])
+    for a in range(1, n + 1):
+        nb6.irr_set_list(a, S["lists"][a - 1])
+    nb6.hermite_open(0.02, 0.125, 2.0 ** -24)
+    nb6.hermite_set_all(S["fi"], S["fid"], S["fr"], S["frd"], S["step"], np.zeros(n), S["stepr"], cl.rs)
+
+
+def test_block_clock_first_block_equals_host_choice_and_corrector(nb6):
+    S = _state(5)
+    n = S["cl"].n
+    tmin = (S["t0"] + S["step"]).min()
+    act_host = np.nonzero(S["t0"] + S["step"] == tmin)[0] + 1
+    _open(nb6, S)
+    try:
+        r0 = nb6.blocks_run(tmin / 2, 10)                 # the first block is past the limit
+        assert r0["reason"] == 2 and r0["blocks"] == 0
+        r1 = nb6.blocks_run(1.0, 1)                       # one block
+        assert r1["blocks"] == 1 and r1["tblock"] == tmin and r1["nact"] == len(act_host)
+        assert r1["reason"] in (0, 1)
+        addr, rows = nb6.blocks_active(n)
+        due, xv = nb6.blocks_regular(n)
+        state = nb6.hermite_get(1, n)
+    finally:
+        nb6.irr_close(0)
+    order = np.argsort(addr)
+    np.testing.assert_array_equal(addr[order], act_host)
+    rows = rows[order]
+    # the due list: the rows' regular-due flags, ascending, with x0 and v0
+    flagged = act_host[rows[:, 19] != 0]
+    np.testing.assert_array_equal(due, flagged)
+    np.testing.assert_array_equal(xv, rows[rows[:, 19] != 0][:, :6])
+    assert r1["reason"] == 1 and len(flagged) > 0
+    # the same set through nb6_irr_correct_ on a fresh copy of the state
+    _open(nb6, S)
+    try:
+        ref = nb6.irr_correct(tmin, act_host)
+    finally:
+        nb6.irr_close(0)
+    np.testing.assert_array_equal(rows, ref)
+    # the resident state took the corrected values
+    np.testing.assert_array_equal(state[act_host - 1][:, :6], ref[:, :6])
+    np.testing.assert_array_equal(state[act_host - 1][:, 24], np.full(len(act_host), tmin))
+
+
+def test_block_clock_runs_to_the_limit(nb6):
+    """Blocks run back to back until a regular step is due or the limit is
+    passed; every block time is a multiple of the smallest step, increasing."""
+    S = _state(6)
+    S["stepr"][:] = 1.0            # no regular step due before t = 1
+    n = S["cl"].n
+    _open(nb6, S)
+    try:
+        r = nb6.blocks_run(0.25, 100000)
+        state = nb6.hermite_get(1, n)
+    finally:
+        nb6.irr_close(0)
+    assert r["reason"] == 2 and r["blocks"] > 1 and r["tblock"] <= 0.25
+    t0 = state[:, 24]
+    step = state[:, 25]
+    assert np.all(t0 <= 0.25) and np.all(t0 + step > 0.25 - 1e-15)
+    assert r["irr_steps"] >= n
