@@ -182,6 +182,23 @@ def cpu_reference_rate(m, x, v, rs, dtr, args, seconds: float, max_calls: int | 
     return pairs / t_used, threads, calls, t_used
 
 
+def mufu_peak_per_s() -> float:
+    """Nominal MUFU (rsqrt) rate: 16 results per SM per clock (the CUDA
+    throughput table's figure for reciprocal square root) x SMs x the GPU's
+    maximum SM clock."""
+    import torch
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    mhz = 1965.0
+    try:
+        import subprocess
+        out = subprocess.run(["nvidia-smi", "--query-gpu=clocks.max.sm", "--format=csv,noheader,nounits",
+                              "-i", "0"], capture_output=True, text=True, timeout=20).stdout.strip()
+        mhz = float(out.splitlines()[0])
+    except Exception:
+        pass
+    return 16.0 * sms * mhz * 1e6
+
+
 def hbm_peak():
     """Measured HBM copy bandwidth (GB/s) of this pool's B200s, else the
     earlier fallback measurement."""
@@ -448,7 +465,11 @@ def main():
                "flops_per_pair": 27,
                "frac_fp32_peak": 27.0 * n * n / (pot_ms * 1e-3) / 1e12 / peak_tf,
                "note": "27 flops per pair is the reference's count (hi/lo differences); "
-                       "the ordered far loop issues 11 FP32 lane operations per pair"}
+                       "the ordered far loop issues 7 FP32 lane operations and one MUFU "
+                       "rsqrt per pair, so the MUFU pipe bounds it",
+               # one rsqrt per pair against the nominal 16 MUFU results per SM
+               # per clock at the GPU's maximum SM clock
+               "frac_mufu_peak": float(n) * n / (pot_ms * 1e-3) / mufu_peak_per_s()}
         if rank == 0:
             import oracle
             i0 = int(np.random.default_rng(9).integers(1, n - 64))

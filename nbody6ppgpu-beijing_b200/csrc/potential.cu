@@ -359,7 +359,7 @@ __global__ void __launch_bounds__(NT) pot_kernel_ord(const PotOrdArgs a) {
             const float2 nxr = pair2(-__double2float_rn(xd - (double)bc.x));
             const float2 nyr = pair2(-__double2float_rn(yd - (double)bc.y));
             const float2 nzr = pair2(-__double2float_rn(zd - (double)bc.z));
-            float2 acc = make_float2(0.f, 0.f);  // -(sum m 2/r), lane = j parity
+            float2 acc = make_float2(0.f, 0.f);  // sum m / r, lane = j parity
 #pragma unroll 4
             for (int q = 0; q < JT; q += 4) {
                 const float4 X = *reinterpret_cast<const float4 *>(&sr[st][0][q]);
@@ -376,16 +376,17 @@ __global__ void __launch_bounds__(NT) pot_kernel_ord(const PotOrdArgs a) {
                     const float2 dy = __fadd2_rn(yr, nyr);
                     const float2 dz = __fadd2_rn(zr, nzr);
                     const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+                    // 1/r straight from rsqrt.approx: every term of the
+                    // sum is positive, so its relative error bound carries
+                    // over to the sum unamplified (no Newton step needed,
+                    // unlike the cancelling force sums)
                     float2 y0;
                     asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y0.x) : "f"(r2.x));
                     asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y0.y) : "f"(r2.y));
-                    const float2 ra = __fmul2_rn(r2, y0);
-                    const float2 nb = __ffma2_rn(ra, y0, pair2(-3.0f));   // -(3 - r2 y0^2)
-                    const float2 ny = __fmul2_rn(y0, nb);                // -2/r
-                    acc = __ffma2_rn(mm, ny, acc);
+                    acc = __ffma2_rn(mm, y0, acc);
                 }
             }
-            p = -(acc.x + acc.y);
+            p = 2.0f * (acc.x + acc.y);  // the 2/r units of the hi/lo loop
         } else {
             const float4 *A = sh[st][0];
             const float4 *B = sh[st][1];
