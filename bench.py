@@ -146,6 +146,23 @@ class Clocks:
                 "power_w_max": float(max(pw))}
 
 
+def reduce_max(value: float, pg, device=None) -> float:
+    """The maximum of value over all ranks (the slowest rank's time); the
+    value itself on one rank."""
+    if pg is None:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world: int, pairs_per_step: float, steps: int, total_ms_max: float) -> float:
+    """Pairs per second of the whole job: every rank runs its own replica of
+    the workload (weak scaling), timed by the slowest rank."""
+    return world * pairs_per_step * steps / (total_ms_max * 1e-3)
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -400,13 +417,9 @@ def main():
     barrier()
     clk = clocks.stop()
     ms = float(np.mean(step_ms))
-    total_ms = float(np.sum(step_ms))
-    if pg is not None:
-        t = torch.tensor([total_ms], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = reduce_max(float(np.sum(step_ms)), pg, dev)
     pairs_step = float(n) * float(n)
-    value = world * pairs_step * args.steps / (total_ms * 1e-3)
+    value = whole_job_rate(world, pairs_step, args.steps, total_ms)
 
     # e2e through the C ABI with host buffers: gpunb_send_ + gpunb_regf_ calls
     e2e = None
@@ -432,11 +445,7 @@ def main():
         e2e_steps = max(1, min(args.steps, 2))
         for _ in range(e2e_steps):
             e2e_step()
-        e2e_s = (time.perf_counter() - t0) / e2e_steps
-        if pg is not None:
-            t = torch.tensor([e2e_s], device=dev)
-            pg.all_reduce(t, op=pg.ReduceOp.MAX)
-            e2e_s = float(t.item())
+        e2e_s = reduce_max((time.perf_counter() - t0) / e2e_steps, pg, dev)
         # bytes moved per step: the j set (m, x, v) and the i data up; the
         # force rows (8 doubles) and each list row's count + ids down (the
         # library writes only the used part of a row into pinned memory);
