@@ -372,7 +372,8 @@ __global__ void __launch_bounds__(NT) regf_kernel(const RegArgs a) {
 // so one LDS.128 brings four consecutive j of one component.  The arithmetic
 // is the scalar reg_pair's, operation for operation (negated i operands turn
 // subtractions into adds; sums are kept negated), so candidates and results
-// are bit-identical to the scalar kernels.
+// are bit-identical to the scalar kernels -- except on the far tiles of an
+// ordered j set, which take tile-relative differences (pair_x2_rel).
 // ----------------------------------------------------------------------------
 struct IP2 {
     float2 nxh, nyh, nzh, nxl, nyl, nzl, nvx, nvy, nvz, h2c, dt;  // i data, negated, duplicated
@@ -427,41 +428,6 @@ NB6_DEV unsigned pair_x2(const IP2 &ip, float2 xh, float2 yh, float2 zh, float2 
     s.jy = __ffma2_rn(nmy3, __ffma2_rn(al, dy, dvy), s.jy);
     s.jz = __ffma2_rn(nmy3, __ffma2_rn(al, dz, dvz), s.jz);
     return (c0 ? 1u : 0u) | (c1 ? 2u : 0u);
-}
-
-// pair_x2 for a pair known not to be a neighbour candidate: the same
-// operations in the same order minus the candidate test, so its results are
-// bit-identical to pair_x2's for such a pair.  (Kept for reference and for
-// a j set without relative coordinates; the far tiles of an ordered set
-// take pair_x2_rel.)
-template <bool MFLAG>
-NB6_DEV void pair_x2_far(const IP2 &ip, float2 xh, float2 yh, float2 zh, float2 m, float2 xl, float2 yl,
-                         float2 zl, float2 vx, float2 vy, float2 vz, S2 &s) {
-    const float2 dx = __fadd2_rn(__fadd2_rn(xh, ip.nxh), __fadd2_rn(xl, ip.nxl));
-    const float2 dy = __fadd2_rn(__fadd2_rn(yh, ip.nyh), __fadd2_rn(yl, ip.nyl));
-    const float2 dz = __fadd2_rn(__fadd2_rn(zh, ip.nzh), __fadd2_rn(zl, ip.nzl));
-    const float2 dvx = __fadd2_rn(vx, ip.nvx);
-    const float2 dvy = __fadd2_rn(vy, ip.nvy);
-    const float2 dvz = __fadd2_rn(vz, ip.nvz);
-    const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
-    const float2 rv = __ffma2_rn(dz, dvz, __ffma2_rn(dy, dvy, __fmul2_rn(dx, dvx)));
-    float2 y0;
-    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y0.x) : "f"(r2.x));
-    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y0.y) : "f"(r2.y));
-    const float2 ra = __fmul2_rn(r2, y0);
-    const float2 nb = __ffma2_rn(ra, y0, dup2(-3.0f));
-    const float2 ny = __fmul2_rn(y0, nb);
-    const float2 y2 = __fmul2_rn(ny, ny);
-    const float2 nmy = __fmul2_rn(m, ny);
-    const float2 nmy3 = __fmul2_rn(nmy, y2);
-    const float2 al = __fmul2_rn(__fmul2_rn(y2, dup2(-0.75f)), rv);
-    s.po = __fadd2_rn(s.po, nmy);
-    s.ax = __ffma2_rn(nmy3, dx, s.ax);
-    s.ay = __ffma2_rn(nmy3, dy, s.ay);
-    s.az = __ffma2_rn(nmy3, dz, s.az);
-    s.jx = __ffma2_rn(nmy3, __ffma2_rn(al, dx, dvx), s.jx);
-    s.jy = __ffma2_rn(nmy3, __ffma2_rn(al, dy, dvy), s.jy);
-    s.jz = __ffma2_rn(nmy3, __ffma2_rn(al, dz, dvz), s.jz);
 }
 
 // Far pair from tile-relative coordinates: xr = fl32(x_j - c) (stored with
