@@ -113,16 +113,30 @@ struct Ensemble : Bodies {
     // any regular correction of this block, as the host snapshot has it);
     // rows that overflowed come back untouched, get a smaller radius here
     // and go again.  The host keeps the new steps and radii of the rows.
-    void regular_on_device(const std::vector<int> &idx) {
+    // per-call buffers of regular_on_device, kept across calls
+    std::vector<int> r_runc, r_segq, r_addr0, r_count, r_segj0, r_pend, r_again, r_addr;
+    std::vector<double> r_rs;
+
+    // xv: when given, x0, v0 of the bodies in idx order (6 doubles each),
+    // else the host copies x0, v0 are read
+    void regular_on_device(const std::vector<int> &idx, const double *xv = nullptr) {
         const double t_0 = wtime();
         const size_t ni = idx.size();
-        std::vector<int> runc, seg_of_q(ni);
+        auto grow = [](auto &v, size_t k) {
+            if (v.size() < k) v.resize(k);
+        };
+        std::vector<int> &runc = r_runc, &seg_of_q = r_segq;
+        runc.clear();
+        grow(seg_of_q, ni);
         for (size_t q = 0; q < ni; ++q) {
             if (q == 0 || cl_of[idx[q]] != cl_of[idx[q - 1]]) runc.push_back(cl_of[idx[q]]);
             seg_of_q[q] = (int)runc.size() - 1;
         }
         int nseg = (int)runc.size();
-        std::vector<int> addr0(nseg), count(nseg), seg_j0(nseg + 1, 0);
+        std::vector<int> &addr0 = r_addr0, &count = r_count, &seg_j0 = r_segj0;
+        addr0.resize(nseg);
+        count.resize(nseg);
+        seg_j0.assign(nseg + 1, 0);
         for (int r = 0; r < nseg; ++r) {
             addr0[r] = base[runc[r]] + 1;
             count[r] = cnt[runc[r]];
@@ -134,23 +148,20 @@ struct Ensemble : Bodies {
         t_pred += wtime() - tp;
         double prm[6] = {P.eta_r, P.smax, P.dtmin, std::max(25.0 / tcr, 0.0), (double)P.nnbopt,
                          (double)P.mlp_mode};
-        std::vector<int> pend(ni);
+        std::vector<int> &pend = r_pend, &again = r_again, &addr = r_addr;
+        std::vector<double> &rsv = r_rs;
+        pend.resize(ni);
         for (size_t q = 0; q < ni; ++q) pend[q] = (int)q;
-        std::vector<int> addr;
-        std::vector<double> rsv;
         while (!pend.empty()) {
             const int np = (int)pend.size();
-            auto grow = [](auto &v, size_t k) {
-                if (v.size() < k) v.resize(k);
-            };
             grow(b_iseg, np);
             grow(b_h2, np);
             grow(b_dtr, np);
             grow(b_xi, 3 * (size_t)np);
             grow(b_vi, 3 * (size_t)np);
-            rrow.resize(32 * (size_t)np);
-            addr.resize(np);
-            rsv.resize(np);
+            grow(rrow, 32 * (size_t)np);
+            grow(addr, np);
+            grow(rsv, np);
             for (int p = 0; p < np; ++p) {
                 const int q = pend[p], i = idx[q];
                 addr[p] = i + 1;
@@ -158,9 +169,12 @@ struct Ensemble : Bodies {
                 b_h2[p] = h2_of(i, 1.0 / cnt[cl_of[i]]);
                 b_dtr[p] = stepr[i];
                 rsv[p] = rs[i];
-                for (int c = 0; c < 3; ++c) {  // t0 = time: the body is at x0, v0
-                    b_xi[3 * (size_t)p + c] = x0[3 * (size_t)i + c];
-                    b_vi[3 * (size_t)p + c] = v0[3 * (size_t)i + c];
+                // t0 = time: the body is at x0, v0
+                const double *px = xv ? xv + 6 * (size_t)q : &x0[3 * (size_t)i];
+                const double *pv = xv ? xv + 6 * (size_t)q + 3 : &v0[3 * (size_t)i];
+                for (int c = 0; c < 3; ++c) {
+                    b_xi[3 * (size_t)p + c] = px[c];
+                    b_vi[3 * (size_t)p + c] = pv[c];
                 }
             }
             int nni = np, lmax = P.lmax, nnbmax = P.nnbmax, mf = P.m_flag;
@@ -170,7 +184,7 @@ struct Ensemble : Bodies {
                            &nnbmax, &mf, prm, rrow.data());
             t_rcall += wtime() - tc;
             st.reg_calls++;
-            std::vector<int> again;
+            again.clear();
             for (int p = 0; p < np; ++p) {
                 const int q = pend[p], i = idx[q];
                 st.reg_pairs += cnt[cl_of[i]];
@@ -457,22 +471,15 @@ struct Ensemble : Bodies {
                 // the block's bodies due a regular step, ascending, with
                 // their corrected x0, v0 (the i of the regular call)
                 const double w0 = wtime();
-                act.resize(std::max(nact, 1));
-                rows.resize(6 * (size_t)std::max(nact, 1));
+                if (act.size() < (size_t)std::max(nact, 1)) act.resize(std::max(nact, 1));
+                if (rows.size() < 6 * (size_t)std::max(nact, 1)) rows.resize(6 * (size_t)std::max(nact, 1));
                 int nr = 0;
                 const double tq = wtime();
                 B.blocks_regular(&nr, act.data(), rows.data());
                 t_breg += wtime() - tq;
                 reg.resize(nr);
-                for (int q = 0; q < nr; ++q) {
-                    const int i = act[q] - 1;
-                    reg[q] = i;
-                    for (int c = 0; c < 3; ++c) {
-                        x0[3 * (size_t)i + c] = rows[6 * (size_t)q + c];
-                        v0[3 * (size_t)i + c] = rows[6 * (size_t)q + 3 + c];
-                    }
-                }
-                regular_on_device(reg);
+                for (int q = 0; q < nr; ++q) reg[q] = act[q] - 1;
+                regular_on_device(reg, rows.data());  // (the host copies of x0, v0 are refreshed at output)
                 t_reg += wtime() - w0;
             }
             if (time >= tnext_out - 1e-15) {
