@@ -585,22 +585,28 @@ __global__ void reg_corrector_kernel(int ni, const int *__restrict__ addr, const
 
 // ----------------------------------------------------------------------------
 // Device block clock (nb6_blocks_run_): blocks of irregular steps run back to
-// back on the device, each as four launches of one CUDA graph --
-//   blk_min      the block time, min over all bodies of tn = t0 + step;
+// back on the device, each as three launches of one CUDA graph --
 //   blk_collect  the active set {i : tn_i == block time} (next_tlist.f picks
 //                the same set from its level lists), or a stop when the
-//                block time passes the caller's limit;
+//                block time passes the caller's limit; also the earliest tn
+//                of the other bodies, which this block leaves as they are;
 //   blk_irr      the neighbour force of every active body (irr_force_warp);
 //   blk_corr     the irregular corrector of every active body (the same
 //                correct_irr_body as nb6_irr_correct_), then, in the last CTA
-//                to finish, the block's bookkeeping and a stop when a body is
-//                due a regular step (the host runs the regular part).
+//                to finish, the block's bookkeeping, the next block time (the
+//                earlier of the others' earliest tn and the block's new
+//                ones) and a stop when a body is due a regular step (the
+//                host runs the regular part).
+// The first block time of a run is the minimum over every body (blk_min,
+// launched once per run).
 // A stopped control block turns every later launch into an early return, so
 // the host enqueues many blocks and synchronises once.  No kernel waits on
 // another: the ordering is the stream's, the last-CTA test is one atomic.
 // ----------------------------------------------------------------------------
 struct BlockCtl {
-    unsigned long long tmin_bits[2];  // per parity: min tn as the bits of a non-negative double
+    unsigned long long tmin_bits[2];  // per parity: the block time, min tn (bits of a non-negative double)
+    unsigned long long m2_bits[2];    // per parity: min tn over the bodies not in the block
+    unsigned long long mact_bits[2];  // per parity: min of the block's new tn
     int nact[2];                      // per parity: active count
     int parity;
     int stop;                         // 0 run; 1 a regular-due block's irregular part is done; 2 block time > tlimit
@@ -614,21 +620,28 @@ struct BlockCtl {
 
 constexpr int BLK_NT = 256;
 
+// Minimum over the CTA (BLK_NT threads), valid in thread 0; every thread
+// must call it.
+NB6_DEV unsigned long long cta_min(unsigned long long m) {
+    __shared__ unsigned long long wm[BLK_NT / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = min(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int w = 1; w < BLK_NT / 32; ++w) m = min(m, wm[w]);
+    __syncthreads();
+    return m;
+}
+
 __global__ void __launch_bounds__(BLK_NT) blk_min(int n, const double *__restrict__ tn, BlockCtl *c) {
     if (c->stop) return;
     const int p = c->parity;
     unsigned long long m = ~0ull;
     for (size_t i = blockIdx.x * (size_t)BLK_NT + threadIdx.x; i < (size_t)n; i += (size_t)gridDim.x * BLK_NT)
         m = min(m, (unsigned long long)__double_as_longlong(tn[i]));
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) m = min(m, __shfl_xor_sync(0xffffffffu, m, o));
-    __shared__ unsigned long long wm[BLK_NT / 32];
-    if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = m;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        for (int w = 1; w < BLK_NT / 32; ++w) m = min(m, wm[w]);
-        atomicMin(&c->tmin_bits[p], m);
-    }
+    m = cta_min(m);
+    if (threadIdx.x == 0) atomicMin(&c->tmin_bits[p], m);
 }
 
 __global__ void __launch_bounds__(BLK_NT) blk_collect(int n, const double *__restrict__ tn, BlockCtl *c,
@@ -641,9 +654,12 @@ __global__ void __launch_bounds__(BLK_NT) blk_collect(int n, const double *__res
         return;
     }
     const int lane = threadIdx.x & 31;
+    unsigned long long m2 = ~0ull;  // the others' earliest time (they keep it through this block)
     for (size_t i0 = blockIdx.x * (size_t)BLK_NT; i0 < (size_t)n; i0 += (size_t)gridDim.x * BLK_NT) {
         const size_t i = i0 + threadIdx.x;
-        const bool on = i < (size_t)n && tn[i] == t;
+        const double ti = i < (size_t)n ? tn[i] : 0.0;
+        const bool on = i < (size_t)n && ti == t;
+        if (i < (size_t)n && !on) m2 = min(m2, (unsigned long long)__double_as_longlong(ti));
         const unsigned b = __ballot_sync(0xffffffffu, on);
         if (b) {
             int base = 0;
@@ -652,10 +668,10 @@ __global__ void __launch_bounds__(BLK_NT) blk_collect(int n, const double *__res
             if (on) act[base + __popc(b & ((1u << lane) - 1u))] = (int)i;
         }
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {  // the next block's accumulators; this block's list
-        c->tmin_bits[p ^ 1] = ~0ull;
-        c->nact[p ^ 1] = 0;
-        c->nreg = 0;
+    m2 = cta_min(m2);  // one atomic per CTA (not per warp: they would queue on one address)
+    if (threadIdx.x == 0) {
+        atomicMin(&c->m2_bits[p], m2);
+        if (blockIdx.x == 0) c->nreg = 0;  // this block's due list
     }
 }
 
@@ -693,26 +709,38 @@ __global__ void __launch_bounds__(BLK_NT)
     const int p = c->parity, na = c->nact[p];
     const double t = __longlong_as_double((long long)c->tmin_bits[p]);
     bool due = false;
+    unsigned long long mact = ~0ull;  // earliest new tn of this thread's bodies
     for (int k = blockIdx.x * BLK_NT + threadIdx.x; k < na; k += gridDim.x * BLK_NT) {
         double *o = rows + (size_t)k * 24;
-        if (correct_irr_body(act[k], t, force + (size_t)k * 8, rec, aux, hp, o, tn)) {
+        const int i = act[k];
+        if (correct_irr_body(i, t, force + (size_t)k * 8, rec, aux, hp, o, tn)) {
             due = true;
             const int q = atomicAdd(&c->nreg, 1);  // (q < na <= nmax)
-            reg[q] = act[k];
+            reg[q] = i;
             for (int d = 0; d < 6; ++d) regxv[6 * (size_t)q + d] = o[d];  // x0, v0
         }
+        mact = min(mact, (unsigned long long)__double_as_longlong(tn[i]));
     }
+    mact = cta_min(mact);
+    if (threadIdx.x == 0) atomicMin(&c->mact_bits[p], mact);
     if (__syncthreads_or(due) && threadIdx.x == 0) atomicOr(&c->regdue, 1);
     if (threadIdx.x == 0) {
         __threadfence();
         if (atomicAdd(&c->cta_done, 1u) == gridDim.x - 1) {  // last CTA: the block is done
             __threadfence();
+            const int q = p ^ 1;
             c->cta_done = 0;
             c->blocks += 1;
             c->irr_steps += na;
             c->tblock = t;
             c->last_nact = na;
-            c->parity = p ^ 1;
+            // the next block's time: the earliest of the bodies outside this
+            // block (unchanged by it) and of this block's new times
+            c->tmin_bits[q] = min(atomicAdd(&c->m2_bits[p], 0ull), atomicAdd(&c->mact_bits[p], 0ull));
+            c->m2_bits[q] = ~0ull;
+            c->mact_bits[q] = ~0ull;
+            c->nact[q] = 0;
+            c->parity = q;
             if (atomicExch(&c->regdue, 0)) c->stop = 1;
         }
     }
@@ -1400,7 +1428,6 @@ bool blocks_graph(cudaStream_t st) {
     const int sms = nb6_num_sms();
     cudaGraph_t g = nullptr;
     if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return false;
-    blk_min<<<sms * 4, BLK_NT, 0, st>>>(I.nmax, I.tn.ptr, I.bctl.ptr);
     blk_collect<<<sms * 4, BLK_NT, 0, st>>>(I.nmax, I.tn.ptr, I.bctl.ptr, I.bact.ptr);
     if (ks.slot)
         blk_irr<true><<<sms * 12, IRR_WARPS * 32, 0, st>>>(I.bctl.ptr, I.bact.ptr, I.rec.ptr, I.lists.ptr, I.lmax,
@@ -1451,9 +1478,13 @@ void blocks_run_impl(double tlimit, int max_blocks, int *reason, long long *nblo
     }
     BlockCtl &h = *I.hctl.ptr;
     memset(&h, 0, sizeof(h));
-    h.tmin_bits[0] = h.tmin_bits[1] = ~0ull;
+    for (int q = 0; q < 2; ++q) h.tmin_bits[q] = h.m2_bits[q] = h.mact_bits[q] = ~0ull;
     h.tlimit = tlimit;
     NB6_CUDA_CHECK(cudaMemcpyAsync(I.bctl.ptr, &h, sizeof(BlockCtl), cudaMemcpyHostToDevice, st));
+    // the first block's time from every body; each later one comes from the
+    // block before it (blk_collect and blk_corr)
+    blk_min<<<nb6_num_sms() * 4, BLK_NT, 0, st>>>(I.nmax, I.tn.ptr, I.bctl.ptr);
+    NB6_CUDA_CHECK(cudaGetLastError());
     if (!blocks_graph(st)) {
         fprintf(stderr, "nb6_blocks_run: the block graph could not be built\n");
         nb6_fatal(NB6_ERR_CUDA);
