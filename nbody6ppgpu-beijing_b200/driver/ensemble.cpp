@@ -454,11 +454,13 @@ struct Ensemble : Bodies {
         std::vector<int> act, reg;
         std::vector<double> rows;
         double t_reg = 0;
+        bool step_past = false;  // run one block past the output time (see below)
         for (;;) {
-            double tlimit = std::min(tnext_out, P.tcrit);
+            double tlimit = step_past ? P.tcrit : std::min(tnext_out, P.tcrit);
             const long long left = P.max_blocks - st.blocks;
             if (left <= 0) break;
-            int maxb = (int)std::min<long long>(left, 1 << 30), reason = 0, nact = 0;
+            int maxb = (int)std::min<long long>(step_past ? 1 : left, 1 << 30), reason = 0, nact = 0;
+            step_past = false;
             long long nb = 0, nirr = 0;
             double tb = time;
             const double ti0 = wtime();
@@ -489,8 +491,15 @@ struct Ensemble : Bodies {
                 tnext_out += P.dt_out;
                 t_out += wtime() - to;
             }
-            if (reason == 0) break;                           // block budget spent
             if (reason == 2 && tlimit >= P.tcrit) break;      // next block beyond the end
+            // No block fell on the output time (steps that do not divide
+            // it): the host clock records after the first block past it,
+            // so run exactly that one block next.
+            if (reason == 2 && time < tnext_out - 1e-15) {
+                step_past = true;
+                continue;
+            }
+            if (reason == 0 && P.max_blocks - st.blocks <= 0) break;  // block budget spent
         }
         pull_state();
         st.t_end = time;
