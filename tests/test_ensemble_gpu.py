@@ -112,3 +112,20 @@ def test_device_regular_corrector_equals_host_corrector_bit_for_bit(nb6, small_l
         np.testing.assert_array_equal(run.energy, host.energy)
         np.testing.assert_array_equal(run.times, host.times)
 
+
+
+def test_device_clock_output_times_off_the_block_grid(nb6):
+    """An output interval that no block time falls on (0.1): the device
+    clock records after the first block past each output time, as the host
+    clock does, with the same energies and state."""
+    from nb6b200 import drive
+    ours = drive.backend_paths("nb6b200")
+    cls = _clusters(3, 95)
+    kw = dict(batched=True, tcrit=0.3, dt_out=0.1)
+    clk = drive.run_ensemble(ours, cls, dev_corrector=3, **kw)
+    host = drive.run_ensemble(ours, cls, dev_corrector=2, **kw)
+    assert clk.stats["blocks"] == host.stats["blocks"]
+    np.testing.assert_array_equal(clk.times, host.times)
+    np.testing.assert_array_equal(clk.energy, host.energy)
+    for c in range(len(cls)):
+        np.testing.assert_array_equal(clk.x[c], host.x[c])
