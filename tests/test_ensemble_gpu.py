@@ -82,8 +82,8 @@ def test_device_corrector_equals_host_corrector_bit_for_bit(nb6):
     np.testing.assert_array_equal(dev.energy, host.energy)
 
 
-@pytest.mark.parametrize("small_lists", [False, True])
-def test_device_regular_corrector_equals_host_corrector_bit_for_bit(nb6, small_lists):
+@pytest.mark.parametrize("small_lists,m_flag", [(False, 0), (True, 0), (False, 1)])
+def test_device_regular_corrector_equals_host_corrector_bit_for_bit(nb6, small_lists, m_flag):
     """Both correctors on the device (nb6_irr_correct_ + nb6_regf_correct_),
     and both plus the block clock (nb6_blocks_run_), against both on the
     host (the same segmented regular-force call for every block): same
@@ -93,7 +93,7 @@ def test_device_regular_corrector_equals_host_corrector_bit_for_bit(nb6, small_l
     from nb6b200 import drive
     ours = drive.backend_paths("nb6b200")
     cls = _clusters(4, 90)
-    kw = dict(batched=True, tcrit=0.5, dt_out=0.125)
+    kw = dict(batched=True, tcrit=0.5, dt_out=0.125, m_flag=m_flag)
     if small_lists:
         kw.update(nnbopt=12, nnbmax=24, lmax=32, tcrit=0.25)
     dev = drive.run_ensemble(ours, cls, dev_corrector=2, **kw)
