@@ -65,6 +65,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-ref-gpu", action="store_true",
+                    help="skip timing the reference's CUDA library (oracle/_ref) on the same workload")
     ap.add_argument("--no-pot", action="store_true", help="skip the N^2 potential leg")
     ap.add_argument("--no-irr", action="store_true", help="skip the irregular-force leg")
     ap.add_argument("--seed", type=int, default=20260)
@@ -197,6 +199,43 @@ def cpu_reference_rate(m, x, v, rs, dtr, args, seconds: float, max_calls: int | 
     lib.gpunb_close()
     threads = int(os.environ.get("OMP_NUM_THREADS", "1"))
     return pairs / t_used, threads, calls, t_used
+
+
+def reference_gpu_rate(m, x, v, rs, dtr, args, seconds: float):
+    """The reference's own CUDA regular-force library (gpunb.velocity.cu,
+    built for sm_100a into oracle/_ref) on the same workload, through its C
+    ABI with host buffers: gpunb_send_ once, then the 1024-i gpunb_regf_
+    calls in order (synchronous calls, wall clock), a bounded sample.
+    Returns None when the library was not built."""
+    import oracle
+    from nb6b200.abi import ForceLib
+    if not oracle.ref_available("gpunb_velocity"):
+        return None
+    lib = ForceLib(oracle.ref_lib("gpunb_velocity"), "ref-gpunb-velocity")
+    n = m.shape[0]
+    h2 = rs ** 2 if not args.m_flag else rs ** 2 / m.mean()
+    lib.gpunb_open(n + 10, 0)
+    t0 = time.perf_counter()
+    lib.gpunb_send(m, x, v)
+    t_send = time.perf_counter() - t0
+    chunks = [(s, min(n, s + args.chunk)) for s in range(0, n, args.chunk)]
+    for s, e in chunks[:2]:                                   # warm-up
+        lib.gpunb_regf(h2[s:e], dtr[s:e], x[s:e], v[s:e], args.lmax, args.nnbmax, args.m_flag)
+    pairs, t_used, calls = 0.0, 0.0, 0
+    for s, e in chunks:
+        t0 = time.perf_counter()
+        lib.gpunb_regf(h2[s:e], dtr[s:e], x[s:e], v[s:e], args.lmax, args.nnbmax, args.m_flag)
+        t_used += time.perf_counter() - t0
+        pairs += (e - s) * float(n)
+        calls += 1
+        if t_used >= seconds:
+            break
+    lib.gpunb_close()
+    return {"value": pairs / t_used, "unit": "pairs/s", "calls": calls,
+            "send_s": t_send,
+            "kind": "the reference's CUDA library gpunb.velocity.cu built for sm_100a "
+                    "(oracle/_ref), through its C ABI with host buffers: compare with e2e",
+            "sample": f"{calls} calls x {args.chunk} i x {n} j of the same workload, {t_used:.1f} s"}
 
 
 def mufu_peak_per_s() -> float:
@@ -527,6 +566,10 @@ def main():
                              f"reg.avx.cpp gpunb_regf_ (oracle/_ref), {t_used:.1f} s"}
 
     lib.gpunb_close()
+    # the reference's own GPU code on this GPU, same workload (rank 0)
+    ref_gpu = None
+    if rank == 0 and not args.no_ref_gpu:
+        ref_gpu = reference_gpu_rate(m, x, v, rs, dtr, args, seconds=5.0)
     achieved = FLOPS_PER_PAIR * args.chunk * n / (kernel_ms * 1e-3) / 1e12
     nominal = 2 * 128 * 148 * (clk.get("sm_max_mhz") or 1965.0) * 1e6 / 1e12
     roof = {"bound": "fp32", "achieved": achieved, "peak": peak_tf, "unit": "TFLOP/s",
@@ -560,6 +603,7 @@ def main():
             # when the j set is spatially ordered (>= 32768 bodies)
             "gpu_launches": int(args.steps * len(chunks) * (3 if n >= 32768 else 2)),
             "clocks": clk, "roofline": roof, "e2e": e2e, "cpu_baseline": cpu,
+            "reference_gpu": ref_gpu,
             "err_vs_fp64": err,
             "gpupot": pot,
             "irregular": irr,
