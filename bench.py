@@ -522,8 +522,21 @@ def main():
             import oracle
             i0 = int(np.random.default_rng(9).integers(1, n - 64))
             po = oracle.pot(m, x, i0, 64)
-            pg_ = lib.gpupot(m, x)[i0 - 1:i0 - 1 + 64]   # the whole-set call, as timed
+            t0 = time.perf_counter()
+            pg_full = lib.gpupot(m, x)                      # the whole-set call, as timed
+            pot["e2e_s"] = time.perf_counter() - t0         # through gpupot_ with host arrays
+            pg_ = pg_full[i0 - 1:i0 - 1 + 64]
             pot["rel_err_max_sample64"] = float(np.max(np.abs(pg_ / po - 1)))
+            # the reference's own CUDA potential (gpupot.gpu.cu built for
+            # sm_100a), same call with host arrays, when it was built
+            if not args.no_ref_gpu and oracle.ref_available("gpupot_gpu"):
+                from nb6b200.abi import ForceLib
+                rlib = ForceLib(oracle.ref_lib("gpupot_gpu"), "ref-gpupot-gpu")
+                rlib.gpupot(m[:4096], x[:4096])             # warm-up (context, module)
+                t0 = time.perf_counter()
+                pr_ = rlib.gpupot(m, x)
+                pot["reference_gpu_s"] = time.perf_counter() - t0
+                pot["reference_gpu_rel_diff_max"] = float(np.max(np.abs(pr_ / pg_full - 1)))
         del d_m
 
     # the irregular path on the same cluster: neighbour lists of a sample

@@ -52,10 +52,10 @@ def fp64():
 
 
 def ref_path(name: str) -> str:
-    """name in {"reg", "pot", "irr"} (the AVX CPU libraries) or
-    "gpunb_velocity" (the reference's CUDA regular-force library)."""
-    if name == "gpunb_velocity":
-        return os.path.join(REF_DIR, "libref_gpunb_velocity.so")
+    """name in {"reg", "pot", "irr"} (the AVX CPU libraries),
+    "gpunb_velocity" or "gpupot_gpu" (the reference's CUDA libraries)."""
+    if name in ("gpunb_velocity", "gpupot_gpu"):
+        return os.path.join(REF_DIR, f"libref_{name}.so")
     return os.path.join(REF_DIR, f"libref_{name}_avx.so")
 
 

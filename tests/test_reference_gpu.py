@@ -41,3 +41,18 @@ def test_lists_and_forces_match_the_reference_cuda_library(nb6, orc, m_flag):
     assert np.median(ea) < 2e-5 and ea.max() < 5e-4, (np.median(ea), ea.max())
     assert np.median(ej) < 5e-5 and ej.max() < 5e-3, (np.median(ej), ej.max())
     assert np.median(ep) < 2e-5 and ep.max() < 5e-4, (np.median(ep), ep.max())
+
+
+def test_potential_matches_the_reference_cuda_library(nb6, orc):
+    """gpupot_ of this library (ordered path above 32,768 bodies) against
+    the reference's gpupot.gpu.cu built for sm_100a, whole set."""
+    from nb6b200 import ics
+    from nb6b200.abi import ForceLib
+    if not orc.ref_available("gpupot_gpu"):
+        pytest.skip("the reference CUDA potential was not built (oracle/Makefile ref_gpu)")
+    ref = ForceLib(orc.ref_lib("gpupot_gpu"), "ref-gpupot-gpu")
+    for n in (3000, 40000):
+        cl = ics.plummer(n, seed=n, imf=True)
+        p = nb6.gpupot(cl.mass, cl.pos)
+        pr = ref.gpupot(cl.mass, cl.pos)
+        assert rel_err_vec(p, pr).max() < 2e-6          # both hi/lo differences, FP32 pair math
