@@ -451,9 +451,12 @@ NB6_DEV void pair_x2_rel(const IP2 &ip, float2 nxr, float2 nyr, float2 nzr, floa
     float2 y0;
     asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y0.x) : "f"(r2.x));
     asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y0.y) : "f"(r2.y));
-    const float2 ra = __fmul2_rn(r2, y0);
-    const float2 nb = __ffma2_rn(ra, y0, dup2(-3.0f));
-    const float2 ny = __fmul2_rn(y0, nb);
+    // No Newton step on a far pair: -2/r straight from the approximation
+    // (one exact scaling instead of three operations).  A far pair is
+    // individually weak, so the approximation's relative error enters the
+    // force as a near-uniform scaling of the far field; the parity tests
+    // and the bench's FP64 check bound the result.
+    const float2 ny = __fmul2_rn(y0, dup2(-2.0f));
     const float2 y2 = __fmul2_rn(ny, ny);
     const float2 nmy = __fmul2_rn(m, ny);
     const float2 nmy3 = __fmul2_rn(nmy, y2);
