@@ -373,7 +373,8 @@ __global__ void __launch_bounds__(NT) regf_kernel(const RegArgs a) {
 // is the scalar reg_pair's, operation for operation (negated i operands turn
 // subtractions into adds; sums are kept negated), so candidates and results
 // are bit-identical to the scalar kernels -- except on the far tiles of an
-// ordered j set, which take tile-relative differences (pair_x2_rel).
+// ordered j set, which take tile-relative differences and 1/r without the
+// Newton step (pair_x2_rel).
 // ----------------------------------------------------------------------------
 struct IP2 {
     float2 nxh, nyh, nzh, nxl, nyl, nzl, nvx, nvy, nvz, h2c, dt;  // i data, negated, duplicated
@@ -451,23 +452,24 @@ NB6_DEV void pair_x2_rel(const IP2 &ip, float2 nxr, float2 nyr, float2 nzr, floa
     float2 y0;
     asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y0.x) : "f"(r2.x));
     asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y0.y) : "f"(r2.y));
-    // No Newton step on a far pair: -2/r straight from the approximation
-    // (one exact scaling instead of three operations).  A far pair is
-    // individually weak, so the approximation's relative error enters the
-    // force as a near-uniform scaling of the far field; the parity tests
-    // and the bench's FP64 check bound the result.
-    const float2 ny = __fmul2_rn(y0, dup2(-2.0f));
-    const float2 y2 = __fmul2_rn(ny, ny);
-    const float2 nmy = __fmul2_rn(m, ny);
-    const float2 nmy3 = __fmul2_rn(nmy, y2);
-    const float2 al = __fmul2_rn(__fmul2_rn(y2, dup2(-0.75f)), rv);
-    s.po = __fadd2_rn(s.po, nmy);
-    s.ax = __ffma2_rn(nmy3, dx, s.ax);
-    s.ay = __ffma2_rn(nmy3, dy, s.ay);
-    s.az = __ffma2_rn(nmy3, dz, s.az);
-    s.jx = __ffma2_rn(nmy3, __ffma2_rn(al, dx, dvx), s.jx);
-    s.jy = __ffma2_rn(nmy3, __ffma2_rn(al, dy, dvy), s.jy);
-    s.jz = __ffma2_rn(nmy3, __ffma2_rn(al, dz, dvz), s.jz);
+    // No Newton step on a far pair: 1/r straight from the approximation.
+    // A far pair is individually weak, so the approximation's relative
+    // error enters the force as a near-uniform scaling of the far field;
+    // the parity tests and the bench's FP64 check bound the result.
+    // The sums of a far tile are kept unscaled and positive (m/r, m dx/r^3,
+    // ...); the tile's fold applies the exact factors 2 and 8 of the
+    // other paths' convention, so a far pair costs 27 lane operations.
+    const float2 u = __fmul2_rn(m, y0);   // m/r
+    const float2 w = __fmul2_rn(y0, y0);  // 1/r^2
+    const float2 u3 = __fmul2_rn(u, w);   // m/r^3
+    const float2 al = __fmul2_rn(__fmul2_rn(w, dup2(-3.0f)), rv);
+    s.po = __fadd2_rn(s.po, u);
+    s.ax = __ffma2_rn(u3, dx, s.ax);
+    s.ay = __ffma2_rn(u3, dy, s.ay);
+    s.az = __ffma2_rn(u3, dz, s.az);
+    s.jx = __ffma2_rn(u3, __ffma2_rn(al, dx, dvx), s.jx);
+    s.jy = __ffma2_rn(u3, __ffma2_rn(al, dy, dvy), s.jy);
+    s.jz = __ffma2_rn(u3, __ffma2_rn(al, dz, dvz), s.jz);
 }
 
 // True when no body of tile box (bc, bh) can be a neighbour candidate of the
@@ -802,13 +804,15 @@ __global__ void __launch_bounds__(NT, X2_MINB / NI) regf_x2_kernel(const RegArgs
             issue_tile_soa<F64DX>(a, sj[st], &bar[st], t_begin + (t + NSTAGE) * t_step);
             issued = t + NSTAGE + 1;
         }
-        // fold: positive partial = rare-path sums - packed (negated) lane sums
+        // fold: positive partial = rare-path sums - packed (negated) lane
+        // sums; a far tile's lane sums are unscaled and positive (x8, x2)
+        const float fa = far ? 8.0f : -1.0f, fp = far ? 2.0f : -1.0f;
 #pragma unroll
         for (int k = 0; k < NI; ++k) {
-            const float p[7] = {fx[k].ax - (s[k].ax.x + s[k].ax.y), fx[k].ay - (s[k].ay.x + s[k].ay.y),
-                                fx[k].az - (s[k].az.x + s[k].az.y), fx[k].jx - (s[k].jx.x + s[k].jx.y),
-                                fx[k].jy - (s[k].jy.x + s[k].jy.y), fx[k].jz - (s[k].jz.x + s[k].jz.y),
-                                fx[k].po - (s[k].po.x + s[k].po.y)};
+            const float p[7] = {fx[k].ax + fa * (s[k].ax.x + s[k].ax.y), fx[k].ay + fa * (s[k].ay.x + s[k].ay.y),
+                                fx[k].az + fa * (s[k].az.x + s[k].az.y), fx[k].jx + fa * (s[k].jx.x + s[k].jx.y),
+                                fx[k].jy + fa * (s[k].jy.x + s[k].jy.y), fx[k].jz + fa * (s[k].jz.x + s[k].jz.y),
+                                fx[k].po + fp * (s[k].po.x + s[k].po.y)};
 #pragma unroll
             for (int c = 0; c < 7; ++c) {
                 float2 d = dsum[k][c][tid];
