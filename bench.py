@@ -19,7 +19,10 @@ Reported on one JSON line (rank 0):
   cpu_baseline  the reference's own reg.avx.cpp (oracle/_ref) on the host
              cores, bounded sample of the same workload;
   err_vs_fp64   force/jerk/potential error against the FP64 oracle on a
-             sample of i-particles.
+             sample of i-particles;
+  gpupot, irregular, predictor   the N^2 potential, the irregular force and
+             the Hermite predictor on the same bodies, each against its own
+             roofline (MUFU rate, HBM bandwidth).
 
 --impl reference runs the reference's CPU library (the timed CPU arm).
 Multi-GPU (torchrun, --gpus N): every rank evaluates its own cluster of the
@@ -69,6 +72,7 @@ def parse():
                     help="skip timing the reference's CUDA library (oracle/_ref) on the same workload")
     ap.add_argument("--no-pot", action="store_true", help="skip the N^2 potential leg")
     ap.add_argument("--no-irr", action="store_true", help="skip the irregular-force leg")
+    ap.add_argument("--no-pred", action="store_true", help="skip the Hermite predictor leg")
     ap.add_argument("--seed", type=int, default=20260)
     return ap.parse_args()
 
@@ -263,6 +267,48 @@ def hbm_peak():
             return float(json.load(f)["hbm_gbs"]), "measured (MEASURED_PEAKS.json)"
     except (OSError, KeyError, ValueError):
         return 6650.0, "fallback"
+
+
+def predictor_leg(lib, m, x, v, flush_l2, reps: int = 10):
+    """The Hermite j predictor (xbpredall.F:48-62) over every body, state
+    resident in HBM (nb6_state_set_, nb6_predict_device_): 104 bytes read
+    (T0, X0, X0DOT, F, FDOT) and 48 written (X, XDOT) per body, HBM-bound.
+    Kernel time from the library's CUDA events, L2 flushed before each
+    launch; the prediction checked against the FP64 oracle's."""
+    import oracle
+    raw = lib.lib
+    n = m.shape[0]
+    rng = np.random.default_rng(11)
+    a = {"body": m, "t0": -rng.integers(0, 64, n) / 8192.0, "x0": x, "x0dot": v,
+         "f": rng.normal(size=(n, 3)) * 0.3, "fdot": rng.normal(size=(n, 3)) * 0.1}
+    a = {k: np.ascontiguousarray(val, dtype=np.float64) for k, val in a.items()}
+    dp = C.POINTER(C.c_double)
+    t = C.c_double(1.0 / 1024)
+    ms = []
+    raw.nb6_state_open_(C.byref(C.c_int(n)))
+    try:
+        raw.nb6_state_set_(C.byref(C.c_int(n)), *(a[k].ctypes.data_as(dp)
+                                                  for k in ("body", "t0", "x0", "x0dot", "f", "fdot")))
+        dx, dv = dp(), dp()
+        for _ in range(3):
+            raw.nb6_predict_device_(C.byref(t), C.byref(dx), C.byref(dv))
+        for _ in range(reps):
+            flush_l2()
+            raw.nb6_predict_device_(C.byref(t), C.byref(dx), C.byref(dv))
+            ms.append(float(raw.nb6_predict_last_kernel_ms_()))
+        xs, xds = np.zeros((n, 3)), np.zeros((n, 3))
+        raw.nb6_predict_(C.byref(t), xs.ctypes.data_as(dp), xds.ctypes.data_as(dp))
+    finally:
+        raw.nb6_state_close_()
+    ox, oxd = oracle.predict(t.value, a["t0"], a["x0"], a["x0dot"], a["f"], a["fdot"])
+    k_ms = float(np.median(ms))
+    gbs = 152.0 * n / (k_ms * 1e-3) / 1e9
+    hbm, src = hbm_peak()
+    return {"bodies": n, "kernel_ms": k_ms, "bytes_per_body": 152, "gbs_algorithmic": gbs,
+            "frac_hbm": gbs / hbm, "hbm_peak_gbs": hbm, "hbm_peak_source": src,
+            "x_diff_vs_oracle_max_over_extent": float(np.max(np.abs(xs - ox)) / np.max(np.abs(ox))),
+            "timing": f"median of {reps} launches, CUDA events on the library stream, "
+                      "L2 flushed (256 MiB write) before each"}
 
 
 def irregular_leg(lib, m, x, v, h2, dtr, args, nsample: int = 65536):
@@ -548,6 +594,11 @@ def main():
     if not args.no_irr and rank == 0:
         irr = irregular_leg(lib, m, x, v, h2, dtr, args)
 
+    # the Hermite predictor over the same bodies (rank 0)
+    pred = None
+    if not args.no_pred and rank == 0:
+        pred = predictor_leg(lib, m, x, v, flush_l2)
+
     # accuracy against the FP64 oracle on one call of the timed shape (a
     # chunk of i, so the same tuned kernel and its far-tile path run; rank 0)
     err = None
@@ -620,6 +671,7 @@ def main():
             "err_vs_fp64": err,
             "gpupot": pot,
             "irregular": irr,
+            "predictor": pred,
             "pct_fp32_peak": 100.0 * FLOPS_PER_PAIR * pairs_step / (ms * 1e-3) / 1e12 / peak_tf,
         }
         print(json.dumps(out), flush=True)
