@@ -609,16 +609,31 @@ struct BlockCtl {
     unsigned long long mact_bits[2];  // per parity: min of the block's new tn
     int nact[2];                      // per parity: active count
     int parity;
-    int stop;                         // 0 run; 1 a regular-due block's irregular part is done; 2 block time > tlimit
+    int stop;                         // 0 run; 1 a regular-due block's irregular part is done; 2 block time > tlimit;
+                                      // 3 the run's block limit reached
     int regdue;                       // the running block has a regular-due body
     unsigned cta_done;                // blk_corr CTAs finished (last-CTA test)
     long long blocks, irr_steps;      // since the last reset by the host
     double tlimit, tblock;            // run limit; time of the last block done
     int last_nact;
     int nreg;                         // regular-due bodies of the running block (breg, bregxv)
+    long long blimit;                 // blocks this run may do (stop 3 when reached)
 };
 
 constexpr int BLK_NT = 256;
+
+// Programmatic dependent launch (the block kernels are captured with
+// programmatic edges, so each may be scheduled while the one before it
+// drains).  griddepcontrol.wait returns once the kernels this one depends
+// on have completed and their memory is visible -- the guarantee of a
+// kernel boundary -- so every block kernel calls it before its first
+// access to the control block or to data an earlier kernel wrote, and then
+// lets its own dependants be scheduled.  Both are no-ops for a launch
+// without a programmatic dependency.
+NB6_DEV void blk_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
 
 // Minimum over the CTA (BLK_NT threads), valid in thread 0; every thread
 // must call it.
@@ -635,6 +650,7 @@ NB6_DEV unsigned long long cta_min(unsigned long long m) {
 }
 
 __global__ void __launch_bounds__(BLK_NT) blk_min(int n, const double *__restrict__ tn, BlockCtl *c) {
+    blk_enter();
     if (c->stop) return;
     const int p = c->parity;
     unsigned long long m = ~0ull;
@@ -646,7 +662,12 @@ __global__ void __launch_bounds__(BLK_NT) blk_min(int n, const double *__restric
 
 __global__ void __launch_bounds__(BLK_NT) blk_collect(int n, const double *__restrict__ tn, BlockCtl *c,
                                                       int *__restrict__ act) {
+    blk_enter();
     if (c->stop) return;
+    if (c->blocks >= c->blimit) {  // every thread reads the same count: all return
+        if (blockIdx.x == 0 && threadIdx.x == 0) c->stop = 3;
+        return;
+    }
     const int p = c->parity;
     const double t = __longlong_as_double((long long)c->tmin_bits[p]);
     if (t > c->tlimit) {  // every thread reads the same t: all return
@@ -679,6 +700,7 @@ template <bool KS>
 __global__ void __launch_bounds__(IRR_WARPS * 32)
     blk_irr(const BlockCtl *c, const int *__restrict__ act, const Rec *__restrict__ rec,
             const int *__restrict__ lists, int ls, int nmax, KsArgs ks, double *__restrict__ out) {
+    blk_enter();
     if (c->stop) return;
     const int p = c->parity, na = c->nact[p];
     const double t = __longlong_as_double((long long)c->tmin_bits[p]);
@@ -705,6 +727,7 @@ __global__ void __launch_bounds__(BLK_NT)
     blk_corr(BlockCtl *c, const int *__restrict__ act, const double *__restrict__ force, Rec *__restrict__ rec,
              Aux *__restrict__ aux, HermiteParams hp, double *__restrict__ rows, double *__restrict__ tn,
              int *__restrict__ reg, double *__restrict__ regxv) {
+    blk_enter();
     if (c->stop) return;
     const int p = c->parity, na = c->nact[p];
     const double t = __longlong_as_double((long long)c->tmin_bits[p]);
@@ -908,7 +931,9 @@ struct IrrState {
     HostBuf<BlockCtl> hctl;
     cudaGraphExec_t bgraph = nullptr;
     const void *bgraph_key[8] = {};   // buffers and pair-table flag the graph was made with
-    int blk_batch = 16;               // graph launches per synchronisation
+    int blk_batch = 16;               // blocks per synchronisation
+    int blk_unroll = 0;               // blocks per graph (NB6_BLK_UNROLL, default 4)
+    bool blk_pdl = true;              // programmatic edges between the block kernels (NB6_BLK_PDL=0: off)
     DevBuf<int> breg;                 // regular-due bodies of the running block
     DevBuf<double> bregxv;            // their x0, v0
     DevBuf<int> bsort;                // [sorted addresses | slots in | slots out], 3 x nmax
@@ -1428,17 +1453,52 @@ bool blocks_graph(cudaStream_t st) {
     const int sms = nb6_num_sms();
     cudaGraph_t g = nullptr;
     if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return false;
-    blk_collect<<<sms * 4, BLK_NT, 0, st>>>(I.nmax, I.tn.ptr, I.bctl.ptr, I.bact.ptr);
-    if (ks.slot)
-        blk_irr<true><<<sms * 12, IRR_WARPS * 32, 0, st>>>(I.bctl.ptr, I.bact.ptr, I.rec.ptr, I.lists.ptr, I.lmax,
-                                                           I.nmax, ks, I.bforce.ptr);
-    else
-        blk_irr<false><<<sms * 12, IRR_WARPS * 32, 0, st>>>(I.bctl.ptr, I.bact.ptr, I.rec.ptr, I.lists.ptr, I.lmax,
-                                                            I.nmax, ks, I.bforce.ptr);
-    blk_corr<<<sms * 2, BLK_NT, 0, st>>>(I.bctl.ptr, I.bact.ptr, I.bforce.ptr, I.rec.ptr, I.aux.ptr, I.hp,
-                                          I.brows.ptr, I.tn.ptr, I.breg.ptr, I.bregxv.ptr);
-    if (cudaStreamEndCapture(st, &g) != cudaSuccess || !g) return false;
-    const bool ok = cudaGraphInstantiate(&I.bgraph, g, 0) == cudaSuccess;
+    // blk_unroll blocks back to back; with blk_pdl every kernel after the
+    // first is captured with a programmatic edge to the one before it
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    auto cfg = [&](int grid, int threads, bool first) {
+        cudaLaunchConfig_t c = {};
+        c.gridDim = dim3(grid);
+        c.blockDim = dim3(threads);
+        c.dynamicSmemBytes = 0;
+        c.stream = st;
+        c.attrs = at;
+        c.numAttrs = (I.blk_pdl && !first) ? 1 : 0;
+        return c;
+    };
+    bool ok = true;
+    for (int u = 0; u < I.blk_unroll && ok; ++u) {
+        cudaLaunchConfig_t c0 = cfg(sms * 4, BLK_NT, u == 0);
+        ok = cudaLaunchKernelEx(&c0, blk_collect, I.nmax, (const double *)I.tn.ptr, I.bctl.ptr, I.bact.ptr) ==
+             cudaSuccess;
+        cudaLaunchConfig_t c1 = cfg(sms * 12, IRR_WARPS * 32, false);
+        const BlockCtl *cc = I.bctl.ptr;
+        const int *ca = I.bact.ptr, *cl = I.lists.ptr;
+        const Rec *cr = I.rec.ptr;
+        if (ok && ks.slot)
+            ok = cudaLaunchKernelEx(&c1, blk_irr<true>, cc, ca, cr, cl, I.lmax, I.nmax, ks, I.bforce.ptr) ==
+                 cudaSuccess;
+        else if (ok)
+            ok = cudaLaunchKernelEx(&c1, blk_irr<false>, cc, ca, cr, cl, I.lmax, I.nmax, ks, I.bforce.ptr) ==
+                 cudaSuccess;
+        cudaLaunchConfig_t c2 = cfg(sms * 2, BLK_NT, false);
+        if (ok)
+            ok = cudaLaunchKernelEx(&c2, blk_corr, I.bctl.ptr, ca, (const double *)I.bforce.ptr, I.rec.ptr,
+                                    I.aux.ptr, I.hp, I.brows.ptr, I.tn.ptr, I.breg.ptr, I.bregxv.ptr) ==
+                 cudaSuccess;
+    }
+    if (cudaStreamEndCapture(st, &g) != cudaSuccess || !g || !ok) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        if (I.blk_pdl) {  // a runtime without programmatic edges in capture: plain edges
+            I.blk_pdl = false;
+            return blocks_graph(st);
+        }
+        return false;
+    }
+    ok = cudaGraphInstantiate(&I.bgraph, g, 0) == cudaSuccess;
     cudaGraphDestroy(g);
     if (!ok) {
         I.bgraph = nullptr;
@@ -1480,6 +1540,13 @@ void blocks_run_impl(double tlimit, int max_blocks, int *reason, long long *nblo
     memset(&h, 0, sizeof(h));
     for (int q = 0; q < 2; ++q) h.tmin_bits[q] = h.m2_bits[q] = h.mact_bits[q] = ~0ull;
     h.tlimit = tlimit;
+    h.blimit = max_blocks;
+    if (I.blk_unroll == 0) {
+        const char *e = getenv("NB6_BLK_UNROLL");
+        I.blk_unroll = std::max(1, std::min(32, e ? atoi(e) : 4));
+        const char *q = getenv("NB6_BLK_PDL");
+        I.blk_pdl = !(q && q[0] == '0');
+    }
     NB6_CUDA_CHECK(cudaMemcpyAsync(I.bctl.ptr, &h, sizeof(BlockCtl), cudaMemcpyHostToDevice, st));
     // the first block's time from every body; each later one comes from the
     // block before it (blk_collect and blk_corr)
@@ -1493,8 +1560,9 @@ void blocks_run_impl(double tlimit, int max_blocks, int *reason, long long *nblo
     long long done = 0;
     int batch = I.blk_batch;
     for (;;) {
+        // blocks past the run's limit or a stop return at once (blimit)
         const int k = (int)std::min<long long>(batch, (long long)max_blocks - done);
-        for (int b = 0; b < k; ++b) NB6_CUDA_CHECK(cudaGraphLaunch(I.bgraph, st));
+        for (int b = 0; b < k; b += I.blk_unroll) NB6_CUDA_CHECK(cudaGraphLaunch(I.bgraph, st));
         NB6_CUDA_CHECK(cudaMemcpyAsync(&h, I.bctl.ptr, sizeof(BlockCtl), cudaMemcpyDeviceToHost, st));
         nb6_status_fetch(st);
         NB6_CUDA_CHECK(cudaStreamSynchronize(st));
@@ -1505,7 +1573,7 @@ void blocks_run_impl(double tlimit, int max_blocks, int *reason, long long *nblo
     }
     // next run's first batch: about twice this run's length
     I.blk_batch = (int)std::max<long long>(2, std::min<long long>(128, 2 * done));
-    *reason = h.stop;
+    *reason = h.stop == 3 ? 0 : h.stop;
     *nblocks = h.blocks;
     *nirr = h.irr_steps;
     *tblock = h.tblock;
