@@ -1,0 +1,147 @@
+"""Regular force of one cluster split over ranks by active particle.
+
+This is the multi-rank form of the regular block in the reference's parallel
+build (``intgrt.F:942-1100``).  Every rank holds the whole predicted state and
+sends the whole j set to its own GPU (``intgrt.F:875-882``); the active list
+is cut into contiguous pieces, one per rank (``intgrt.F:955-968``); each rank
+evaluates its piece (``CALC_REG_ON_GPU(IREG,istart,iend)``, ``intgrt.F:992``);
+then the per-particle results travel to every rank (the ``MPI_SENDRECV`` ring
+of ``intgrt.F:1046-1095``), so that each rank ends the block with the results
+of the whole active list.
+
+Here the exchange is one all-gather per result kind over ``torch.distributed``
+(NCCL between GPUs, gloo between host processes): the FP64 rows
+(acc, jrk, pot) and the neighbour-list rows (``lmax`` ints each).  The pieces
+are padded to the largest piece so that every rank contributes the same
+number of rows.  Every rank takes the same collective steps in the same
+order, including ranks whose piece is empty; a block with no active
+particles takes none on any rank, since the active count is the same
+everywhere.
+
+The force itself goes through :class:`nb6b200.abi.ForceLib` (``gpunb_regf_``
+of ``libnb6b200.so``) in calls of at most 1024 particles, the reference's
+per-call limit (``util_gpu.F:7``).  Results are those of a single-rank call
+over the whole list, row for row: each particle's force is computed
+independently of how the list is cut.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+NIMAX = 1024  # particles per gpunb_regf_ call (util_gpu.F:7)
+NREC = 7      # FP64 values per result row: acc[3], jrk[3], pot
+
+
+def active_split(nl: int, size: int) -> tuple[list[int], list[int]]:
+    """Contiguous pieces of an active list of ``nl`` particles over ``size``
+    ranks, as ``intgrt.F:955-968`` cuts it: each rank gets ``nl // size``
+    and the first ``nl % size`` ranks one more.  Returns (start, count) per
+    rank, starts 0-based (the Fortran ``ista`` minus one)."""
+    if size < 1 or nl < 0:
+        raise ValueError(f"active_split: nl={nl}, size={size}")
+    inl, idiff = divmod(nl, size)
+    start, count, run = [], [], 0
+    for r in range(size):
+        n = inl + (1 if r < idiff else 0)
+        start.append(run)
+        count.append(n)
+        run += n
+    return start, count
+
+
+class RegularRankSplit:
+    """``gpunb_send_`` / ``gpunb_regf_`` for one cluster over the ranks of a
+    process group, split by active particle.
+
+    ``lib`` is this rank's :class:`ForceLib`, already opened
+    (``gpunb_open``) on this rank's GPU.  ``group`` is a ``torch.distributed``
+    process group (None: the default group; no initialised group: one rank,
+    no exchange).  ``chunk`` is the largest ``gpunb_regf_`` call.
+    """
+
+    def __init__(self, lib, group=None, chunk: int = NIMAX):
+        if not 1 <= chunk <= NIMAX:
+            raise ValueError(f"chunk={chunk} outside [1, {NIMAX}]")
+        self.lib = lib
+        self.chunk = chunk
+        self.group = group
+        self.rank, self.size = 0, 1
+        self.dist = None
+        try:
+            import torch.distributed as dist
+            if dist.is_available() and dist.is_initialized():
+                self.dist = dist
+                self.rank = dist.get_rank(group)
+                self.size = dist.get_world_size(group)
+        except ImportError:
+            pass
+        self.device = None
+        if self.dist is not None:
+            import torch
+            if self.dist.get_backend(group) == "nccl":
+                # NCCL buffers live on the GPU the library opened on
+                # (gpunb_open_ picks irank modulo the visible devices).
+                dev = -1
+                query = getattr(getattr(lib, "lib", None), "nb6_device_", None)
+                if query is not None:
+                    dev = int(query())
+                if dev < 0:
+                    dev = torch.cuda.current_device()
+                torch.cuda.set_device(dev)
+                self.device = torch.device("cuda", dev)
+            else:
+                self.device = torch.device("cpu")
+
+    def send(self, m, x, v) -> None:
+        """Every rank sends the whole predicted j set to its own GPU
+        (``intgrt.F:882``); list ids are then the same on every rank."""
+        self.lib.gpunb_send(m, x, v)
+
+    def piece(self, nl: int) -> tuple[int, int]:
+        """(start, count) of this rank's piece of an ``nl``-particle list."""
+        start, count = active_split(nl, self.size)
+        return start[self.rank], count[self.rank]
+
+    def _own(self, h2, dtr, xi, vi, lmax, nnbmax, m_flag, s, n):
+        rec = np.zeros((n, NREC))
+        lst = np.zeros((n, lmax), dtype=np.int32)
+        for a in range(0, n, self.chunk):
+            b = min(n, a + self.chunk)
+            acc, jrk, pot, l = self.lib.gpunb_regf(h2[s + a:s + b], dtr[s + a:s + b], xi[s + a:s + b],
+                                                   vi[s + a:s + b], lmax, nnbmax, m_flag)
+            rec[a:b, 0:3] = acc
+            rec[a:b, 3:6] = jrk
+            rec[a:b, 6] = pot
+            lst[a:b] = l
+        return rec, lst
+
+    def _gather(self, rows: np.ndarray, width: int, counts: list[int]) -> np.ndarray:
+        """All-gather of each rank's first ``counts[rank]`` rows, padded to
+        ``counts[0]`` (the largest piece); returns the rows in rank order."""
+        import torch
+        pad = counts[0]
+        buf = np.zeros((pad, width), dtype=rows.dtype)
+        buf[:rows.shape[0]] = rows
+        src = torch.from_numpy(buf).to(self.device)
+        out = torch.empty((self.size * pad, width), dtype=src.dtype, device=self.device)
+        self.dist.all_gather_into_tensor(out, src, group=self.group)
+        full = out.cpu().numpy().reshape(self.size, pad, width)
+        return np.concatenate([full[r, :counts[r]] for r in range(self.size)], axis=0)
+
+    def regf(self, h2, dtr, xi, vi, lmax: int, nnbmax: int, m_flag: int = 0):
+        """Regular force of the whole active list (``gpunb_regf_`` semantics:
+        acc, jrk, pot exclude neighbours; list rows ``[nnb, ids...]`` or
+        ``-nnb`` on overflow).  Every rank passes the same list and gets every
+        particle's results back; it evaluates only its own piece."""
+        h2 = np.ascontiguousarray(h2, dtype=np.float64)
+        nl = h2.shape[0]
+        dtr = np.ascontiguousarray(dtr, dtype=np.float64).reshape(nl)
+        xi = np.ascontiguousarray(xi, dtype=np.float64).reshape(nl, 3)
+        vi = np.ascontiguousarray(vi, dtype=np.float64).reshape(nl, 3)
+        start, count = active_split(nl, self.size)
+        s, n = start[self.rank], count[self.rank]
+        rec, lst = self._own(h2, dtr, xi, vi, lmax, nnbmax, m_flag, s, n)
+        if self.dist is not None and self.size > 1 and nl > 0:
+            rec = self._gather(rec, NREC, count)
+            lst = self._gather(lst, lmax, count)
+        return rec[:, 0:3].copy(), rec[:, 3:6].copy(), rec[:, 6].copy(), lst

@@ -36,7 +36,7 @@ def test_two_ranks_take_the_slowest_time():
     import torch.multiprocessing as mp
     world, port = 2, _free_port()
     times = [1500.0, 1750.0]
-    with mp.Manager() as mgr:
+    with mp.get_context("spawn").Manager() as mgr:
         out = mgr.dict()
         mp.spawn(_rank, args=(world, port, times, out), nprocs=world, join=True)
         res = dict(out)

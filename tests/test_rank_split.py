@@ -1,0 +1,153 @@
+"""The regular force split over ranks by active particle (nb6b200.rank_split)
+on CPU: gloo ranks, one process each as torchrun launches them, with the FP64
+oracle standing in for each rank's GPU library.  Every rank must end with the
+results of a single-rank call over the whole active list, bit for bit:
+ragged pieces, pieces that are empty, pieces that cross the per-call limit,
+and overflowing neighbour lists (-nnb rows) included."""
+import os
+import socket
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+class _OracleForceLib:
+    """gpunb_send / gpunb_regf of the FP64 oracle (the checker), with the
+    ForceLib call signatures."""
+
+    def __init__(self, orc):
+        self.orc = orc
+        self.j = None
+
+    def gpunb_send(self, m, x, v):
+        self.j = (np.array(m), np.array(x), np.array(v))
+
+    def gpunb_regf(self, h2, dtr, xi, vi, lmax, nnbmax, m_flag=0):
+        return self.orc.regf(*self.j, h2, dtr, xi, vi, lmax, nnbmax, m_flag)
+
+
+# (active count, chunk, nnbmax): ragged pieces, an empty list, fewer active
+# particles than ranks, pieces crossing the call limit, overflowing lists.
+CASES = [(256, 1024, 40), (5, 1024, 40), (1, 1024, 40), (0, 1024, 40), (200, 7, 40), (97, 16, 3)]
+
+
+def _cases():
+    import oracle
+    from nb6b200 import ics
+    cl = ics.plummer(256, seed=43532, nnbopt=20)
+    h2 = cl.h2(0)
+    rng = np.random.default_rng(7)
+    out = []
+    for nl, chunk, nnbmax in CASES:
+        act = np.sort(rng.choice(cl.n, size=nl, replace=False))
+        out.append((cl, h2[act], cl.dtr[act], cl.pos[act], cl.vel[act], chunk, nnbmax))
+    return oracle, out
+
+
+def _rank(rank, world, port, out):
+    import datetime
+    import sys
+    for p in (os.path.join(ROOT, "nbody6ppgpu-beijing_b200"), os.path.join(ROOT, "oracle")):
+        sys.path.insert(0, p)
+    import torch.distributed as dist
+    from nb6b200.rank_split import RegularRankSplit
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        orc, cases = _cases()
+        res = []
+        for cl, h2, dtr, xi, vi, chunk, nnbmax in cases:
+            lmax = 64
+            split = RegularRankSplit(_OracleForceLib(orc), chunk=chunk)
+            split.send(cl.mass, cl.pos, cl.vel)
+            got = split.regf(h2, dtr, xi, vi, lmax, nnbmax, 0)
+            want = orc.regf(cl.mass, cl.pos, cl.vel, h2, dtr, xi, vi, lmax, nnbmax, 0)
+            same = all(np.array_equal(g, w) for g, w in zip(got, want))
+            shapes = tuple(g.shape for g in got)
+            nover = int((got[3][:, 0] < 0).sum()) if len(got[3]) else 0
+            res.append((same, shapes, split.piece(len(h2)), nover))
+        out[rank] = res
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_ranks_end_with_the_single_rank_results(world):
+    import torch.multiprocessing as mp
+    port = _free_port()
+    with mp.get_context("spawn").Manager() as mgr:
+        out = mgr.dict()
+        mp.spawn(_rank, args=(world, port, out), nprocs=world, join=True)
+        res = dict(out)
+    from nb6b200.rank_split import active_split
+    for rank in range(world):
+        assert len(res[rank]) == len(CASES)
+        for (nl, chunk, nnbmax), (same, shapes, piece, nover) in zip(CASES, res[rank]):
+            assert same, (rank, nl, chunk, nnbmax)
+            assert shapes == ((nl, 3), (nl, 3), (nl,), (nl, 64))
+            start, count = active_split(nl, world)
+            assert piece == (start[rank], count[rank])
+            if nnbmax == 3 and nl > 0:
+                assert nover > 0  # the overflow rows travelled too
+
+
+def _fortran_split(nl, isize):
+    """intgrt.F:955-968 as written, 1-based ista, inum zeroed past the list."""
+    inl = nl // isize
+    idiff = nl - isize * inl
+    irun, ista, inum = 0, [], []
+    for ix in range(1, isize + 1):
+        n = inl + (1 if ix <= idiff else 0)
+        s = irun + 1
+        if s > nl:
+            n = 0
+        ista.append(s)
+        inum.append(n)
+        irun += n
+    return ista, inum
+
+
+def test_active_split_matches_the_reference_cut():
+    from nb6b200.rank_split import active_split
+    for size in range(1, 9):
+        for nl in list(range(0, 40)) + [1023, 1024, 1025, 65536, 996147]:
+            ista, inum = _fortran_split(nl, size)
+            start, count = active_split(nl, size)
+            assert count == inum
+            assert sum(count) == nl
+            for s, i, c in zip(start, ista, count):
+                if c:
+                    assert s == i - 1
+
+
+def test_one_rank_without_a_process_group_evaluates_everything():
+    import oracle
+    from nb6b200 import ics
+    from nb6b200.rank_split import RegularRankSplit
+    cl = ics.plummer(128, seed=5, nnbopt=20)
+    h2 = cl.h2(0)
+    split = RegularRankSplit(_OracleForceLib(oracle), chunk=50)
+    assert (split.rank, split.size) == (0, 1)
+    split.send(cl.mass, cl.pos, cl.vel)
+    got = split.regf(h2, cl.dtr, cl.pos, cl.vel, 64, 40, 0)
+    want = oracle.regf(cl.mass, cl.pos, cl.vel, h2, cl.dtr, cl.pos, cl.vel, 64, 40, 0)
+    for g, w in zip(got, want):
+        assert np.array_equal(g, w)
+
+
+def test_chunk_outside_the_call_limit_is_rejected():
+    from nb6b200.rank_split import RegularRankSplit
+    with pytest.raises(ValueError):
+        RegularRankSplit(None, chunk=0)
+    with pytest.raises(ValueError):
+        RegularRankSplit(None, chunk=1025)
