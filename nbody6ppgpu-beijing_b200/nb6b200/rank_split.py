@@ -1,4 +1,4 @@
-"""Regular force of one cluster split over ranks by active particle.
+"""Regular force and potential of one cluster split over ranks.
 
 This is the multi-rank form of the regular block in the reference's parallel
 build (``intgrt.F:942-1100``).  Every rank holds the whole predicted state and
@@ -23,6 +23,13 @@ of ``libnb6b200.so``) in calls of at most 1024 particles, the reference's
 per-call limit (``util_gpu.F:7``).  Results are those of a single-rank call
 over the whole list, row for row: each particle's force is computed
 independently of how the list is cut.
+
+The potential follows the reference's parallel ENERGY (``energy_mpi.F``):
+a set of more than 5e4 bodies is cut the same way (``energy_mpi.F:59-77``),
+each rank evaluates the potential of its own range against all bodies
+(``GPUPOT(rank,istart,NN,...)``, ``energy_mpi.F:101``), and the potentials
+travel to every rank (``energy_mpi.F:179-181``); a smaller set is evaluated
+whole on every rank (``energy_mpi.F:216``).
 """
 from __future__ import annotations
 
@@ -30,6 +37,7 @@ import numpy as np
 
 NIMAX = 1024  # particles per gpunb_regf_ call (util_gpu.F:7)
 NREC = 7      # FP64 values per result row: acc[3], jrk[3], pot
+POT_SPLIT_MIN = 50000  # bodies above which the potential is split (energy_mpi.F:60)
 
 
 def active_split(nl: int, size: int) -> tuple[list[int], list[int]]:
@@ -49,7 +57,7 @@ def active_split(nl: int, size: int) -> tuple[list[int], list[int]]:
     return start, count
 
 
-class RegularRankSplit:
+class RankSplit:
     """``gpunb_send_`` / ``gpunb_regf_`` for one cluster over the ranks of a
     process group, split by active particle.
 
@@ -145,3 +153,18 @@ class RegularRankSplit:
             rec = self._gather(rec, NREC, count)
             lst = self._gather(lst, lmax, count)
         return rec[:, 0:3].copy(), rec[:, 3:6].copy(), rec[:, 6].copy(), lst
+
+    def gpupot(self, m, x, split_min: int = POT_SPLIT_MIN) -> np.ndarray:
+        """Potential of every body against all bodies (``gpupot_``
+        semantics: positive, self excluded).  Every rank passes the whole set
+        and gets every body's potential back; above ``split_min`` bodies each
+        rank evaluates only its own range."""
+        m = np.ascontiguousarray(m, dtype=np.float64)
+        n = m.shape[0]
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(n, 3)
+        if self.dist is None or self.size == 1 or n <= split_min:
+            return self.lib.gpupot(m, x, 1, n, self.rank) if n else np.zeros(0)
+        start, count = active_split(n, self.size)
+        s, c = start[self.rank], count[self.rank]
+        own = self.lib.gpupot(m, x, s + 1, c, self.rank) if c else np.zeros(0)
+        return self._gather(own.reshape(c, 1), 1, count).reshape(n)

@@ -1,9 +1,10 @@
-"""The regular force split over ranks by active particle (nb6b200.rank_split)
+"""The regular force and the potential split over ranks (nb6b200.rank_split)
 on CPU: gloo ranks, one process each as torchrun launches them, with the FP64
 oracle standing in for each rank's GPU library.  Every rank must end with the
 results of a single-rank call over the whole active list, bit for bit:
 ragged pieces, pieces that are empty, pieces that cross the per-call limit,
-and overflowing neighbour lists (-nnb rows) included."""
+and overflowing neighbour lists (-nnb rows) included; and likewise for the
+potential of every body, split above a size threshold."""
 import os
 import socket
 
@@ -35,10 +36,16 @@ class _OracleForceLib:
     def gpunb_regf(self, h2, dtr, xi, vi, lmax, nnbmax, m_flag=0):
         return self.orc.regf(*self.j, h2, dtr, xi, vi, lmax, nnbmax, m_flag)
 
+    def gpupot(self, m, x, istart=1, ni=None, irank=0):
+        return self.orc.pot(m, x, istart, ni)
+
 
 # (active count, chunk, nnbmax): ragged pieces, an empty list, fewer active
 # particles than ranks, pieces crossing the call limit, overflowing lists.
 CASES = [(256, 1024, 40), (5, 1024, 40), (1, 1024, 40), (0, 1024, 40), (200, 7, 40), (97, 16, 3)]
+# (bodies, split threshold): split with ragged pieces, a piece that is empty,
+# and a set small enough to be evaluated whole on every rank.
+POT_CASES = [(256, 100), (5, 0), (2, 0), (256, 50000)]
 
 
 def _cases():
@@ -60,7 +67,7 @@ def _rank(rank, world, port, out):
     for p in (os.path.join(ROOT, "nbody6ppgpu-beijing_b200"), os.path.join(ROOT, "oracle")):
         sys.path.insert(0, p)
     import torch.distributed as dist
-    from nb6b200.rank_split import RegularRankSplit
+    from nb6b200.rank_split import RankSplit
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     try:
@@ -68,7 +75,7 @@ def _rank(rank, world, port, out):
         res = []
         for cl, h2, dtr, xi, vi, chunk, nnbmax in cases:
             lmax = 64
-            split = RegularRankSplit(_OracleForceLib(orc), chunk=chunk)
+            split = RankSplit(_OracleForceLib(orc), chunk=chunk)
             split.send(cl.mass, cl.pos, cl.vel)
             got = split.regf(h2, dtr, xi, vi, lmax, nnbmax, 0)
             want = orc.regf(cl.mass, cl.pos, cl.vel, h2, dtr, xi, vi, lmax, nnbmax, 0)
@@ -76,7 +83,13 @@ def _rank(rank, world, port, out):
             shapes = tuple(g.shape for g in got)
             nover = int((got[3][:, 0] < 0).sum()) if len(got[3]) else 0
             res.append((same, shapes, split.piece(len(h2)), nover))
-        out[rank] = res
+        pots = []
+        for n, split_min in POT_CASES:
+            cl = cases[0][0]
+            m, x = cl.mass[:n], cl.pos[:n]
+            got = split.gpupot(m, x, split_min)
+            pots.append((got.shape, bool(np.array_equal(got, orc.pot(m, x)))))
+        out[rank] = (res, pots)
     finally:
         dist.destroy_process_group()
 
@@ -91,8 +104,11 @@ def test_ranks_end_with_the_single_rank_results(world):
         res = dict(out)
     from nb6b200.rank_split import active_split
     for rank in range(world):
-        assert len(res[rank]) == len(CASES)
-        for (nl, chunk, nnbmax), (same, shapes, piece, nover) in zip(CASES, res[rank]):
+        regs, pots = res[rank]
+        assert len(regs) == len(CASES)
+        for (n, _), (shape, same) in zip(POT_CASES, pots):
+            assert shape == (n,) and same, (rank, n)
+        for (nl, chunk, nnbmax), (same, shapes, piece, nover) in zip(CASES, regs):
             assert same, (rank, nl, chunk, nnbmax)
             assert shapes == ((nl, 3), (nl, 3), (nl,), (nl, 64))
             start, count = active_split(nl, world)
@@ -133,21 +149,22 @@ def test_active_split_matches_the_reference_cut():
 def test_one_rank_without_a_process_group_evaluates_everything():
     import oracle
     from nb6b200 import ics
-    from nb6b200.rank_split import RegularRankSplit
+    from nb6b200.rank_split import RankSplit
     cl = ics.plummer(128, seed=5, nnbopt=20)
     h2 = cl.h2(0)
-    split = RegularRankSplit(_OracleForceLib(oracle), chunk=50)
+    split = RankSplit(_OracleForceLib(oracle), chunk=50)
     assert (split.rank, split.size) == (0, 1)
     split.send(cl.mass, cl.pos, cl.vel)
     got = split.regf(h2, cl.dtr, cl.pos, cl.vel, 64, 40, 0)
     want = oracle.regf(cl.mass, cl.pos, cl.vel, h2, cl.dtr, cl.pos, cl.vel, 64, 40, 0)
     for g, w in zip(got, want):
         assert np.array_equal(g, w)
+    assert np.array_equal(split.gpupot(cl.mass, cl.pos, 0), oracle.pot(cl.mass, cl.pos))
 
 
 def test_chunk_outside_the_call_limit_is_rejected():
-    from nb6b200.rank_split import RegularRankSplit
+    from nb6b200.rank_split import RankSplit
     with pytest.raises(ValueError):
-        RegularRankSplit(None, chunk=0)
+        RankSplit(None, chunk=0)
     with pytest.raises(ValueError):
-        RegularRankSplit(None, chunk=1025)
+        RankSplit(None, chunk=1025)
