@@ -30,6 +30,13 @@ each rank evaluates the potential of its own range against all bodies
 (``GPUPOT(rank,istart,NN,...)``, ``energy_mpi.F:101``), and the potentials
 travel to every rank (``energy_mpi.F:179-181``); a smaller set is evaluated
 whole on every rank (``energy_mpi.F:216``).
+
+The irregular force follows the parallel irregular step
+(``intgrt.F:600-720``): every rank keeps the whole irregular state
+(``IRR_SIMD_SET_JP`` / ``SET_LIST`` for all bodies), the block's active list
+is cut the same way, each rank evaluates its piece
+(``IRR_SIMD_FIRR_VEC(TIME,NPART_LEN,NXTLST_MPI(istart_lst),...)``,
+``intgrt.F:648``), and the rows travel to every rank (``intgrt.F:690-720``).
 """
 from __future__ import annotations
 
@@ -168,3 +175,23 @@ class RankSplit:
         s, c = start[self.rank], count[self.rank]
         own = self.lib.gpupot(m, x, s + 1, c, self.rank) if c else np.zeros(0)
         return self._gather(own.reshape(c, 1), 1, count).reshape(n)
+
+    def firr(self, ti: float, addr):
+        """Irregular force of the whole active list ``addr`` (1-based
+        addresses, ``irr_simd_firr_vec_`` semantics): acc, jrk over each
+        body's neighbour list and ``nnbid``, the 1-based nearest neighbour.
+        Every rank passes the same list and gets every body's results back;
+        it evaluates only its own piece."""
+        addr = np.ascontiguousarray(addr, dtype=np.int32)
+        nl = addr.shape[0]
+        start, count = active_split(nl, self.size)
+        s, c = start[self.rank], count[self.rank]
+        rec = np.zeros((c, NREC))
+        if c:
+            acc, jrk, nnbid = self.lib.irr_firr_vec(ti, addr[s:s + c])
+            rec[:, 0:3] = acc
+            rec[:, 3:6] = jrk
+            rec[:, 6] = nnbid  # int32 ids are exact in FP64
+        if self.dist is not None and self.size > 1 and nl > 0:
+            rec = self._gather(rec, NREC, count)
+        return rec[:, 0:3].copy(), rec[:, 3:6].copy(), rec[:, 6].astype(np.int32)

@@ -4,7 +4,8 @@ oracle standing in for each rank's GPU library.  Every rank must end with the
 results of a single-rank call over the whole active list, bit for bit:
 ragged pieces, pieces that are empty, pieces that cross the per-call limit,
 and overflowing neighbour lists (-nnb rows) included; and likewise for the
-potential of every body, split above a size threshold."""
+potential of every body, split above a size threshold, and for the
+irregular force of an active list."""
 import os
 import socket
 
@@ -39,6 +40,12 @@ class _OracleForceLib:
     def gpupot(self, m, x, istart=1, ni=None, irank=0):
         return self.orc.pot(m, x, istart, ni)
 
+    def irr_state(self, *state):
+        self.irr = state
+
+    def irr_firr_vec(self, ti, addr):
+        return self.orc.firr(ti, addr, *self.irr)
+
 
 # (active count, chunk, nnbmax): ragged pieces, an empty list, fewer active
 # particles than ranks, pieces crossing the call limit, overflowing lists.
@@ -46,6 +53,24 @@ CASES = [(256, 1024, 40), (5, 1024, 40), (1, 1024, 40), (0, 1024, 40), (200, 7, 
 # (bodies, split threshold): split with ragged pieces, a piece that is empty,
 # and a set small enough to be evaluated whole on every rank.
 POT_CASES = [(256, 100), (5, 0), (2, 0), (256, 50000)]
+# active counts of an irregular block: ragged, fewer than ranks, empty.
+IRR_CASES = [256, 77, 2, 0]
+
+
+def _irr_state(cl, k=12):
+    """Irregular state of the cluster: records at t0 = 0 and lists of the k
+    nearest bodies (rows [nnb, 1-based ids])."""
+    rng = np.random.default_rng(3)
+    n = cl.n
+    d2 = ((cl.pos[:, None, :] - cl.pos[None, :, :]) ** 2).sum(-1)
+    np.fill_diagonal(d2, np.inf)
+    near = np.argsort(d2, axis=1)[:, :k]
+    lists = np.zeros((n, k + 4), dtype=np.int32)
+    lists[:, 0] = k
+    lists[:, 1:k + 1] = np.sort(near, axis=1) + 1
+    acc2 = rng.normal(scale=0.5, size=(n, 3))
+    jrk6 = rng.normal(scale=0.1, size=(n, 3))
+    return (cl.pos, cl.vel, acc2, jrk6, cl.mass, np.zeros(n), lists)
 
 
 def _cases():
@@ -89,7 +114,18 @@ def _rank(rank, world, port, out):
             m, x = cl.mass[:n], cl.pos[:n]
             got = split.gpupot(m, x, split_min)
             pots.append((got.shape, bool(np.array_equal(got, orc.pot(m, x)))))
-        out[rank] = (res, pots)
+        irrs = []
+        cl = cases[0][0]
+        lib = _OracleForceLib(orc)
+        lib.irr_state(*_irr_state(cl))
+        split = RankSplit(lib)
+        rng = np.random.default_rng(11)
+        for nl in IRR_CASES:
+            addr = (np.sort(rng.choice(cl.n, size=nl, replace=False)) + 1).astype(np.int32)
+            got = split.firr(0.01, addr)
+            want = orc.firr(0.01, addr, *lib.irr)
+            irrs.append((tuple(g.shape for g in got), all(np.array_equal(g, w) for g, w in zip(got, want))))
+        out[rank] = (res, pots, irrs)
     finally:
         dist.destroy_process_group()
 
@@ -104,8 +140,10 @@ def test_ranks_end_with_the_single_rank_results(world):
         res = dict(out)
     from nb6b200.rank_split import active_split
     for rank in range(world):
-        regs, pots = res[rank]
+        regs, pots, irrs = res[rank]
         assert len(regs) == len(CASES)
+        for nl, (shapes, same) in zip(IRR_CASES, irrs):
+            assert shapes == ((nl, 3), (nl, 3), (nl,)) and same, (rank, nl)
         for (n, _), (shape, same) in zip(POT_CASES, pots):
             assert shape == (n,) and same, (rank, n)
         for (nl, chunk, nnbmax), (same, shapes, piece, nover) in zip(CASES, regs):
