@@ -65,13 +65,15 @@ def active_split(nl: int, size: int) -> tuple[list[int], list[int]]:
 
 
 class RankSplit:
-    """``gpunb_send_`` / ``gpunb_regf_`` for one cluster over the ranks of a
-    process group, split by active particle.
+    """Regular force (``regf``), potential (``gpupot``) and irregular force
+    (``firr``) of one cluster over the ranks of a process group, each split
+    into one piece of its particle list per rank.
 
-    ``lib`` is this rank's :class:`ForceLib`, already opened
-    (``gpunb_open``) on this rank's GPU.  ``group`` is a ``torch.distributed``
-    process group (None: the default group; no initialised group: one rank,
-    no exchange).  ``chunk`` is the largest ``gpunb_regf_`` call.
+    ``lib`` is this rank's :class:`ForceLib`, already opened on this rank's
+    GPU (``gpunb_open``; ``irr_open`` with every body's state set, for
+    ``firr``).  ``group`` is a ``torch.distributed`` process group (None: the
+    default group; no initialised group: one rank, no exchange).  ``chunk``
+    is the largest ``gpunb_regf_`` call.
     """
 
     def __init__(self, lib, group=None, chunk: int = NIMAX):
