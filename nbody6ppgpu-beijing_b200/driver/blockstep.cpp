@@ -14,6 +14,8 @@
 //   regular step                 regcor_gpu.F:593-737
 //   F, FDOT bookkeeping          intgrt.F:558-581,911-935
 //   energy                       energy.F:28-62 (GPUPOT), ZKIN
+//   radius-rule quantities       adjust.F:104-199, core.f, output.F:61,271
+//                                at every output time
 // The per-body steps live in hermite.h (shared with the ensemble driver).
 // Left out: KS/chain regularisation, stellar evolution, external fields,
 // the checkl/fpcorr options (KZ(37), KZ(38)) and the SMIN neighbour retention.
@@ -51,7 +53,7 @@ struct Sim : Bodies {
     // Regular force for the bodies in idx (chunks of P.chunk) against all
     // bodies predicted to `time`; returns the new lists through nlist
     // (rows of LS, 1-based, self removed).  Overflow shrinks RS and re-runs the
-    // chunk (util_gpu.F:69-100, NB_FLAG branch).
+    // row (util_gpu.F:69-100).
     void regular_forces(const std::vector<int> &idx, std::vector<double> &freg,
                         std::vector<double> &fdr, std::vector<int> &nlist) {
         const double t_0 = wtime();
@@ -92,6 +94,7 @@ struct Sim : Bodies {
 
 bool Sim::init() {
     alloc();
+    adjust_init(1);
     xp.assign(3 * (size_t)n, 0);
     vp.assign(3 * (size_t)n, 0);
     for (int i = 0; i < n; ++i) init_radius(i, &x0[3 * (size_t)i]);
@@ -105,7 +108,9 @@ bool Sim::init() {
     for (int i = 0; i < n; ++i) all[i] = i;
     std::vector<double> freg, fdr;
     std::vector<int> nl;
+    fpoly0 = true;
     regular_forces(all, freg, fdr, nl);
+    fpoly0 = false;
     for (int i = 0; i < n; ++i) memcpy(row(i), &nl[(size_t)i * LS], sizeof(int) * LS);
     // irregular force from the lists: state at t = 0 with F = FDOT = 0 so the
     // libraries' prediction is the identity
@@ -164,6 +169,7 @@ bool Sim::run(double *eout, int nout_max) {
     int nout = 0;
     double ek, ep;
     energy(ek, ep);
+    adjust(0, 0, n, xp.data(), vp.data(), ek, -ep, list.data(), (size_t)LS, time);
     if (nout < nout_max) {
         eout[4 * nout] = 0.0;
         eout[4 * nout + 1] = ek;
@@ -201,6 +207,7 @@ bool Sim::run(double *eout, int nout_max) {
         clock_push(active);
         if (time >= tnext_out - 1e-15) {
             energy(ek, ep);
+            adjust(0, 0, n, xp.data(), vp.data(), ek, -ep, list.data(), (size_t)LS, time);
             if (nout < nout_max) {
                 eout[4 * nout] = time;
                 eout[4 * nout + 1] = ek;
@@ -250,6 +257,48 @@ int nb6drive_run(const char *reg_lib, const char *irr_lib, const char *pot_lib, 
     s.B.gpunb_close();
     if (stats) *stats = s.st;
     return 0;
+}
+
+// The driver's Ahmad-Cohen radius rule (ac_radius) for n bodies of one
+// cluster, with the argument layout of the oracle's restatement:
+// kz39 selects NB_FLAG and M_FLAG as regcor_gpu.F:21-22 does; adj =
+// RDENS[3], RSCALE, RC2, RSFAC, BODYM; xnb/vnb[n][3][3] the first
+// min(nnb, 3) new neighbours.  rs in/out; dfirr/dfd[n][3] out.  For tests.
+void nb6drive_ac_radius(int n, int kz39, int nnbopt, int nnbmax, const double *adj, const int *nnb,
+                        const int *nnb0, const double *dtr, const double *xi, const double *vi,
+                        const double *xnb, const double *vnb, double *rs, double *dfirr, double *dfd) {
+    ACPar a;
+    for (int k = 0; k < 3; ++k) a.rdens[k] = adj[k];
+    a.rscale = adj[3];
+    a.rc2 = adj[4];
+    a.rsfac = adj[5];
+    a.bodym = adj[6];
+    const int nb_flag = (kz39 == 0 || kz39 == 2), m_flag = (kz39 == 2 || kz39 == 3);
+    for (int i = 0; i < n; ++i)
+        rs[i] = ac_radius(nb_flag, m_flag, nnbopt, nnbmax, a, nnb[i], nnb0[i], dtr[i], xi + 3 * i, vi + 3 * i,
+                          xnb + 9 * i, vnb + 9 * i, rs[i], dfirr + 3 * i, dfd + 3 * i);
+}
+
+// The driver's overflow shrink (ac_shrink) of n radii; nnb_neg[i] = -NNB.
+void nb6drive_ac_shrink(int n, int kz39, int nnbopt, int nnbmax, const int *nnb_neg, double *rs) {
+    const int nb_flag = (kz39 == 0 || kz39 == 2);
+    for (int i = 0; i < n; ++i) rs[i] = ac_shrink(nb_flag, nnbopt, nnbmax, nnb_neg[i], rs[i]);
+}
+
+// The driver's core.f restatement (ac_core) on one cluster of n bodies:
+// rows[n][ls] = [nnb, 1-based neighbour ids]; io = {RDENS[3], RSCALE, RC
+// of the last call} in, {RDENS[3], RSCALE, RC, RC2, VC} out.  For tests.
+void nb6drive_core(int n, const double *m, const double *x, const double *v, const double *rs, const int *rows,
+                   int ls, double time, double *io) {
+    ACPar a;
+    for (int k = 0; k < 3; ++k) a.rdens[k] = io[k];
+    a.rscale = io[3];
+    double rc = io[4];
+    const double vc = ac_core(n, m, x, v, rs, rows, (size_t)ls, 0, time, a, rc);
+    for (int k = 0; k < 3; ++k) io[k] = a.rdens[k];
+    io[4] = rc;
+    io[5] = a.rc2;
+    io[6] = vc;
 }
 
 }  // extern "C"

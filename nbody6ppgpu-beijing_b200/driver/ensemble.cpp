@@ -199,6 +199,7 @@ struct Ensemble : Bodies {
                 rs[i] = o[26];
                 t0r[i] = time;
                 const int nnb = (int)o[27];
+                if (nnb > 0) rsmin_seen(i);
                 st.nb_sum += nnb;
                 st.nb_absdev += fabs((double)(nnb - P.nnbopt));
                 st.reg_steps++;
@@ -371,6 +372,8 @@ struct Ensemble : Bodies {
         cl_of.assign(n, 0);
         for (int c = 0; c < ncl; ++c)
             for (int k = 0; k < cnt[c]; ++k) cl_of[base[c] + k] = c;
+        adjust_init(ncl);
+        acl = cl_of;
         for (int i = 0; i < n; ++i) init_radius(i, &x0[3 * (size_t)i]);
         int nb = n + 10, rank = 0;
         B.gpunb_open(&nb, &rank);
@@ -383,7 +386,9 @@ struct Ensemble : Bodies {
         for (int i = 0; i < n; ++i) all[i] = i;
         std::vector<double> freg, fdr;
         std::vector<int> nl;
+        fpoly0 = true;
         regular_forces(all, freg, fdr, nl);
+        fpoly0 = false;
         for (int i = 0; i < n; ++i) {
             const int *src = &nl[(size_t)i * LS];
             memcpy(row(i), src, sizeof(int) * std::min(LS, src[0] + 1));  // rows start zeroed
@@ -408,10 +413,13 @@ struct Ensemble : Bodies {
         return true;
     }
 
-    // Kinetic and potential energy of cluster c at `time`.
-    void energy(int c, double &ekin, double &epot) {
+    // Kinetic and potential energy of cluster c at `time`; xp, vp receive
+    // its bodies at `time`.
+    void energy(int c, double &ekin, double &epot, std::vector<double> &xp, std::vector<double> &vp) {
         const int nc = cnt[c], b = base[c];
-        std::vector<double> xp(3 * (size_t)nc), vp(3 * (size_t)nc), phi(nc + 8);
+        xp.resize(3 * (size_t)nc);
+        vp.resize(3 * (size_t)nc);
+        std::vector<double> phi(nc + 8);
         for (int j = 0; j < nc; ++j) pred(b + j, time, &xp[3 * (size_t)j], &vp[3 * (size_t)j]);
         int rank = 0, istart = 1, ni = nc, nn = nc;
         B.gpupot(&rank, &istart, &ni, &nn, &m[b], (double(*)[3])xp.data(), phi.data());
@@ -424,18 +432,50 @@ struct Ensemble : Bodies {
         }
     }
 
+    // Energy output of every cluster, and the radius rule's quantities of
+    // each (Bodies::adjust) from the same bodies at `time`; with the
+    // regular corrector on the device the neighbour rows are read back for
+    // it first, and the new quantities go to the device.
     void record(double *tout, double *eout, int &nout, int nout_max) {
-        if (nout >= nout_max) return;
-        tout[nout] = time;
+        if (dev_reg() && B.lists_get) {
+            int a0 = 1, nn = n, ls = LS;
+            B.lists_get(&a0, &nn, &ls, list.data());
+        }
+        std::vector<double> xp, vp;
         for (int c = 0; c < ncl; ++c) {
             double ek, ep;
-            energy(c, ek, ep);
-            double *e = eout + ((size_t)nout * ncl + c) * 3;
-            e[0] = ek;
-            e[1] = ep;
-            e[2] = ek + ep;
+            energy(c, ek, ep, xp, vp);
+            adjust(c, base[c], cnt[c], xp.data(), vp.data(), ek, -ep, list.data(), (size_t)LS, time);
+            if (nout < nout_max) {
+                double *e = eout + ((size_t)nout * ncl + c) * 3;
+                e[0] = ek;
+                e[1] = ep;
+                e[2] = ek + ep;
+            }
         }
-        nout++;
+        if (dev_reg() && B.hermite_adjust) push_adjust();
+        if (nout < nout_max) tout[nout++] = time;
+    }
+
+    // The radius rule's quantities of every cluster to the device corrector.
+    void push_adjust() {
+        std::vector<int> a0(ncl + 1);
+        std::vector<double> par(8 * (size_t)ncl, 0.0);
+        for (int c = 0; c < ncl; ++c) {
+            a0[c] = base[c] + 1;
+            const ACPar &a = acp[c];
+            double *q = &par[8 * (size_t)c];
+            q[0] = a.rdens[0];
+            q[1] = a.rdens[1];
+            q[2] = a.rdens[2];
+            q[3] = a.rscale;
+            q[4] = a.rc2;
+            q[5] = a.rsfac;
+            q[6] = a.bodym;
+        }
+        a0[ncl] = n + 1;
+        int nbf = P.nb_flag, nc = ncl;
+        B.hermite_adjust(&nbf, &nc, a0.data(), par.data());
     }
 
     // block clock on the device too

@@ -59,6 +59,13 @@ struct nb6drive_params {
     // belong to one cluster also takes the segmented call (nb6_regf_seg_,
     // as the device regular corrector does); 0 = gpunb_regf_ for it
     int seg_single;
+    // form of the Ahmad-Cohen radius rule, NB_FLAG of regcor_gpu.F:22 /
+    // util_gpu.F:29 (KZ(39) = 0 or 2 give 1, the reference's default):
+    // 1 = distances from the density centre, membership reduced outside
+    // the half-mass radius, radial-velocity volume factor, overflow shrink
+    // by (NNBOPT/NNB)^0.333; 0 = distances from the origin, overflow shrink
+    // by 0.9
+    int nb_flag;
 };
 
 // Counters returned by the drivers.
@@ -106,6 +113,8 @@ typedef void (*fn_hermite_get)(int *, int *, double *);
 typedef void (*fn_blocks_run)(double *, int *, int *, long long *, long long *, double *, int *);
 typedef void (*fn_blocks_active)(int *, int *, double *);
 typedef void (*fn_blocks_regular)(int *, int *, double *);
+typedef void (*fn_hermite_adjust)(int *, int *, int *, double *);
+typedef void (*fn_lists_get)(int *, int *, int *, int *);
 
 struct Backend {
     void *hreg = nullptr, *hirr = nullptr, *hpot = nullptr;
@@ -132,6 +141,8 @@ struct Backend {
     fn_blocks_run blocks_run = nullptr;                        // device block clock
     fn_blocks_active blocks_active = nullptr;
     fn_blocks_regular blocks_regular = nullptr;
+    fn_hermite_adjust hermite_adjust = nullptr;                // radius-rule quantities per cluster
+    fn_lists_get lists_get = nullptr;                          // resident neighbour rows
 };
 
 inline void *must_sym(void *h, const char *name) {
@@ -175,6 +186,8 @@ inline bool load_backend(Backend &b, const char *reg, const char *irr, const cha
     b.blocks_run = (fn_blocks_run)dlsym(b.hirr, "nb6_blocks_run_");
     b.blocks_active = (fn_blocks_active)dlsym(b.hirr, "nb6_blocks_active_");
     b.blocks_regular = (fn_blocks_regular)dlsym(b.hirr, "nb6_blocks_regular_");
+    b.hermite_adjust = (fn_hermite_adjust)dlsym(b.hirr, "nb6_hermite_adjust_");
+    b.lists_get = (fn_lists_get)dlsym(b.hirr, "nb6_irr_lists_get_");
     return b.gpunb_open && b.gpunb_close && b.gpunb_send && b.gpunb_regf && b.gpupot &&
            b.irr_open && b.irr_close && b.irr_set_jp && b.irr_set_list && b.irr_firr_vec;
 }
@@ -183,6 +196,210 @@ inline double wtime() {
     struct timespec ts;
     clock_gettime(CLOCK_MONOTONIC, &ts);
     return ts.tv_sec + 1e-9 * ts.tv_nsec;
+}
+
+// Constants of the reference's integrator (zero.f:113-116), multiplied as
+// the Fortran multiplies them.
+constexpr double ONE3 = 1.0 / 3.0, ONE6 = 1.0 / 6.0, ONE12 = 1.0 / 12.0;
+// The reference is compiled without -fdefault-real-8: a real literal such
+// as 0.6 is REAL*4 and enters a REAL*8 expression as its single-precision
+// value; R4(0.6) writes that value.
+#define R4(c) ((double)(c##f))
+
+// Per-cluster quantities of the radius rule, refreshed at each adjust time
+// (adjust.F:104-199, core.f): density centre RDENS, half-mass radius
+// RSCALE, core radius squared RC2, RSFAC = MAX(25/TCR, 1.5 VC/RSMIN) and
+// the mean mass BODYM.
+struct ACPar {
+    double rdens[3] = {0.0, 0.0, 0.0};
+    double rscale = 1.0, rc2 = 1.0, rsfac = 0.0, bodym = 1.0;
+};
+
+// Ahmad-Cohen radius update of a single body at its regular step,
+// regcor_gpu.F:19-238.  nnb: new membership (self removed), nnb0: old;
+// xi, vi: the body at TIME; xnb, vnb: its first min(nnb, 3) new neighbours
+// at TIME.  Returns the new RS; dfirr, dfd receive the irregular force
+// change the neighbour moves start from (non-zero only for nnb = 0, the
+// small central mass of :108-121).  Single-precision terms as the
+// reference computes them (FLOAT() and literals are REAL*4).
+inline double ac_radius(int nb_flag, int m_flag, int nnbopt, int nnbmax, const ACPar &a, int nnb,
+                        int nnb0, double dtr, const double *xi, const double *vi, const double *xnb,
+                        const double *vnb, double rs, double *dfirr, double *dfd) {
+    const float zs = 0.01f * (float)nnbmax;                     // input.F:133
+    const double znbmin = (double)(zs > 1.0f ? zs : 1.0f);
+    for (int k = 0; k < 3; ++k) dfirr[k] = dfd[k] = 0.0;
+    double ri2, rh2;
+    if (nb_flag) {                                             // :30-37
+        const double e0 = xi[0] - a.rdens[0], e1 = xi[1] - a.rdens[1], e2 = xi[2] - a.rdens[2];
+        ri2 = e0 * e0 + e1 * e1 + e2 * e2;
+        rh2 = a.rscale * a.rscale;
+    } else {
+        ri2 = xi[0] * xi[0] + xi[1] * xi[1] + xi[2] * xi[2];
+        rh2 = R4(9.0) * (a.rscale * a.rscale);
+    }
+    if (nnb == 0) {                                            // :108-131
+        const double r2 = xi[0] * xi[0] + xi[1] * xi[1] + xi[2] * xi[2];
+        const double fij = R4(0.01) * a.bodym / (r2 * sqrt(r2));
+        const double rdot = 3.0 * (xi[0] * vi[0] + xi[1] * vi[1] + xi[2] * vi[2]) / r2;
+        for (int k = 0; k < 3; ++k) {
+            dfirr[k] = -fij * xi[k];
+            dfd[k] = -(vi[k] - rdot * xi[k]) * fij;
+        }
+        if (rdot > 0.0) return std::max(R4(0.75) * rs, R4(0.1) * a.rscale);
+        return R4(1.1) * rs;
+    }
+    const float fac_s = 1.0f + 0.1f * ((float)nnbopt - (float)nnb) / (float)nnb;   // :139-150
+    double a3 = (double)(float)nnb * (double)fac_s;
+    const int nbave = std::min(nnbopt + 150, std::max(nnbmax - 50, (int)znbmin));
+    const double cap = (double)(0.9f * (float)nbave);
+    a3 = a3 < cap ? a3 : cap;
+    const int nbp = (int)a3;
+    if (ri2 > rh2 && nb_flag) {                                // :152-156
+        const double f = a.rscale / sqrt(ri2);
+        a3 = a3 * (f > R4(0.1) ? f : R4(0.1));
+    } else {
+        a3 = a3 > znbmin ? a3 : znbmin;
+    }
+    double a4 = a3 / (double)(float)nnb;
+    if ((a3 - (double)(float)nnb0) * (a3 - (double)(float)nnb) < 0.0) a4 = sqrt(a4);
+    const double ridot = (xi[0] - a.rdens[0]) * vi[0] + (xi[1] - a.rdens[1]) * vi[1] +
+                         (xi[2] - a.rdens[2]) * vi[2];              // :162-164
+    if (ri2 > a.rc2 && nb_flag && ri2 < R4(100.0) * rh2) a4 = a4 * (1.0 + ridot * dtr / ri2);
+    // (:170-181, the perturber range of a c.m. body, applies to I > N only)
+    double a5 = a.rsfac * dtr;                                 // :184-192
+    a5 = a5 < 0.25 ? a5 : 0.25;
+    a4 = a4 - 1.0;
+    if (a4 > a5) a4 = a5;
+    else a4 = a4 > -a5 ? a4 : -a5;
+    const double a3b = ONE3 * a4;                              // :195-213
+    double a1 = 1.0 + a3b - a3b * a3b;
+    if (nnb < znbmin && nbp > znbmin && a1 < 1.0) a1 = R4(1.05);
+    if (fabs(a1 - 1.0) > R4(0.003)) {
+        if (rs * rs > ri2 && rs * rs < 2.0 * ri2 && nnb > 5) a1 = sqrt(a1);
+        rs = a1 * rs;
+    }
+    if (nnb > nbave && ridot < 0.0) {                          // :215-220
+        const float drs = ((float)nnb - (float)nbave) / (3.0f * (float)nnb);
+        rs = rs * (1.0 - (double)drs);
+    }
+    if (!m_flag && nnb <= 3 && ri2 < R4(100.0) * rh2) {        // :223-238
+        double b1 = 2.0 * rs;
+        for (int l = 0; l < nnb; ++l) {
+            const double *xj = xnb + 3 * l, *vj = vnb + 3 * l;
+            const double e0 = xi[0] - xj[0], e1 = xi[1] - xj[1], e2 = xi[2] - xj[2];
+            const double rij = sqrt(e0 * e0 + e1 * e1 + e2 * e2);
+            const double rsdot = (e0 * (vi[0] - vj[0]) + e1 * (vi[1] - vj[1]) + e2 * (vi[2] - vj[2])) / rij;
+            const double t = rij + rsdot * dtr;
+            b1 = b1 < t ? b1 : t;
+        }
+        const double g = R4(1.1) * rs;
+        rs = b1 > g ? b1 : g;
+    }
+    return rs;
+}
+
+// Radius of a row that overflowed (util_gpu.F:69-100, fpoly0.F:134-160);
+// nb_neg = -NNB.
+inline double ac_shrink(int nb_flag, int nnbopt, int nnbmax, int nb_neg, double rs) {
+    if (!nb_flag) return R4(0.9) * rs;
+    if (-nb_neg > nnbopt) return (double)powf(-(float)nnbopt / (float)nb_neg, 0.333f) * rs;
+    return (double)powf((float)nnbopt / (float)nnbmax, 0.4f) * rs;
+}
+
+// Density centre, core radius and core rms velocity of a cluster (core.f),
+// from the bodies' positions and velocities x, v at TIME, masses m, radii
+// rs and neighbour rows (rows[k*ls] = nnb, then 1-based addresses, address
+// a0 + 1 being body 0 of the cluster).  In: a.rdens and rc_prev from the
+// last call (zero and unused at TIME = 0), a.rscale.  Out: a.rdens, a.rc2,
+// the returned VC, and rc_prev.
+inline double ac_core(int nc, const double *m, const double *x, const double *v, const double *rs,
+                      const int *rows, size_t ls, int a0, double time, ACPar &a, double &rc_prev) {
+    double rcore2 = a.rscale * a.rscale;
+    if (time > 0.0) rcore2 = std::max(9.0 * (rc_prev * rc_prev), rcore2);
+    std::vector<int> jl;
+    for (;;) {
+        jl.clear();
+        for (int i = 0; i < nc; ++i) {
+            const double *p = x + 3 * (size_t)i;
+            const double e0 = p[0] - a.rdens[0], e1 = p[1] - a.rdens[1], e2 = p[2] - a.rdens[2];
+            if (e0 * e0 + e1 * e1 + e2 * e2 < rcore2) jl.push_back(i);
+        }
+        if ((int)jl.size() >= nc / 5) break;
+        rcore2 = R4(1.5) * rcore2;
+    }
+    std::vector<double> rho(jl.size(), 0.0), rl;
+    std::vector<int> il;
+    for (size_t l = 0; l < jl.size(); ++l) {
+        const int i = jl[l];
+        const int *row = rows + (size_t)i * ls;
+        const int nnb = row[0];
+        if (nnb <= 0) continue;
+        const double *xi = x + 3 * (size_t)i;
+        double d6 = (double)(2.0f * powf(6.0f / (float)nnb, 0.66f)) * (rs[i] * rs[i]);
+        int n6;
+        for (;;) {
+            il.clear();
+            rl.clear();
+            for (int lj = 1; lj <= nnb; ++lj) {
+                const int j = row[lj] - 1 - a0;
+                const double *xj = x + 3 * (size_t)j;
+                const double e0 = xi[0] - xj[0], e1 = xi[1] - xj[1], e2 = xi[2] - xj[2];
+                const double rij2 = e0 * e0 + e1 * e1 + e2 * e2;
+                if (rij2 < d6) {
+                    il.push_back(j);
+                    rl.push_back(rij2);
+                }
+            }
+            n6 = (int)il.size();
+            if (n6 >= 6) break;
+            d6 = R4(1.5) * d6;
+            if (n6 >= nnb) break;
+        }
+        for (int ii = 0; ii < n6; ++ii)                        // the exchange sort of :73-84
+            for (int jj = ii + 1; jj < n6; ++jj)
+                if (rl[jj] < rl[ii]) {
+                    std::swap(rl[ii], rl[jj]);
+                    std::swap(il[ii], il[jj]);
+                }
+        const int i6 = std::min(n6, 6);
+        double xmass = 0.0;
+        for (int lj = 0; lj < i6 - 1; ++lj) xmass += m[il[lj]];
+        const double r6 = rl[i6 - 1];
+        const double rinv32 = r6 > 0.0 ? 1.0 / (r6 * sqrt(r6)) : 0.0;
+        rho[l] = n6 < 6 ? 0.0 : xmass * rinv32;
+    }
+    double zmass = 0.0;
+    for (int i = 0; i < nc; ++i) zmass += m[i];
+    double rd[3] = {0.0, 0.0, 0.0}, rho1 = 0.0;
+    for (size_t l = 0; l < jl.size(); ++l) {
+        for (int k = 0; k < 3; ++k) rd[k] += rho[l] * x[3 * (size_t)jl[l] + k];
+        rho1 += rho[l];
+    }
+    rho1 = std::max(rho1, zmass / (a.rscale * a.rscale * a.rscale));
+    for (int k = 0; k < 3; ++k) a.rdens[k] = rd[k] / rho1;
+    double rc = 0.0, rho2 = 0.0;
+    for (size_t l = 0; l < jl.size(); ++l) {
+        const double *p = x + 3 * (size_t)jl[l];
+        const double e0 = p[0] - a.rdens[0], e1 = p[1] - a.rdens[1], e2 = p[2] - a.rdens[2];
+        rc += rho[l] * rho[l] * (e0 * e0 + e1 * e1 + e2 * e2);
+        rho2 += rho[l] * rho[l];
+    }
+    if (rho2 > 0.0) rc = sqrt(rc / rho2);
+    if (rc == 0.0) rc = a.rscale;
+    a.rc2 = rc * rc;
+    rc_prev = rc;
+    int nc1 = 0;
+    double vc = 0.0;
+    for (size_t l = 0; l < jl.size(); ++l) {
+        const double *p = x + 3 * (size_t)jl[l];
+        const double e0 = p[0] - a.rdens[0], e1 = p[1] - a.rdens[1], e2 = p[2] - a.rdens[2];
+        if (e0 * e0 + e1 * e1 + e2 * e2 < a.rc2) {
+            const double *u = v + 3 * (size_t)jl[l];
+            nc1++;
+            vc += u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+        }
+    }
+    return sqrt(vc / (double)(float)std::max(nc1, 2));
 }
 
 // STEP = sqrt(ETA (|F||F2| + |F1|^2) / (|F1||F3| + |F2|^2))   (tstep.f)
@@ -217,6 +434,52 @@ struct Bodies {
     std::vector<int> list;  // n x LS: [nnb, 1-based addresses ascending] (self excluded)
     int LS = 0;             // row stride (lmax + 8 so the AVX library can over-read)
     double tcr = 2.0 * sqrt(2.0);  // crossing time in Henon units
+    // initial evaluation (fpoly0.F:100-206): a row holding only the body
+    // itself is evaluated again with a larger radius
+    bool fpoly0 = false;
+    // radius-rule quantities per cluster (one cluster unless set by the
+    // ensemble driver): acl[i] = cluster of body i; RSMIN since the last
+    // adjust (intgrt.F:927, reset at output, output.F:271); core radius of
+    // the last core() call
+    std::vector<ACPar> acp{ACPar()};
+    std::vector<int> acl;
+    std::vector<double> rsmin{0.0}, rc_last{0.0};
+    const ACPar &acpar(int i) const { return acp[acl.empty() ? 0 : acl[i]]; }
+    void rsmin_seen(int i) {
+        double &r = rsmin[acl.empty() ? 0 : acl[i]];
+        r = std::min(r, rs[i]);
+    }
+    void adjust_init(int ncl) {
+        acp.assign(ncl, ACPar());
+        rsmin.assign(ncl, P.rs0);   // RSMIN = RS0 from the input (input.F:137)
+        rc_last.assign(ncl, 0.0);
+    }
+
+    // Adjust-time quantities of cluster c, whose nc bodies start at body b:
+    // what ADJUST computes for the radius rule (adjust.F:104 TCR, :136
+    // RSCALE, :150 RSMIN, :154 CORE, :199 RSFAC) followed by OUTPUT's own
+    // CORE call and RSMIN reset (output.F:61,271).  x, v: the bodies at
+    // `time`; ekin, pot (> 0): the cluster's kinetic and potential energy;
+    // rows: neighbour rows of every body (stride ls, 1-based addresses).
+    void adjust(int c, int b, int nc, const double *x, const double *v, double ekin, double pot,
+                const int *rows, size_t ls, double time) {
+        ACPar &a = acp[c];
+        double zmass = 0.0;
+        for (int k = 0; k < nc; ++k) zmass += m[b + k];
+        const double tcr_c = pow(zmass, 2.5) / pow(2.0 * fabs(ekin - pot), 1.5);
+        a.rscale = 0.5 * (zmass * zmass) / pot;
+        a.bodym = zmass / (double)(float)nc;
+        if (rsmin[c] == 0.0) {                                 // adjust.F:139-150
+            double r0 = a.rscale;
+            for (int k = 0; k < nc; ++k)
+                if (rows[(size_t)(b + k) * ls] > 0) r0 = std::min(r0, rs[b + k]);
+            rsmin[c] = r0;
+        }
+        const double vc = ac_core(nc, &m[b], x, v, &rs[b], rows + (size_t)b * ls, ls, b, time, a, rc_last[c]);
+        a.rsfac = std::max(R4(25.0) / tcr_c, 3.0 * vc / (2.0 * rsmin[c]));
+        ac_core(nc, &m[b], x, v, &rs[b], rows + (size_t)b * ls, ls, b, time, a, rc_last[c]);
+        rsmin[c] = R4(100.0);
+    }
     nb6drive_stats st{};
 
     // State at the block time of the bodies being regular-corrected, taken
@@ -308,7 +571,7 @@ struct Bodies {
             fi[3 * i + k] = a[k];
             fidot[3 * i + k] = jd[k];
             f[3 * i + k] = 0.5 * (fi[3 * i + k] + fr[3 * i + k]);
-            fdot[3 * i + k] = (fidot[3 * i + k] + frdot[3 * i + k]) / 6.0;
+            fdot[3 * i + k] = ONE6 * (fidot[3 * i + k] + frdot[3 * i + k]);
             ft[k] = fi[3 * i + k] + fr[3 * i + k];
             fdt[k] = fidot[3 * i + k] + frdot[3 * i + k];
         }
@@ -337,7 +600,7 @@ struct Bodies {
             vi[k] = (fdot[c] * s1 + f[c]) * s2 + v0[c];
         }
         const double dt = s, dtsq = dt * dt, dt6 = 6.0 / (dt * dtsq), dt2 = 2.0 / dtsq;
-        const double dtsq12 = dtsq / 12.0, dt13 = dt / 3.0;
+        const double dtsq12 = ONE12 * dtsq, dt13 = ONE3 * dt;
         double ftot[3];
         for (int k = 0; k < 3; ++k) {  // nbint_cor.f:130-150
             const size_t c = 3 * (size_t)i + k;
@@ -346,7 +609,7 @@ struct Bodies {
             const double sum = fid + jd[k];
             const double at3 = 2.0 * df + dt * sum;
             const double bt2 = -3.0 * df - dt * (sum + fid);
-            x0[c] = xi[k] + (0.6 * at3 + bt2) * dtsq12;
+            x0[c] = xi[k] + (R4(0.6) * at3 + bt2) * dtsq12;
             v0[c] = vi[k] + (0.75 * at3 + bt2) * dt13;
             fi[c] = a[k];
             fidot[c] = jd[k];
@@ -373,7 +636,7 @@ struct Bodies {
         for (int k = 0; k < 3; ++k) {
             const size_t c = 3 * (size_t)i + k;
             f[c] = 0.5 * (frdot[c] * dtr + fr[c] + fi[c]);
-            fdot[c] = (frdot[c] + fidot[c]) / 6.0;
+            fdot[c] = ONE6 * (frdot[c] + fidot[c]);
         }
         // keep the irregular step inside the regular interval
         while (t0[i] + step[i] > t0r[i] + stepr[i] && step[i] > P.dtmin) step[i] *= 0.5;
@@ -382,10 +645,7 @@ struct Bodies {
 
     // Overflow handling of one regular-force row (util_gpu.F:69-100, NB_FLAG
     // branch): shrink RS; the caller re-runs the force.
-    void shrink_radius(int i, int nb_neg) {
-        if (-nb_neg > P.nnbopt) rs[i] *= pow((double)P.nnbopt / (double)(-nb_neg), 0.333);
-        else rs[i] *= pow((double)P.nnbopt / (double)P.nnbmax, 0.4);
-    }
+    void shrink_radius(int i, int nb_neg) { rs[i] = ac_shrink(P.nb_flag, P.nnbopt, P.nnbmax, nb_neg, rs[i]); }
 
     // Regular corrector of body i at `time`: Ahmad-Cohen radius update, force
     // moves for neighbours gained and lost, Hermite corrector on the regular
@@ -397,37 +657,17 @@ struct Bodies {
         const double dtr = time - t0r[i];
         double xi[3], vi[3];
         pred_at(i, time, xi, vi);
-        const double ri2 = xi[0] * xi[0] + xi[1] * xi[1] + xi[2] * xi[2];
-        const double znbmin = 0.2 * P.nnbopt;
-        const double rsfac = std::max(25.0 / tcr, 0.0);
-        // Ahmad-Cohen radius update (regcor_gpu.F:131-196, NB_FLAG = 0 form)
-        if (nnb > 0) {
-            const double fac = 1.0 + 0.1 * (double)(P.nnbopt - nnb) / (double)nnb;
-            double a3 = nnb * fac;
-            const double nbave = std::min(P.nnbopt + 150, std::max(P.nnbmax - 50, (int)znbmin));
-            a3 = std::min(a3, 0.9 * nbave);
-            const int nbp = (int)a3;
-            a3 = std::max(a3, znbmin);
-            double a4 = a3 / nnb;
-            if ((a3 - nnb0) * (a3 - nnb) < 0.0) a4 = sqrt(a4);
-            const double a5 = std::min(rsfac * dtr, 0.25);
-            a4 -= 1.0;
-            a4 = a4 > a5 ? a5 : std::max(a4, -a5);
-            const double a3b = a4 / 3.0;
-            double a1 = 1.0 + a3b - a3b * a3b;
-            if (nnb < znbmin && nbp > znbmin && a1 < 1.0) a1 = 1.05;
-            if (fabs(a1 - 1.0) > 0.003) {
-                if (rs[i] * rs[i] > ri2 && rs[i] * rs[i] < 2.0 * ri2 && nnb > 5) a1 = sqrt(a1);
-                rs[i] *= a1;
-            }
-            const double ridot = xi[0] * vi[0] + xi[1] * vi[1] + xi[2] * vi[2];
-            if (nnb > nbave && ridot < 0.0) rs[i] *= 1.0 - (nnb - nbave) / (3.0 * nnb);
-        } else {
-            rs[i] *= 1.5;  // zero membership (fpoly0.F:140-160)
-        }
+        // Ahmad-Cohen radius update (regcor_gpu.F:19-238) from the first
+        // min(nnb, 3) new neighbours at `time`; for nnb = 0 it also gives
+        // the irregular force change the neighbour moves start from
+        double xnb[9] = {0}, vnb[9] = {0};
+        for (int l = 0; l < std::min(nnb, 3); ++l) pred_at(nlist[1 + l] - 1, time, &xnb[3 * l], &vnb[3 * l]);
+        double dfirr[3], dfd[3];
+        rs[i] = ac_radius(P.nb_flag, P.m_flag, P.nnbopt, P.nnbmax, acpar(i), nnb, nnb0, dtr, xi, vi, xnb, vnb,
+                          rs[i], dfirr, dfd);
+        if (nnb > 0) rsmin_seen(i);
         // neighbour gains and losses: move their force between the parts
         // (regcor_gpu.F:284-444)
-        double dfirr[3] = {0, 0, 0}, dfd[3] = {0, 0, 0};
         const int *old = row(i);
         int a = 1, b = 1;
         while (a <= nnb0 || b <= nnb) {
@@ -455,7 +695,7 @@ struct Bodies {
         }
         // regular corrector (regcor_gpu.F:442-537)
         const double dtsq = dtr * dtr, dt6 = 6.0 / (dtr * dtsq), dt2 = 2.0 / dtsq;
-        const double dtsq12 = dtsq / 12.0, dtr13 = dtr / 3.0;
+        const double dtsq12 = ONE12 * dtsq, dtr13 = ONE3 * dtr;
         for (int k = 0; k < 3; ++k) {
             const size_t c = 3 * (size_t)i + k;
             const double dfr = fr[c] - freg[k] - dfirr[k];
@@ -464,7 +704,7 @@ struct Bodies {
             const double sum = frd + fdr0;
             const double at3 = 2.0 * dfr + dtr * sum;
             const double bt2 = -3.0 * dfr - dtr * (sum + frd);
-            x0[c] += (0.6 * at3 + bt2) * dtsq12;
+            x0[c] += (R4(0.6) * at3 + bt2) * dtsq12;
             v0[c] += (0.75 * at3 + bt2) * dtr13;
             fi[c] += dfirr[k];
             fr[c] = freg[k];
@@ -497,7 +737,7 @@ struct Bodies {
         for (int k = 0; k < 3; ++k) {
             const size_t c = 3 * (size_t)i + k;
             f[c] = 0.5 * (fi[c] + fr[c]);
-            fdot[c] = (fidot[c] + frdot[c]) / 6.0;
+            fdot[c] = ONE6 * (fidot[c] + frdot[c]);
         }
         if (step[i] > stepr[i]) step[i] = stepr[i];
         st.reg_steps++;
@@ -671,6 +911,11 @@ struct Bodies {
                     const int *row = &lst[(size_t)p * P.lmax];
                     if (row[0] < 0) {
                         shrink_radius(i, row[0]);
+                        again.push_back(q);
+                        continue;
+                    }
+                    if (fpoly0 && row[0] < 2) {  // only itself: RS = 1.5 RS (fpoly0.F:157)
+                        rs[i] = R4(1.5) * rs[i];
                         again.push_back(q);
                         continue;
                     }

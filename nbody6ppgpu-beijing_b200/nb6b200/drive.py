@@ -32,7 +32,7 @@ class Params(C.Structure):
                 ("max_blocks", C.c_longlong), ("mlp_mode", C.c_int), ("mlp_pad", C.c_int),
                 ("samples", C.POINTER(C.c_float)), ("sample_cap", C.c_longlong),
                 ("rs_init", C.POINTER(C.c_double)), ("dev_corrector", C.c_int),
-                ("seg_single", C.c_int)]
+                ("seg_single", C.c_int), ("nb_flag", C.c_int)]
 
 
 class Stats(C.Structure):
@@ -74,6 +74,9 @@ def _lib():
         _LIB = C.CDLL(DRIVER_LIB, mode=C.RTLD_LOCAL)
         _LIB.nb6drive_run.restype = C.c_int
         _LIB.nb6drive_ensemble.restype = C.c_int
+        _LIB.nb6drive_ac_radius.restype = None
+        _LIB.nb6drive_ac_shrink.restype = None
+        _LIB.nb6drive_core.restype = None
     return _LIB
 
 
@@ -111,11 +114,15 @@ def _rs_field(p: "Params", rs_init, n: int):
 
 def run(backend: dict, mass, pos, vel, *, tcrit=1.0, eta_i=0.02, eta_r=0.03, smax=0.125,
         dtmin=2.0 ** -24, dt_out=0.125, rs0=0.3, nnbopt=50, nnbmax=400, lmax=512, m_flag=0,
-        chunk=1024, max_blocks=10_000_000, mlp_mode=0, sample_cap=0, rs_init=None) -> RunResult:
+        chunk=1024, max_blocks=10_000_000, mlp_mode=0, sample_cap=0, rs_init=None,
+        nb_flag=1) -> RunResult:
     """mlp_mode: 0 Ahmad-Cohen radii; 1 Ahmad-Cohen and log up to sample_cap
     (features, target) samples into RunResult.samples; 2 the library's learned
     proposals (nb6b200.mlp.enable(True) first), Ahmad-Cohen as fallback.
-    rs_init: initial neighbour radii per body (default RS0 sqrt(1 + r^2))."""
+    rs_init: initial neighbour radii per body (default RS0 sqrt(1 + r^2)).
+    nb_flag: form of the Ahmad-Cohen rule, NB_FLAG of regcor_gpu.F:22 (1,
+    the reference's default KZ(39) = 0 or 2: density-centre distances; 0:
+    KZ(39) = 1 or 3)."""
     mass = np.ascontiguousarray(mass, dtype=np.float64)
     n = mass.shape[0]
     x = np.ascontiguousarray(pos, dtype=np.float64).reshape(n, 3).copy()
@@ -123,6 +130,7 @@ def run(backend: dict, mass, pos, vel, *, tcrit=1.0, eta_i=0.02, eta_r=0.03, sma
     p = Params(eta_i, eta_r, smax, dtmin, tcrit, dt_out, rs0, nnbopt, nnbmax, lmax, m_flag,
                chunk, max_blocks)
     buf = _mlp_fields(p, mlp_mode, sample_cap)
+    p.nb_flag = int(nb_flag)
     rs_arr = _rs_field(p, rs_init, n)
     nout_max = int(tcrit / dt_out) + 4
     eout = np.zeros((nout_max, 4))
@@ -160,7 +168,7 @@ def run_ensemble(backend: dict, clusters, *, batched=True, tcrit=1.0, eta_i=0.02
                  smax=0.125, dtmin=2.0 ** -24, dt_out=0.125, rs0=0.3, nnbopt=50, nnbmax=400,
                  lmax=512, m_flag=0, chunk=1024, max_blocks=100_000_000, mlp_mode=0,
                  sample_cap=0, rs_init=None, rs_from_clusters=False,
-                 dev_corrector=True, seg_single=False) -> EnsembleResult:
+                 dev_corrector=True, seg_single=False, nb_flag=1) -> EnsembleResult:
     """clusters: sequence of (mass, pos, vel) (or objects with .mass/.pos/.vel),
     each in its own Henon units.  batched=False issues the regular force per
     cluster (what running each alone does); the result is then identical to
@@ -187,6 +195,7 @@ def run_ensemble(backend: dict, clusters, *, batched=True, tcrit=1.0, eta_i=0.02
     buf = _mlp_fields(p, mlp_mode, sample_cap)
     p.dev_corrector = int(dev_corrector)
     p.seg_single = 1 if seg_single else 0
+    p.nb_flag = int(nb_flag)
     if rs_init is None and all(hasattr(c, "rs") for c in clusters) and rs_from_clusters:
         rs_init = np.concatenate([c.rs for c in clusters])
     rs_arr = _rs_field(p, rs_init, len(mass))

@@ -248,3 +248,136 @@ void orc_ks_cmcorr(double ti, int ni, const int *addr, const double *x0,
         }
     }
 }
+
+/* ------------------------------------------------------------------------
+ * Ahmad-Cohen neighbour-radius rule of the regular corrector,
+ * regcor_gpu.F:19-238 (single bodies, I <= N), and the overflow shrink of
+ * util_gpu.F:69-100 / fpoly0.F:134-160.
+ *
+ * The reference is compiled without -fdefault-real-8, so its real literals
+ * (0.1, 0.9, 0.003, 1.05, 1.1, ...) and FLOAT(int) are REAL*4: mixed with a
+ * REAL*8 operand such a literal enters as its single-precision value, and an
+ * expression of REAL*4 terms only (FAC, DRS, the overflow factors) is
+ * evaluated in single precision.  R4() writes those literals; the single
+ * precision expressions are computed in float.  No FMA contraction (the
+ * Fortran is compiled for -mavx without FMA).
+ * ------------------------------------------------------------------------ */
+#define R4(c) ((double)(c##f))
+
+void orc_ac_radius(int n, int kz39, int nnbopt, int nnbmax, const double *adj,
+                   const int *nnb_in, const int *nnb0_in, const double *dtr_in,
+                   const double *xi, const double *vi,
+                   const double *xnb, const double *vnb,
+                   double *rs, double *dfirr, double *dfd)
+{
+    const int m_flag = (kz39 == 2 || kz39 == 3);   /* regcor_gpu.F:21-22 */
+    const int nb_flag = (kz39 == 0 || kz39 == 2);
+    const double *rdens = adj;
+    const double rscale = adj[3], rc2 = adj[4], rsfac = adj[5], bodym = adj[6];
+    const double one3 = 1.0 / 3.0;                 /* zero.f:113 */
+    /* input.F:133: ZNBMIN = MAX(0.01*FLOAT(NNBMAX),1.0) */
+    const float zs = 0.01f * (float)nnbmax;
+    const double znbmin = (double)(zs > 1.0f ? zs : 1.0f);
+    for (int i = 0; i < n; i++) {
+        const double *x = xi + 3 * i, *v = vi + 3 * i;
+        const int nnb = nnb_in[i], nnb0 = nnb0_in[i];
+        const double dtr = dtr_in[i];
+        double *df = dfirr + 3 * i, *dd = dfd + 3 * i;
+        df[0] = df[1] = df[2] = dd[0] = dd[1] = dd[2] = 0.0;
+        double ri2, rh2;
+        if (nb_flag) {                                /* :30-37 */
+            const double a = x[0] - rdens[0], b = x[1] - rdens[1], c = x[2] - rdens[2];
+            ri2 = a * a + b * b + c * c;
+            rh2 = rscale * rscale;
+        } else {
+            ri2 = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
+            rh2 = R4(9.0) * (rscale * rscale);
+        }
+        if (nnb == 0) {                               /* :108-131 */
+            const double r2 = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
+            const double fij = R4(0.01) * bodym / (r2 * sqrt(r2));
+            const double rdot = 3.0 * (x[0] * v[0] + x[1] * v[1] + x[2] * v[2]) / r2;
+            for (int k = 0; k < 3; k++) {
+                df[k] = -fij * x[k];
+                dd[k] = -(v[k] - rdot * x[k]) * fij;
+            }
+            if (rdot > 0.0) {
+                const double a = R4(0.75) * rs[i], b = R4(0.1) * rscale;
+                rs[i] = a > b ? a : b;
+            } else {
+                rs[i] = R4(1.1) * rs[i];
+            }
+            continue;                                 /* GO TO 50 */
+        }
+        /* :139-150 */
+        const float fac_s = 1.0f + 0.1f * ((float)nnbopt - (float)nnb) / (float)nnb;
+        const double fac = (double)fac_s;
+        double a3 = (double)(float)nnb * fac;
+        int nbave = nnbmax - 50 > (int)znbmin ? nnbmax - 50 : (int)znbmin;
+        nbave = nnbopt + 150 < nbave ? nnbopt + 150 : nbave;
+        const double cap = (double)(0.9f * (float)nbave);
+        a3 = a3 < cap ? a3 : cap;
+        const int nbp = (int)a3;
+        if (ri2 > rh2 && nb_flag) {                   /* :152-156 */
+            const double f = rscale / sqrt(ri2);
+            a3 = a3 * (f > R4(0.1) ? f : R4(0.1));
+        } else {
+            a3 = a3 > znbmin ? a3 : znbmin;
+        }
+        double a4 = a3 / (double)(float)nnb;
+        if ((a3 - (double)(float)nnb0) * (a3 - (double)(float)nnb) < 0.0) a4 = sqrt(a4);
+        /* :162-167, RIDOT relative to the density centre in both forms */
+        const double ridot = (x[0] - rdens[0]) * v[0] + (x[1] - rdens[1]) * v[1] +
+                             (x[2] - rdens[2]) * v[2];
+        if (ri2 > rc2 && nb_flag && ri2 < R4(100.0) * rh2)
+            a4 = a4 * (1.0 + ridot * dtr / ri2);
+        /* (:170-181, the c.m. perturber range, applies to I > N only) */
+        double a5 = rsfac * dtr;                      /* :184-192 */
+        a5 = a5 < 0.25 ? a5 : 0.25;
+        a4 = a4 - 1.0;
+        if (a4 > a5) a4 = a5;
+        else a4 = a4 > -a5 ? a4 : -a5;
+        const double a3b = one3 * a4;                 /* :195-213 */
+        double a1 = 1.0 + a3b - a3b * a3b;
+        if (nnb < znbmin && nbp > znbmin)
+            if (a1 < 1.0) a1 = R4(1.05);
+        if (fabs(a1 - 1.0) > R4(0.003)) {
+            if (rs[i] * rs[i] > ri2 && rs[i] * rs[i] < 2.0 * ri2 && nnb > 5) a1 = sqrt(a1);
+            rs[i] = a1 * rs[i];
+        }
+        if (nnb > nbave && ridot < 0.0) {             /* :215-220 */
+            const float drs = ((float)nnb - (float)nbave) / (3.0f * (float)nnb);
+            rs[i] = rs[i] * (1.0 - (double)drs);
+        }
+        if (!m_flag && nnb <= 3 && ri2 < R4(100.0) * rh2) {   /* :223-238 */
+            double a1b = 2.0 * rs[i];
+            for (int l = 0; l < nnb; l++) {
+                const double *xj = xnb + 9 * i + 3 * l, *vj = vnb + 9 * i + 3 * l;
+                const double ex = x[0] - xj[0], ey = x[1] - xj[1], ez = x[2] - xj[2];
+                const double rij = sqrt(ex * ex + ey * ey + ez * ez);
+                const double rsdot = (ex * (v[0] - vj[0]) + ey * (v[1] - vj[1]) +
+                                      ez * (v[2] - vj[2])) / rij;
+                const double t = rij + rsdot * dtr;
+                a1b = a1b < t ? a1b : t;
+            }
+            const double g = R4(1.1) * rs[i];
+            rs[i] = a1b > g ? a1b : g;
+        }
+    }
+}
+
+void orc_ac_shrink(int n, int kz39, int nnbopt, int nnbmax, const int *nnb_neg, double *rs)
+{
+    const int nb_flag = (kz39 == 0 || kz39 == 2);
+    for (int i = 0; i < n; i++) {
+        const int nnb = nnb_neg[i];                   /* negative: the overflow count */
+        if (nb_flag) {                                /* util_gpu.F:80-85 */
+            float f;
+            if (-nnb > nnbopt) f = powf(-(float)nnbopt / (float)nnb, 0.333f);
+            else f = powf((float)nnbopt / (float)nnbmax, 0.4f);
+            rs[i] = (double)f * rs[i];
+        } else {
+            rs[i] = R4(0.9) * rs[i];                  /* :87 */
+        }
+    }
+}

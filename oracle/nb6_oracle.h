@@ -78,6 +78,29 @@ void orc_ks_cmcorr(double ti, int ni, const int *addr, const double *x0,
                    const double *vk, const double *mk, const int *pofs,
                    const int *plist, double *acc, double *jrk);
 
+
+/* Ahmad-Cohen neighbour-radius rule of the regular corrector for single
+ * bodies, regcor_gpu.F:19-238, with the reference's KZ(39) switch
+ * (kz39 = 0 or 2: NB_FLAG = 1; 2 or 3: M_FLAG = 1).  adj = {RDENS[3],
+ * RSCALE, RC2, RSFAC, BODYM}: density centre and core radius squared
+ * (core.f), half-mass radius (adjust.F:136), RSFAC (adjust.F:199), mean
+ * mass.  Per body i: nnb (new list, self removed), nnb0 (old list), dtr =
+ * TIME - T0R, xi/vi at TIME, and for nnb <= 3 the first nnb neighbours of
+ * the new list at TIME in xnb/vnb[i][3][3].  rs[i] is RS(I) in, the new RS
+ * out; dfirr/dfd[i][3] receive the irregular force change the rule starts
+ * the neighbour moves with (non-zero only for nnb = 0: the small central
+ * mass of :108-118).  Real literals and FLOAT() are single precision as in
+ * the reference's build. */
+void orc_ac_radius(int n, int kz39, int nnbopt, int nnbmax, const double *adj,
+                   const int *nnb, const int *nnb0, const double *dtr,
+                   const double *xi, const double *vi,
+                   const double *xnb, const double *vnb,
+                   double *rs, double *dfirr, double *dfd);
+
+/* Radius shrink of an overflowed regular-force row (util_gpu.F:69-100,
+ * fpoly0.F:134-160): nnb_neg[i] < 0 is the row's -NNB. */
+void orc_ac_shrink(int n, int kz39, int nnbopt, int nnbmax, const int *nnb_neg, double *rs);
+
 #ifdef __cplusplus
 }
 #endif

@@ -163,3 +163,33 @@ def ks_cmcorr(ti, addr, x0, v0, acc2, jrk6, mass, t0, lists, slot, xk, vk, mk, p
                          pofs.ctypes.data_as(_i), plist.ctypes.data_as(_i),
                          acc.ctypes.data_as(_d), jrk.ctypes.data_as(_d))
     return acc, jrk
+
+
+def ac_radius(kz39, nnbopt, nnbmax, adj, nnb, nnb0, dtr, xi, vi, rs, xnb=None, vnb=None):
+    """Ahmad-Cohen radius rule (regcor_gpu.F:19-238).  adj = (RDENS[3],
+    RSCALE, RC2, RSFAC, BODYM).  Returns (new rs, dfirr, dfd)."""
+    nnb = np.ascontiguousarray(nnb, dtype=np.int32)
+    n = nnb.shape[0]
+    nnb0 = np.ascontiguousarray(nnb0, dtype=np.int32)
+    dtr, xi, vi = _f(np.broadcast_to(dtr, (n,))), _f(xi).reshape(n, 3), _f(vi).reshape(n, 3)
+    xnb = np.zeros((n, 3, 3)) if xnb is None else _f(xnb).reshape(n, 3, 3)
+    vnb = np.zeros((n, 3, 3)) if vnb is None else _f(vnb).reshape(n, 3, 3)
+    adj = _f(adj).reshape(7)
+    out = _f(rs).reshape(n).copy()
+    dfirr = np.zeros((n, 3))
+    dfd = np.zeros((n, 3))
+    fp64().orc_ac_radius(int(n), int(kz39), int(nnbopt), int(nnbmax), adj.ctypes.data_as(_d),
+                         nnb.ctypes.data_as(_i), nnb0.ctypes.data_as(_i), dtr.ctypes.data_as(_d),
+                         xi.ctypes.data_as(_d), vi.ctypes.data_as(_d), xnb.ctypes.data_as(_d),
+                         vnb.ctypes.data_as(_d), out.ctypes.data_as(_d), dfirr.ctypes.data_as(_d),
+                         dfd.ctypes.data_as(_d))
+    return out, dfirr, dfd
+
+
+def ac_shrink(kz39, nnbopt, nnbmax, nnb_neg, rs):
+    """Overflow shrink of RS (util_gpu.F:69-100)."""
+    nnb_neg = np.ascontiguousarray(nnb_neg, dtype=np.int32)
+    out = _f(rs).reshape(-1).copy()
+    fp64().orc_ac_shrink(int(out.shape[0]), int(kz39), int(nnbopt), int(nnbmax),
+                         nnb_neg.ctypes.data_as(_i), out.ctypes.data_as(_d))
+    return out
