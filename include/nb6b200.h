@@ -186,7 +186,7 @@ void nb6_hermite_set_(int *addr, double fi[3], double fidot[3], double fr[3], do
 void nb6_irr_correct_(double *time, int *ni, int *addr, double *out);
 
 /* Regular force plus regular corrector on the device (the host's REGCOR_GPU
- * work of regcor_gpu.F:131-196 radius update, :284-444 neighbour gain/loss
+ * work of regcor_gpu.F:19-238 radius update, :284-444 neighbour gain/loss
  * force moves, :442-537 corrector, :593-737 new regular step), after
  * nb6_irr_predict_send_ has put the j set of the segments on the device and
  * the irregular corrector of the block has run.  addr[ni] are the bodies
@@ -195,7 +195,9 @@ void nb6_irr_correct_(double *time, int *ni, int *addr, double *out);
  * h2, dtr, xi, vi, lmax, nnbmax, m_flag as for nb6_regf_seg_; rs[k] is the
  * radius h2[k] was formed from; prm = {ETAR, SMAX, DTMIN, 25 / TCR, NNBOPT,
  * learned-radius mode (0, or 2 to take the network's proposal as in the
- * driver)}.  Each body whose list fits gets its
+ * driver)}.  The radius rule takes its form and per-cluster quantities from
+ * nb6_hermite_adjust_ (prm[3] is RSFAC only while no table is set).  Each
+ * body whose list fits gets its
  * radius, neighbour list, Hermite state and regular step updated on the
  * device; out[k][32] = x0[3], v0[3], fi[3], fidot[3], fr[3], frdot[3],
  * F[3], FDOT[3], step, stepr, rs, nnb, overflow (-nnb, else 0),
@@ -207,6 +209,24 @@ void nb6_irr_correct_(double *time, int *ni, int *addr, double *out);
 void nb6_regf_correct_(double *time, int *ni, int *addr, int *iseg, int *nseg, int *seg_j0, int *seg_a0,
                        double *h2, double *dtr, double *rs, double (*xi)[3], double (*vi)[3], int *lmax,
                        int *nnbmax, int *m_flag, double *prm, double *out);
+/* The Ahmad-Cohen radius rule's form and quantities for nb6_regf_correct_
+ * (no reference counterpart as a call: the reference keeps them in common
+ * blocks set by ADJUST and CORE, adjust.F:104-199, core.f).  *nb_flag is
+ * NB_FLAG of regcor_gpu.F:22 (1 for KZ(39) = 0 or 2: distances from the
+ * density centre, membership reduced outside the half-mass radius,
+ * radial-velocity volume factor).  Cluster c holds the bodies of 1-based
+ * addresses [a0[c], a0[c+1]) (*ncl + 1 entries) with par[8c .. 8c+7] =
+ * RDENS[3], RSCALE, RC2, RSFAC = MAX(25/TCR, 1.5 VC/RSMIN), BODYM, 0.  With
+ * *ncl = 0 each segment of a call is its own cluster with RDENS = 0,
+ * RSCALE = RC2 = 1, RSFAC = prm[3], BODYM = 1 / its body count. */
+void nb6_hermite_adjust_(int *nb_flag, int *ncl, int *a0, double *par);
+/* The resident neighbour rows of bodies *a0 .. *a0 + *n - 1 (1-based) into
+ * out[*n][*ls]: [nnb, 1-based ids ascending] with at most *ls - 1 ids and
+ * zeros over the 8 entries after the last (no reference counterpart: the
+ * reference's host keeps LIST; this is for a host that lets the device
+ * regular corrector keep the lists, e.g. for the density centre of
+ * core.f). */
+void nb6_irr_lists_get_(int *a0, int *n, int *ls, int *out);
 /* KS c.m. corrections of the irregular force (cmfirr_cor.f:13-130,
  * cmfirr_ucor.f:14-116, called from nbint_cor.f:37-65; no reference
  * counterpart in the force libraries: the reference applies them on the

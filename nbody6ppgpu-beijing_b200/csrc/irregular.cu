@@ -97,10 +97,49 @@ NB6_DEV void cm_pair(const double *xi, const double *vi, const double *xj, const
 // term (cmfirr_ucor.f:14-116); for i itself the c.m. of a perturbed pair,
 // the perturbation terms over its perturber list are added instead
 // (cmfirr_cor.f:13-130).  An empty list gets no corrections.
+// Per-warp staging of 32 gathered records (4 KB of shared memory): record
+// r's 16-byte chunk t sits at slot 8 r + (t ^ (r & 7)), so that both the
+// cooperative writes (8 lanes per record) and each lane's reads of its own
+// record (chunk t of 8 consecutive records per quarter warp) are free of
+// bank conflicts.
+constexpr int IRR_STAGE = 32 * 8;  // double2 per warp
+
+// The records of the 32 neighbours l = base + lane of this batch into each
+// lane's rj: 8 lanes load one record together (chunk t = lane & 7, one
+// 128-byte line per record, four lines per load instruction, eight loads in
+// flight per lane), the warp transposes them through shared memory.  j is
+// this lane's neighbour (nmax, the zero padding record, when it has none).
+NB6_DEV void gather_batch(const Rec *__restrict__ rec, int j, int lane, double2 *__restrict__ stage, Rec &rj) {
+    const int g = lane >> 3, t = lane & 7;
+    double2 buf[8];
+#pragma unroll
+    for (int s = 0; s < 8; ++s) {
+        const int r = 4 * s + g;
+        const int jr = __shfl_sync(0xffffffffu, j, r);
+        buf[s] = t < 7 ? __ldg(reinterpret_cast<const double2 *>(rec + jr) + t) : make_double2(0.0, 0.0);
+    }
+    __syncwarp();  // the previous batch's reads are done
+#pragma unroll
+    for (int s = 0; s < 8; ++s) {
+        const int r = 4 * s + g;
+        stage[8 * r + (t ^ (r & 7))] = buf[s];
+    }
+    __syncwarp();
+    const double2 *q = stage + 8 * lane;
+    const int sw = lane & 7;
+    const double2 c0 = q[0 ^ sw], c1 = q[1 ^ sw], c2 = q[2 ^ sw], c3 = q[3 ^ sw];
+    const double2 c4 = q[4 ^ sw], c5 = q[5 ^ sw], c6 = q[6 ^ sw];
+    rj.x[0] = c0.x; rj.x[1] = c0.y; rj.x[2] = c1.x;
+    rj.v[0] = c1.y; rj.v[1] = c2.x; rj.v[2] = c2.y;
+    rj.f[0] = c3.x; rj.f[1] = c3.y; rj.f[2] = c4.x;
+    rj.fd[0] = c4.y; rj.fd[1] = c5.x; rj.fd[2] = c5.y;
+    rj.m = c6.x; rj.t0 = c6.y;
+}
+
 template <bool KS>
 NB6_DEV void irr_force_warp(int i, int lane, double ti, const Rec *__restrict__ rec,
                             const int *__restrict__ lists, int ls, int nmax, const KsArgs &ks, double *a,
-                            double *jd, int &nnbid) {
+                            double *jd, int &nnbid, double2 *__restrict__ stage) {
     Rec ri;
     load_rec(rec + i, ri);
     double xi[3], vi[3];
@@ -112,11 +151,14 @@ NB6_DEV void irr_force_warp(int i, int lane, double ti, const Rec *__restrict__ 
     double ax = 0, ay = 0, az = 0, jx = 0, jy = 0, jz = 0;
     double rmin = 1.0e300;
     int jmin = 0x7fffffff;
-    for (int l = lane; l < nnb; l += 32) {
-        const int j = row[1 + l];
-        if (j < 0 || j >= nmax) continue;   // ids are checked at set_list time
+    for (int base = 0; base < nnb; base += 32) {  // warp-uniform: every lane takes every batch
+        const int l = base + lane;
+        int j = l < nnb ? row[1 + l] : nmax;
+        const bool valid = l < nnb && j >= 0 && j < nmax;   // ids are checked at set_list time
+        if (!valid) j = nmax;
         Rec rj;
-        load_rec(rec + j, rj);
+        gather_batch(rec, j, lane, stage, rj);
+        if (!valid) continue;
         double xj[3], vj[3];
         predict(rj, ti, xj, vj);
         const double dxd = xj[0] - xi[0], dyd = xj[1] - xi[1], dzd = xj[2] - xi[2];
@@ -205,20 +247,39 @@ NB6_DEV void irr_force_warp(int i, int lane, double ti, const Rec *__restrict__ 
     nnbid = (nnb > 0 && jmin != 0x7fffffff) ? jmin + 1 : -1;
 }
 
-// out row k = (ax, ay, az, jx, jy, jz, nnbid, 0): one download per call.
+// out row k = (ax, ay, az, jx, jy, jz, nnbid, 0) (the correctors' rows),
+// or, with out null, the caller's layout in fv: acc[ni][3] | jrk[ni][3]
+// (doubles) | nnbid[ni] | nnb[ni] (ints), one download per call and plain
+// block copies into the caller's arrays.
 // KS: with the pair table (a separate instance: the corrections double the
 // registers of the plain walk).
 template <bool KS>
 __global__ void __launch_bounds__(IRR_WARPS * 32)
     irr_kernel(int ni, const int *__restrict__ addr, double ti, const Rec *__restrict__ rec,
-               const int *__restrict__ lists, int ls, int nmax, KsArgs ks, double *__restrict__ out) {
+               const int *__restrict__ lists, int ls, int nmax, KsArgs ks, double *__restrict__ out,
+               double *__restrict__ fv) {
+    __shared__ __align__(16) double2 stage[IRR_WARPS][IRR_STAGE];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int k = blockIdx.x * IRR_WARPS + warp;
     if (k >= ni) return;
     double a[3], jd[3];
     int id;
-    irr_force_warp<KS>(addr[k] - 1, lane, ti, rec, lists, ls, nmax, ks, a, jd, id);
-    if (lane == 0) {
+    irr_force_warp<KS>(addr[k] - 1, lane, ti, rec, lists, ls, nmax, ks, a, jd, id, stage[warp]);
+    if (lane == 0 && !out) {
+        // the caller's layout, in the blocks of the output staging:
+        // acc[ni][3] | jrk[ni][3] (doubles) | nnbid[ni] | nnb[ni] (ints)
+        double *oa = fv;
+        int *oi = reinterpret_cast<int *>(oa + 6 * (size_t)ni);
+        oa[3 * (size_t)k] = a[0];
+        oa[3 * (size_t)k + 1] = a[1];
+        oa[3 * (size_t)k + 2] = a[2];
+        oa[3 * (size_t)ni + 3 * (size_t)k] = jd[0];
+        oa[3 * (size_t)ni + 3 * (size_t)k + 1] = jd[1];
+        oa[3 * (size_t)ni + 3 * (size_t)k + 2] = jd[2];
+        oi[k] = id;
+        oi[ni + k] = max(lists[(size_t)(addr[k] - 1) * ls], 0);
+    }
+    if (lane == 0 && out) {
         double *o = out + (size_t)k * 8;
         o[0] = a[0];
         o[1] = a[1];
@@ -253,6 +314,12 @@ NB6_DEV double dadd(double a, double b) { return __dadd_rn(a, b); }
 NB6_DEV double dmul(double a, double b) { return __dmul_rn(a, b); }
 NB6_DEV double dsub(double a, double b) { return __dsub_rn(a, b); }
 NB6_DEV double ddiv(double a, double b) { return __ddiv_rn(a, b); }
+
+// Constants of the reference's integrator (zero.f:113-116), multiplied as
+// the Fortran multiplies them, and its REAL*4 literals (it is compiled
+// without -fdefault-real-8, so 0.6 enters a REAL*8 product as 0.6f).
+constexpr double ONE3 = 1.0 / 3.0, ONE6 = 1.0 / 6.0, ONE12 = 1.0 / 12.0;
+#define R4(c) ((double)(c##f))
 
 // tstep.f: sqrt(eta (|F||F2| + |F1|^2) / (|F1||F3| + |F2|^2))
 NB6_DEV double tstep_dev(const double *f, const double *f1, const double *f2, const double *f3, double eta) {
@@ -291,7 +358,7 @@ NB6_DEV bool correct_irr_body(int i, double time, const double *__restrict__ fk,
         vi[c] = dadd(dmul(dadd(dmul(r.fd[c], s1), r.f[c]), s2), r.v[c]);
     }
     const double dt = s, dtsq = dmul(dt, dt), dt6 = ddiv(6.0, dmul(dt, dtsq)), dt2 = ddiv(2.0, dtsq);
-    const double dtsq12 = ddiv(dtsq, 12.0), dt13 = ddiv(dt, 3.0);
+    const double dtsq12 = dmul(ONE12, dtsq), dt13 = dmul(ONE3, dt);
     double ftot[3], d2[3], d3[3];
     for (int c = 0; c < 3; ++c) {  // nbint_cor.f:130-150
         const double df = dsub(x.fi[c], a[c]);
@@ -299,7 +366,7 @@ NB6_DEV bool correct_irr_body(int i, double time, const double *__restrict__ fk,
         const double sum = dadd(fid, jd[c]);
         const double at3 = dadd(dmul(2.0, df), dmul(dt, sum));
         const double bt2 = dsub(dmul(-3.0, df), dmul(dt, dadd(sum, fid)));
-        r.x[c] = dadd(xi[c], dmul(dadd(dmul(0.6, at3), bt2), dtsq12));
+        r.x[c] = dadd(xi[c], dmul(dadd(dmul(R4(0.6), at3), bt2), dtsq12));
         r.v[c] = dadd(vi[c], dmul(dadd(dmul(0.75, at3), bt2), dt13));
         x.fi[c] = a[c];
         x.fid[c] = jd[c];
@@ -326,7 +393,7 @@ NB6_DEV bool correct_irr_body(int i, double time, const double *__restrict__ fk,
         const double dtr = dsub(time, x.t0r);
         for (int c = 0; c < 3; ++c) {
             r.f[c] = dmul(0.5, dadd(dadd(dmul(x.frd[c], dtr), x.fr[c]), x.fi[c]));
-            r.fd[c] = ddiv(dadd(x.frd[c], x.fid[c]), 6.0);
+            r.fd[c] = dmul(ONE6, dadd(x.frd[c], x.fid[c]));
         }
         // keep the irregular step inside the regular interval
         while (dadd(r.t0, x.step) > dadd(x.t0r, x.stepr) && x.step > hp.dtmin) x.step = dmul(x.step, 0.5);
@@ -372,7 +439,109 @@ __global__ void irr_apply_corrector(int ni, const int *__restrict__ addr, double
 struct RegCorrParams {
     double eta_r, smax, dtmin, rsfac;
     int nnbopt, nnbmax, cap, mlp_mode;
+    int nb_flag, m_flag;
+    // radius-rule quantities per cluster (nb6_hermite_adjust_): cluster c
+    // holds bodies [acl_a0[c], acl_a0[c+1]) (0-based), acpar[8c..] = RDENS[3],
+    // RSCALE, RC2, RSFAC, BODYM; nacl = 0: none set
+    int nacl;
+    const int *acl_a0;
+    const double *acpar;
 };
+
+// Radius-rule quantities of one cluster (as Bodies::adjust sets them).
+struct ACParDev {
+    double rdens[3], rscale, rc2, rsfac, bodym;
+};
+
+// Ahmad-Cohen radius update of one body at its regular step
+// (regcor_gpu.F:19-238), the host's ac_radius (driver/hermite.h) operation
+// for operation: REAL*4 terms of the reference (FLOAT(), literals) in float,
+// the rest in double, every operation rounded separately.  xnb/vnb: the
+// first min(nnb, 3) new neighbours at TIME.  dfirr/dfd: the irregular force
+// change the neighbour moves start from (the small central mass, nnb = 0).
+NB6_DEV double ac_radius_dev(int nb_flag, int m_flag, int nnbopt, int nnbmax, const ACParDev &a, int nnb,
+                             int nnb0, double dtr, const double *xi, const double *vi, const double *xnb,
+                             const double *vnb, double rs, double *dfirr, double *dfd) {
+    const float zs = __fmul_rn(0.01f, (float)nnbmax);
+    const double znbmin = (double)(zs > 1.0f ? zs : 1.0f);
+    for (int k = 0; k < 3; ++k) dfirr[k] = dfd[k] = 0.0;
+    double ri2, rh2;
+    if (nb_flag) {
+        const double e0 = dsub(xi[0], a.rdens[0]), e1 = dsub(xi[1], a.rdens[1]), e2 = dsub(xi[2], a.rdens[2]);
+        ri2 = dadd(dadd(dmul(e0, e0), dmul(e1, e1)), dmul(e2, e2));
+        rh2 = dmul(a.rscale, a.rscale);
+    } else {
+        ri2 = dadd(dadd(dmul(xi[0], xi[0]), dmul(xi[1], xi[1])), dmul(xi[2], xi[2]));
+        rh2 = dmul(R4(9.0), dmul(a.rscale, a.rscale));
+    }
+    if (nnb == 0) {
+        const double r2 = dadd(dadd(dmul(xi[0], xi[0]), dmul(xi[1], xi[1])), dmul(xi[2], xi[2]));
+        const double fij = ddiv(dmul(R4(0.01), a.bodym), dmul(r2, __dsqrt_rn(r2)));
+        const double rdot =
+            ddiv(dmul(3.0, dadd(dadd(dmul(xi[0], vi[0]), dmul(xi[1], vi[1])), dmul(xi[2], vi[2]))), r2);
+        for (int k = 0; k < 3; ++k) {
+            dfirr[k] = dmul(-fij, xi[k]);
+            dfd[k] = dmul(-dsub(vi[k], dmul(rdot, xi[k])), fij);
+        }
+        if (rdot > 0.0) {
+            const double u = dmul(R4(0.75), rs), w = dmul(R4(0.1), a.rscale);
+            return u > w ? u : w;
+        }
+        return dmul(R4(1.1), rs);
+    }
+    const float fac_s =
+        __fadd_rn(1.0f, __fdiv_rn(__fmul_rn(0.1f, __fsub_rn((float)nnbopt, (float)nnb)), (float)nnb));
+    double a3 = dmul((double)(float)nnb, (double)fac_s);
+    const int zi = (int)znbmin;
+    const int nbave = min(nnbopt + 150, max(nnbmax - 50, zi));
+    const double cap = (double)__fmul_rn(0.9f, (float)nbave);
+    a3 = a3 < cap ? a3 : cap;
+    const int nbp = (int)a3;
+    if (ri2 > rh2 && nb_flag) {
+        const double f = ddiv(a.rscale, __dsqrt_rn(ri2));
+        a3 = dmul(a3, f > R4(0.1) ? f : R4(0.1));
+    } else {
+        a3 = a3 > znbmin ? a3 : znbmin;
+    }
+    double a4 = ddiv(a3, (double)(float)nnb);
+    if (dmul(dsub(a3, (double)(float)nnb0), dsub(a3, (double)(float)nnb)) < 0.0) a4 = __dsqrt_rn(a4);
+    const double ridot = dadd(dadd(dmul(dsub(xi[0], a.rdens[0]), vi[0]), dmul(dsub(xi[1], a.rdens[1]), vi[1])),
+                              dmul(dsub(xi[2], a.rdens[2]), vi[2]));
+    if (ri2 > a.rc2 && nb_flag && ri2 < dmul(R4(100.0), rh2)) a4 = dmul(a4, dadd(1.0, ddiv(dmul(ridot, dtr), ri2)));
+    double a5 = dmul(a.rsfac, dtr);
+    a5 = a5 < 0.25 ? a5 : 0.25;
+    a4 = dsub(a4, 1.0);
+    if (a4 > a5) a4 = a5;
+    else a4 = a4 > -a5 ? a4 : -a5;
+    const double a3b = dmul(ONE3, a4);
+    double a1 = dsub(dadd(1.0, a3b), dmul(a3b, a3b));
+    if (nnb < znbmin && nbp > znbmin && a1 < 1.0) a1 = R4(1.05);
+    if (fabs(dsub(a1, 1.0)) > R4(0.003)) {
+        const double rs2 = dmul(rs, rs);
+        if (rs2 > ri2 && rs2 < dmul(2.0, ri2) && nnb > 5) a1 = __dsqrt_rn(a1);
+        rs = dmul(a1, rs);
+    }
+    if (nnb > nbave && ridot < 0.0) {
+        const float drs = __fdiv_rn(__fsub_rn((float)nnb, (float)nbave), __fmul_rn(3.0f, (float)nnb));
+        rs = dmul(rs, dsub(1.0, (double)drs));
+    }
+    if (!m_flag && nnb <= 3 && ri2 < dmul(R4(100.0), rh2)) {
+        double b1 = dmul(2.0, rs);
+        for (int l = 0; l < nnb; ++l) {
+            const double *xj = xnb + 3 * l, *vj = vnb + 3 * l;
+            const double e0 = dsub(xi[0], xj[0]), e1 = dsub(xi[1], xj[1]), e2 = dsub(xi[2], xj[2]);
+            const double rij = __dsqrt_rn(dadd(dadd(dmul(e0, e0), dmul(e1, e1)), dmul(e2, e2)));
+            const double rsdot = ddiv(dadd(dadd(dmul(e0, dsub(vi[0], vj[0])), dmul(e1, dsub(vi[1], vj[1]))),
+                                           dmul(e2, dsub(vi[2], vj[2]))),
+                                      rij);
+            const double t = dadd(rij, dmul(rsdot, dtr));
+            b1 = b1 < t ? b1 : t;
+        }
+        const double g = dmul(R4(1.1), rs);
+        rs = b1 > g ? b1 : g;
+    }
+    return rs;
+}
 
 // host Bodies::pair_force: FP64 force and jerk of j (at xj, vj, mass mj) on i
 NB6_DEV void pair_force_dev(const double *xi, const double *vi, const double *xj, const double *vj, double mj,
@@ -423,45 +592,42 @@ __global__ void reg_corrector_kernel(int ni, const int *__restrict__ addr, const
     const int nnb = raw - self_in;
     const double dtr = dsub(time, x.t0r);
     const double xi[3] = {r.x[0], r.x[1], r.x[2]}, vi[3] = {r.v[0], r.v[1], r.v[2]};
-    const double ri2 = dadd(dadd(dmul(xi[0], xi[0]), dmul(xi[1], xi[1])), dmul(xi[2], xi[2]));
-    const double znbmin = dmul(0.2, (double)p.nnbopt);
     double rs = rs_in[k];  // the radius the call's h2 was formed from
     const double rs_used = rs;
-    // Ahmad-Cohen radius update (regcor_gpu.F:131-196, NB_FLAG = 0 form)
-    if (nnb > 0) {
-        const double fac = dadd(1.0, ddiv(dmul(0.1, (double)(p.nnbopt - nnb)), (double)nnb));
-        double a3 = dmul((double)nnb, fac);
-        const int zi = (int)znbmin;
-        const int nbave_i = min(p.nnbopt + 150, max(p.nnbmax - 50, zi));
-        const double nbave = (double)nbave_i;
-        const double cap9 = dmul(0.9, nbave);
-        a3 = (cap9 < a3) ? cap9 : a3;
-        const int nbp = (int)a3;
-        a3 = (a3 < znbmin) ? znbmin : a3;
-        double a4 = ddiv(a3, (double)nnb);
-        if (dmul(dsub(a3, (double)nnb0), dsub(a3, (double)nnb)) < 0.0) a4 = __dsqrt_rn(a4);
-        const double rd = dmul(p.rsfac, dtr);
-        const double a5 = (0.25 < rd) ? 0.25 : rd;
-        a4 = dsub(a4, 1.0);
-        const double na5 = -a5;
-        a4 = a4 > a5 ? a5 : ((a4 < na5) ? na5 : a4);
-        const double a3b = ddiv(a4, 3.0);
-        double a1 = dsub(dadd(1.0, a3b), dmul(a3b, a3b));
-        if (nnb < znbmin && nbp > znbmin && a1 < 1.0) a1 = 1.05;
-        if (fabs(dsub(a1, 1.0)) > 0.003) {
-            const double rs2 = dmul(rs, rs);
-            if (rs2 > ri2 && rs2 < dmul(2.0, ri2) && nnb > 5) a1 = __dsqrt_rn(a1);
-            rs = dmul(rs, a1);
+    // the body's cluster and its radius-rule quantities
+    ACParDev ap;
+    if (p.nacl > 0) {
+        int lo = 0, hi = p.nacl - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (p.acl_a0[mid] <= i) lo = mid;
+            else hi = mid - 1;
         }
-        const double ridot = dadd(dadd(dmul(xi[0], vi[0]), dmul(xi[1], vi[1])), dmul(xi[2], vi[2]));
-        if ((double)nnb > nbave && ridot < 0.0)
-            rs = dmul(rs, dsub(1.0, ddiv((double)nnb - nbave, dmul(3.0, (double)nnb))));
+        const double *q = p.acpar + 8 * (size_t)lo;
+        ap = {{q[0], q[1], q[2]}, q[3], q[4], q[5], q[6]};
     } else {
-        rs = dmul(rs, 1.5);  // zero membership (fpoly0.F:140-160)
+        ap = {{0.0, 0.0, 0.0}, 1.0, 1.0, p.rsfac, ddiv(1.0, (double)nj)};
     }
+    // Ahmad-Cohen radius update (regcor_gpu.F:19-238) from the first
+    // min(nnb, 3) new neighbours of the call's j set
+    double xnb[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, vnb[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    {
+        int l3 = 0;
+        for (int l = 1; l <= raw && l3 < 3; ++l) {
+            if (base + ol[l] == i) continue;
+            const size_t q = (size_t)(jb + ol[l]);
+            for (int c = 0; c < 3; ++c) {
+                xnb[3 * l3 + c] = ro.jx[3 * q + c];
+                vnb[3 * l3 + c] = ro.jv[3 * q + c];
+            }
+            ++l3;
+        }
+    }
+    double dfirr[3], dfd[3];
+    rs = ac_radius_dev(p.nb_flag, p.m_flag, p.nnbopt, p.nnbmax, ap, nnb, nnb0, dtr, xi, vi, xnb, vnb, rs, dfirr,
+                       dfd);
     // neighbour gains and losses (regcor_gpu.F:284-444); ids are 0-based
     // global addresses, the new list's are relative to the segment
-    double dfirr[3] = {0, 0, 0}, dfd[3] = {0, 0, 0};
     int a = 1, b = 1;
     auto next_new = [&](int &bb) {  // skip self in the new list
         while (bb <= raw && base + ol[bb] == i) ++bb;
@@ -503,7 +669,7 @@ __global__ void reg_corrector_kernel(int ni, const int *__restrict__ addr, const
     }
     // regular corrector (regcor_gpu.F:442-537)
     const double dtsq = dmul(dtr, dtr), dt6 = ddiv(6.0, dmul(dtr, dtsq)), dt2 = ddiv(2.0, dtsq);
-    const double dtsq12 = ddiv(dtsq, 12.0), dtr13 = ddiv(dtr, 3.0);
+    const double dtsq12 = dmul(ONE12, dtsq), dtr13 = dmul(ONE3, dtr);
     double d2r[3], d3r[3];
     for (int c = 0; c < 3; ++c) {
         const double dfr = dsub(dsub(x.fr[c], of[c]), dfirr[c]);
@@ -512,7 +678,7 @@ __global__ void reg_corrector_kernel(int ni, const int *__restrict__ addr, const
         const double sum = dadd(frd, fdr0);
         const double at3 = dadd(dmul(2.0, dfr), dmul(dtr, sum));
         const double bt2 = dsub(dmul(-3.0, dfr), dmul(dtr, dadd(sum, frd)));
-        r.x[c] = dadd(r.x[c], dmul(dadd(dmul(0.6, at3), bt2), dtsq12));
+        r.x[c] = dadd(r.x[c], dmul(dadd(dmul(R4(0.6), at3), bt2), dtsq12));
         r.v[c] = dadd(r.v[c], dmul(dadd(dmul(0.75, at3), bt2), dtr13));
         x.fi[c] = dadd(x.fi[c], dfirr[c]);
         x.fr[c] = of[c];
@@ -544,7 +710,7 @@ __global__ void reg_corrector_kernel(int ni, const int *__restrict__ addr, const
     x.t0r = time;
     for (int c = 0; c < 3; ++c) {
         r.f[c] = dmul(0.5, dadd(x.fi[c], x.fr[c]));
-        r.fd[c] = ddiv(dadd(x.fid[c], x.frd[c]), 6.0);
+        r.fd[c] = dmul(ONE6, dadd(x.fid[c], x.frd[c]));
     }
     if (x.step > x.stepr) x.step = x.stepr;
     // learned radius (Bodies::learn_apply): take RS_used exp(dlog) when the
@@ -700,6 +866,7 @@ template <bool KS>
 __global__ void __launch_bounds__(IRR_WARPS * 32)
     blk_irr(const BlockCtl *c, const int *__restrict__ act, const Rec *__restrict__ rec,
             const int *__restrict__ lists, int ls, int nmax, KsArgs ks, double *__restrict__ out) {
+    __shared__ __align__(16) double2 stage[IRR_WARPS][IRR_STAGE];
     blk_enter();
     if (c->stop) return;
     const int p = c->parity, na = c->nact[p];
@@ -708,7 +875,7 @@ __global__ void __launch_bounds__(IRR_WARPS * 32)
     for (int k = blockIdx.x * IRR_WARPS + (threadIdx.x >> 5); k < na; k += gridDim.x * IRR_WARPS) {
         double a[3], jd[3];
         int id;
-        irr_force_warp<KS>(act[k], lane, t, rec, lists, ls, nmax, ks, a, jd, id);
+        irr_force_warp<KS>(act[k], lane, t, rec, lists, ls, nmax, ks, a, jd, id, stage[threadIdx.x >> 5]);
         if (lane == 0) {
             double *o = out + (size_t)k * 8;
             o[0] = a[0];
@@ -941,6 +1108,13 @@ struct IrrState {
     DevBuf<char> bsort_tmp;
     long long rc_calls = 0;           // nb6_regf_correct_ calls and their host-side phases
     double rc_t[4] = {0, 0, 0, 0};
+    // radius-rule quantities per cluster (nb6_hermite_adjust_)
+    int ac_nb_flag = 0, nacl = 0;
+    DevBuf<int> acl_a0;
+    DevBuf<double> acpar;
+    // neighbour rows read back (nb6_irr_lists_get_)
+    DevBuf<int> lg_dev;
+    HostBuf<int> lg_host;
 };
 IrrState I;
 
@@ -958,11 +1132,14 @@ KsArgs ks_args() {
     return k;
 }
 
-void launch_irr_kernel(int ni, const int *daddr, double ti, double *out, cudaStream_t st) {
+// out: rows of 8 doubles; or, out null, the caller's layout in fv
+void launch_irr_kernel(int ni, const int *daddr, double ti, double *out, cudaStream_t st, double *fv = nullptr) {
     const KsArgs ks = ks_args();
     const dim3 grid((ni + IRR_WARPS - 1) / IRR_WARPS), block(IRR_WARPS * 32);
-    if (ks.slot) irr_kernel<true><<<grid, block, 0, st>>>(ni, daddr, ti, I.rec.ptr, I.lists.ptr, I.lmax, I.nmax, ks, out);
-    else irr_kernel<false><<<grid, block, 0, st>>>(ni, daddr, ti, I.rec.ptr, I.lists.ptr, I.lmax, I.nmax, ks, out);
+    if (ks.slot)
+        irr_kernel<true><<<grid, block, 0, st>>>(ni, daddr, ti, I.rec.ptr, I.lists.ptr, I.lmax, I.nmax, ks, out, fv);
+    else
+        irr_kernel<false><<<grid, block, 0, st>>>(ni, daddr, ti, I.rec.ptr, I.lists.ptr, I.lmax, I.nmax, ks, out, fv);
 }
 
 __global__ void ks_scatter_slots(int npair, const int *__restrict__ cm, int *__restrict__ slot) {
@@ -1034,6 +1211,12 @@ void irr_close_impl() {
     I.aux_slot.clear();
     I.naux = 0;
     I.hermite = false;
+    I.nacl = 0;
+    I.ac_nb_flag = 0;
+    I.acl_a0.release();
+    I.acpar.release();
+    I.lg_dev.release();
+    I.lg_host.release();
     I.ks_slot.release();
     I.ks_int.release();
     I.ks_dbl.release();
@@ -1218,25 +1401,32 @@ void irr_firr_vec_impl(double ti, int ni, const int *addr, double (*acc)[3], dou
         return;
     }
     if (ni <= 0) return;
-    for (int k = 0; k < ni; ++k) {
-        if (addr[k] < 1 || addr[k] > I.nmax) {
-            fprintf(stderr, "irr_simd_firr_vec: address %d outside [1, %d]\n", addr[k], I.nmax);
-            nb6_fatal(NB6_ERR_BAD_ARG);
-            return;
-        }
+    int bad = 0;
+    for (int k = 0; k < ni; ++k) bad |= (addr[k] < 1) | (addr[k] > I.nmax);
+    if (bad) {
+        for (int k = 0; k < ni; ++k)
+            if (addr[k] < 1 || addr[k] > I.nmax) {
+                fprintf(stderr, "irr_simd_firr_vec: address %d outside [1, %d]\n", addr[k], I.nmax);
+                break;
+            }
+        nb6_fatal(NB6_ERR_BAD_ARG);
+        return;
     }
     const double t0 = nb6_wtime();
     cudaStream_t st = nb6_stream();
     // the pinned staging is reused only after this call's synchronize, so
     // the uploads enqueued here read it intact
     const int *daddr = irr_flush(st, addr, ni);
-    I.hout.reserve((size_t)ni * 8);
-    // results go straight to pinned host memory when small, else through
-    // one device buffer and one copy
-    const bool direct = sizeof(double) * 8 * (size_t)ni <= zero_copy_bytes();
+    // results in the caller's layout: acc | jrk (6 ni doubles) | nnbid | nnb
+    // (2 ni ints), written straight to pinned host memory when small, else
+    // through one device buffer and one copy
+    const size_t nd = 7 * (size_t)ni;   // 6 ni doubles + 2 ni ints
+    const size_t bytes = sizeof(double) * nd;
+    I.hout.reserve(nd);
+    const bool direct = bytes <= zero_copy_bytes();
     double *out = I.hout.ptr;
     if (!direct) {
-        I.dout.reserve((size_t)ni * 8);
+        I.dout.reserve(nd);
         out = I.dout.ptr;
     }
     if (!I.ev0) {
@@ -1244,27 +1434,21 @@ void irr_firr_vec_impl(double ti, int ni, const int *addr, double (*acc)[3], dou
         NB6_CUDA_CHECK(cudaEventCreate(&I.ev1));
     }
     NB6_CUDA_CHECK(cudaEventRecord(I.ev0, st));
-    launch_irr_kernel(ni, daddr, ti, out, st);
+    launch_irr_kernel(ni, daddr, ti, nullptr, st, out);
     NB6_CUDA_CHECK(cudaGetLastError());
     NB6_CUDA_CHECK(cudaEventRecord(I.ev1, st));
-    if (!direct)
-        NB6_CUDA_CHECK(cudaMemcpyAsync(I.hout.ptr, I.dout.ptr, sizeof(double) * 8 * ni, cudaMemcpyDeviceToHost, st));
+    if (!direct) NB6_CUDA_CHECK(cudaMemcpyAsync(I.hout.ptr, I.dout.ptr, bytes, cudaMemcpyDeviceToHost, st));
     nb6_status_fetch(st);
     NB6_CUDA_CHECK(cudaStreamSynchronize(st));
     if (nb6_check_dev_status() != 0) return;
+    const double *h = I.hout.ptr;
+    memcpy(&acc[0][0], h, sizeof(double) * 3 * (size_t)ni);
+    memcpy(&jrk[0][0], h + 3 * (size_t)ni, sizeof(double) * 3 * (size_t)ni);
+    const int *hi = reinterpret_cast<const int *>(h + 6 * (size_t)ni);
+    memcpy(nnbid, hi, sizeof(int) * (size_t)ni);
     unsigned long long inter = 0;
-    for (int k = 0; k < ni; ++k) inter += (unsigned long long)I.nnb_host[addr[k] - 1];
+    for (int k = 0; k < ni; ++k) inter += (unsigned)hi[ni + k];
     I.num_inter += inter;
-    for (int k = 0; k < ni; ++k) {
-        const double *o = I.hout.ptr + (size_t)k * 8;
-        acc[k][0] = o[0];
-        acc[k][1] = o[1];
-        acc[k][2] = o[2];
-        jrk[k][0] = o[3];
-        jrk[k][1] = o[4];
-        jrk[k][2] = o[5];
-        nnbid[k] = (int)o[6];
-    }
     I.time_grav += nb6_wtime() - t0;
     I.num_fcall++;
     I.num_steps += ni;
@@ -1709,6 +1893,11 @@ void regf_correct_impl(double time, int ni, const int *addr, int *iseg, int nseg
     p.nnbmax = nnbmax;
     p.cap = std::max(0, std::min(nnbmax, lmax - 1));
     p.mlp_mode = (int)prm[5];
+    p.nb_flag = I.ac_nb_flag;
+    p.m_flag = mflag ? 1 : 0;
+    p.nacl = I.nacl;
+    p.acl_a0 = I.acl_a0.ptr;
+    p.acpar = I.acpar.ptr;
     const size_t rowd = 32;
     I.hout.reserve((size_t)ni * rowd);
     const bool direct = sizeof(double) * rowd * (size_t)ni <= zero_copy_bytes();
@@ -1801,6 +1990,102 @@ void irr_profile_impl(int rank) {
 }
 
 }  // namespace
+
+// Radius-rule quantities per cluster for the device regular corrector.
+void hermite_adjust_impl(int nb_flag, int ncl, const int *a0, const double *par) {
+    if (!I.open) {
+        nb6_fatal(NB6_ERR_NOT_OPEN);
+        return;
+    }
+    bool bad = ncl < 0 || (ncl > 0 && (a0[0] < 1 || a0[ncl] > I.nmax + 1));
+    for (int c = 0; c < ncl && !bad; ++c) bad = a0[c + 1] < a0[c];
+    for (int c = 0; c < 8 * ncl && !bad; ++c) bad = par[c] != par[c];
+    if (bad) {
+        fprintf(stderr, "nb6_hermite_adjust: bad cluster table\n");
+        nb6_fatal(NB6_ERR_BAD_ARG);
+        return;
+    }
+    I.ac_nb_flag = nb_flag ? 1 : 0;
+    I.nacl = ncl;
+    if (ncl == 0) return;
+    cudaStream_t st = nb6_stream();
+    std::vector<int> h(ncl + 1);
+    for (int c = 0; c <= ncl; ++c) h[c] = a0[c] - 1;
+    I.acl_a0.reserve((size_t)ncl + 1);
+    I.acpar.reserve(8 * (size_t)ncl);
+    NB6_CUDA_CHECK(cudaMemcpyAsync(I.acl_a0.ptr, h.data(), sizeof(int) * (ncl + 1), cudaMemcpyHostToDevice, st));
+    NB6_CUDA_CHECK(cudaMemcpyAsync(I.acpar.ptr, par, sizeof(double) * 8 * ncl, cudaMemcpyHostToDevice, st));
+    NB6_CUDA_CHECK(cudaStreamSynchronize(st));
+}
+
+// Row lengths of bodies [a0, a0 + n) (0-based), capped at cap ids.
+__global__ void lists_count(int n, int a0, const int *__restrict__ lists, int ls, int cap, int *__restrict__ cnt) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int c = lists[(size_t)(a0 + k) * ls];
+    cnt[k] = min(max(c, 0), cap);
+}
+
+// One warp per body: its row [nnb, ids] packed at offs[k], ids 1-based.
+__global__ void lists_pack(int n, int a0, const int *__restrict__ lists, int ls, const int *__restrict__ cnt,
+                           const long long *__restrict__ offs, int *__restrict__ packed) {
+    const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (k >= n) return;
+    const int *row = lists + (size_t)(a0 + k) * ls;
+    int *o = packed + offs[k];
+    const int c = cnt[k];
+    if (lane == 0) o[0] = c;
+    for (int l = lane; l < c; l += 32) o[1 + l] = row[1 + l] + 1;
+}
+
+void lists_get_impl(int a0, int n, int ls, int *out) {
+    if (!I.open) {
+        nb6_fatal(NB6_ERR_NOT_OPEN);
+        return;
+    }
+    if (n <= 0) return;
+    if (a0 < 1 || (long long)a0 - 1 + n > I.nmax || ls < 1) {
+        nb6_fatal(NB6_ERR_BAD_ARG);
+        return;
+    }
+    cudaStream_t st = nb6_stream();
+    irr_flush(st);
+    const int cap = std::min(I.lmax, ls) - 1;
+    const size_t nn = (size_t)n;
+    // [counts n | offsets 2n (long long)] on both sides, then the packed rows
+    I.lg_dev.reserve(3 * nn + 2);
+    I.lg_host.reserve(3 * nn + 2);
+    int *dcnt = I.lg_dev.ptr;
+    lists_count<<<(n + 255) / 256, 256, 0, st>>>(n, a0 - 1, I.lists.ptr, I.lmax, cap, dcnt);
+    NB6_CUDA_CHECK(cudaGetLastError());
+    NB6_CUDA_CHECK(cudaMemcpyAsync(I.lg_host.ptr, dcnt, sizeof(int) * nn, cudaMemcpyDeviceToHost, st));
+    NB6_CUDA_CHECK(cudaStreamSynchronize(st));
+    long long *hoff = reinterpret_cast<long long *>(I.lg_host.ptr + ((nn + 1) & ~(size_t)1));
+    long long tot = 0;
+    for (size_t k = 0; k < nn; ++k) {
+        hoff[k] = tot;
+        tot += 1 + I.lg_host.ptr[k];
+    }
+    long long *doff = reinterpret_cast<long long *>(I.lg_dev.ptr + ((nn + 1) & ~(size_t)1));
+    NB6_CUDA_CHECK(cudaMemcpyAsync(doff, hoff, sizeof(long long) * nn, cudaMemcpyHostToDevice, st));
+    DevBuf<int> dpk;
+    HostBuf<int> hpk;
+    dpk.reserve((size_t)tot);
+    hpk.reserve((size_t)tot);
+    lists_pack<<<(unsigned)((nn * 32 + 255) / 256), 256, 0, st>>>(n, a0 - 1, I.lists.ptr, I.lmax, dcnt, doff, dpk.ptr);
+    NB6_CUDA_CHECK(cudaGetLastError());
+    NB6_CUDA_CHECK(cudaMemcpyAsync(hpk.ptr, dpk.ptr, sizeof(int) * tot, cudaMemcpyDeviceToHost, st));
+    NB6_CUDA_CHECK(cudaStreamSynchronize(st));
+    for (size_t k = 0; k < nn; ++k) {
+        const int *src = hpk.ptr + hoff[k];
+        int *row = out + k * (size_t)ls;
+        const int c = src[0];
+        memcpy(row, src, sizeof(int) * (size_t)(1 + c));
+        for (int l = 1 + c; l < std::min(ls, 1 + c + 8); ++l) row[l] = 0;
+    }
+    dpk.release();
+    hpk.release();
+}
 
 extern "C" {
 
@@ -1932,5 +2217,23 @@ float nb6_irr_last_kernel_ms_() {
 void nb6_irr_predict_send_(double *t, int *nseg, int *addr0, int *count) {
     irr_predict_send_impl(*t, *nseg, addr0, count);
 }
+
+// Extension (no reference counterpart; the reference keeps these in common
+// blocks, set by ADJUST and CORE, adjust.F:104-199, core.f): the Ahmad-Cohen
+// radius rule's quantities for the device regular corrector.  *nb_flag
+// selects the rule's form (NB_FLAG of regcor_gpu.F:22: 1 for KZ(39) = 0 or
+// 2).  Cluster c holds the bodies of 1-based addresses [a0[c], a0[c+1])
+// (a0 has *ncl + 1 entries) and par[8c .. 8c+7] = RDENS[3], RSCALE, RC2,
+// RSFAC, BODYM, 0.  Without a table (*ncl = 0) each segment of a call is
+// its own cluster with RDENS = 0, RSCALE = RC2 = 1, RSFAC = prm[3] and
+// BODYM = 1 / (its body count).
+void nb6_hermite_adjust_(int *nb_flag, int *ncl, int *a0, double *par) { hermite_adjust_impl(*nb_flag, *ncl, a0, par); }
+
+// Extension (no reference counterpart): the resident neighbour rows of the
+// bodies of 1-based addresses *a0 .. *a0 + *n - 1 into out[*n][*ls], each
+// [nnb, 1-based ids ascending] (at most *ls - 1 ids), zeros over the 8
+// entries after the last id.  For a host that lets the device regular
+// corrector keep the lists (density centre, core.f).
+void nb6_irr_lists_get_(int *a0, int *n, int *ls, int *out) { lists_get_impl(*a0, *n, *ls, out); }
 
 }  // extern "C"

@@ -38,6 +38,7 @@ ABI_SYMBOLS = (
     "nb6_state_close_",
     "nb6_fp32_peak_probe_",
     "nb6_regf_noalloc_",
+    "nb6_hermite_adjust_", "nb6_irr_lists_get_",
 )
 
 _LIB: C.CDLL | None = None

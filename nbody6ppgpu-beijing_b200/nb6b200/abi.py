@@ -230,6 +230,41 @@ class ForceLib:
         self.lib.nb6_irr_correct_(_cd(time), _ci(addr.shape[0]), _ip(addr), _dp(out))
         return out[:addr.shape[0]]
 
+    def regf_correct(self, time: float, addr, iseg, seg_j0, seg_a0, h2, dtr, rs, xi, vi, lmax: int,
+                     nnbmax: int, m_flag: int, prm) -> np.ndarray:
+        """nb6_regf_correct_ (extension): regular force and regular corrector
+        of the bodies addr (1-based, grouped by segment iseg) on the device,
+        after irr_predict_send; rows (ni, 32)."""
+        addr = np.ascontiguousarray(addr, dtype=np.int32)
+        ni = addr.shape[0]
+        iseg = np.ascontiguousarray(iseg, dtype=np.int32)
+        seg_j0 = np.ascontiguousarray(seg_j0, dtype=np.int32)
+        seg_a0 = np.ascontiguousarray(seg_a0, dtype=np.int32)
+        h2, dtr, rs = _f64(h2), _f64(dtr), _f64(rs)
+        xi, vi = _f64(xi, (ni, 3)), _f64(vi, (ni, 3))
+        prm = _f64(prm)
+        out = np.zeros((max(ni, 1), 32))
+        self.lib.nb6_regf_correct_(_cd(time), _ci(ni), _ip(addr), _ip(iseg), _ci(seg_a0.shape[0]),
+                                   _ip(seg_j0), _ip(seg_a0), _dp(h2), _dp(dtr), _dp(rs), _dp(xi), _dp(vi),
+                                   _ci(lmax), _ci(nnbmax), _ci(m_flag), _dp(prm), _dp(out))
+        return out[:ni]
+
+    def hermite_adjust(self, nb_flag: int, a0, par) -> None:
+        """nb6_hermite_adjust_ (extension): the Ahmad-Cohen rule's form and
+        per-cluster quantities (RDENS[3], RSCALE, RC2, RSFAC, BODYM, 0) for
+        the device regular corrector; cluster c = addresses [a0[c], a0[c+1])."""
+        a0 = np.ascontiguousarray(a0, dtype=np.int32)
+        par = _f64(par).reshape(-1)
+        ncl = a0.shape[0] - 1
+        self.lib.nb6_hermite_adjust_(_ci(nb_flag), _ci(ncl), _ip(a0), _dp(par if par.size else np.zeros(8)))
+
+    def lists_get(self, a0: int, n: int, ls: int) -> np.ndarray:
+        """nb6_irr_lists_get_ (extension): resident neighbour rows (n, ls),
+        [nnb, 1-based ids]."""
+        out = np.zeros((max(n, 1), ls), dtype=np.int32)
+        self.lib.nb6_irr_lists_get_(_ci(a0), _ci(n), _ci(ls), _ip(out))
+        return out[:n]
+
     def blocks_run(self, tlimit: float, max_blocks: int) -> dict:
         """nb6_blocks_run_: blocks of irregular steps on the device."""
         reason, nact = C.c_int(0), C.c_int(0)
@@ -277,11 +312,20 @@ class ForceLib:
         cmp = cm if npair else np.zeros(1, dtype=np.int32)
         self.lib.nb6_ks_set_(_ci(npair), _ip(cmp), _dp(xk), _dp(vk), _dp(mk), _ip(pofs), _ip(plist))
 
-    def irr_firr_vec(self, ti: float, addr) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    def irr_firr_vec(self, ti: float, addr, out=None) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+        """irr_simd_firr_vec_: (acc, jrk, nnbid) of the bodies addr (1-based).
+        out: optional (acc (ni, 3), jrk (ni, 3), nnbid (ni,) int32) arrays to
+        fill, as a Fortran caller passes its own static arrays."""
         addr = np.ascontiguousarray(addr, dtype=np.int32)
         ni = addr.shape[0]
-        acc = np.zeros((max(ni, 1), 3))
-        jrk = np.zeros((max(ni, 1), 3))
-        nnbid = np.zeros(max(ni, 1), dtype=np.int32)
+        if out is None:
+            acc = np.zeros((max(ni, 1), 3))
+            jrk = np.zeros((max(ni, 1), 3))
+            nnbid = np.zeros(max(ni, 1), dtype=np.int32)
+        else:
+            acc, jrk, nnbid = out
+            assert acc.dtype == np.float64 and jrk.dtype == np.float64 and nnbid.dtype == np.int32
+            assert acc.flags.c_contiguous and jrk.flags.c_contiguous and nnbid.flags.c_contiguous
+            assert acc.shape[0] >= ni and jrk.shape[0] >= ni and nnbid.shape[0] >= ni
         self.lib.irr_simd_firr_vec_(_cd(ti), _ci(ni), _ip(addr), _dp(acc), _dp(jrk), _ip(nnbid))
         return acc[:ni], jrk[:ni], nnbid[:ni]
