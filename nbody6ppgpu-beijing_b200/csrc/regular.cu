@@ -31,6 +31,7 @@
 #include <algorithm>
 #include <climits>
 #include <map>
+#include <mutex>
 #include <vector>
 #include <math.h>
 #include <string.h>
@@ -849,58 +850,145 @@ __global__ void __launch_bounds__(NT, X2_MINB / NI) regf_x2_kernel(const RegArgs
 // in FP64 and written as (hi, lo) slice partials for regf_finalize.
 constexpr int JPAR_NT = 256;
 
-template <int IB, bool MFLAG>
-__global__ void __launch_bounds__(JPAR_NT) regf_jpar_kernel(const RegArgs a) {
-    __shared__ float4 sip[IB][3];
-    __shared__ double red[JPAR_NT / 32][IB][7];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int i0 = blockIdx.x * IB;
-    if (tid < IB) {
-        const int i = i0 + tid;
-        float4 p = make_float4(0.f, 0.f, 0.f, 0.f), q = p, r = p;  // padding: never a candidate
-        if (i < a.ni) {
-            split_hl(a.ix[3 * i], p.x, q.x);
-            split_hl(a.ix[3 * i + 1], p.y, q.y);
-            split_hl(a.ix[3 * i + 2], p.z, q.z);
-            p.w = (float)a.ih2[i] * CAND_SLACK;
-            q.w = (float)a.idtr[i];
-            r = make_float4((float)a.iv[3 * i], (float)a.iv[3 * i + 1], (float)a.iv[3 * i + 2], 0.f);
-        }
-        sip[tid][0] = p;
-        sip[tid][1] = q;
-        sip[tid][2] = r;
+// The i-particles of a j-parallel CTA in shared memory: sip[k] = (xH, yH, zH,
+// 1.01 h2), (xL, yL, zL, dtr), (vx, vy, vz, 0) of particle k, and, for the
+// packed loop, the same data as IP2 pairs (particles 2p and 2p+1 in the two
+// lanes, negated as pair_x2 takes them).  Padding particles (k >= nvalid)
+// have h2 = 0: never a candidate, results unused.
+template <int IB> struct JparI {
+    float4 sip[IB][3];
+    IP2 sip2[IB > 1 ? IB / 2 : 1];
+};
+
+template <int IB, bool X2>
+NB6_DEV void jpar_stage_i(const RegArgs &a, JparI<IB> &S, int i0, int nvalid) {
+    const int k = threadIdx.x;
+    if (k >= IB) return;
+    float4 p = make_float4(0.f, 0.f, 0.f, 0.f), q = p, r = p;
+    if (k < nvalid) {
+        const int i = i0 + k;
+        split_hl(a.ix[3 * i], p.x, q.x);
+        split_hl(a.ix[3 * i + 1], p.y, q.y);
+        split_hl(a.ix[3 * i + 2], p.z, q.z);
+        p.w = (float)a.ih2[i] * CAND_SLACK;
+        q.w = (float)a.idtr[i];
+        r = make_float4((float)a.iv[3 * i], (float)a.iv[3 * i + 1], (float)a.iv[3 * i + 2], 0.f);
     }
-    __syncthreads();
-    const int j_begin = (int)(((long long)blockIdx.y * a.nj) / a.nslices);
-    const int j_end = (int)(((long long)(blockIdx.y + 1) * a.nj) / a.nslices);
-    Sums s[IB];
+    S.sip[k][0] = p;
+    S.sip[k][1] = q;
+    S.sip[k][2] = r;
+    if constexpr (X2 && IB > 1) {
+        IP2 &d = S.sip2[k >> 1];
+        float *l = reinterpret_cast<float *>(&d) + (k & 1);  // lane k & 1 of every float2
+        const float v[11] = {-p.x, -p.y, -p.z, -q.x, -q.y, -q.z, -r.x, -r.y, -r.z, p.w, q.w};
 #pragma unroll
-    for (int k = 0; k < IB; ++k) zero(s[k]);
-    for (int j = j_begin + tid; j < j_end; j += JPAR_NT) {
-        const float4 pa = __ldg(a.posH + j);
-        const float4 pb = __ldg(a.posL + j);
-        const float4 pc = __ldg(a.vel + j);
-        bool any = false;
+        for (int c = 0; c < 11; ++c) l[2 * c] = v[c];
+    }
+}
+
+// The j-parallel inner loop: this thread's j's of [j_begin, j_end) against
+// the IB staged i-particles, results into s[k] (scaled as reg_pair keeps
+// them).  X2 (IB >= 2): two i-particles per f32x2 instruction (pair_x2 on
+// IP2 pairs, the j operands duplicated into both lanes).  pair_x2 is
+// reg_pair operation for operation and each lane accumulates its particle's
+// pairs in the same j order, and the rare path subtracts reg_exact's exact
+// contribution from the (negated) lane sum at the same point of the
+// sequence, so both forms give the same bits.
+template <int IB, bool MFLAG, bool X2>
+NB6_DEV void jpar_loop(const RegArgs &a, const JparI<IB> &S, int j_begin, int j_end, int i0, int nvalid,
+                       int jbase, Sums *s) {
+    if constexpr (X2 && IB > 1) {
+        constexpr int NP = IB / 2;
+        S2 acc[NP];
+#pragma unroll
+        for (int p = 0; p < NP; ++p) zero2(acc[p]);
+        for (int j = j_begin + (int)threadIdx.x; j < j_end; j += JPAR_NT) {
+            const float4 pa = __ldg(a.posH + j);
+            const float4 pb = __ldg(a.posL + j);
+            const float4 pc = __ldg(a.vel + j);
+            unsigned cm = 0u;
+#pragma unroll
+            for (int p = 0; p < NP; ++p) {
+                const IP2 ip = S.sip2[p];
+                cm |= pair_x2<MFLAG>(ip, dup2(pa.x), dup2(pa.y), dup2(pa.z), dup2(pa.w), dup2(pb.x),
+                                     dup2(pb.y), dup2(pb.z), dup2(pc.x), dup2(pc.y), dup2(pc.z), acc[p])
+                      << (2 * p);
+            }
+            if (cm) {
+                // unrolled: acc stays in registers (a dynamic index into it
+                // would put the array in local memory)
+#pragma unroll
+                for (int k = 0; k < IB; ++k) {
+                    if (k >= nvalid || !((cm >> k) & 1u)) continue;
+                    Sums t;
+                    zero(t);
+                    reg_exact<MFLAG>(a, i0 + k, j, t, jbase);
+                    S2 &q = acc[k >> 1];
+                    if (k & 1) {
+                        q.ax.y -= t.ax; q.ay.y -= t.ay; q.az.y -= t.az;
+                        q.jx.y -= t.jx; q.jy.y -= t.jy; q.jz.y -= t.jz; q.po.y -= t.po;
+                    } else {
+                        q.ax.x -= t.ax; q.ay.x -= t.ay; q.az.x -= t.az;
+                        q.jx.x -= t.jx; q.jy.x -= t.jy; q.jz.x -= t.jz; q.po.x -= t.po;
+                    }
+                }
+            }
+        }
 #pragma unroll
         for (int k = 0; k < IB; ++k) {
-            const float4 p = sip[k][0], q = sip[k][1], r = sip[k][2];
-            IPart ip;
-            ip.xh = p.x; ip.yh = p.y; ip.zh = p.z; ip.h2c = p.w;
-            ip.xl = q.x; ip.yl = q.y; ip.zl = q.z; ip.dt = q.w;
-            ip.vx = r.x; ip.vy = r.y; ip.vz = r.z;
-            any |= reg_pair<MFLAG>(ip, pa, pb, pc, s[k]);
+            const S2 &q = acc[k >> 1];
+            const bool hi = k & 1;
+            s[k].ax = -(hi ? q.ax.y : q.ax.x);
+            s[k].ay = -(hi ? q.ay.y : q.ay.x);
+            s[k].az = -(hi ? q.az.y : q.az.x);
+            s[k].jx = -(hi ? q.jx.y : q.jx.x);
+            s[k].jy = -(hi ? q.jy.y : q.jy.x);
+            s[k].jz = -(hi ? q.jz.y : q.jz.x);
+            s[k].po = -(hi ? q.po.y : q.po.x);
         }
-        if (any) {
+    } else {
+#pragma unroll
+        for (int k = 0; k < IB; ++k) zero(s[k]);
+        for (int j = j_begin + (int)threadIdx.x; j < j_end; j += JPAR_NT) {
+            const float4 pa = __ldg(a.posH + j);
+            const float4 pb = __ldg(a.posL + j);
+            const float4 pc = __ldg(a.vel + j);
+            bool any = false;
+#pragma unroll
             for (int k = 0; k < IB; ++k) {
-                const float4 p = sip[k][0], q = sip[k][1], r = sip[k][2];
+                const float4 p = S.sip[k][0], q = S.sip[k][1], r = S.sip[k][2];
                 IPart ip;
                 ip.xh = p.x; ip.yh = p.y; ip.zh = p.z; ip.h2c = p.w;
                 ip.xl = q.x; ip.yl = q.y; ip.zl = q.z; ip.dt = q.w;
                 ip.vx = r.x; ip.vy = r.y; ip.vz = r.z;
-                if (reg_geom<MFLAG>(ip, pa, pb, pc).cand) reg_exact<MFLAG>(a, i0 + k, j, s[k]);
+                any |= reg_pair<MFLAG>(ip, pa, pb, pc, s[k]);
+            }
+            if (any) {
+                for (int k = 0; k < IB && k < nvalid; ++k) {
+                    const float4 p = S.sip[k][0], q = S.sip[k][1], r = S.sip[k][2];
+                    IPart ip;
+                    ip.xh = p.x; ip.yh = p.y; ip.zh = p.z; ip.h2c = p.w;
+                    ip.xl = q.x; ip.yl = q.y; ip.zl = q.z; ip.dt = q.w;
+                    ip.vx = r.x; ip.vy = r.y; ip.vz = r.z;
+                    if (reg_geom<MFLAG>(ip, pa, pb, pc).cand) reg_exact<MFLAG>(a, i0 + k, j, s[k], jbase);
+                }
             }
         }
     }
+}
+
+template <int IB, bool MFLAG, bool X2 = false>
+__global__ void __launch_bounds__(JPAR_NT) regf_jpar_kernel(const RegArgs a) {
+    __shared__ __align__(16) JparI<IB> S;
+    __shared__ double red[JPAR_NT / 32][IB][7];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int i0 = blockIdx.x * IB;
+    jpar_stage_i<IB, X2>(a, S, i0, a.ni - i0);
+    __syncthreads();
+    const int j_begin = (int)(((long long)blockIdx.y * a.nj) / a.nslices);
+    const int j_end = (int)(((long long)(blockIdx.y + 1) * a.nj) / a.nslices);
+    Sums s[IB];
+    jpar_loop<IB, MFLAG, X2>(a, S, j_begin, j_end, i0, a.ni - i0, 0, s);
     // CTA reduction in FP64: warp shuffles, then across warps in shared memory
 #pragma unroll
     for (int k = 0; k < IB; ++k) {
@@ -1057,61 +1145,21 @@ struct SegItem {
     int i0, ni, j0, j1, jbase, q, pad0, pad1;
 };
 
-template <int IB, bool MFLAG>
+template <int IB, bool MFLAG, bool X2 = false>
 __global__ void __launch_bounds__(JPAR_NT)
     regf_seg_kernel(const RegArgs a, const SegItem *__restrict__ items, const int *__restrict__ nitems_p,
                     const int2 *__restrict__ pinfo) {
-    __shared__ float4 sip[IB][3];
+    __shared__ __align__(16) JparI<IB> S;
     __shared__ double red[JPAR_NT / 32][IB][7];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nitems = *nitems_p;
     for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
         const SegItem it = items[w];
-        __syncthreads();  // the previous item is done with sip and red
-        if (tid < IB) {
-            float4 p = make_float4(0.f, 0.f, 0.f, 0.f), q = p, r = p;  // padding: never a candidate
-            if (tid < it.ni) {
-                const int i = it.i0 + tid;
-                split_hl(a.ix[3 * i], p.x, q.x);
-                split_hl(a.ix[3 * i + 1], p.y, q.y);
-                split_hl(a.ix[3 * i + 2], p.z, q.z);
-                p.w = (float)a.ih2[i] * CAND_SLACK;
-                q.w = (float)a.idtr[i];
-                r = make_float4((float)a.iv[3 * i], (float)a.iv[3 * i + 1], (float)a.iv[3 * i + 2], 0.f);
-            }
-            sip[tid][0] = p;
-            sip[tid][1] = q;
-            sip[tid][2] = r;
-        }
+        __syncthreads();  // the previous item is done with the staged i and red
+        jpar_stage_i<IB, X2>(a, S, it.i0, it.ni);
         __syncthreads();
         Sums s[IB];
-#pragma unroll
-        for (int k = 0; k < IB; ++k) zero(s[k]);
-        for (int j = it.j0 + tid; j < it.j1; j += JPAR_NT) {
-            const float4 pa = __ldg(a.posH + j);
-            const float4 pb = __ldg(a.posL + j);
-            const float4 pc = __ldg(a.vel + j);
-            bool any = false;
-#pragma unroll
-            for (int k = 0; k < IB; ++k) {
-                const float4 p = sip[k][0], q = sip[k][1], r = sip[k][2];
-                IPart ip;
-                ip.xh = p.x; ip.yh = p.y; ip.zh = p.z; ip.h2c = p.w;
-                ip.xl = q.x; ip.yl = q.y; ip.zl = q.z; ip.dt = q.w;
-                ip.vx = r.x; ip.vy = r.y; ip.vz = r.z;
-                any |= reg_pair<MFLAG>(ip, pa, pb, pc, s[k]);
-            }
-            if (any) {
-                for (int k = 0; k < it.ni && k < IB; ++k) {
-                    const float4 p = sip[k][0], q = sip[k][1], r = sip[k][2];
-                    IPart ip;
-                    ip.xh = p.x; ip.yh = p.y; ip.zh = p.z; ip.h2c = p.w;
-                    ip.xl = q.x; ip.yl = q.y; ip.zl = q.z; ip.dt = q.w;
-                    ip.vx = r.x; ip.vy = r.y; ip.vz = r.z;
-                    if (reg_geom<MFLAG>(ip, pa, pb, pc).cand) reg_exact<MFLAG>(a, it.i0 + k, j, s[k], it.jbase);
-                }
-            }
-        }
+        jpar_loop<IB, MFLAG, X2>(a, S, it.j0, it.j1, it.i0, it.ni, it.jbase, s);
 #pragma unroll
         for (int k = 0; k < IB; ++k) {
             double v[7] = {s[k].ax, s[k].ay, s[k].az, s[k].jx, s[k].jy, s[k].jz, s[k].po};
@@ -1287,6 +1335,17 @@ bool valid_variant(int v) {
 
 int i_per_thread(int v) { return v == 13 ? 1 : v > 10 ? v - 10 : v; }
 
+// The j-parallel and segmented kernels with two or more i per CTA run the
+// packed (f32x2) inner loop; NB6_JPAR_X2=0 in the environment selects the
+// scalar loop (the same bits, for comparison).
+bool jpar_x2() {
+    static const bool on = [] {
+        const char *e = getenv("NB6_JPAR_X2");
+        return !(e && atoi(e) == 0);
+    }();
+    return on;
+}
+
 template <bool MF> int occupancy_t(int variant) {
     switch (variant) {
         case 1: return occ_of(regf_kernel<1, MF>, NT);
@@ -1296,9 +1355,9 @@ template <bool MF> int occupancy_t(int variant) {
         case 12: return occ_of(regf_x2_kernel<2, MF>, NT);
         case 13: return occ_of(regf_x2_kernel<1, MF, true>, NT);
         case -1: return occ_of(regf_jpar_kernel<1, MF>, JPAR_NT);
-        case -2: return occ_of(regf_jpar_kernel<2, MF>, JPAR_NT);
-        case -4: return occ_of(regf_jpar_kernel<4, MF>, JPAR_NT);
-        default: return occ_of(regf_jpar_kernel<8, MF>, JPAR_NT);
+        case -2: return jpar_x2() ? occ_of(regf_jpar_kernel<2, MF, true>, JPAR_NT) : occ_of(regf_jpar_kernel<2, MF>, JPAR_NT);
+        case -4: return jpar_x2() ? occ_of(regf_jpar_kernel<4, MF, true>, JPAR_NT) : occ_of(regf_jpar_kernel<4, MF>, JPAR_NT);
+        default: return jpar_x2() ? occ_of(regf_jpar_kernel<8, MF, true>, JPAR_NT) : occ_of(regf_jpar_kernel<8, MF>, JPAR_NT);
     }
 }
 
@@ -1354,9 +1413,18 @@ template <bool MF> void launch_plan(const Plan &p, const RegArgs &a, cudaStream_
         case 12: regf_x2_kernel<2, MF><<<grid, NT, 0, st>>>(a); break;
         case 13: regf_x2_kernel<1, MF, true><<<grid, NT, 0, st>>>(a); break;
         case -1: regf_jpar_kernel<1, MF><<<grid, JPAR_NT, 0, st>>>(a); break;
-        case -2: regf_jpar_kernel<2, MF><<<grid, JPAR_NT, 0, st>>>(a); break;
-        case -4: regf_jpar_kernel<4, MF><<<grid, JPAR_NT, 0, st>>>(a); break;
-        default: regf_jpar_kernel<8, MF><<<grid, JPAR_NT, 0, st>>>(a); break;
+        case -2:
+            if (jpar_x2()) regf_jpar_kernel<2, MF, true><<<grid, JPAR_NT, 0, st>>>(a);
+            else regf_jpar_kernel<2, MF><<<grid, JPAR_NT, 0, st>>>(a);
+            break;
+        case -4:
+            if (jpar_x2()) regf_jpar_kernel<4, MF, true><<<grid, JPAR_NT, 0, st>>>(a);
+            else regf_jpar_kernel<4, MF><<<grid, JPAR_NT, 0, st>>>(a);
+            break;
+        default:
+            if (jpar_x2()) regf_jpar_kernel<8, MF, true><<<grid, JPAR_NT, 0, st>>>(a);
+            else regf_jpar_kernel<8, MF><<<grid, JPAR_NT, 0, st>>>(a);
+            break;
     }
 }
 
@@ -1370,9 +1438,9 @@ template <bool MF> const void *kernel_of(int variant) {
         case 12: return (const void *)regf_x2_kernel<2, MF>;
         case 13: return (const void *)regf_x2_kernel<1, MF, true>;
         case -1: return (const void *)regf_jpar_kernel<1, MF>;
-        case -2: return (const void *)regf_jpar_kernel<2, MF>;
-        case -4: return (const void *)regf_jpar_kernel<4, MF>;
-        default: return (const void *)regf_jpar_kernel<8, MF>;
+        case -2: return jpar_x2() ? (const void *)regf_jpar_kernel<2, MF, true> : (const void *)regf_jpar_kernel<2, MF>;
+        case -4: return jpar_x2() ? (const void *)regf_jpar_kernel<4, MF, true> : (const void *)regf_jpar_kernel<4, MF>;
+        default: return jpar_x2() ? (const void *)regf_jpar_kernel<8, MF, true> : (const void *)regf_jpar_kernel<8, MF>;
     }
 }
 
@@ -1689,6 +1757,20 @@ struct FinArgs {
     }
 };
 
+// The neighbour counters of ni rows.  A new buffer is cleared over its
+// whole capacity: the kernels count into rows [0, ni) of every call and
+// regf_finalize resets the rows it reads, so rows beyond the calls so far
+// must start at zero too (a later, larger call reads them without a
+// clear).  Returns whether the buffer was replaced.
+static bool nbcnt_reserve(int ni, cudaStream_t st) {
+    const int *before = R.nbcnt.ptr;
+    const size_t cap_before = R.nbcnt.cap;
+    R.nbcnt.reserve(ni);
+    if (R.nbcnt.ptr == before && R.nbcnt.cap == cap_before) return false;
+    NB6_CUDA_CHECK(cudaMemsetAsync(R.nbcnt.ptr, 0, sizeof(int) * R.nbcnt.cap, st));
+    return true;
+}
+
 static void regf_prepare(int ni, const double *d_h2, const double *d_dtr, const double *d_x,
                          const double *d_v, int lmax, int nnbmax, int mflag, cudaStream_t st,
                          RegLaunch &L) {
@@ -1739,10 +1821,7 @@ static void regf_prepare(int ni, const double *d_h2, const double *d_dtr, const 
         for (int c = 0; c < ncand; ++c)
             part_need = std::max<size_t>(part_need, (size_t)make_plan(cands[c], nt, R.nj, R.ntile, mf, 0).nslices * nt);
     R.part.reserve(part_need * 4);
-    const int *cnt_before = R.nbcnt.ptr;
-    const size_t cnt_cap_before = R.nbcnt.cap;
-    R.nbcnt.reserve(ni);
-    if (R.nbcnt.ptr != cnt_before || R.nbcnt.cap != cnt_cap_before) R.nbcnt_dirty = true;
+    nbcnt_reserve(ni, st);
     R.nbbuf.reserve((size_t)ni * std::max(cap, 1));
     R.outf.reserve((size_t)ni * 8);
     R.outl.reserve((size_t)ni * W);
@@ -1901,7 +1980,7 @@ static void regf_copy_out(const RegLaunch &L, cudaStream_t st) {
 static void regf_eager(const RegLaunch &L, cudaStream_t st) {
     if (L.hin)
         NB6_CUDA_CHECK(cudaMemcpyAsync(R.iin.ptr, L.hin, L.in_bytes, cudaMemcpyHostToDevice, st));
-    NB6_CUDA_CHECK(cudaMemsetAsync(R.nbcnt.ptr, 0, sizeof(int) * L.ni, st));
+    NB6_CUDA_CHECK(cudaMemsetAsync(R.nbcnt.ptr, 0, sizeof(int) * (R.nbcnt_dirty ? R.nbcnt.cap : (size_t)L.ni), st));
     // kernel-only timing of the main force kernel (read by
     // nb6_regf_last_kernel_ms_ after the stream has drained)
     NB6_CUDA_CHECK(cudaEventRecord(R.ev0, st));
@@ -2025,7 +2104,9 @@ static void regf_submit(const RegLaunch &L, cudaStream_t st) {
     RegState::Graph &G = R.graph[L.hin ? 1 : 0];
     bool ok = G.x ? graph_update(G, L) : graph_build(G, L);
     if (ok) {
-        if (R.nbcnt_dirty) NB6_CUDA_CHECK(cudaMemsetAsync(R.nbcnt.ptr, 0, sizeof(int) * L.ni, st));
+        // (a call that failed or the tuner's trials may have left any row
+        // counted: clear them all)
+        if (R.nbcnt_dirty) NB6_CUDA_CHECK(cudaMemsetAsync(R.nbcnt.ptr, 0, sizeof(int) * R.nbcnt.cap, st));
         ok = cudaGraphLaunch(G.x, st) == cudaSuccess;
     }
     if (!ok) {
@@ -2266,9 +2347,9 @@ static bool g_seg_keep_device = false;
 template <bool MF> static const void *seg_kernel_of(int ib) {
     switch (ib) {
         case 1: return (const void *)regf_seg_kernel<1, MF>;
-        case 2: return (const void *)regf_seg_kernel<2, MF>;
-        case 4: return (const void *)regf_seg_kernel<4, MF>;
-        default: return (const void *)regf_seg_kernel<8, MF>;
+        case 2: return jpar_x2() ? (const void *)regf_seg_kernel<2, MF, true> : (const void *)regf_seg_kernel<2, MF>;
+        case 4: return jpar_x2() ? (const void *)regf_seg_kernel<4, MF, true> : (const void *)regf_seg_kernel<4, MF>;
+        default: return jpar_x2() ? (const void *)regf_seg_kernel<8, MF, true> : (const void *)regf_seg_kernel<8, MF>;
     }
 }
 
@@ -2288,7 +2369,8 @@ static int seg_occupancy(int ib, bool mf) {
 template <int IB, bool MF>
 static void launch_seg_t(int grid, const RegArgs &a, const SegItem *items, const int *nit,
                          const int2 *pinfo, cudaStream_t st) {
-    regf_seg_kernel<IB, MF><<<grid, JPAR_NT, 0, st>>>(a, items, nit, pinfo);
+    if (IB > 1 && jpar_x2()) regf_seg_kernel<IB, MF, true><<<grid, JPAR_NT, 0, st>>>(a, items, nit, pinfo);
+    else regf_seg_kernel<IB, MF><<<grid, JPAR_NT, 0, st>>>(a, items, nit, pinfo);
 }
 
 static void launch_seg(int ib, bool mf, int grid, const RegArgs &a, const SegItem *items, const int *nit,
@@ -2529,7 +2611,7 @@ void nb6_regf_seg_(int *ni_, int *iseg, double *h2, double *dtr, double (*xi)[3]
     const int2 *d_pinfo = reinterpret_cast<const int2 *>(R.dseg.ptr + 4 + (size_t)8 * nitems);
 
     R.part.reserve((size_t)std::max<long long>(slots, 1) * 4);
-    R.nbcnt.reserve(ni);
+    nbcnt_reserve(ni, st);
     R.nbbuf.reserve((size_t)ni * std::max(cap, 1));
     R.outf.reserve((size_t)ni * 8);
     R.outl.reserve((size_t)ni * W);
@@ -2947,10 +3029,13 @@ __global__ void __launch_bounds__(FIN_WARPS * 32)
 }
 
 // Device address of the scratch array, looked up once per device (up to 64
-// devices) with that device current.
+// devices) with that device current.  The lookup is serialised, so host
+// threads making their first calls at the same time all get the address.
 unsigned char *na_scratch_address(int dev) {
     static unsigned char *addr[64] = {nullptr};
+    static std::mutex mu;
     if (dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lock(mu);
     if (!addr[dev]) {
         void *p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, nb6_noalloc_scratch);
@@ -3023,7 +3108,12 @@ void nb6_regf_noalloc_(int *nj_, const double *d_mj, const double *d_xj, const d
     a.lcap = std::max(cap, 1);
     a.part = reinterpret_cast<float4 *>(base + NA_OFF_PART);
     const int igroups = (ni + NA_IB - 1) / NA_IB;
-    a.nslices = std::max(1, std::min(std::min(2 * sms / igroups, nj / (JPAR_NT * 4)), NA_SLICES_MAX));
+    // Two waves of CTAs, and at most 64 j per thread and slice: each
+    // thread's FP32 sums then cover as few pairs as a tile of the other
+    // kernels before they reach FP64 (up to 2M j within NA_SLICES_MAX).
+    const int by_waves = std::min(2 * sms / igroups, nj / (JPAR_NT * 4));
+    const int by_sums = (int)(((long long)nj + JPAR_NT * 64 - 1) / (JPAR_NT * 64));
+    a.nslices = std::max(1, std::min(std::max(by_waves, by_sums), NA_SLICES_MAX));
 
     na_clear_counts<<<(ni + 255) / 256, 256, 0, st>>>(a.nbcnt, ni);
     dim3 grid(igroups, a.nslices);

@@ -293,3 +293,41 @@ def test_regular_spatial_order_matches_caller_order(nb6, orc):
                 check_vs_oracle(orc, inp, run_gpu(nb6, **inp))
     finally:
         raw.nb6_regf_jsort_(C.byref(C.c_int(1)))
+
+
+def test_regular_counts_stay_clean_across_growing_calls(nb6, orc):
+    """Neighbour counters of rows beyond every earlier call start at zero: a
+    segmented call, a close and a re-open leave the device memory the next
+    counter buffer comes from in use before; then calls of growing ni on the
+    j-parallel kernels (every row's count is exact, overflowed rows give the
+    oracle's -nnb) must match the oracle row for row."""
+    import ctypes as C
+    from nb6b200 import ics
+    raw = nb6.lib
+    ens = [ics.plummer(3000, seed=s) for s in (1, 2)]
+    m = np.concatenate([c.mass for c in ens])
+    x = np.concatenate([c.pos for c in ens])
+    v = np.concatenate([c.vel for c in ens])
+    rs = np.concatenate([c.rs for c in ens])
+    dtr = np.concatenate([c.dtr for c in ens])
+    iseg = np.repeat([0, 1], 3000).astype(np.int32)
+    nb6.gpunb_open(6010, 0)
+    try:
+        nb6.gpunb_send(m, x, v)
+        nb6.regf_seg(rs ** 2, dtr, x, v, iseg, np.array([0, 3000, 6000], dtype=np.int32), 512, 400, 0)
+    finally:
+        nb6.gpunb_close()
+    cl = ics.plummer(40000, seed=6)
+    h2 = (cl.rs * 2.0) ** 2          # large radii: hundreds of neighbours, some rows overflow
+    nb6.gpunb_open(cl.n + 10, 0)
+    try:
+        nb6.gpunb_send(cl.mass, cl.pos, cl.vel)
+        for ni, var in ((2, -2), (4, -4), (8, -8), (64, -8), (16, -4), (200, -8)):
+            raw.nb6_regf_tune_(C.byref(C.c_int(var)), C.byref(C.c_int(0)))
+            sel = np.arange(100, 100 + ni)
+            got = nb6.gpunb_regf(h2[sel], cl.dtr[sel], cl.pos[sel], cl.vel[sel], 512, 400, 0)
+            want = orc.regf(cl.mass, cl.pos, cl.vel, h2[sel], cl.dtr[sel], cl.pos[sel], cl.vel[sel], 512, 400, 0)
+            np.testing.assert_array_equal(got[3][:, 0], want[3][:, 0], err_msg=f"ni={ni}")
+    finally:
+        raw.nb6_regf_tune_(C.byref(C.c_int(0)), C.byref(C.c_int(0)))
+        nb6.gpunb_close()
