@@ -73,6 +73,13 @@ def parse():
     ap.add_argument("--no-pot", action="store_true", help="skip the N^2 potential leg")
     ap.add_argument("--no-irr", action="store_true", help="skip the irregular-force leg")
     ap.add_argument("--no-pred", action="store_true", help="skip the Hermite predictor leg")
+    ap.add_argument("--no-err", action="store_true", help="skip the error check against the FP64 oracle")
+    ap.add_argument("--no-northstar", action="store_true",
+                    help="skip the config 3/4 driver leg (plain GPU method vs batched device form)")
+    ap.add_argument("--ns-t3", type=float, default=1.0 / 64, help="config 3 end time")
+    ap.add_argument("--ns-t4", type=float, default=1.0, help="config 4 end time")
+    ap.add_argument("--ns-clusters", type=int, default=256)
+    ap.add_argument("--ns-alone", type=int, default=8, help="config 4 clusters run alone")
     ap.add_argument("--seed", type=int, default=20260)
     return ap.parse_args()
 
@@ -167,6 +174,28 @@ def whole_job_rate(world: int, pairs_per_step: float, steps: int, total_ms_max: 
     """Pairs per second of the whole job: every rank runs its own replica of
     the workload (weak scaling), timed by the slowest rank."""
     return world * pairs_per_step * steps / (total_ms_max * 1e-3)
+
+
+def bench_config(args, n: int, world: int) -> dict:
+    """The workload description shared by both arms' JSON lines."""
+    return {"workload": f"king-w0=6 N={args.n} ({n} c.m. bodies), full regular "
+                        f"evaluation in {args.chunk}-i calls",
+            "n_bodies": n, "chunk": args.chunk, "calls_per_step": (n + args.chunk - 1) // args.chunk,
+            "nnbopt": 50, "nnbmax": args.nnbmax, "lmax": args.lmax,
+            "m_flag": args.m_flag, "parallelism": f"replicas x{world}",
+            "l2": "flushed (256 MiB write) between timed steps"}
+
+
+def cpu_model() -> str:
+    """The host CPU's model name (lscpu), for the CPU baselines."""
+    try:
+        out = subprocess.run(["lscpu"], capture_output=True, text=True, timeout=20).stdout
+        for ln in out.splitlines():
+            if ln.startswith("Model name:"):
+                return ln.split(":", 1)[1].strip()
+    except (OSError, subprocess.SubprocessError):
+        pass
+    return "unknown"
 
 
 def dist_setup(args):
@@ -340,11 +369,15 @@ def irregular_leg(lib, m, x, v, h2, dtr, args, nsample: int = 65536):
         flib.irr_set_jp_all(x, v, zeros, zeros, m, t0)
         for i in range(ns):
             flib.irr_set_list(i + 1, rows[i])
-        flib.irr_firr_vec(0.0, addr)               # uploads the staged state
+        # the caller's own result arrays (a Fortran caller's static FIRR,
+        # FD and neighbour-id arrays), reused call after call
+        out = (np.zeros((ns, 3)), np.zeros((ns, 3)), np.zeros(ns, dtype=np.int32))
+        flib.irr_firr_vec(0.0, addr, out)          # uploads the staged state
         t = time.perf_counter()
         for _ in range(reps):
-            res = flib.irr_firr_vec(0.0, addr)
+            res = flib.irr_firr_vec(0.0, addr, out)
         dt = (time.perf_counter() - t) / reps
+        res = tuple(a.copy() for a in res)
         flib.irr_close(0)
         return res, dt
 
@@ -374,6 +407,142 @@ def irregular_leg(lib, m, x, v, h2, dtr, args, nsample: int = 65536):
     return out
 
 
+def northstar_leg(m, x, v, rs, args):
+    """N-body time per wall second of the block-step drivers on this GPU,
+    the plain GPU method against the batched, device-resident form:
+
+    config 3  the bench's King W0=6 cluster (N = 1M, 5% binaries as c.m.
+              bodies), radii from its NNBOPT-th neighbour, to T = args.ns_t3:
+              plain = the single-cluster driver (host prediction and
+              gpunb_send_ per regular block, host correctors, 1024-i
+              gpunb_regf_ calls, util_gpu.F); batched = the ensemble driver
+              with the j set predicted, both correctors and the block clock
+              on the device (dev_corrector 3);
+    config 4  args.ns_clusters Plummer clusters (Kroupa IMF, N log-uniform
+              512-8192) to T = args.ns_t4 as one batched ensemble, against
+              each cluster run alone with the plain method, measured on
+              args.ns_alone clusters spread over the size range and scaled
+              by the ensemble's total N^2 over theirs.
+
+    Wall times are the drivers' own (block loop and energy outputs; the
+    start-up evaluation is reported beside them).  Energy errors are the
+    largest |E(t) - E(0)| / |E(0)| over the outputs, per cluster."""
+    from nb6b200 import drive
+    from nb6b200.ensemble_bench import make_clusters
+    ours = drive.backend_paths("nb6b200")
+    out = {}
+    t3 = args.ns_t3
+    t = time.perf_counter()
+    plain = drive.run(ours, m, x, v, tcrit=t3, dt_out=t3, rs_init=rs)
+    t_plain = time.perf_counter() - t
+    t = time.perf_counter()
+    batch = drive.run_ensemble(ours, [(m, x, v)], batched=True, tcrit=t3, dt_out=t3, rs_init=rs,
+                               dev_corrector=3)
+    t_batch = time.perf_counter() - t
+    wp, wb = plain.stats["wall_total"], batch.stats["wall_total"]
+    out["config3"] = {
+        "workload": f"king-w0=6 N={args.n} ({m.shape[0]} c.m. bodies) to T = {t3}",
+        "plain": {"wall_s": wp, "wall_with_startup_s": t_plain, "nbody_time_per_wall_s": t3 / wp,
+                  "dE": plain.de_max, "reg_calls": plain.stats["reg_calls"],
+                  "reg_steps": plain.stats["reg_steps"], "irr_steps": plain.stats["irr_steps"]},
+        "batched_device": {"wall_s": wb, "wall_with_startup_s": t_batch, "nbody_time_per_wall_s": t3 / wb,
+                           "dE": float(batch.de_max[0]), "reg_calls": batch.stats["reg_calls"],
+                           "reg_steps": batch.stats["reg_steps"], "irr_steps": batch.stats["irr_steps"]},
+        "speedup": wp / wb,
+        "dE_ratio_batched_over_plain": float(batch.de_max[0]) / plain.de_max if plain.de_max > 0 else None}
+    cls = make_clusters(args.ns_clusters)
+    sizes = np.array([c.n for c in cls])
+    t4 = args.ns_t4
+    dt_out = min(t4, 0.25)
+    t = time.perf_counter()
+    ens = drive.run_ensemble(ours, cls, batched=True, tcrit=t4, dt_out=dt_out, dev_corrector=3)
+    t_ens = time.perf_counter() - t
+    order = np.argsort(sizes)
+    pick = order[np.linspace(0, len(cls) - 1, min(args.ns_alone, len(cls))).astype(int)]
+    w_alone, ratios = 0.0, []
+    for c in pick:
+        cl = cls[c]
+        r = drive.run(ours, cl.mass, cl.pos, cl.vel, tcrit=t4, dt_out=dt_out)
+        w_alone += r.stats["wall_total"]
+        ratios.append(float(ens.de_max[c]) / r.de_max if r.de_max > 0 else float("nan"))
+    scale = float((sizes.astype(float) ** 2).sum() / (sizes[pick].astype(float) ** 2).sum())
+    we = ens.stats["wall_total"]
+    out["config4"] = {
+        "workload": f"{len(cls)} Plummer clusters, Kroupa IMF, N log-uniform 512-8192, "
+                    f"total {int(sizes.sum())} bodies, to T = {t4}",
+        "ensemble": {"wall_s": we, "wall_with_startup_s": t_ens, "nbody_time_per_wall_s": t4 / we,
+                     "dE_median": float(np.median(ens.de_max)), "dE_p90": float(np.percentile(ens.de_max, 90))},
+        "alone": {"clusters_run": int(len(pick)), "wall_s_measured": w_alone, "scale_sum_n2": scale,
+                  "wall_s": w_alone * scale, "nbody_time_per_wall_s": t4 / (w_alone * scale)},
+        "speedup": w_alone * scale / we,
+        "dE_ratio_ensemble_over_alone": {"median": float(np.nanmedian(ratios)),
+                                         "max": float(np.nanmax(ratios)), "clusters": len(ratios)}}
+    return out
+
+
+def _rel(a, b):
+    """Per-row relative error |a - b| / |b| (vector rows or scalars)."""
+    if a.ndim == 1:
+        return np.abs(a - b) / np.maximum(np.abs(b), 1e-300)
+    return np.sqrt(((a - b) ** 2).sum(1) / np.maximum((b ** 2).sum(1), 1e-300))
+
+
+def fp64_error_leg(lib, m, x, v, h2, dtr, args, ncalls: int = 16, ncore: int = 2):
+    """Force, jerk and potential error against the FP64 oracle over many
+    calls of the timed shape: `ncalls` of the step's 1024-i calls, evenly
+    spaced over the call sequence (the bodies are in random radial order, so
+    each is a sample of the whole cluster), plus `ncore` calls of the bodies
+    nearest the centre -- the King core, where the near field is densest
+    and the regular force of a body cancels most.  Every i of every call is
+    checked; lists are compared row for row."""
+    import oracle
+    n = m.shape[0]
+    chunks = [(s, min(n, s + args.chunk)) for s in range(0, n, args.chunk)]
+    picks = sorted(set(np.linspace(0, len(chunks) - 1, min(ncalls, len(chunks))).astype(int).tolist()))
+    calls = [("timed", np.arange(*chunks[k])) for k in picks]
+    centre = (m[:, None] * x).sum(0) / m.sum()
+    byr = np.argsort(((x - centre) ** 2).sum(1), kind="stable")
+    for c in range(ncore):
+        calls.append(("core", np.sort(byr[c * args.chunk:(c + 1) * args.chunk])))
+    ea, ej, ep, core_a, core_j = [], [], [], [], []
+    rows_differ, nnb, t_orc = 0, [], 0.0
+    for kind, idx in calls:
+        a_g, j_g, p_g, l_g = lib.gpunb_regf(h2[idx], dtr[idx], x[idx], v[idx], args.lmax,
+                                            args.nnbmax, args.m_flag)
+        t0 = time.perf_counter()
+        a_o, j_o, p_o, l_o = oracle.regf(m, x, v, h2[idx], dtr[idx], x[idx], v[idx],
+                                         args.lmax, args.nnbmax, args.m_flag)
+        t_orc += time.perf_counter() - t0
+        rows_differ += int(np.sum(np.any(l_g != l_o, axis=1)))
+        ok = l_o[:, 0] >= 0
+        ra, rj, rp = _rel(a_g, a_o)[ok], _rel(j_g, j_o)[ok], _rel(p_g, p_o)[ok]
+        ea.append(ra)
+        ej.append(rj)
+        ep.append(rp)
+        nnb.append(l_o[ok, 0])
+        if kind == "core":
+            core_a.append(ra)
+            core_j.append(rj)
+    ea, ej, ep = np.concatenate(ea), np.concatenate(ej), np.concatenate(ep)
+    core_a, core_j = np.concatenate(core_a), np.concatenate(core_j)
+
+    def q(e, p):
+        return float(np.quantile(e, p))
+    return {"calls": len(calls), "timed_calls_checked": len(picks), "core_calls": ncore,
+            "sample_i": int(ea.size),
+            "core_radius_max": float(np.sqrt(((x[byr[ncore * args.chunk - 1]] - centre) ** 2).sum())),
+            "acc_rel_max": float(ea.max()), "acc_rel_p999": q(ea, 0.999),
+            "acc_rel_median": q(ea, 0.5),
+            "jrk_rel_max": float(ej.max()), "jrk_rel_p999": q(ej, 0.999),
+            "jrk_rel_median": q(ej, 0.5),
+            "pot_rel_max": float(ep.max()), "pot_rel_p999": q(ep, 0.999),
+            "core_acc_rel_max": float(core_a.max()), "core_jrk_rel_max": float(core_j.max()),
+            "rows_acc_above_1e-6": int(np.sum(ea > 1e-6)),
+            "lists_identical": rows_differ == 0, "list_rows_differing": rows_differ,
+            "nnb_mean": float(np.concatenate(nnb).mean()),
+            "oracle_s": t_orc}
+
+
 def run_reference(args):
     world, rank, _ = dist_setup(args)
     if rank != 0:
@@ -391,18 +560,20 @@ def run_reference(args):
         rates.append(r)
         times.append(t)
     value = float(np.sum([r * t for r, t in zip(rates, times)]) / np.sum(times))
-    sample = f"{calls} calls x {args.chunk} i x {n} j per step (reg.avx.cpp gpunb_regf_)"
+    sample = (f"{calls} of the step's {(n + args.chunk - 1) // args.chunk} calls (random ones) x "
+              f"{args.chunk} i x {n} j per timed step, reg.avx.cpp gpunb_regf_; the rate is "
+              f"pairs over the time of those calls")
     out = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "pairs/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * float(np.mean(times)), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic King W0=6, Kroupa IMF, 5% binaries as c.m. bodies",
-        "config": {"workload": f"king-w0=6 N={args.n} ({n} c.m. bodies), 1024-i gpunb_regf calls",
-                   "n_bodies": n, "chunk": args.chunk, "nnbmax": args.nnbmax,
-                   "lmax": args.lmax, "m_flag": args.m_flag},
+        "data": "synthetic King W0=6 (seeded), Kroupa IMF 0.08-100 Msun, 5% binaries "
+                "as c.m. bodies, Henon units",
+        "config": bench_config(args, n, args.gpus),
+        "sample": sample,
         "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": threads,
-                         "kind": "reference", "sample": sample},
+                         "cpu": cpu_model(), "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -556,11 +727,9 @@ def main():
                                 C.c_void_p(d_m.data_ptr()), C.c_void_p(d_x.data_ptr()), C.byref(outp))
         pot_ms = float(raw.nb6_pot_last_kernel_ms_())
         pot = {"pairs_per_s": float(n) * n / (pot_ms * 1e-3), "kernel_ms": pot_ms,
-               "flops_per_pair": 27,
-               "frac_fp32_peak": 27.0 * n * n / (pot_ms * 1e-3) / 1e12 / peak_tf,
-               "note": "27 flops per pair is the reference's count (hi/lo differences); "
-                       "the ordered far loop issues 7 FP32 lane operations and one MUFU "
-                       "rsqrt per pair, so the MUFU pipe bounds it",
+               "note": "the ordered far loop issues 7 FP32 lane operations and one MUFU "
+                       "rsqrt per pair, so the MUFU pipe bounds it: the fraction below is "
+                       "rsqrt results per second against the nominal MUFU rate",
                # one rsqrt per pair against the nominal 16 MUFU results per SM
                # per clock at the GPU's maximum SM clock
                "frac_mufu_peak": float(n) * n / (pot_ms * 1e-3) / mufu_peak_per_s()}
@@ -599,37 +768,27 @@ def main():
     if not args.no_pred and rank == 0:
         pred = predictor_leg(lib, m, x, v, flush_l2)
 
-    # accuracy against the FP64 oracle on one call of the timed shape (a
-    # chunk of i, so the same tuned kernel and its far-tile path run; rank 0)
+    # accuracy against the FP64 oracle on calls of the timed shape (chunks of
+    # 1024 i, so the same tuned kernel and its far-tile path run; rank 0)
     err = None
     cpu = None
     if rank == 0:
-        import oracle
-        rng = np.random.default_rng(5)
-        isel = np.sort(rng.choice(n, min(args.chunk, n), replace=False))
-        a_g, j_g, p_g, l_g = lib.gpunb_regf(h2[isel], dtr[isel], x[isel], v[isel], args.lmax,
-                                            args.nnbmax, args.m_flag)
-        a_o, j_o, p_o, l_o = oracle.regf(m, x, v, h2[isel], dtr[isel], x[isel], v[isel],
-                                         args.lmax, args.nnbmax, args.m_flag)
-        ok = l_o[:, 0] >= 0
-
-        def rel(a, b):
-            if a.ndim == 1:
-                return np.abs(a - b) / np.abs(b)
-            return np.sqrt(((a - b) ** 2).sum(1) / (b ** 2).sum(1))
-        err = {"sample_i": int(len(isel)), "acc_rel_max": float(rel(a_g, a_o)[ok].max()),
-               "jrk_rel_max": float(rel(j_g, j_o)[ok].max()),
-               "pot_rel_max": float(rel(p_g, p_o)[ok].max()),
-               "lists_identical": bool(np.array_equal(l_g, l_o)),
-               "nnb_mean": float(l_o[ok, 0].mean())}
+        if not args.no_err:
+            err = fp64_error_leg(lib, m, x, v, h2, dtr, args)
         if not args.no_cpu_baseline:
             rate, threads, calls, t_used = cpu_reference_rate(m, x, v, rs, dtr, args,
                                                               seconds=args.cpu_seconds)
-            cpu = {"value": rate, "unit": "pairs/s", "cores": threads, "kind": "reference",
+            cpu = {"value": rate, "unit": "pairs/s", "cores": threads, "cpu": cpu_model(),
+                   "kind": "reference",
                    "sample": f"{calls} calls x {args.chunk} i x {n} j of the same workload, "
                              f"reg.avx.cpp gpunb_regf_ (oracle/_ref), {t_used:.1f} s"}
 
     lib.gpunb_close()
+    # configs 3 and 4 end to end: the plain GPU method against the batched,
+    # device-resident drivers (rank 0)
+    ns = None
+    if rank == 0 and not args.no_northstar:
+        ns = northstar_leg(m, x, v, rs, args)
     # the reference's own GPU code on this GPU, same workload (rank 0)
     ref_gpu = None
     if rank == 0 and not args.no_ref_gpu:
@@ -657,12 +816,7 @@ def main():
             "dtype": "f32",
             "data": "synthetic King W0=6 (seeded), Kroupa IMF 0.08-100 Msun, 5% binaries "
                     "as c.m. bodies, Henon units",
-            "config": {"workload": f"king-w0=6 N={args.n} ({n} c.m. bodies), full regular "
-                                   f"evaluation in {args.chunk}-i calls",
-                       "n_bodies": n, "chunk": args.chunk, "calls_per_step": len(chunks),
-                       "nnbopt": 50, "nnbmax": args.nnbmax, "lmax": args.lmax,
-                       "m_flag": args.m_flag, "parallelism": f"replicas x{world}",
-                       "l2": "flushed (256 MiB write) between timed steps"},
+            "config": bench_config(args, n, world),
             # per call: force kernel + finalize, plus the active-set order
             # when the j set is spatially ordered (>= 32768 bodies)
             "gpu_launches": int(args.steps * len(chunks) * (3 if n >= 32768 else 2)),
@@ -672,6 +826,7 @@ def main():
             "gpupot": pot,
             "irregular": irr,
             "predictor": pred,
+            "northstar": ns,
             "pct_fp32_peak": 100.0 * FLOPS_PER_PAIR * pairs_step / (ms * 1e-3) / 1e12 / peak_tf,
         }
         print(json.dumps(out), flush=True)

@@ -47,6 +47,16 @@ NREC = 7      # FP64 values per result row: acc[3], jrk[3], pot
 POT_SPLIT_MIN = 50000  # bodies above which the potential is split (energy_mpi.F:60)
 
 
+def _device_view(ptr: int, shape, typestr: str, device):
+    """A torch tensor over device memory the library owns (no copy)."""
+    import torch
+
+    class _Buf:
+        __cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr, "data": (ptr, False),
+                                    "version": 3, "strides": None}
+    return torch.as_tensor(_Buf(), device=device)
+
+
 def active_split(nl: int, size: int) -> tuple[list[int], list[int]]:
     """Contiguous pieces of an active list of ``nl`` particles over ``size``
     ranks, as ``intgrt.F:955-968`` cuts it: each rank gets ``nl // size``
@@ -162,6 +172,74 @@ class RankSplit:
             rec = self._gather(rec, NREC, count)
             lst = self._gather(lst, lmax, count)
         return rec[:, 0:3].copy(), rec[:, 3:6].copy(), rec[:, 6].copy(), lst
+
+    # ------------------------------------------------ device-resident form
+    def _own_device(self, d_h2, d_dtr, d_xi, d_vi, lmax, nnbmax, m_flag, s, n, pad):
+        """This rank's piece [s, s + n) of device-resident i data through
+        nb6_regf_device_ in calls of at most ``chunk``, each call's output
+        rows copied on the library's stream into (pad, 7) FP64 and (pad, W)
+        int32 device tensors (rows past n stay zero)."""
+        import ctypes as C
+        import torch
+        raw = self.lib.lib
+        W = max(0, min(nnbmax, lmax - 1)) + 1
+        dev = self.device
+        rec = torch.zeros((pad, NREC), dtype=torch.float64, device=dev)
+        lst = torch.zeros((pad, W), dtype=torch.int32, device=dev)
+        stream = torch.cuda.ExternalStream(raw.nb6_stream_(), device=dev)
+        ci = C.c_int
+        po, pl = C.POINTER(C.c_double)(), C.POINTER(C.c_int)()
+        with torch.cuda.stream(stream):
+            for a in range(0, n, self.chunk):
+                b = min(n, a + self.chunk)
+                k = s + a
+                raw.nb6_regf_device_(C.byref(ci(b - a)), C.c_void_p(d_h2.data_ptr() + 8 * k),
+                                     C.c_void_p(d_dtr.data_ptr() + 8 * k),
+                                     C.c_void_p(d_xi.data_ptr() + 24 * k),
+                                     C.c_void_p(d_vi.data_ptr() + 24 * k),
+                                     C.byref(ci(lmax)), C.byref(ci(nnbmax)), C.byref(ci(m_flag)))
+                raw.nb6_regf_outputs_(C.byref(po), C.byref(pl))
+                outf = _device_view(C.cast(po, C.c_void_p).value, (b - a, 8), "<f8", dev)
+                outl = _device_view(C.cast(pl, C.c_void_p).value, (b - a, W), "<i4", dev)
+                rec[a:b].copy_(outf[:, :NREC])
+                lst[a:b].copy_(outl)
+        return rec, lst, stream
+
+    def regf_device(self, d_h2, d_dtr, d_xi, d_vi, lmax: int, nnbmax: int, m_flag: int = 0):
+        """``regf`` with the i data and the results on the device: d_h2,
+        d_dtr (nl,), d_xi, d_vi (nl, 3) FP64 CUDA tensors on this rank's
+        GPU, the same on every rank.  Returns (rec, lst): (nl, 7) FP64 rows
+        (acc, jrk, pot) and (nl, W) int32 list rows (W = min(nnbmax,
+        lmax-1) + 1) of the whole list, on the device: each rank's rows go
+        from the library's output buffers into the all-gather's send buffer
+        and come back from NCCL without touching the host."""
+        import contextlib
+        import torch
+        nl = int(d_h2.shape[0])
+        start, count = active_split(nl, self.size)
+        s, n = start[self.rank], count[self.rank]
+        pad = count[0] if nl else 0
+        rec, lst, stream = self._own_device(d_h2, d_dtr, d_xi, d_vi, lmax, nnbmax, m_flag, s, n, pad)
+        if self.dist is not None and self.size > 1 and nl > 0:
+            # the collective follows the library's work in stream order
+            with torch.cuda.stream(stream) if stream is not None else contextlib.nullcontext():
+                rec = self._gather_device(rec, count)
+                lst = self._gather_device(lst, count)
+        else:
+            rec, lst = rec[:n], lst[:n]
+        if stream is not None:
+            torch.cuda.current_stream(self.device).wait_stream(stream)
+        return rec, lst
+
+    def _gather_device(self, rows, counts: list[int]):
+        """All-gather of every rank's (counts[0], width) padded tensor on
+        its device; the first counts[r] rows of rank r, in rank order."""
+        import torch
+        pad = rows.shape[0]
+        out = torch.empty((self.size * pad,) + tuple(rows.shape[1:]), dtype=rows.dtype, device=rows.device)
+        self.dist.all_gather_into_tensor(out, rows.contiguous(), group=self.group)
+        out = out.view(self.size, pad, *rows.shape[1:])
+        return torch.cat([out[r, :counts[r]] for r in range(self.size)], dim=0)
 
     def gpupot(self, m, x, split_min: int = POT_SPLIT_MIN) -> np.ndarray:
         """Potential of every body against all bodies (``gpupot_``

@@ -206,3 +206,64 @@ def test_chunk_outside_the_call_limit_is_rejected():
         RankSplit(None, chunk=0)
     with pytest.raises(ValueError):
         RankSplit(None, chunk=1025)
+
+
+def _rank_device(rank, world, port, out):
+    """The device-resident split with gloo ranks on CPU: each rank's piece
+    comes from the FP64 oracle as CPU tensors in place of the library's
+    device output rows, then the padded all-gather of regf_device."""
+    import datetime
+    import sys
+    for p in (os.path.join(ROOT, "nbody6ppgpu-beijing_b200"), os.path.join(ROOT, "oracle")):
+        sys.path.insert(0, p)
+    import torch
+    import torch.distributed as dist
+    from nb6b200.rank_split import NREC, RankSplit
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        orc, cases = _cases()
+        res = []
+        for cl, h2, dtr, xi, vi, chunk, nnbmax in cases:
+            lmax = 64
+            W = min(nnbmax, lmax - 1) + 1
+            split = RankSplit(None, chunk=chunk)
+
+            def own(d_h2, d_dtr, d_xi, d_vi, lmax_, nnbmax_, m_flag, s, n, pad):
+                rec = torch.zeros((pad, NREC), dtype=torch.float64)
+                lst = torch.zeros((pad, W), dtype=torch.int32)
+                if n:
+                    a, j, p, l = orc.regf(cl.mass, cl.pos, cl.vel, d_h2[s:s + n].numpy(), d_dtr[s:s + n].numpy(),
+                                          d_xi[s:s + n].numpy(), d_vi[s:s + n].numpy(), lmax_, nnbmax_, m_flag)
+                    rec[:n, 0:3] = torch.from_numpy(a)
+                    rec[:n, 3:6] = torch.from_numpy(j)
+                    rec[:n, 6] = torch.from_numpy(p)
+                    lst[:n] = torch.from_numpy(l[:, :W])
+                return rec, lst, None
+
+            split._own_device = own
+            t = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64))
+            rec, lst = split.regf_device(t(h2), t(dtr), t(xi), t(vi), lmax, nnbmax, 0)
+            want = orc.regf(cl.mass, cl.pos, cl.vel, h2, dtr, xi, vi, lmax, nnbmax, 0)
+            same = (np.array_equal(rec[:, 0:3].numpy(), want[0]) and np.array_equal(rec[:, 3:6].numpy(), want[1])
+                    and np.array_equal(rec[:, 6].numpy(), want[2])
+                    and np.array_equal(lst.numpy(), want[3][:, :W]))
+            res.append((same, tuple(rec.shape), tuple(lst.shape)))
+        out[rank] = res
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_device_split_gathers_the_single_rank_rows(world):
+    import torch.multiprocessing as mp
+    port = _free_port()
+    with mp.get_context("spawn").Manager() as mgr:
+        out = mgr.dict()
+        mp.spawn(_rank_device, args=(world, port, out), nprocs=world, join=True)
+        res = dict(out)
+    for rank in range(world):
+        assert len(res[rank]) == len(CASES)
+        for (nl, chunk, nnbmax), (same, rshape, lshape) in zip(CASES, res[rank]):
+            assert same, (rank, nl, chunk, nnbmax)
+            assert rshape == (nl, 7) and lshape == (nl, min(nnbmax, 63) + 1)
