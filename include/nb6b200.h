@@ -220,13 +220,13 @@ void nb6_regf_correct_(double *time, int *ni, int *addr, int *iseg, int *nseg, i
  * *ncl = 0 each segment of a call is its own cluster with RDENS = 0,
  * RSCALE = RC2 = 1, RSFAC = prm[3], BODYM = 1 / its body count. */
 void nb6_hermite_adjust_(int *nb_flag, int *ncl, int *a0, double *par);
-/* The resident neighbour rows of bodies *a0 .. *a0 + *n - 1 (1-based) into
- * out[*n][*ls]: [nnb, 1-based ids ascending] with at most *ls - 1 ids and
- * zeros over the 8 entries after the last (no reference counterpart: the
- * reference's host keeps LIST; this is for a host that lets the device
+/* The resident neighbour rows of the *n bodies of 1-based addresses addr[]
+ * into out[*n][*ls]: [nnb, 1-based ids ascending] with at most *ls - 1 ids
+ * and zeros over the 8 entries after the last (no reference counterpart:
+ * the reference's host keeps LIST; this is for a host that lets the device
  * regular corrector keep the lists, e.g. for the density centre of
  * core.f). */
-void nb6_irr_lists_get_(int *a0, int *n, int *ls, int *out);
+void nb6_irr_lists_get_(int *n, const int *addr, int *ls, int *out);
 /* KS c.m. corrections of the irregular force (cmfirr_cor.f:13-130,
  * cmfirr_ucor.f:14-116, called from nbint_cor.f:37-65; no reference
  * counterpart in the force libraries: the reference applies them on the

@@ -59,7 +59,7 @@ def build_driver(force: bool = False, verbose: bool = False) -> str:
             and all(os.path.getmtime(DRIVER_LIB) >= os.path.getmtime(d) for d in DRIVER_DEPS)):
         return DRIVER_LIB
     cxx = shutil.which("g++") or "g++"
-    cmd = [cxx, "-O2", "-std=c++17", "-fPIC", "-shared", "-Wall", "-o", DRIVER_LIB + ".tmp",
+    cmd = [cxx, "-O2", "-std=c++17", "-fPIC", "-shared", "-Wall", "-pthread", "-o", DRIVER_LIB + ".tmp",
            *DRIVER_SRCS, "-ldl"]
     if verbose:
         print(" ".join(cmd), flush=True)

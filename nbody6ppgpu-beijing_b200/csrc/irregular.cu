@@ -97,49 +97,10 @@ NB6_DEV void cm_pair(const double *xi, const double *vi, const double *xj, const
 // term (cmfirr_ucor.f:14-116); for i itself the c.m. of a perturbed pair,
 // the perturbation terms over its perturber list are added instead
 // (cmfirr_cor.f:13-130).  An empty list gets no corrections.
-// Per-warp staging of 32 gathered records (4 KB of shared memory): record
-// r's 16-byte chunk t sits at slot 8 r + (t ^ (r & 7)), so that both the
-// cooperative writes (8 lanes per record) and each lane's reads of its own
-// record (chunk t of 8 consecutive records per quarter warp) are free of
-// bank conflicts.
-constexpr int IRR_STAGE = 32 * 8;  // double2 per warp
-
-// The records of the 32 neighbours l = base + lane of this batch into each
-// lane's rj: 8 lanes load one record together (chunk t = lane & 7, one
-// 128-byte line per record, four lines per load instruction, eight loads in
-// flight per lane), the warp transposes them through shared memory.  j is
-// this lane's neighbour (nmax, the zero padding record, when it has none).
-NB6_DEV void gather_batch(const Rec *__restrict__ rec, int j, int lane, double2 *__restrict__ stage, Rec &rj) {
-    const int g = lane >> 3, t = lane & 7;
-    double2 buf[8];
-#pragma unroll
-    for (int s = 0; s < 8; ++s) {
-        const int r = 4 * s + g;
-        const int jr = __shfl_sync(0xffffffffu, j, r);
-        buf[s] = t < 7 ? __ldg(reinterpret_cast<const double2 *>(rec + jr) + t) : make_double2(0.0, 0.0);
-    }
-    __syncwarp();  // the previous batch's reads are done
-#pragma unroll
-    for (int s = 0; s < 8; ++s) {
-        const int r = 4 * s + g;
-        stage[8 * r + (t ^ (r & 7))] = buf[s];
-    }
-    __syncwarp();
-    const double2 *q = stage + 8 * lane;
-    const int sw = lane & 7;
-    const double2 c0 = q[0 ^ sw], c1 = q[1 ^ sw], c2 = q[2 ^ sw], c3 = q[3 ^ sw];
-    const double2 c4 = q[4 ^ sw], c5 = q[5 ^ sw], c6 = q[6 ^ sw];
-    rj.x[0] = c0.x; rj.x[1] = c0.y; rj.x[2] = c1.x;
-    rj.v[0] = c1.y; rj.v[1] = c2.x; rj.v[2] = c2.y;
-    rj.f[0] = c3.x; rj.f[1] = c3.y; rj.f[2] = c4.x;
-    rj.fd[0] = c4.y; rj.fd[1] = c5.x; rj.fd[2] = c5.y;
-    rj.m = c6.x; rj.t0 = c6.y;
-}
-
 template <bool KS>
 NB6_DEV void irr_force_warp(int i, int lane, double ti, const Rec *__restrict__ rec,
                             const int *__restrict__ lists, int ls, int nmax, const KsArgs &ks, double *a,
-                            double *jd, int &nnbid, double2 *__restrict__ stage) {
+                            double *jd, int &nnbid) {
     Rec ri;
     load_rec(rec + i, ri);
     double xi[3], vi[3];
@@ -151,14 +112,11 @@ NB6_DEV void irr_force_warp(int i, int lane, double ti, const Rec *__restrict__ 
     double ax = 0, ay = 0, az = 0, jx = 0, jy = 0, jz = 0;
     double rmin = 1.0e300;
     int jmin = 0x7fffffff;
-    for (int base = 0; base < nnb; base += 32) {  // warp-uniform: every lane takes every batch
-        const int l = base + lane;
-        int j = l < nnb ? row[1 + l] : nmax;
-        const bool valid = l < nnb && j >= 0 && j < nmax;   // ids are checked at set_list time
-        if (!valid) j = nmax;
+    for (int l = lane; l < nnb; l += 32) {
+        const int j = row[1 + l];
+        if (j < 0 || j >= nmax) continue;   // ids are checked at set_list time
         Rec rj;
-        gather_batch(rec, j, lane, stage, rj);
-        if (!valid) continue;
+        load_rec(rec + j, rj);
         double xj[3], vj[3];
         predict(rj, ti, xj, vj);
         const double dxd = xj[0] - xi[0], dyd = xj[1] - xi[1], dzd = xj[2] - xi[2];
@@ -258,13 +216,12 @@ __global__ void __launch_bounds__(IRR_WARPS * 32)
     irr_kernel(int ni, const int *__restrict__ addr, double ti, const Rec *__restrict__ rec,
                const int *__restrict__ lists, int ls, int nmax, KsArgs ks, double *__restrict__ out,
                double *__restrict__ fv) {
-    __shared__ __align__(16) double2 stage[IRR_WARPS][IRR_STAGE];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int k = blockIdx.x * IRR_WARPS + warp;
     if (k >= ni) return;
     double a[3], jd[3];
     int id;
-    irr_force_warp<KS>(addr[k] - 1, lane, ti, rec, lists, ls, nmax, ks, a, jd, id, stage[warp]);
+    irr_force_warp<KS>(addr[k] - 1, lane, ti, rec, lists, ls, nmax, ks, a, jd, id);
     if (lane == 0 && !out) {
         // the caller's layout, in the blocks of the output staging:
         // acc[ni][3] | jrk[ni][3] (doubles) | nnbid[ni] | nnb[ni] (ints)
@@ -866,7 +823,6 @@ template <bool KS>
 __global__ void __launch_bounds__(IRR_WARPS * 32)
     blk_irr(const BlockCtl *c, const int *__restrict__ act, const Rec *__restrict__ rec,
             const int *__restrict__ lists, int ls, int nmax, KsArgs ks, double *__restrict__ out) {
-    __shared__ __align__(16) double2 stage[IRR_WARPS][IRR_STAGE];
     blk_enter();
     if (c->stop) return;
     const int p = c->parity, na = c->nact[p];
@@ -875,7 +831,7 @@ __global__ void __launch_bounds__(IRR_WARPS * 32)
     for (int k = blockIdx.x * IRR_WARPS + (threadIdx.x >> 5); k < na; k += gridDim.x * IRR_WARPS) {
         double a[3], jd[3];
         int id;
-        irr_force_warp<KS>(act[k], lane, t, rec, lists, ls, nmax, ks, a, jd, id, stage[threadIdx.x >> 5]);
+        irr_force_warp<KS>(act[k], lane, t, rec, lists, ls, nmax, ks, a, jd, id);
         if (lane == 0) {
             double *o = out + (size_t)k * 8;
             o[0] = a[0];
@@ -2018,33 +1974,37 @@ void hermite_adjust_impl(int nb_flag, int ncl, const int *a0, const double *par)
     NB6_CUDA_CHECK(cudaStreamSynchronize(st));
 }
 
-// Row lengths of bodies [a0, a0 + n) (0-based), capped at cap ids.
-__global__ void lists_count(int n, int a0, const int *__restrict__ lists, int ls, int cap, int *__restrict__ cnt) {
+// Row lengths of the bodies addr[0 .. n) (0-based), capped at cap ids.
+__global__ void lists_count(int n, const int *__restrict__ addr, const int *__restrict__ lists, int ls, int cap,
+                            int *__restrict__ cnt) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
-    const int c = lists[(size_t)(a0 + k) * ls];
+    const int c = lists[(size_t)addr[k] * ls];
     cnt[k] = min(max(c, 0), cap);
 }
 
 // One warp per body: its row [nnb, ids] packed at offs[k], ids 1-based.
-__global__ void lists_pack(int n, int a0, const int *__restrict__ lists, int ls, const int *__restrict__ cnt,
-                           const long long *__restrict__ offs, int *__restrict__ packed) {
+__global__ void lists_pack(int n, const int *__restrict__ addr, const int *__restrict__ lists, int ls,
+                           const int *__restrict__ cnt, const long long *__restrict__ offs, int *__restrict__ packed) {
     const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (k >= n) return;
-    const int *row = lists + (size_t)(a0 + k) * ls;
+    const int *row = lists + (size_t)addr[k] * ls;
     int *o = packed + offs[k];
     const int c = cnt[k];
     if (lane == 0) o[0] = c;
     for (int l = lane; l < c; l += 32) o[1 + l] = row[1 + l] + 1;
 }
 
-void lists_get_impl(int a0, int n, int ls, int *out) {
+void lists_get_impl(int n, const int *addr, int ls, int *out) {
     if (!I.open) {
         nb6_fatal(NB6_ERR_NOT_OPEN);
         return;
     }
     if (n <= 0) return;
-    if (a0 < 1 || (long long)a0 - 1 + n > I.nmax || ls < 1) {
+    bool bad = ls < 1;
+    for (int k = 0; k < n && !bad; ++k) bad = addr[k] < 1 || addr[k] > I.nmax;
+    if (bad) {
+        fprintf(stderr, "nb6_irr_lists_get: address outside [1, %d] or ls < 1\n", I.nmax);
         nb6_fatal(NB6_ERR_BAD_ARG);
         return;
     }
@@ -2052,27 +2012,33 @@ void lists_get_impl(int a0, int n, int ls, int *out) {
     irr_flush(st);
     const int cap = std::min(I.lmax, ls) - 1;
     const size_t nn = (size_t)n;
-    // [counts n | offsets 2n (long long)] on both sides, then the packed rows
-    I.lg_dev.reserve(3 * nn + 2);
-    I.lg_host.reserve(3 * nn + 2);
+    // [counts n | pad | offsets n (long long) | addresses n, 0-based] on the
+    // device; [counts | pad | offsets] on the host; then the packed rows
+    const size_t noff = (nn + 1) & ~(size_t)1;
+    I.lg_dev.reserve(noff + 3 * nn + 2);
+    I.lg_host.reserve(noff + 3 * nn + 2);
     int *dcnt = I.lg_dev.ptr;
-    lists_count<<<(n + 255) / 256, 256, 0, st>>>(n, a0 - 1, I.lists.ptr, I.lmax, cap, dcnt);
+    int *daddr = I.lg_dev.ptr + noff + 2 * nn;
+    int *haddr = I.lg_host.ptr + noff + 2 * nn;
+    for (size_t k = 0; k < nn; ++k) haddr[k] = addr[k] - 1;
+    NB6_CUDA_CHECK(cudaMemcpyAsync(daddr, haddr, sizeof(int) * nn, cudaMemcpyHostToDevice, st));
+    lists_count<<<(n + 255) / 256, 256, 0, st>>>(n, daddr, I.lists.ptr, I.lmax, cap, dcnt);
     NB6_CUDA_CHECK(cudaGetLastError());
     NB6_CUDA_CHECK(cudaMemcpyAsync(I.lg_host.ptr, dcnt, sizeof(int) * nn, cudaMemcpyDeviceToHost, st));
     NB6_CUDA_CHECK(cudaStreamSynchronize(st));
-    long long *hoff = reinterpret_cast<long long *>(I.lg_host.ptr + ((nn + 1) & ~(size_t)1));
+    long long *hoff = reinterpret_cast<long long *>(I.lg_host.ptr + noff);
     long long tot = 0;
     for (size_t k = 0; k < nn; ++k) {
         hoff[k] = tot;
         tot += 1 + I.lg_host.ptr[k];
     }
-    long long *doff = reinterpret_cast<long long *>(I.lg_dev.ptr + ((nn + 1) & ~(size_t)1));
+    long long *doff = reinterpret_cast<long long *>(I.lg_dev.ptr + noff);
     NB6_CUDA_CHECK(cudaMemcpyAsync(doff, hoff, sizeof(long long) * nn, cudaMemcpyHostToDevice, st));
     DevBuf<int> dpk;
     HostBuf<int> hpk;
     dpk.reserve((size_t)tot);
     hpk.reserve((size_t)tot);
-    lists_pack<<<(unsigned)((nn * 32 + 255) / 256), 256, 0, st>>>(n, a0 - 1, I.lists.ptr, I.lmax, dcnt, doff, dpk.ptr);
+    lists_pack<<<(unsigned)((nn * 32 + 255) / 256), 256, 0, st>>>(n, daddr, I.lists.ptr, I.lmax, dcnt, doff, dpk.ptr);
     NB6_CUDA_CHECK(cudaGetLastError());
     NB6_CUDA_CHECK(cudaMemcpyAsync(hpk.ptr, dpk.ptr, sizeof(int) * tot, cudaMemcpyDeviceToHost, st));
     NB6_CUDA_CHECK(cudaStreamSynchronize(st));
@@ -2230,10 +2196,10 @@ void nb6_irr_predict_send_(double *t, int *nseg, int *addr0, int *count) {
 void nb6_hermite_adjust_(int *nb_flag, int *ncl, int *a0, double *par) { hermite_adjust_impl(*nb_flag, *ncl, a0, par); }
 
 // Extension (no reference counterpart): the resident neighbour rows of the
-// bodies of 1-based addresses *a0 .. *a0 + *n - 1 into out[*n][*ls], each
-// [nnb, 1-based ids ascending] (at most *ls - 1 ids), zeros over the 8
-// entries after the last id.  For a host that lets the device regular
-// corrector keep the lists (density centre, core.f).
-void nb6_irr_lists_get_(int *a0, int *n, int *ls, int *out) { lists_get_impl(*a0, *n, *ls, out); }
+// *n bodies of 1-based addresses addr[] into out[*n][*ls], each [nnb,
+// 1-based ids ascending] (at most *ls - 1 ids), zeros over the 8 entries
+// after the last id.  For a host that lets the device regular corrector keep
+// the lists (density centre, core.f).
+void nb6_irr_lists_get_(int *n, const int *addr, int *ls, int *out) { lists_get_impl(*n, addr, *ls, out); }
 
 }  // extern "C"

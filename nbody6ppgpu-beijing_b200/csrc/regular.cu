@@ -858,6 +858,10 @@ constexpr int JPAR_NT = 256;
 template <int IB> struct JparI {
     float4 sip[IB][3];
     IP2 sip2[IB > 1 ? IB / 2 : 1];
+    // packed loop: each warp's queue of neighbour candidates (j << 3 | k)
+    // awaiting the exact FP64 decision; fewer than 32 wait between j
+    // iterations, and one iteration adds at most 32 IB
+    unsigned queue[IB > 1 ? JPAR_NT / 32 : 1][IB > 1 ? 32 + 32 * IB : 1];
 };
 
 template <int IB, bool X2>
@@ -889,11 +893,15 @@ NB6_DEV void jpar_stage_i(const RegArgs &a, JparI<IB> &S, int i0, int nvalid) {
 // The j-parallel inner loop: this thread's j's of [j_begin, j_end) against
 // the IB staged i-particles, results into s[k] (scaled as reg_pair keeps
 // them).  X2 (IB >= 2): two i-particles per f32x2 instruction (pair_x2 on
-// IP2 pairs, the j operands duplicated into both lanes).  pair_x2 is
-// reg_pair operation for operation and each lane accumulates its particle's
-// pairs in the same j order, and the rare path subtracts reg_exact's exact
-// contribution from the (negated) lane sum at the same point of the
-// sequence, so both forms give the same bits.
+// IP2 pairs, the j operands duplicated into both lanes; pair_x2 is reg_pair
+// operation for operation).  Neighbour candidates of the packed loop wait
+// in a per-warp queue and are decided 32 at a time, one per lane: in a small
+// cluster a sizeable share of all pairs are neighbours, and deciding them
+// where they arise would hold the whole warp for every lane that has one.
+// Any lane may decide any queued pair: its contribution joins that lane's
+// partial sum of particle k, which the CTA reduction adds up with the rest.
+// The order is fixed by the data, so results are deterministic; they differ
+// from the scalar loop's (X2 false) in the order of those sums.
 template <int IB, bool MFLAG, bool X2>
 NB6_DEV void jpar_loop(const RegArgs &a, const JparI<IB> &S, int j_begin, int j_end, int i0, int nvalid,
                        int jbase, Sums *s) {
@@ -902,37 +910,72 @@ NB6_DEV void jpar_loop(const RegArgs &a, const JparI<IB> &S, int j_begin, int j_
         S2 acc[NP];
 #pragma unroll
         for (int p = 0; p < NP; ++p) zero2(acc[p]);
-        for (int j = j_begin + (int)threadIdx.x; j < j_end; j += JPAR_NT) {
-            const float4 pa = __ldg(a.posH + j);
-            const float4 pb = __ldg(a.posL + j);
-            const float4 pc = __ldg(a.vel + j);
-            unsigned cm = 0u;
+        const int lane = threadIdx.x & 31;
+        unsigned *qw = const_cast<unsigned *>(S.queue[threadIdx.x >> 5]);
+        int qn = 0;  // queued candidates of this warp (warp-uniform)
+        // decide queued entry e on this lane: its exact contribution (or its
+        // neighbour record) into lane k & 1 of acc[k / 2]
+        auto decide = [&](unsigned e) {
+            const int k = (int)(e & 7u), jj = (int)(e >> 3);
+            Sums t;
+            zero(t);
+            reg_exact<MFLAG>(a, i0 + k, jj, t, jbase);
 #pragma unroll
-            for (int p = 0; p < NP; ++p) {
-                const IP2 ip = S.sip2[p];
-                cm |= pair_x2<MFLAG>(ip, dup2(pa.x), dup2(pa.y), dup2(pa.z), dup2(pa.w), dup2(pb.x),
-                                     dup2(pb.y), dup2(pb.z), dup2(pc.x), dup2(pc.y), dup2(pc.z), acc[p])
-                      << (2 * p);
-            }
-            if (cm) {
-                // unrolled: acc stays in registers (a dynamic index into it
-                // would put the array in local memory)
-#pragma unroll
-                for (int k = 0; k < IB; ++k) {
-                    if (k >= nvalid || !((cm >> k) & 1u)) continue;
-                    Sums t;
-                    zero(t);
-                    reg_exact<MFLAG>(a, i0 + k, j, t, jbase);
-                    S2 &q = acc[k >> 1];
-                    if (k & 1) {
-                        q.ax.y -= t.ax; q.ay.y -= t.ay; q.az.y -= t.az;
-                        q.jx.y -= t.jx; q.jy.y -= t.jy; q.jz.y -= t.jz; q.po.y -= t.po;
-                    } else {
-                        q.ax.x -= t.ax; q.ay.x -= t.ay; q.az.x -= t.az;
-                        q.jx.x -= t.jx; q.jy.x -= t.jy; q.jz.x -= t.jz; q.po.x -= t.po;
-                    }
+            for (int kk = 0; kk < IB; ++kk) {
+                if (kk != k) continue;
+                S2 &q = acc[kk >> 1];
+                if (kk & 1) {
+                    q.ax.y -= t.ax; q.ay.y -= t.ay; q.az.y -= t.az;
+                    q.jx.y -= t.jx; q.jy.y -= t.jy; q.jz.y -= t.jz; q.po.y -= t.po;
+                } else {
+                    q.ax.x -= t.ax; q.ay.x -= t.ay; q.az.x -= t.az;
+                    q.jx.x -= t.jx; q.jy.x -= t.jy; q.jz.x -= t.jz; q.po.x -= t.po;
                 }
             }
+        };
+        const int j_stop = j_begin + (int)((j_end - j_begin + JPAR_NT - 1) / JPAR_NT) * JPAR_NT;
+        for (int j = j_begin + lane + (int)(threadIdx.x & ~31u); j < j_stop; j += JPAR_NT) {
+            // every lane of the warp takes every iteration (the queue is the
+            // warp's); lanes past j_end compute nothing
+            unsigned cm = 0u;
+            if (j < j_end) {
+                const float4 pa = __ldg(a.posH + j);
+                const float4 pb = __ldg(a.posL + j);
+                const float4 pc = __ldg(a.vel + j);
+#pragma unroll
+                for (int p = 0; p < NP; ++p) {
+                    const IP2 ip = S.sip2[p];
+                    cm |= pair_x2<MFLAG>(ip, dup2(pa.x), dup2(pa.y), dup2(pa.z), dup2(pa.w), dup2(pb.x),
+                                         dup2(pb.y), dup2(pb.z), dup2(pc.x), dup2(pc.y), dup2(pc.z), acc[p])
+                          << (2 * p);
+                }
+            }
+            if (__any_sync(0xffffffffu, cm != 0u)) {
+                // append this lane's candidates after those of the lanes below
+                const int c = __popc(cm);
+                int pre = c;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int t = __shfl_up_sync(0xffffffffu, pre, o);
+                    if (lane >= o) pre += t;
+                }
+                const int tot = __shfl_sync(0xffffffffu, pre, 31);
+                int w = qn + pre - c;
+                for (unsigned m = cm; m; m &= m - 1) qw[w++] = ((unsigned)j << 3) | (unsigned)(__ffs(m) - 1);
+                __syncwarp();
+                qn += tot;
+                while (qn >= 32) {  // warp-uniform
+                    const unsigned e = qw[qn - 32 + lane];
+                    __syncwarp();
+                    qn -= 32;
+                    decide(e);
+                }
+            }
+        }
+        if (qn > 0) {
+            const unsigned e = lane < qn ? qw[lane] : 0u;
+            __syncwarp();
+            if (lane < qn) decide(e);
         }
 #pragma unroll
         for (int k = 0; k < IB; ++k) {

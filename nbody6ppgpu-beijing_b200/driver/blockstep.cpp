@@ -15,7 +15,7 @@
 //   F, FDOT bookkeeping          intgrt.F:558-581,911-935
 //   energy                       energy.F:28-62 (GPUPOT), ZKIN
 //   radius-rule quantities       adjust.F:104-199, core.f, output.F:61,271
-//                                at every output time
+//                                at TIME = 0 and every DTADJ (at outputs)
 // The per-body steps live in hermite.h (shared with the ensemble driver).
 // Left out: KS/chain regularisation, stellar evolution, external fields,
 // the checkl/fpcorr options (KZ(37), KZ(38)) and the SMIN neighbour retention.
@@ -84,6 +84,13 @@ struct Sim : Bodies {
         };
         regf_rows(B, idx, 0, (int)idx.size(), n, bodym, fill, take, prop);
         st.wall_reg += wtime() - t_0;
+    }
+
+    // the neighbour rows core.f reads, from the host's lists
+    auto host_rows() {
+        return [this](const std::vector<int> &jl, std::vector<const int *> &rp) {
+            for (size_t l = 0; l < jl.size(); ++l) rp[l] = row(jl[l]);
+        };
     }
 
     bool init();
@@ -169,7 +176,7 @@ bool Sim::run(double *eout, int nout_max) {
     int nout = 0;
     double ek, ep;
     energy(ek, ep);
-    adjust(0, 0, n, xp.data(), vp.data(), ek, -ep, list.data(), (size_t)LS, time);
+    if (adjust_due(time)) adjust(0, 0, n, xp.data(), vp.data(), ek, -ep, host_rows(), time);
     if (nout < nout_max) {
         eout[4 * nout] = 0.0;
         eout[4 * nout + 1] = ek;
@@ -207,7 +214,7 @@ bool Sim::run(double *eout, int nout_max) {
         clock_push(active);
         if (time >= tnext_out - 1e-15) {
             energy(ek, ep);
-            adjust(0, 0, n, xp.data(), vp.data(), ek, -ep, list.data(), (size_t)LS, time);
+            if (adjust_due(time)) adjust(0, 0, n, xp.data(), vp.data(), ek, -ep, host_rows(), time);
             if (nout < nout_max) {
                 eout[4 * nout] = time;
                 eout[4 * nout + 1] = ek;
@@ -294,7 +301,10 @@ void nb6drive_core(int n, const double *m, const double *x, const double *v, con
     for (int k = 0; k < 3; ++k) a.rdens[k] = io[k];
     a.rscale = io[3];
     double rc = io[4];
-    const double vc = ac_core(n, m, x, v, rs, rows, (size_t)ls, 0, time, a, rc);
+    auto rows_of = [rows, ls](const std::vector<int> &jl, std::vector<const int *> &rp) {
+        for (size_t l = 0; l < jl.size(); ++l) rp[l] = rows + (size_t)jl[l] * ls;
+    };
+    const double vc = ac_core(n, m, x, v, rs, rows_of, 0, time, a, rc);
     for (int k = 0; k < 3; ++k) io[k] = a.rdens[k];
     io[4] = rc;
     io[5] = a.rc2;

@@ -23,6 +23,8 @@
 // Energies are computed per cluster (gpupot_ on the cluster's own bodies).
 #include "hermite.h"
 
+#include <functional>
+
 namespace {
 
 using namespace nb6drv;
@@ -437,15 +439,12 @@ struct Ensemble : Bodies {
     // regular corrector on the device the neighbour rows are read back for
     // it first, and the new quantities go to the device.
     void record(double *tout, double *eout, int &nout, int nout_max) {
-        if (dev_reg() && B.lists_get) {
-            int a0 = 1, nn = n, ls = LS;
-            B.lists_get(&a0, &nn, &ls, list.data());
-        }
         std::vector<double> xp, vp;
+        const bool adj = adjust_due(time);
         for (int c = 0; c < ncl; ++c) {
             double ek, ep;
             energy(c, ek, ep, xp, vp);
-            adjust(c, base[c], cnt[c], xp.data(), vp.data(), ek, -ep, list.data(), (size_t)LS, time);
+            if (adj) adjust(c, base[c], cnt[c], xp.data(), vp.data(), ek, -ep, rows_for(c), time);
             if (nout < nout_max) {
                 double *e = eout + ((size_t)nout * ncl + c) * 3;
                 e[0] = ek;
@@ -453,8 +452,29 @@ struct Ensemble : Bodies {
                 e[2] = ek + ep;
             }
         }
-        if (dev_reg() && B.hermite_adjust) push_adjust();
+        if (adj && dev_reg() && B.hermite_adjust) push_adjust();
         if (nout < nout_max) tout[nout++] = time;
+    }
+
+    // The neighbour rows core.f reads for cluster c: the host's lists, or,
+    // once the device regular corrector keeps them, the rows of the central
+    // bodies read back from the device.
+    std::vector<int> core_rows, core_addr;
+    std::function<void(const std::vector<int> &, std::vector<const int *> &)> rows_for(int c) {
+        return [this, c](const std::vector<int> &jl, std::vector<const int *> &rp) {
+            const int b = base[c];
+            if (!(dev_reg() && B.lists_get && time > 0.0)) {   // at TIME = 0 the host's rows are current
+                for (size_t l = 0; l < jl.size(); ++l) rp[l] = row(b + jl[l]);
+                return;
+            }
+            const int k = (int)jl.size();
+            core_addr.resize(std::max(k, 1));
+            core_rows.resize((size_t)std::max(k, 1) * LS);
+            for (int l = 0; l < k; ++l) core_addr[l] = b + jl[l] + 1;
+            int nn = k, ls = LS;
+            if (k) B.lists_get(&nn, core_addr.data(), &ls, core_rows.data());
+            for (int l = 0; l < k; ++l) rp[l] = &core_rows[(size_t)l * LS];
+        };
     }
 
     // The radius rule's quantities of every cluster to the device corrector.

@@ -23,6 +23,7 @@
 
 #include <algorithm>
 #include <map>
+#include <thread>
 #include <vector>
 
 extern "C" {
@@ -66,6 +67,10 @@ struct nb6drive_params {
     // by (NNBOPT/NNB)^0.333; 0 = distances from the origin, overflow shrink
     // by 0.9
     int nb_flag;
+    // interval of the radius rule's adjust times (DTADJ of input.F): the
+    // quantities are refreshed at TIME = 0 and at the first energy output at
+    // or after each multiple of it
+    double dt_adj;
 };
 
 // Counters returned by the drivers.
@@ -114,7 +119,7 @@ typedef void (*fn_blocks_run)(double *, int *, int *, long long *, long long *, 
 typedef void (*fn_blocks_active)(int *, int *, double *);
 typedef void (*fn_blocks_regular)(int *, int *, double *);
 typedef void (*fn_hermite_adjust)(int *, int *, int *, double *);
-typedef void (*fn_lists_get)(int *, int *, int *, int *);
+typedef void (*fn_lists_get)(int *, const int *, int *, int *);
 
 struct Backend {
     void *hreg = nullptr, *hirr = nullptr, *hpot = nullptr;
@@ -307,13 +312,15 @@ inline double ac_shrink(int nb_flag, int nnbopt, int nnbmax, int nb_neg, double 
 }
 
 // Density centre, core radius and core rms velocity of a cluster (core.f),
-// from the bodies' positions and velocities x, v at TIME, masses m, radii
-// rs and neighbour rows (rows[k*ls] = nnb, then 1-based addresses, address
-// a0 + 1 being body 0 of the cluster).  In: a.rdens and rc_prev from the
-// last call (zero and unused at TIME = 0), a.rscale.  Out: a.rdens, a.rc2,
-// the returned VC, and rc_prev.
+// from the bodies' positions and velocities x, v at TIME, masses m and radii
+// rs.  rows_of(jl, rp) gives the neighbour row of each selected central body
+// jl[l] (cluster-local index) in rp[l]: [nnb, 1-based addresses], address
+// a0 + 1 being body 0 of the cluster.  In: a.rdens and rc_prev from the last
+// call (zero and unused at TIME = 0), a.rscale.  Out: a.rdens, a.rc2, the
+// returned VC, and rc_prev.
+template <class RowsOf>
 inline double ac_core(int nc, const double *m, const double *x, const double *v, const double *rs,
-                      const int *rows, size_t ls, int a0, double time, ACPar &a, double &rc_prev) {
+                      RowsOf rows_of, int a0, double time, ACPar &a, double &rc_prev) {
     double rcore2 = a.rscale * a.rscale;
     if (time > 0.0) rcore2 = std::max(9.0 * (rc_prev * rc_prev), rcore2);
     std::vector<int> jl;
@@ -327,11 +334,17 @@ inline double ac_core(int nc, const double *m, const double *x, const double *v,
         if ((int)jl.size() >= nc / 5) break;
         rcore2 = R4(1.5) * rcore2;
     }
-    std::vector<double> rho(jl.size(), 0.0), rl;
-    std::vector<int> il;
-    for (size_t l = 0; l < jl.size(); ++l) {
+    std::vector<const int *> rp(jl.size());
+    rows_of(jl, rp);
+    std::vector<double> rho(jl.size(), 0.0);
+    // each central body's density is its own: blocks of bodies on a few
+    // host threads (joined before the sums below)
+    auto density = [&](size_t l0, size_t l1) {
+      std::vector<double> rl;
+      std::vector<int> il;
+      for (size_t l = l0; l < l1; ++l) {
         const int i = jl[l];
-        const int *row = rows + (size_t)i * ls;
+        const int *row = rp[l];
         const int nnb = row[0];
         if (nnb <= 0) continue;
         const double *xi = x + 3 * (size_t)i;
@@ -367,6 +380,17 @@ inline double ac_core(int nc, const double *m, const double *x, const double *v,
         const double r6 = rl[i6 - 1];
         const double rinv32 = r6 > 0.0 ? 1.0 / (r6 * sqrt(r6)) : 0.0;
         rho[l] = n6 < 6 ? 0.0 : xmass * rinv32;
+      }
+    };
+    const size_t nl = jl.size();
+    const unsigned hw = std::thread::hardware_concurrency();
+    const size_t nth = std::min<size_t>(std::max(1u, std::min(hw, 16u)), (nl + 4095) / 4096);
+    if (nth <= 1) {
+        density(0, nl);
+    } else {
+        std::vector<std::thread> th;
+        for (size_t t = 0; t < nth; ++t) th.emplace_back(density, nl * t / nth, nl * (t + 1) / nth);
+        for (auto &t : th) t.join();
     }
     double zmass = 0.0;
     for (int i = 0; i < nc; ++i) zmass += m[i];
@@ -449,6 +473,15 @@ struct Bodies {
         double &r = rsmin[acl.empty() ? 0 : acl[i]];
         r = std::min(r, rs[i]);
     }
+    // adjust times: TIME = 0, then the first output at or after each
+    // multiple of DTADJ (dt_adj <= 0: every output)
+    double tnext_adj = 0.0;
+    bool adjust_due(double time) {
+        if (time < tnext_adj - 1e-15) return false;
+        const double d = P.dt_adj > 0.0 ? P.dt_adj : 0.0;
+        tnext_adj = d > 0.0 ? (floor(time / d + 1e-12) + 1.0) * d : time;
+        return true;
+    }
     void adjust_init(int ncl) {
         acp.assign(ncl, ACPar());
         rsmin.assign(ncl, P.rs0);   // RSMIN = RS0 from the input (input.F:137)
@@ -460,24 +493,25 @@ struct Bodies {
     // RSCALE, :150 RSMIN, :154 CORE, :199 RSFAC) followed by OUTPUT's own
     // CORE call and RSMIN reset (output.F:61,271).  x, v: the bodies at
     // `time`; ekin, pot (> 0): the cluster's kinetic and potential energy;
-    // rows: neighbour rows of every body (stride ls, 1-based addresses).
+    // rows_of(jl, rp): the neighbour rows of the cluster's bodies jl (see
+    // ac_core).
+    template <class RowsOf>
     void adjust(int c, int b, int nc, const double *x, const double *v, double ekin, double pot,
-                const int *rows, size_t ls, double time) {
+                RowsOf rows_of, double time) {
         ACPar &a = acp[c];
         double zmass = 0.0;
         for (int k = 0; k < nc; ++k) zmass += m[b + k];
         const double tcr_c = pow(zmass, 2.5) / pow(2.0 * fabs(ekin - pot), 1.5);
         a.rscale = 0.5 * (zmass * zmass) / pot;
         a.bodym = zmass / (double)(float)nc;
-        if (rsmin[c] == 0.0) {                                 // adjust.F:139-150
+        if (rsmin[c] == 0.0) {  // adjust.F:139-150 (over every body, not only those with neighbours)
             double r0 = a.rscale;
-            for (int k = 0; k < nc; ++k)
-                if (rows[(size_t)(b + k) * ls] > 0) r0 = std::min(r0, rs[b + k]);
+            for (int k = 0; k < nc; ++k) r0 = std::min(r0, rs[b + k]);
             rsmin[c] = r0;
         }
-        const double vc = ac_core(nc, &m[b], x, v, &rs[b], rows + (size_t)b * ls, ls, b, time, a, rc_last[c]);
+        const double vc = ac_core(nc, &m[b], x, v, &rs[b], rows_of, b, time, a, rc_last[c]);
         a.rsfac = std::max(R4(25.0) / tcr_c, 3.0 * vc / (2.0 * rsmin[c]));
-        ac_core(nc, &m[b], x, v, &rs[b], rows + (size_t)b * ls, ls, b, time, a, rc_last[c]);
+        ac_core(nc, &m[b], x, v, &rs[b], rows_of, b, time, a, rc_last[c]);
         rsmin[c] = R4(100.0);
     }
     nb6drive_stats st{};

@@ -258,11 +258,13 @@ class ForceLib:
         ncl = a0.shape[0] - 1
         self.lib.nb6_hermite_adjust_(_ci(nb_flag), _ci(ncl), _ip(a0), _dp(par if par.size else np.zeros(8)))
 
-    def lists_get(self, a0: int, n: int, ls: int) -> np.ndarray:
+    def lists_get(self, addr, ls: int) -> np.ndarray:
         """nb6_irr_lists_get_ (extension): resident neighbour rows (n, ls),
-        [nnb, 1-based ids]."""
+        [nnb, 1-based ids], of the bodies addr (1-based)."""
+        addr = np.ascontiguousarray(addr, dtype=np.int32)
+        n = addr.shape[0]
         out = np.zeros((max(n, 1), ls), dtype=np.int32)
-        self.lib.nb6_irr_lists_get_(_ci(a0), _ci(n), _ci(ls), _ip(out))
+        self.lib.nb6_irr_lists_get_(_ci(n), _ip(addr if n else np.zeros(1, np.int32)), _ci(ls), _ip(out))
         return out[:n]
 
     def blocks_run(self, tlimit: float, max_blocks: int) -> dict:

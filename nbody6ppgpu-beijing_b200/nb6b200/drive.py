@@ -32,7 +32,7 @@ class Params(C.Structure):
                 ("max_blocks", C.c_longlong), ("mlp_mode", C.c_int), ("mlp_pad", C.c_int),
                 ("samples", C.POINTER(C.c_float)), ("sample_cap", C.c_longlong),
                 ("rs_init", C.POINTER(C.c_double)), ("dev_corrector", C.c_int),
-                ("seg_single", C.c_int), ("nb_flag", C.c_int)]
+                ("seg_single", C.c_int), ("nb_flag", C.c_int), ("dt_adj", C.c_double)]
 
 
 class Stats(C.Structure):
@@ -115,14 +115,16 @@ def _rs_field(p: "Params", rs_init, n: int):
 def run(backend: dict, mass, pos, vel, *, tcrit=1.0, eta_i=0.02, eta_r=0.03, smax=0.125,
         dtmin=2.0 ** -24, dt_out=0.125, rs0=0.3, nnbopt=50, nnbmax=400, lmax=512, m_flag=0,
         chunk=1024, max_blocks=10_000_000, mlp_mode=0, sample_cap=0, rs_init=None,
-        nb_flag=1) -> RunResult:
+        nb_flag=1, dt_adj=1.0) -> RunResult:
     """mlp_mode: 0 Ahmad-Cohen radii; 1 Ahmad-Cohen and log up to sample_cap
     (features, target) samples into RunResult.samples; 2 the library's learned
     proposals (nb6b200.mlp.enable(True) first), Ahmad-Cohen as fallback.
     rs_init: initial neighbour radii per body (default RS0 sqrt(1 + r^2)).
     nb_flag: form of the Ahmad-Cohen rule, NB_FLAG of regcor_gpu.F:22 (1,
     the reference's default KZ(39) = 0 or 2: density-centre distances; 0:
-    KZ(39) = 1 or 3)."""
+    KZ(39) = 1 or 3).  dt_adj: DTADJ, the interval at which the rule's
+    quantities (density centre, core and half-mass radius, RSFAC) are
+    refreshed (at the first energy output at or after each multiple)."""
     mass = np.ascontiguousarray(mass, dtype=np.float64)
     n = mass.shape[0]
     x = np.ascontiguousarray(pos, dtype=np.float64).reshape(n, 3).copy()
@@ -131,6 +133,7 @@ def run(backend: dict, mass, pos, vel, *, tcrit=1.0, eta_i=0.02, eta_r=0.03, sma
                chunk, max_blocks)
     buf = _mlp_fields(p, mlp_mode, sample_cap)
     p.nb_flag = int(nb_flag)
+    p.dt_adj = float(dt_adj)
     rs_arr = _rs_field(p, rs_init, n)
     nout_max = int(tcrit / dt_out) + 4
     eout = np.zeros((nout_max, 4))
@@ -168,7 +171,7 @@ def run_ensemble(backend: dict, clusters, *, batched=True, tcrit=1.0, eta_i=0.02
                  smax=0.125, dtmin=2.0 ** -24, dt_out=0.125, rs0=0.3, nnbopt=50, nnbmax=400,
                  lmax=512, m_flag=0, chunk=1024, max_blocks=100_000_000, mlp_mode=0,
                  sample_cap=0, rs_init=None, rs_from_clusters=False,
-                 dev_corrector=True, seg_single=False, nb_flag=1) -> EnsembleResult:
+                 dev_corrector=True, seg_single=False, nb_flag=1, dt_adj=1.0) -> EnsembleResult:
     """clusters: sequence of (mass, pos, vel) (or objects with .mass/.pos/.vel),
     each in its own Henon units.  batched=False issues the regular force per
     cluster (what running each alone does); the result is then identical to
@@ -196,6 +199,7 @@ def run_ensemble(backend: dict, clusters, *, batched=True, tcrit=1.0, eta_i=0.02
     p.dev_corrector = int(dev_corrector)
     p.seg_single = 1 if seg_single else 0
     p.nb_flag = int(nb_flag)
+    p.dt_adj = float(dt_adj)
     if rs_init is None and all(hasattr(c, "rs") for c in clusters) and rs_from_clusters:
         rs_init = np.concatenate([c.rs for c in clusters])
     rs_arr = _rs_field(p, rs_init, len(mass))

@@ -81,7 +81,8 @@ def test_device_radius_rule_equals_oracle(nb6, orc, kz39):
         over = out[:, 28] != 0
         assert over.sum() > 20 and (~over).sum() > 600
         assert np.all(out[over, 28] < 0)
-        rows = nb6.lists_get(1, n, LMAX)
+        rows = np.zeros((n, LMAX), dtype=np.int32)
+        rows[sel] = nb6.lists_get(sel + 1, LMAX)
         ok = np.nonzero(~over)[0]
         nnb = out[ok, 27].astype(np.int32)
         np.testing.assert_array_equal(rows[sel[ok], 0], nnb)
