@@ -263,6 +263,19 @@ void nb6_blocks_run_(double *tlimit, int *max_blocks, int *reason, long long *nb
                      double *tblock, int *nact);
 void nb6_blocks_regular_(int *nreg, int *addr, double *xv);
 void nb6_blocks_active_(int *nact, int *addr, double *rows);
+/* Launches a large irr_simd_firr_vec_ call is split into (no reference
+ * counterpart): 1-4, anything else restores the default 4.  Each launch's
+ * results are downloaded and copied into the caller's arrays while the
+ * later launches run; 1 gives one launch over every body, then one download
+ * and copy. */
+void nb6_irr_tune_(int *chunks);
+/* Form of the device block clock for the following nb6_blocks_run_ calls
+ * (no reference counterpart): *persistent = 0 (the default) runs each block
+ * as a CUDA graph of three launches; 1 (or environment NB6_BLK_PERSIST=1)
+ * runs a whole call as one cooperative launch that loops over blocks, with
+ * two grid-wide barriers per block.  Both give the same results bit for
+ * bit. */
+void nb6_blocks_mode_(int *persistent);
 
 /* The device-resident state of bodies *a0 .. *a0 + *n - 1 (1-based), for a
  * host that lets the device correctors keep it (energy output, the end of

@@ -16,6 +16,7 @@
 // reference's FP32 (irr.avx.cpp:303-332); the nearest neighbour is the minimum FP64 r2 with the
 // smallest index on ties (irr.avx.cpp:320-323 packs (r2, idx) the same way).
 #include "nb6_common.cuh"
+#include "copy_pool.h"
 
 #include <cub/device/device_radix_sort.cuh>
 
@@ -29,6 +30,10 @@ bool regular_bind_j(int n, double **jm, double **jx, double **jv, JSetOut *out);
 namespace {
 
 constexpr int IRR_WARPS = 4;
+// A large irr_simd_firr_vec_ call runs in up to IRR_CHUNKS launches of at
+// least IRR_CHUNK_MIN bodies, so that each chunk's results are downloaded
+// and copied into the caller's arrays while the next chunks compute.
+constexpr int IRR_CHUNKS = 4, IRR_CHUNK_MIN = 8192;
 
 struct Rec {           // 16 doubles = 128 bytes, one cache line per gather
     double x[3], v[3], f[3], fd[3], m, t0, pad0, pad1;
@@ -44,10 +49,19 @@ NB6_DEV void predict(const Rec &r, double ti, double *x, double *v) {
     }
 }
 
+// CG: load through L2 only (ld.global.cg), for records that other CTAs of
+// the same launch write (the persistent block kernel); else the read-only
+// path.
+template <bool CG = false>
+NB6_DEV double2 ld_d2(const double2 *q) {
+    return CG ? __ldcg(q) : __ldg(q);
+}
+
+template <bool CG = false>
 NB6_DEV void load_rec(const Rec *__restrict__ p, Rec &r) {
     const double2 *q = reinterpret_cast<const double2 *>(p);
-    double2 a = __ldg(q + 0), b = __ldg(q + 1), c = __ldg(q + 2), d = __ldg(q + 3);
-    double2 e = __ldg(q + 4), f = __ldg(q + 5), g = __ldg(q + 6);
+    double2 a = ld_d2<CG>(q + 0), b = ld_d2<CG>(q + 1), c = ld_d2<CG>(q + 2), d = ld_d2<CG>(q + 3);
+    double2 e = ld_d2<CG>(q + 4), f = ld_d2<CG>(q + 5), g = ld_d2<CG>(q + 6);
     r.x[0] = a.x; r.x[1] = a.y; r.x[2] = b.x;
     r.v[0] = b.y; r.v[1] = c.x; r.v[2] = c.y;
     r.f[0] = d.x; r.f[1] = d.y; r.f[2] = e.x;
@@ -97,12 +111,12 @@ NB6_DEV void cm_pair(const double *xi, const double *vi, const double *xj, const
 // term (cmfirr_ucor.f:14-116); for i itself the c.m. of a perturbed pair,
 // the perturbation terms over its perturber list are added instead
 // (cmfirr_cor.f:13-130).  An empty list gets no corrections.
-template <bool KS>
+template <bool KS, bool CG = false>
 NB6_DEV void irr_force_warp(int i, int lane, double ti, const Rec *__restrict__ rec,
                             const int *__restrict__ lists, int ls, int nmax, const KsArgs &ks, double *a,
                             double *jd, int &nnbid) {
     Rec ri;
-    load_rec(rec + i, ri);
+    load_rec<CG>(rec + i, ri);
     double xi[3], vi[3];
     predict(ri, ti, xi, vi);
     const int *row = lists + (size_t)i * ls;
@@ -116,7 +130,7 @@ NB6_DEV void irr_force_warp(int i, int lane, double ti, const Rec *__restrict__ 
         const int j = row[1 + l];
         if (j < 0 || j >= nmax) continue;   // ids are checked at set_list time
         Rec rj;
-        load_rec(rec + j, rj);
+        load_rec<CG>(rec + j, rj);
         double xj[3], vj[3];
         predict(rj, ti, xj, vj);
         const double dxd = xj[0] - xi[0], dyd = xj[1] - xi[1], dzd = xj[2] - xi[2];
@@ -165,7 +179,7 @@ NB6_DEV void irr_force_warp(int i, int lane, double ti, const Rec *__restrict__ 
             const int j = ks.plist[l];
             if (j < 0 || j >= nmax) continue;   // ids are checked at set time
             Rec rj;
-            load_rec(rec + j, rj);
+            load_rec<CG>(rec + j, rj);
             double xj[3], vj[3], fcm[3], fcmd[3];
             predict(rj, ti, xj, vj);
             cm_pair(xi, vi, xj, vj, rj.m, fcm, fcmd);
@@ -298,16 +312,13 @@ NB6_DEV double tstep_dev(const double *f, const double *f1, const double *f2, co
 // predicted from their old state, as on the host), then each body is
 // corrected.  out row k (24 doubles): x0[3], v0[3], fi[3], fidot[3], F[3],
 // FDOT[3], step, regular-due flag, nnbid, 0, 0, 0.
-// The corrector of body i (0-based) at `time` from its force row fk, out row
-// o (24 doubles); tn[i] = t0 + step, the body's next block time, is kept for
-// the device block clock.  Returns the regular-due flag.
-NB6_DEV bool correct_irr_body(int i, double time, const double *__restrict__ fk, Rec *__restrict__ rec,
-                              Aux *__restrict__ aux, const HermiteParams &hp, double *__restrict__ o,
-                              double *__restrict__ tn) {
+// The corrector of one body at `time` from its force row fk: its record r
+// and corrector state x are updated in place and its out row o (24 doubles)
+// written.  Returns the regular-due flag.
+NB6_DEV bool correct_state(Rec &r, Aux &x, double time, const double *__restrict__ fk, const HermiteParams &hp,
+                           double *__restrict__ o) {
     const double a[3] = {fk[0], fk[1], fk[2]}, jd[3] = {fk[3], fk[4], fk[5]};
     const int id = (int)fk[6];
-    Rec r = rec[i];
-    Aux x = aux[i];
     const double s = dsub(time, r.t0), s1 = dmul(1.5, s), s2 = dmul(2.0, s);
     double xi[3], vi[3];
     for (int c = 0; c < 3; ++c) {
@@ -355,9 +366,6 @@ NB6_DEV bool correct_irr_body(int i, double time, const double *__restrict__ fk,
         // keep the irregular step inside the regular interval
         while (dadd(r.t0, x.step) > dadd(x.t0r, x.stepr) && x.step > hp.dtmin) x.step = dmul(x.step, 0.5);
     }
-    rec[i] = r;
-    aux[i] = x;
-    tn[i] = dadd(r.t0, x.step);
     for (int c = 0; c < 3; ++c) {
         o[c] = r.x[c];
         o[3 + c] = r.v[c];
@@ -370,6 +378,20 @@ NB6_DEV bool correct_irr_body(int i, double time, const double *__restrict__ fk,
     o[19] = regdue ? 1.0 : 0.0;
     o[20] = (double)id;
     o[21] = o[22] = o[23] = 0.0;
+    return regdue;
+}
+
+// The corrector of body i (0-based) in place, with out row o; tn[i] = t0 +
+// step, the body's next block time, is kept for the device block clock.
+NB6_DEV bool correct_irr_body(int i, double time, const double *__restrict__ fk, Rec *__restrict__ rec,
+                              Aux *__restrict__ aux, const HermiteParams &hp, double *__restrict__ o,
+                              double *__restrict__ tn) {
+    Rec r = rec[i];
+    Aux x = aux[i];
+    const bool regdue = correct_state(r, x, time, fk, hp, o);
+    rec[i] = r;
+    aux[i] = x;
+    tn[i] = dadd(r.t0, x.step);
     return regdue;
 }
 
@@ -741,6 +763,10 @@ struct BlockCtl {
     int last_nact;
     int nreg;                         // regular-due bodies of the running block (breg, bregxv)
     long long blimit;                 // blocks this run may do (stop 3 when reached)
+    // persistent form (blk_persist): grid barrier, and the act[] half that
+    // holds the last block's active set
+    unsigned bar_count, bar_gen;
+    int last_parity;
 };
 
 constexpr int BLK_NT = 256;
@@ -760,14 +786,15 @@ NB6_DEV void blk_enter() {
 
 // Minimum over the CTA (BLK_NT threads), valid in thread 0; every thread
 // must call it.
+template <int NT = BLK_NT>
 NB6_DEV unsigned long long cta_min(unsigned long long m) {
-    __shared__ unsigned long long wm[BLK_NT / 32];
+    __shared__ unsigned long long wm[NT / 32];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) m = min(m, __shfl_xor_sync(0xffffffffu, m, o));
     if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = m;
     __syncthreads();
     if (threadIdx.x == 0)
-        for (int w = 1; w < BLK_NT / 32; ++w) m = min(m, wm[w]);
+        for (int w = 1; w < NT / 32; ++w) m = min(m, wm[w]);
     __syncthreads();
     return m;
 }
@@ -889,6 +916,214 @@ __global__ void __launch_bounds__(BLK_NT)
             c->parity = q;
             if (atomicExch(&c->regdue, 0)) c->stop = 1;
         }
+    }
+}
+
+// ----------------------------------------------------------------------------
+// Persistent block clock (blk_persist): the same blocks, one cooperative
+// launch for a whole run of them.  Each block is two phases separated by
+// grid-wide barriers:
+//   A  the previous block's new records go into rec[] (see B), then the
+//      active set and the earliest tn of the others, as blk_collect;
+//   B  one warp per active body: its neighbour force (irr_force_warp), then
+//      on lane 0 its corrector (correct_state), with the new aux[i] and
+//      tn[i] written in place and the new record kept in the body's out
+//      row until phase A of the next block -- other warps of this block
+//      still read the old record of i as a neighbour, predicted from its
+//      old state, exactly as blk_irr does before blk_corr runs.
+// The last CTA at the barrier after B does blk_corr's bookkeeping.  Data
+// written by other CTAs of the launch (records, tn, aux, the active set,
+// out rows) is read through L2 only (ld.global.cg), after the barrier's
+// fences.  The active set alternates between two halves of act[] (phase A
+// reads the previous block's half while it writes the next one).
+// Results are those of the three-kernel form, bit for bit.
+// ----------------------------------------------------------------------------
+#ifndef PB_THREADS
+#define PB_THREADS 256
+#endif
+constexpr int PB_NT = PB_THREADS;                         // threads per CTA, one CTA per SM
+constexpr unsigned long long PB_WAIT_NS = 4000000000ull;  // barrier wait limit, 4 s
+
+NB6_DEV unsigned atom_add_acq_rel(unsigned *p, unsigned v) {
+    unsigned old;
+    asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+NB6_DEV unsigned ld_acquire(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+NB6_DEV void st_release(unsigned *p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Grid-wide barrier (every CTA resident: cooperative launch).  Thread 0 of
+// each CTA arrives with one acquire-release atomic (its CTA's writes, ordered
+// before it by the CTA barrier, are released with it); the last to arrive
+// has acquired every other CTA's writes, runs last() and opens the barrier
+// with a release store of the next generation; the others poll the
+// generation with acquire loads for at most PB_WAIT_NS of global time,
+// after which they set the status word and report false (in every thread
+// of the CTA).
+template <class F>
+NB6_DEV bool grid_sync(BlockCtl *c, int *status, F last) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int good = 1;
+        const unsigned g = ld_acquire(&c->bar_gen);
+        if (atom_add_acq_rel(&c->bar_count, 1u) == gridDim.x - 1) {
+            last();
+            c->bar_count = 0;
+            st_release(&c->bar_gen, g + 1);
+        } else {
+            const unsigned long long t0 = globaltimer();
+            while (ld_acquire(&c->bar_gen) == g) {
+                if (globaltimer() - t0 > PB_WAIT_NS) {
+                    set_status(status, NB6_ERR_WAIT_TIMEOUT);
+                    good = 0;
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        ok = good;
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+NB6_DEV void ldcg_aux(const Aux *p, Aux &x) {
+    const double2 *q = reinterpret_cast<const double2 *>(p);
+    double *d = reinterpret_cast<double *>(&x);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const double2 v = __ldcg(q + k);
+        d[2 * k] = v.x;
+        d[2 * k + 1] = v.y;
+    }
+}
+
+// NT threads per CTA, one CTA per SM (the corrected walk of the KS form
+// needs 186 registers: 256 threads).
+template <bool KS, int NT = KS ? 256 : PB_NT>
+__global__ void __launch_bounds__(NT, 1)
+    blk_persist(BlockCtl *c, int *__restrict__ act, int n, Rec *__restrict__ rec, Aux *__restrict__ aux,
+                const int *__restrict__ lists, int ls, KsArgs ks, HermiteParams hp, double *__restrict__ rows,
+                double *__restrict__ tn, int *__restrict__ reg, double *__restrict__ regxv, int *status) {
+    volatile BlockCtl *cv = c;
+    const int lane = threadIdx.x & 31;
+    const int gw = blockIdx.x * (NT / 32) + (threadIdx.x >> 5), nw = gridDim.x * (NT / 32);
+    const int gt = blockIdx.x * NT + threadIdx.x, nt = gridDim.x * NT;
+    int prev_na = 0, prev_p = 0;
+    double prev_t = 0.0;
+    for (;;) {
+        // ---- phase A
+        for (int k = gt; k < prev_na; k += nt) {   // the previous block's new records
+            const int i = __ldcg(act + (size_t)prev_p * n + k);
+            const double *o = rows + (size_t)k * 24;
+            Rec *r = rec + i;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                r->x[d] = __ldcg(o + d);
+                r->v[d] = __ldcg(o + 3 + d);
+                r->f[d] = __ldcg(o + 12 + d);
+                r->fd[d] = __ldcg(o + 15 + d);
+            }
+            r->t0 = prev_t;
+        }
+        if (cv->stop) return;
+        if (cv->blocks >= cv->blimit) {   // every thread reads the same count: all return
+            if (blockIdx.x == 0 && threadIdx.x == 0) c->stop = 3;
+            return;
+        }
+        const int p = cv->parity;
+        const double t = __longlong_as_double((long long)cv->tmin_bits[p]);
+        if (t > cv->tlimit) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) c->stop = 2;
+            return;
+        }
+        int *ap = act + (size_t)p * n;
+        unsigned long long m2 = ~0ull;
+        constexpr int U = 8;   // next times loaded U at a time, all in flight together
+        for (int i0 = gt; i0 - (int)threadIdx.x < n; i0 += U * nt) {
+            double tv[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) tv[u] = i0 + u * nt < n ? __ldcg(tn + i0 + u * nt) : 0.0;
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int i = i0 + u * nt;
+                const bool on = i < n && tv[u] == t;
+                if (i < n && !on) m2 = min(m2, (unsigned long long)__double_as_longlong(tv[u]));
+                const unsigned b = __ballot_sync(0xffffffffu, on);
+                if (b) {
+                    int base = 0;
+                    if (lane == 0) base = atomicAdd(&c->nact[p], __popc(b));
+                    base = __shfl_sync(0xffffffffu, base, 0);
+                    if (on) ap[base + __popc(b & ((1u << lane) - 1u))] = i;
+                }
+            }
+        }
+        m2 = cta_min<NT>(m2);
+        if (threadIdx.x == 0) atomicMin(&c->m2_bits[p], m2);
+        if (blockIdx.x == 0 && threadIdx.x == 0) c->nreg = 0;
+        if (!grid_sync(c, status, [] {})) return;
+        // ---- phase B
+        const int na = cv->nact[p];
+        bool due = false;
+        unsigned long long mact = ~0ull;
+        for (int k = gw; k < na; k += nw) {
+            const int i = __ldcg(ap + k);
+            double fk[8];
+            int id;
+            irr_force_warp<KS, true>(i, lane, t, rec, lists, ls, n, ks, fk, fk + 3, id);
+            if (lane == 0) {
+                fk[6] = (double)id;
+                fk[7] = 0.0;
+                Rec r;
+                Aux x;
+                load_rec<true>(rec + i, r);
+                ldcg_aux(aux + i, x);
+                double *o = rows + (size_t)k * 24;
+                if (correct_state(r, x, t, fk, hp, o)) {
+                    due = true;
+                    const int q = atomicAdd(&c->nreg, 1);  // (q < na <= n)
+                    reg[q] = i;
+                    for (int d = 0; d < 6; ++d) regxv[6 * (size_t)q + d] = o[d];  // x0, v0
+                }
+                aux[i] = x;
+                const double tnew = dadd(r.t0, x.step);
+                tn[i] = tnew;
+                mact = min(mact, (unsigned long long)__double_as_longlong(tnew));
+            }
+        }
+        mact = cta_min<NT>(mact);
+        if (threadIdx.x == 0) atomicMin(&c->mact_bits[p], mact);
+        if (__syncthreads_or(due) && threadIdx.x == 0) atomicOr(&c->regdue, 1);
+        const bool go = grid_sync(c, status, [&] {
+            // the block is done (blk_corr's last-CTA bookkeeping)
+            const int q = p ^ 1;
+            c->blocks += 1;
+            c->irr_steps += na;
+            c->tblock = t;
+            c->last_nact = na;
+            c->last_parity = p;
+            // (the arrival atomic acquired every CTA's minima and flags)
+            c->tmin_bits[q] = min(cv->m2_bits[p], cv->mact_bits[p]);
+            c->m2_bits[q] = ~0ull;
+            c->mact_bits[q] = ~0ull;
+            c->nact[q] = 0;
+            c->parity = q;
+            if (cv->regdue) {
+                c->regdue = 0;
+                c->stop = 1;
+            }
+        });
+        if (!go) return;
+        prev_na = na;
+        prev_p = p;
+        prev_t = t;
     }
 }
 
@@ -1028,6 +1263,10 @@ struct IrrState {
     double time_grav = 0;
     unsigned long long num_inter = 0, num_fcall = 0, num_steps = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // irr_kernel of the last call
+    cudaStream_t cst = nullptr;                // downloads of the chunks' results
+    cudaEvent_t evk[IRR_CHUNKS] = {}, evc[IRR_CHUNKS] = {};   // chunk kernel / download done
+    CopyPool pool;                             // copies into the caller's arrays
+    int chunks_max = IRR_CHUNKS;               // nb6_irr_tune_
     // device-resident corrector state (nb6_hermite_open_)
     bool hermite = false;
     HermiteParams hp{};
@@ -1057,6 +1296,8 @@ struct IrrState {
     int blk_batch = 16;               // blocks per synchronisation
     int blk_unroll = 0;               // blocks per graph (NB6_BLK_UNROLL, default 4)
     bool blk_pdl = true;              // programmatic edges between the block kernels (NB6_BLK_PDL=0: off)
+    int blk_persist = -1;             // 1: one persistent launch per run (NB6_BLK_PERSIST=1; default 0)
+    const int *bact_last = nullptr;   // the last block's active set (a half of bact in the persistent form)
     DevBuf<int> breg;                 // regular-due bodies of the running block
     DevBuf<double> bregxv;            // their x0, v0
     DevBuf<int> bsort;                // [sorted addresses | slots in | slots out], 3 x nmax
@@ -1151,6 +1392,7 @@ void irr_close_impl() {
     I.bgraph = nullptr;
     memset(I.bgraph_key, 0, sizeof(I.bgraph_key));
     I.bact.release();
+    I.bact_last = nullptr;
     I.breg.release();
     I.bregxv.release();
     I.bsort.release();
@@ -1186,6 +1428,7 @@ void irr_close_impl() {
     I.hout.release();
     I.jp_slot.clear();
     I.list_slot.clear();
+    I.pool.stop();
 }
 
 void irr_set_jp_impl(int a, const double *pos, const double *vel, const double *acc2,
@@ -1373,9 +1616,15 @@ void irr_firr_vec_impl(double ti, int ni, const int *addr, double (*acc)[3], dou
     // the pinned staging is reused only after this call's synchronize, so
     // the uploads enqueued here read it intact
     const int *daddr = irr_flush(st, addr, ni);
-    // results in the caller's layout: acc | jrk (6 ni doubles) | nnbid | nnb
-    // (2 ni ints), written straight to pinned host memory when small, else
-    // through one device buffer and one copy
+    // Results in the caller's layout, per chunk of bodies [a, a+m): at
+    // double offset 7a, acc[m][3] | jrk[m][3] (doubles) | nnbid[m] | nnb[m]
+    // (ints) -- one chunk covering all ni is exactly the caller's three
+    // arrays back to back.  Small calls write straight to pinned host
+    // memory; large ones into one device buffer, each chunk downloaded on a
+    // second stream as soon as its kernel ends, then copied into the
+    // caller's arrays by the copy pool while later chunks run.  (With a
+    // device status error and NB6_ABORT_ON_ERROR=0 the caller's arrays may
+    // hold part of the results.)
     const size_t nd = 7 * (size_t)ni;   // 6 ni doubles + 2 ni ints
     const size_t bytes = sizeof(double) * nd;
     I.hout.reserve(nd);
@@ -1385,25 +1634,68 @@ void irr_firr_vec_impl(double ti, int ni, const int *addr, double (*acc)[3], dou
         I.dout.reserve(nd);
         out = I.dout.ptr;
     }
+    const int nch = direct ? 1 : std::max(1, std::min(I.chunks_max, ni / IRR_CHUNK_MIN));
     if (!I.ev0) {
         NB6_CUDA_CHECK(cudaEventCreate(&I.ev0));
         NB6_CUDA_CHECK(cudaEventCreate(&I.ev1));
     }
+    if (!direct && !I.cst) {
+        NB6_CUDA_CHECK(cudaStreamCreateWithFlags(&I.cst, cudaStreamNonBlocking));
+        for (int c = 0; c < IRR_CHUNKS; ++c) {
+            NB6_CUDA_CHECK(cudaEventCreateWithFlags(&I.evk[c], cudaEventDisableTiming));
+            NB6_CUDA_CHECK(cudaEventCreateWithFlags(&I.evc[c], cudaEventDisableTiming));
+        }
+    }
+    if (!direct) I.pool.start(CopyPool::default_parts());
+    auto chunk_lo = [&](int c) { return (int)((long long)ni * c / nch); };
     NB6_CUDA_CHECK(cudaEventRecord(I.ev0, st));
-    launch_irr_kernel(ni, daddr, ti, nullptr, st, out);
-    NB6_CUDA_CHECK(cudaGetLastError());
+    for (int c = 0; c < nch; ++c) {
+        const int a = chunk_lo(c), m = chunk_lo(c + 1) - a;
+        launch_irr_kernel(m, daddr + a, ti, nullptr, st, out + 7 * (size_t)a);
+        NB6_CUDA_CHECK(cudaGetLastError());
+        if (!direct) {
+            NB6_CUDA_CHECK(cudaEventRecord(I.evk[c], st));
+            NB6_CUDA_CHECK(cudaStreamWaitEvent(I.cst, I.evk[c], 0));
+            NB6_CUDA_CHECK(cudaMemcpyAsync(I.hout.ptr + 7 * (size_t)a, out + 7 * (size_t)a,
+                                           sizeof(double) * 7 * (size_t)m, cudaMemcpyDeviceToHost, I.cst));
+            NB6_CUDA_CHECK(cudaEventRecord(I.evc[c], I.cst));
+        }
+    }
     NB6_CUDA_CHECK(cudaEventRecord(I.ev1, st));
-    if (!direct) NB6_CUDA_CHECK(cudaMemcpyAsync(I.hout.ptr, I.dout.ptr, bytes, cudaMemcpyDeviceToHost, st));
     nb6_status_fetch(st);
+    unsigned long long inter = 0;
+    if (!direct) I.pool.arm();
+    if (!direct) {
+        const int np = I.pool.parts();
+        std::vector<unsigned long long> part(np);
+        for (int c = 0; c < nch; ++c) {
+            NB6_CUDA_CHECK(cudaEventSynchronize(I.evc[c]));
+            const int a = chunk_lo(c), m = chunk_lo(c + 1) - a;
+            const double *h = I.hout.ptr + 7 * (size_t)a;
+            I.pool.run([&](int p) {
+                const int lo = (int)((long long)m * p / np), hi = (int)((long long)m * (p + 1) / np);
+                if (hi <= lo) return;
+                memcpy(&acc[a + lo][0], h + 3 * (size_t)lo, sizeof(double) * 3 * (size_t)(hi - lo));
+                memcpy(&jrk[a + lo][0], h + 3 * (size_t)m + 3 * (size_t)lo, sizeof(double) * 3 * (size_t)(hi - lo));
+                const int *hi_ = reinterpret_cast<const int *>(h + 6 * (size_t)m);
+                memcpy(nnbid + a + lo, hi_ + lo, sizeof(int) * (size_t)(hi - lo));
+                unsigned long long s = 0;
+                for (int k = lo; k < hi; ++k) s += (unsigned)hi_[m + k];
+                part[p] += s;
+            });
+        }
+        for (int p = 0; p < np; ++p) inter += part[p];
+    }
     NB6_CUDA_CHECK(cudaStreamSynchronize(st));
     if (nb6_check_dev_status() != 0) return;
-    const double *h = I.hout.ptr;
-    memcpy(&acc[0][0], h, sizeof(double) * 3 * (size_t)ni);
-    memcpy(&jrk[0][0], h + 3 * (size_t)ni, sizeof(double) * 3 * (size_t)ni);
-    const int *hi = reinterpret_cast<const int *>(h + 6 * (size_t)ni);
-    memcpy(nnbid, hi, sizeof(int) * (size_t)ni);
-    unsigned long long inter = 0;
-    for (int k = 0; k < ni; ++k) inter += (unsigned)hi[ni + k];
+    if (direct) {
+        const double *h = I.hout.ptr;
+        memcpy(&acc[0][0], h, sizeof(double) * 3 * (size_t)ni);
+        memcpy(&jrk[0][0], h + 3 * (size_t)ni, sizeof(double) * 3 * (size_t)ni);
+        const int *hi = reinterpret_cast<const int *>(h + 6 * (size_t)ni);
+        memcpy(nnbid, hi, sizeof(int) * (size_t)ni);
+        for (int k = 0; k < ni; ++k) inter += (unsigned)hi[ni + k];
+    }
     I.num_inter += inter;
     I.time_grav += nb6_wtime() - t0;
     I.num_fcall++;
@@ -1580,6 +1872,45 @@ void ks_set_impl(int npair, const int *cm, const double *xk, const double *vk, c
 
 // Capture the four launches of one block as a graph (rebuilt when a buffer
 // moved or the pair table came or went).
+// One cooperative launch of blk_persist for the whole run; false when the
+// device cannot hold the grid (then the graph form runs).  On return h holds
+// the control block.
+bool blocks_persist(cudaStream_t st, int max_blocks, BlockCtl &h) {
+    (void)max_blocks;   // in the control block (blimit)
+    const KsArgs ks = ks_args();
+    const void *fn = ks.slot ? (const void *)blk_persist<true> : (const void *)blk_persist<false>;
+    const int nt = ks.slot ? 256 : PB_NT;
+    static int coop = -1;
+    if (coop < 0) {
+        int dev = 0, v = 0;
+        NB6_CUDA_CHECK(cudaGetDevice(&dev));
+        coop = (cudaDeviceGetAttribute(&v, cudaDevAttrCooperativeLaunch, dev) == cudaSuccess && v) ? 1 : 0;
+    }
+    int occ = 0;
+    if (!coop || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, nt, 0) != cudaSuccess || occ < 1) {
+        cudaGetLastError();
+        return false;
+    }
+    const int grid = nb6_num_sms();
+    BlockCtl *cp = I.bctl.ptr;
+    int *ap = I.bact.ptr;
+    int n = I.nmax, ls = I.lmax;
+    Rec *rp = I.rec.ptr;
+    Aux *xp = I.aux.ptr;
+    const int *lp = I.lists.ptr;
+    KsArgs ka = ks;
+    HermiteParams hp = I.hp;
+    double *rows = I.brows.ptr, *tn = I.tn.ptr, *rxv = I.bregxv.ptr;
+    int *reg = I.breg.ptr, *status = nb6_dev_status();
+    void *args[] = {&cp, &ap, &n, &rp, &xp, &lp, &ls, &ka, &hp, &rows, &tn, &reg, &rxv, &status};
+    NB6_CUDA_CHECK(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(nt), args, 0, st));
+    NB6_CUDA_CHECK(cudaMemcpyAsync(&h, I.bctl.ptr, sizeof(BlockCtl), cudaMemcpyDeviceToHost, st));
+    nb6_status_fetch(st);
+    NB6_CUDA_CHECK(cudaStreamSynchronize(st));
+    nb6_check_dev_status();
+    return true;
+}
+
 bool blocks_graph(cudaStream_t st) {
     const KsArgs ks = ks_args();
     const void *key[8] = {I.bact.ptr, I.bforce.ptr, I.brows.ptr, I.bctl.ptr, I.tn.ptr, I.breg.ptr, I.bregxv.ptr,
@@ -1664,7 +1995,7 @@ void blocks_run_impl(double tlimit, int max_blocks, int *reason, long long *nblo
     const double t0 = nb6_wtime();
     cudaStream_t st = nb6_stream();
     irr_flush(st);
-    I.bact.reserve((size_t)I.nmax);
+    I.bact.reserve((size_t)I.nmax * 2);
     I.bforce.reserve((size_t)I.nmax * 8);
     I.brows.reserve((size_t)I.nmax * 24);
     I.breg.reserve((size_t)I.nmax);
@@ -1687,11 +2018,28 @@ void blocks_run_impl(double tlimit, int max_blocks, int *reason, long long *nblo
         const char *q = getenv("NB6_BLK_PDL");
         I.blk_pdl = !(q && q[0] == '0');
     }
+    if (I.blk_persist < 0) {
+        const char *e = getenv("NB6_BLK_PERSIST");
+        I.blk_persist = (e && e[0] == '1') ? 1 : 0;
+    }
     NB6_CUDA_CHECK(cudaMemcpyAsync(I.bctl.ptr, &h, sizeof(BlockCtl), cudaMemcpyHostToDevice, st));
     // the first block's time from every body; each later one comes from the
     // block before it (blk_collect and blk_corr)
     blk_min<<<nb6_num_sms() * 4, BLK_NT, 0, st>>>(I.nmax, I.tn.ptr, I.bctl.ptr);
     NB6_CUDA_CHECK(cudaGetLastError());
+    if (I.blk_persist && blocks_persist(st, max_blocks, h)) {
+        I.bact_last = I.bact.ptr + (size_t)h.last_parity * I.nmax;
+        *reason = h.stop == 3 ? 0 : h.stop;
+        *nblocks = h.blocks;
+        *nirr = h.irr_steps;
+        *tblock = h.tblock;
+        *nact = h.last_nact;
+        I.time_grav += nb6_wtime() - t0;
+        I.num_fcall += (unsigned long long)h.blocks;
+        I.num_steps += (unsigned long long)h.irr_steps;
+        return;
+    }
+    I.bact_last = I.bact.ptr;
     if (!blocks_graph(st)) {
         fprintf(stderr, "nb6_blocks_run: the block graph could not be built\n");
         nb6_fatal(NB6_ERR_CUDA);
@@ -1732,7 +2080,8 @@ void blocks_active_impl(int *nact, int *addr, double *rows) {
     *nact = na;
     if (na <= 0) return;
     cudaStream_t st = nb6_stream();
-    NB6_CUDA_CHECK(cudaMemcpyAsync(addr, I.bact.ptr, sizeof(int) * na, cudaMemcpyDeviceToHost, st));
+    NB6_CUDA_CHECK(cudaMemcpyAsync(addr, I.bact_last ? I.bact_last : I.bact.ptr, sizeof(int) * na,
+                                   cudaMemcpyDeviceToHost, st));
     NB6_CUDA_CHECK(cudaMemcpyAsync(rows, I.brows.ptr, sizeof(double) * 24 * (size_t)na, cudaMemcpyDeviceToHost, st));
     NB6_CUDA_CHECK(cudaStreamSynchronize(st));
     for (int k = 0; k < na; ++k) addr[k] += 1;
@@ -2122,6 +2471,10 @@ void nb6_ks_set_(int *npair, int *cm, double *xk, double *vk, double *mk, int *p
 // of this call, *tblock is the last block's time, *nact its active count.
 // The host's block clock is not needed meanwhile (next_tlist.f's choice is
 // made on the device, bit for bit the same).
+void nb6_blocks_mode_(int *persistent) { I.blk_persist = *persistent ? 1 : 0; }
+
+void nb6_irr_tune_(int *chunks) { I.chunks_max = (*chunks >= 1 && *chunks <= IRR_CHUNKS) ? *chunks : IRR_CHUNKS; }
+
 void nb6_blocks_run_(double *tlimit, int *max_blocks, int *reason, long long *nblocks, long long *nirr,
                      double *tblock, int *nact) {
     blocks_run_impl(*tlimit, *max_blocks, reason, nblocks, nirr, tblock, nact);

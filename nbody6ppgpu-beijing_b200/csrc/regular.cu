@@ -2391,8 +2391,7 @@ template <bool MF> static const void *seg_kernel_of(int ib) {
     switch (ib) {
         case 1: return (const void *)regf_seg_kernel<1, MF>;
         case 2: return jpar_x2() ? (const void *)regf_seg_kernel<2, MF, true> : (const void *)regf_seg_kernel<2, MF>;
-        case 4: return jpar_x2() ? (const void *)regf_seg_kernel<4, MF, true> : (const void *)regf_seg_kernel<4, MF>;
-        default: return jpar_x2() ? (const void *)regf_seg_kernel<8, MF, true> : (const void *)regf_seg_kernel<8, MF>;
+        default: return jpar_x2() ? (const void *)regf_seg_kernel<4, MF, true> : (const void *)regf_seg_kernel<4, MF>;
     }
 }
 
@@ -2424,9 +2423,7 @@ static void launch_seg(int ib, bool mf, int grid, const RegArgs &a, const SegIte
         case 4: launch_seg_t<2, false>(grid, a, items, nit, pinfo, st); break;
         case 5: launch_seg_t<2, true>(grid, a, items, nit, pinfo, st); break;
         case 8: launch_seg_t<4, false>(grid, a, items, nit, pinfo, st); break;
-        case 9: launch_seg_t<4, true>(grid, a, items, nit, pinfo, st); break;
-        case 16: launch_seg_t<8, false>(grid, a, items, nit, pinfo, st); break;
-        default: launch_seg_t<8, true>(grid, a, items, nit, pinfo, st); break;
+        default: launch_seg_t<4, true>(grid, a, items, nit, pinfo, st); break;
     }
 }
 
@@ -2595,8 +2592,11 @@ void nb6_regf_seg_(int *ni_, int *iseg, double *h2, double *dtr, double (*xi)[3]
         }
     const int nrun = (int)run_k0.size();
     run_k0.push_back(ni);
+    // at most 4: the IB = 8 form needs 184 registers (one CTA of 8 warps per
+    // SM) against 112 for IB = 4 (two CTAs), and ran 15-17% slower on
+    // ensembles of 2-100% active bodies
     int ib = 1;
-    while (ib < 8 && ib * nrun < ni) ib <<= 1;
+    while (ib < 4 && ib * nrun < ni) ib <<= 1;
     const int grid_max = nb6_num_sms() * seg_occupancy(ib, mf);
     double work = 0.0;
     for (int r = 0; r < nrun; ++r)

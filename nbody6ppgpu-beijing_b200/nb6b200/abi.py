@@ -277,6 +277,11 @@ class ForceLib:
         return {"reason": reason.value, "blocks": nb.value, "irr_steps": nirr.value, "tblock": tb.value,
                 "nact": nact.value}
 
+    def blocks_mode(self, persistent: bool) -> None:
+        """nb6_blocks_mode_: 1 one persistent launch per nb6_blocks_run_ call,
+        0 (the default) a graph of three launches per block (same results)."""
+        self.lib.nb6_blocks_mode_(_ci(1 if persistent else 0))
+
     def blocks_active(self, nmax: int) -> tuple[np.ndarray, np.ndarray]:
         """nb6_blocks_active_: the last block's active bodies (1-based) and
         corrector rows."""

@@ -101,3 +101,63 @@ def test_block_clock_runs_to_the_limit(nb6):
     step = state[:, 25]
     assert np.all(t0 <= 0.25) and np.all(t0 + step > 0.25 - 1e-15)
     assert r["irr_steps"] >= n
+
+
+@pytest.mark.parametrize("stepr_all", [None, 1.0])
+def test_persistent_and_graph_forms_agree_bit_for_bit(nb6, stepr_all):
+    """The persistent form (one cooperative launch per call, grid barriers
+    between the phases of a block) and the graph form (three launches per
+    block) give the same blocks, active sets, corrector rows, due lists and
+    final state.  stepr_all = 1.0: no regular step due, the run ends at the
+    time limit after many blocks; None: it stops at the first block with a
+    regular-due body."""
+    S = _state(7)
+    if stepr_all is not None:
+        S["stepr"][:] = stepr_all
+    n = S["cl"].n
+    out = {}
+    for persistent in (True, False):
+        _open(nb6, S)
+        try:
+            nb6.blocks_mode(persistent)
+            runs = [nb6.blocks_run(0.25, 100000) for _ in range(3 if stepr_all is None else 1)]
+            addr, rows = nb6.blocks_active(n)
+            due, xv = nb6.blocks_regular(n)
+            out[persistent] = (runs, addr, rows, due, xv, nb6.hermite_get(1, n))
+        finally:
+            nb6.blocks_mode(False)
+            nb6.irr_close(0)
+    (r1, a1, w1, d1, x1, s1), (r0, a0, w0, d0, x0, s0) = out[True], out[False]
+    assert r1 == r0
+    assert sum(r["blocks"] for r in r1) > (1 if stepr_all is None else 10)
+    o1, o0 = np.argsort(a1), np.argsort(a0)
+    np.testing.assert_array_equal(a1[o1], a0[o0])
+    np.testing.assert_array_equal(w1[o1], w0[o0])
+    np.testing.assert_array_equal(d1, d0)
+    np.testing.assert_array_equal(x1, x0)
+    np.testing.assert_array_equal(s1, s0)
+
+
+def test_persistent_form_in_the_ensemble_driver_bit_for_bit(nb6):
+    """The ensemble driver with the device block clock, run once per form
+    (the library call switches the form the driver's calls use): same
+    blocks, steps, state and energies."""
+    from nb6b200 import drive, ics
+    ours = drive.backend_paths("nb6b200")
+    cls = [ics.plummer(n, seed=40 + n, imf=True) for n in (700, 1500, 2300)]
+    kw = dict(batched=True, tcrit=0.25, dt_out=0.125, dev_corrector=3)
+    runs = {}
+    for persistent in (True, False):
+        nb6.blocks_mode(persistent)
+        try:
+            runs[persistent] = drive.run_ensemble(ours, cls, **kw)
+        finally:
+            nb6.blocks_mode(False)
+    a, b = runs[True], runs[False]
+    for key in ("blocks", "irr_steps", "reg_steps", "reg_calls", "nb_sum"):
+        assert a.stats[key] == b.stats[key], key
+    assert a.stats["blocks"] > 100
+    for c in range(len(cls)):
+        np.testing.assert_array_equal(a.x[c], b.x[c])
+        np.testing.assert_array_equal(a.v[c], b.v[c])
+    np.testing.assert_array_equal(a.energy, b.energy)

@@ -77,6 +77,49 @@ def test_irregular_random(nb6, orc, n, lmax, ni):
         nb6.irr_close(0)
 
 
+def test_irregular_large_call_in_chunks(nb6, orc):
+    """A large call runs in chunks whose results are downloaded and copied
+    into the caller's arrays while later chunks compute: 50,000 bodies (four
+    ragged chunks) against the oracle, and bit for bit against the same
+    bodies split over two calls, with preallocated output arrays reused."""
+    from nb6b200 import ics
+    n, lmax, ni = 60000, 80, 50000
+    rng = np.random.default_rng(21)
+    cl = ics.plummer(n, seed=21)
+    lists = np.zeros((n, lmax), dtype=np.int32)
+    for i in range(n):
+        ids = np.unique((i + rng.integers(1, n, int(rng.integers(0, lmax)))) % n) + 1
+        lists[i, 0] = len(ids)
+        lists[i, 1:1 + len(ids)] = ids
+    g = {"x0": cl.pos, "v0": cl.vel, "acc2": rng.normal(size=(n, 3)) * 0.5,
+         "jrk6": rng.normal(size=(n, 3)) * 0.2, "mass": cl.mass,
+         "t0": -rng.integers(0, 16, n) / 2048.0, "lists": lists}
+    addr = np.sort(rng.choice(n, ni, replace=False) + 1).astype(np.int32)
+    load_state(nb6, g)
+    try:
+        ti = 1.0 / 1024
+        out = (np.full((ni, 3), np.nan), np.full((ni, 3), np.nan), np.full(ni, -7, np.int32))
+        acc, jrk, nnbid = nb6.irr_firr_vec(ti, addr, out)
+        oa, oj, oid = orc.firr(ti, addr, g["x0"], g["v0"], g["acc2"], g["jrk6"], g["mass"], g["t0"], lists)
+        ok = lists[addr - 1, 0] > 0
+        assert ok.sum() > 0.9 * ni
+        assert rel_err_vec(acc[ok], oa[ok]).max() <= 1e-6
+        assert rel_err_vec(jrk[ok], oj[ok]).max() <= 1e-5
+        np.testing.assert_array_equal(nnbid, oid)
+        first = [a.copy() for a in (acc, jrk, nnbid)]
+        h = 23457
+        for part in (slice(0, h), slice(h, ni)):
+            pa, pj, pn = nb6.irr_firr_vec(ti, addr[part])
+            np.testing.assert_array_equal(pa, first[0][part])
+            np.testing.assert_array_equal(pj, first[1][part])
+            np.testing.assert_array_equal(pn, first[2][part])
+        acc, jrk, nnbid = nb6.irr_firr_vec(ti, addr, out)        # the same arrays again
+        for a, b in zip((acc, jrk, nnbid), first):
+            np.testing.assert_array_equal(a, b)
+    finally:
+        nb6.irr_close(0)
+
+
 def test_irregular_updates_between_calls(nb6, orc):
     """set_jp / set_list after a firr call take effect on the next call; a
     second set of the same particle before a flush wins."""
