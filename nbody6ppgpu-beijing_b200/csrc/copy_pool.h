@@ -6,12 +6,15 @@
 // the caller's arrays.  One core copies at about 10 GB/s, so for a large
 // irregular call (65,536 bodies, 3.7 MB of acc, jrk and nnbid) that second
 // copy takes longer than the force kernel.  The pool runs it on `parts()`
-// threads (the calling thread is part 0).  Idle helpers spin for up to 1 ms
-// after each job or arm() (calls of a block loop come in quick succession),
-// then sleep on a condition variable.
+// threads (the calling thread is part 0).  Idle helpers spin for up to 2 ms
+// after each job or arm() (force calls come in quick succession: a
+// 1,024-body regular call takes ~1.4 ms), then sleep on a condition
+// variable.
 //
 // NB6_COPY_THREADS sets the number of parts (1 = the calling thread alone);
-// the default is min(4, hardware threads / 2).
+// the default is min(4, hardware threads / 2).  One pool serves the whole
+// library (nb6_copy_pool); its threads start with the first large call and
+// stop when the last of the regular and irregular libraries is closed.
 #pragma once
 
 #include <atomic>
@@ -22,6 +25,8 @@
 #include <mutex>
 #include <thread>
 #include <vector>
+
+#include <unistd.h>
 
 #if defined(__x86_64__) || defined(_M_X64)
 #include <immintrin.h>
@@ -47,13 +52,14 @@ class CopyPool {
     // Start nparts - 1 helpers (no-op when already running).
     void start(int nparts) {
         if (!th_.empty() || nparts <= 1) return;
+        pid_ = getpid();
         quit_.store(false);
         const unsigned g0 = gen_.load();   // helpers wait for the next generation
         for (int p = 1; p < nparts; ++p) th_.emplace_back(&CopyPool::loop, this, p, g0);
     }
 
     void stop() {
-        if (th_.empty()) return;
+        if (th_.empty() || getpid() != pid_) return;
         {
             std::lock_guard<std::mutex> lk(mu_);
             quit_.store(true);
@@ -72,6 +78,10 @@ class CopyPool {
             f(0);
             return;
         }
+        if (getpid() != pid_) {   // a forked child has none of the helpers
+            for (int p = 0; p < parts(); ++p) f(p);
+            return;
+        }
         job_ = std::move(f);
         left_.store((int)th_.size(), std::memory_order_relaxed);
         {
@@ -87,7 +97,7 @@ class CopyPool {
     // caller still waits for the GPU (a futex wake-up can take longer than
     // the copy itself).
     void arm() {
-        if (th_.empty()) return;
+        if (th_.empty() || getpid() != pid_) return;
         {
             std::lock_guard<std::mutex> lk(mu_);
             ++wake_;
@@ -96,7 +106,7 @@ class CopyPool {
     }
 
   private:
-    static constexpr long long SPIN_NS = 1000000;   // spin up to 1 ms before sleeping
+    static constexpr long long SPIN_NS = 2000000;   // spin up to 2 ms before sleeping
 
     void loop(int p, unsigned seen) {
         unsigned woken = 0;
@@ -136,5 +146,6 @@ class CopyPool {
     std::atomic<int> left_{0};
     std::atomic<bool> quit_{false};
     unsigned wake_ = 0;   // under mu_
+    pid_t pid_ = 0;       // the process that started the helpers
     std::function<void(int)> job_;
 };

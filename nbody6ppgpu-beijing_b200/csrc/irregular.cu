@@ -826,17 +826,29 @@ __global__ void __launch_bounds__(BLK_NT) blk_collect(int n, const double *__res
     }
     const int lane = threadIdx.x & 31;
     unsigned long long m2 = ~0ull;  // the others' earliest time (they keep it through this block)
-    for (size_t i0 = blockIdx.x * (size_t)BLK_NT; i0 < (size_t)n; i0 += (size_t)gridDim.x * BLK_NT) {
-        const size_t i = i0 + threadIdx.x;
-        const double ti = i < (size_t)n ? tn[i] : 0.0;
-        const bool on = i < (size_t)n && ti == t;
-        if (i < (size_t)n && !on) m2 = min(m2, (unsigned long long)__double_as_longlong(ti));
-        const unsigned b = __ballot_sync(0xffffffffu, on);
-        if (b) {
-            int base = 0;
-            if (lane == 0) base = atomicAdd(&c->nact[p], __popc(b));
-            base = __shfl_sync(0xffffffffu, base, 0);
-            if (on) act[base + __popc(b & ((1u << lane) - 1u))] = (int)i;
+    // the next times are loaded U per thread at once, all in flight together
+    // (one pass for up to U x grid threads bodies), then tested
+    constexpr int U = 8;
+    const size_t nt = (size_t)gridDim.x * BLK_NT;
+    for (size_t i0 = blockIdx.x * (size_t)BLK_NT; i0 < (size_t)n; i0 += U * nt) {
+        double tv[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const size_t i = i0 + u * nt + threadIdx.x;
+            tv[u] = i < (size_t)n ? tn[i] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const size_t i = i0 + u * nt + threadIdx.x;
+            const bool on = i < (size_t)n && tv[u] == t;
+            if (i < (size_t)n && !on) m2 = min(m2, (unsigned long long)__double_as_longlong(tv[u]));
+            const unsigned b = __ballot_sync(0xffffffffu, on);
+            if (b) {
+                int base = 0;
+                if (lane == 0) base = atomicAdd(&c->nact[p], __popc(b));
+                base = __shfl_sync(0xffffffffu, base, 0);
+                if (on) act[base + __popc(b & ((1u << lane) - 1u))] = (int)i;
+            }
         }
     }
     m2 = cta_min(m2);  // one atomic per CTA (not per warp: they would queue on one address)
@@ -1265,7 +1277,6 @@ struct IrrState {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // irr_kernel of the last call
     cudaStream_t cst = nullptr;                // downloads of the chunks' results
     cudaEvent_t evk[IRR_CHUNKS] = {}, evc[IRR_CHUNKS] = {};   // chunk kernel / download done
-    CopyPool pool;                             // copies into the caller's arrays
     int chunks_max = IRR_CHUNKS;               // nb6_irr_tune_
     // device-resident corrector state (nb6_hermite_open_)
     bool hermite = false;
@@ -1355,6 +1366,7 @@ void irr_open_impl(int nmax, int lmax, int rank) {
         return;
     }
     I.open = true;
+    nb6_lib_opened();
     I.nmax = nmax;
     I.lmax = lmax;
     I.rec.reserve((size_t)nmax + 1);
@@ -1428,7 +1440,7 @@ void irr_close_impl() {
     I.hout.release();
     I.jp_slot.clear();
     I.list_slot.clear();
-    I.pool.stop();
+    nb6_lib_closed();
 }
 
 void irr_set_jp_impl(int a, const double *pos, const double *vel, const double *acc2,
@@ -1646,7 +1658,7 @@ void irr_firr_vec_impl(double ti, int ni, const int *addr, double (*acc)[3], dou
             NB6_CUDA_CHECK(cudaEventCreateWithFlags(&I.evc[c], cudaEventDisableTiming));
         }
     }
-    if (!direct) I.pool.start(CopyPool::default_parts());
+    CopyPool *pool = direct ? nullptr : &nb6_copy_pool();
     auto chunk_lo = [&](int c) { return (int)((long long)ni * c / nch); };
     NB6_CUDA_CHECK(cudaEventRecord(I.ev0, st));
     for (int c = 0; c < nch; ++c) {
@@ -1664,15 +1676,15 @@ void irr_firr_vec_impl(double ti, int ni, const int *addr, double (*acc)[3], dou
     NB6_CUDA_CHECK(cudaEventRecord(I.ev1, st));
     nb6_status_fetch(st);
     unsigned long long inter = 0;
-    if (!direct) I.pool.arm();
+    if (pool) pool->arm();
     if (!direct) {
-        const int np = I.pool.parts();
+        const int np = pool->parts();
         std::vector<unsigned long long> part(np);
         for (int c = 0; c < nch; ++c) {
             NB6_CUDA_CHECK(cudaEventSynchronize(I.evc[c]));
             const int a = chunk_lo(c), m = chunk_lo(c + 1) - a;
             const double *h = I.hout.ptr + 7 * (size_t)a;
-            I.pool.run([&](int p) {
+            pool->run([&](int p) {
                 const int lo = (int)((long long)m * p / np), hi = (int)((long long)m * (p + 1) / np);
                 if (hi <= lo) return;
                 memcpy(&acc[a + lo][0], h + 3 * (size_t)lo, sizeof(double) * 3 * (size_t)(hi - lo));
@@ -1922,6 +1934,13 @@ bool blocks_graph(cudaStream_t st) {
         I.bgraph = nullptr;
     }
     const int sms = nb6_num_sms();
+    // blk_irr: one resident wave of CTAs (they stride over the active set)
+    int irr_occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &irr_occ, ks.slot ? (const void *)blk_irr<true> : (const void *)blk_irr<false>, IRR_WARPS * 32, 0) !=
+            cudaSuccess ||
+        irr_occ < 1)
+        irr_occ = 4;
     cudaGraph_t g = nullptr;
     if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return false;
     // blk_unroll blocks back to back; with blk_pdl every kernel after the
@@ -1944,7 +1963,7 @@ bool blocks_graph(cudaStream_t st) {
         cudaLaunchConfig_t c0 = cfg(sms * 4, BLK_NT, u == 0);
         ok = cudaLaunchKernelEx(&c0, blk_collect, I.nmax, (const double *)I.tn.ptr, I.bctl.ptr, I.bact.ptr) ==
              cudaSuccess;
-        cudaLaunchConfig_t c1 = cfg(sms * 12, IRR_WARPS * 32, false);
+        cudaLaunchConfig_t c1 = cfg(sms * irr_occ, IRR_WARPS * 32, false);
         const BlockCtl *cc = I.bctl.ptr;
         const int *ca = I.bact.ptr, *cl = I.lists.ptr;
         const Rec *cr = I.rec.ptr;

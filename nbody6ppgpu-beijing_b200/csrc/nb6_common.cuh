@@ -258,6 +258,10 @@ int nb6_device_id();               // device picked at devinit (GPU_LIST / NB_GP
 void nb6_devinit_once(int irank);
 cudaStream_t nb6_stream();         // the library's stream (non-blocking)
 int *nb6_dev_status();             // device status word (zeroed at init)
+class CopyPool;
+CopyPool &nb6_copy_pool();         // host copy threads, started on first use (copy_pool.h)
+void nb6_lib_opened();             // gpunb_open_ / irr_simd_open_
+void nb6_lib_closed();             // their closes: the pool stops with the last
 int nb6_check_dev_status();        // read (and clear) after a stream sync
 void nb6_status_fetch(cudaStream_t st);  // enqueue the status copy before that sync
 bool nb6_uva();                    // device reads/writes pinned host memory in place

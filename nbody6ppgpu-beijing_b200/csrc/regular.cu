@@ -24,6 +24,7 @@
 // sent, ascending, self included; nnb > nnbmax -> list[0] = -nnb and no ids
 // (reg.avx.cpp:320-327).
 #include "nb6_common.cuh"
+#include "copy_pool.h"
 #include "mlp.cuh"
 
 #include <cub/device/device_radix_sort.cuh>
@@ -2196,6 +2197,7 @@ void gpunb_open_(int *nbmax, int *irank) {
         return;
     }
     R.open = true;
+    nb6_lib_opened();
     R.nbodymax = *nbmax;
     size_j_buffers(std::max(*nbmax, 1));
     R.nj = 0;
@@ -2234,6 +2236,7 @@ void gpunb_close_() {
     R.houtl.release();
     R.nbodymax = 0;
     R.nj = 0;
+    nb6_lib_closed();
 }
 
 void gpunb_send_(int *nj, double *mj, double (*xj)[3], double (*vj)[3]) {
@@ -2298,11 +2301,15 @@ bool regular_bind_j(int n, double **jm, double **jx, double **jv, JSetOut *out) 
 
 // Results of a finished call, from the pinned staging into the caller's
 // arrays (reference layout: acc/jrk [ni][3], pot [ni], list rows of lmax).
-static void unpack_results(int ni, int W, int lmax, double (*acc)[3], double (*jrk)[3], double *pot,
-                           int *list) {
+// Calls of at least this many bodies stage their inputs and unpack their
+// results on the library's copy threads (copy_pool.h).
+constexpr int POOL_MIN_NI = 256;
+
+static void unpack_rows(int lo, int hi, int W, int lmax, double (*acc)[3], double (*jrk)[3], double *pot,
+                        int *list) {
     const double *of = R.houtf.ptr;
     const int *ol = R.houtl.ptr;
-    for (int i = 0; i < ni; ++i) {
+    for (int i = lo; i < hi; ++i) {
         acc[i][0] = of[8 * i + 0];
         acc[i][1] = of[8 * i + 1];
         acc[i][2] = of[8 * i + 2];
@@ -2316,6 +2323,49 @@ static void unpack_results(int ni, int W, int lmax, double (*acc)[3], double (*j
         dst[0] = nnb;
         if (nnb > 0) memcpy(dst + 1, src + 1, sizeof(int) * nnb);
     }
+}
+
+static void unpack_results(int ni, int W, int lmax, double (*acc)[3], double (*jrk)[3], double *pot,
+                           int *list) {
+    if (ni < POOL_MIN_NI) {
+        unpack_rows(0, ni, W, lmax, acc, jrk, pot, list);
+        return;
+    }
+    CopyPool &pool = nb6_copy_pool();
+    const int np = pool.parts();
+    pool.run([&](int p) {
+        unpack_rows((int)((long long)ni * p / np), (int)((long long)ni * (p + 1) / np), W, lmax, acc, jrk, pot,
+                    list);
+    });
+}
+
+// Stage a call's i data as [h2 | dtr | x | v] in the pinned block h and
+// report whether any value is NaN, in one pass (split over the copy threads
+// for large calls).
+static bool stage_inputs(int ni, double *h, const double *h2, const double *dtr, const double *xi,
+                         const double *vi) {
+    auto part = [&](int lo, int hi) {
+        bool nan = false;
+        for (int k = lo; k < hi; ++k) {
+            h[k] = h2[k];
+            h[ni + k] = dtr[k];
+            nan |= (h2[k] != h2[k]) | (dtr[k] != dtr[k]);
+        }
+        for (int k = 3 * lo; k < 3 * hi; ++k) {
+            h[2 * (size_t)ni + k] = xi[k];
+            h[5 * (size_t)ni + k] = vi[k];
+            nan |= (xi[k] != xi[k]) | (vi[k] != vi[k]);
+        }
+        return nan;
+    };
+    if (ni < POOL_MIN_NI) return part(0, ni);
+    CopyPool &pool = nb6_copy_pool();
+    const int np = pool.parts();
+    bool nan[64] = {};
+    pool.run([&](int p) { nan[p] = part((int)((long long)ni * p / np), (int)((long long)ni * (p + 1) / np)); });
+    bool any = false;
+    for (int p = 0; p < np; ++p) any |= nan[p];
+    return any;
 }
 
 // Diagnostic (NB6_SELFCHECK=1, off by default): re-derive sample rows of a
@@ -2445,8 +2495,12 @@ void gpunb_regf_(int *ni_, double *h2, double *dtr, double (*xi)[3], double (*vi
         nb6_fatal(NB6_ERR_BAD_ARG);
         return;
     }
-    if (any_nan(h2, ni) || any_nan(dtr, ni) || any_nan(&xi[0][0], 3 * (size_t)ni) ||
-        any_nan(&vi[0][0], 3 * (size_t)ni)) {
+    // stage i data: [h2 | dtr | x | v] in one pinned block, one H2D
+    const size_t nin = (size_t)8 * ni;
+    R.hin.reserve(nin);
+    R.iin.reserve(nin);
+    double *h = R.hin.ptr;
+    if (stage_inputs(ni, h, h2, dtr, &xi[0][0], &vi[0][0])) {
         fprintf(stderr, "gpunb_regf: NaN in i-particle input\n");
         nb6_fatal(NB6_ERR_NAN_INPUT);
         return;
@@ -2456,16 +2510,6 @@ void gpunb_regf_(int *ni_, double *h2, double *dtr, double (*xi)[3], double (*vi
     R.ini += ni;
     R.icall++;
     cudaStream_t st = nb6_stream();
-
-    // stage i data: [h2 | dtr | x | v] in one pinned block, one H2D
-    const size_t nin = (size_t)8 * ni;
-    R.hin.reserve(nin);
-    R.iin.reserve(nin);
-    double *h = R.hin.ptr;
-    memcpy(h, h2, sizeof(double) * ni);
-    memcpy(h + ni, dtr, sizeof(double) * ni);
-    memcpy(h + 2 * (size_t)ni, xi, sizeof(double) * 3 * ni);
-    memcpy(h + 5 * (size_t)ni, vi, sizeof(double) * 3 * ni);
     const double *d = R.iin.ptr;
 
     // one submission: H2D of the staged i data, force kernel, finalize and
@@ -2477,6 +2521,7 @@ void gpunb_regf_(int *ni_, double *h2, double *dtr, double (*xi)[3], double (*vi
     const int W = L.W;
     regf_submit(L, st);
     nb6_status_fetch(st);
+    if (ni >= POOL_MIN_NI) nb6_copy_pool().arm();   // the helpers spin while the GPU works
     NB6_CUDA_CHECK(cudaStreamSynchronize(st));
     NB6_CUDA_CHECK(cudaEventElapsedTime(&R.last_kernel_ms, R.ev0, R.ev1));
     const double wt = nb6_wtime();

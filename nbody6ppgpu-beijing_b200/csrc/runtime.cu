@@ -12,6 +12,7 @@
 // default.  nb6_set_abort_on_error_(0) switches to "record and return": the
 // call does no work and nb6_last_status_() reports the code.
 #include "nb6_common.cuh"
+#include "copy_pool.h"
 
 #include <string.h>
 
@@ -84,6 +85,21 @@ void nb6_devinit_once(int irank) {
 }
 
 int nb6_device_id() { return g_device; }
+static CopyPool g_pool;
+static int g_open_libs = 0;
+
+CopyPool &nb6_copy_pool() {
+    g_pool.start(CopyPool::default_parts());
+    return g_pool;
+}
+void nb6_lib_opened() { ++g_open_libs; }
+void nb6_lib_closed() {
+    if (--g_open_libs <= 0) {
+        g_open_libs = 0;
+        g_pool.stop();
+    }
+}
+
 int nb6_num_sms() { return g_num_sms; }
 cudaStream_t nb6_stream() { return g_stream; }
 int *nb6_dev_status() { return g_dev_status; }
