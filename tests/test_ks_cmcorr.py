@@ -1,6 +1,7 @@
 """KS c.m. corrections of the irregular force (cmfirr_cor.f, cmfirr_ucor.f).
 
-CPU: the oracle's restatement against an independent numpy evaluation of
+CPU: the oracle's restatement against the two routines restated statement
+by statement (bit for bit), against an independent numpy evaluation of
 what the corrections stand for (each perturbed pair's components in place
 of its point mass) and against the limit of components at the c.m.
 GPU: irr_simd_firr_vec_ / nb6_irr_correct_ with a pair table set
@@ -60,7 +61,7 @@ def _system(seed, ns=600, npair=40, nperturbed=30, sep=3e-3, lmax=96):
     slot[cm - 1] = np.arange(nperturbed)
     active = np.sort(np.concatenate([rng.choice(ns, 150, replace=False) + 1, cm[:20],
                                      ns + 1 + np.setdiff1d(np.arange(npair), pert)[:5]])).astype(np.int32)
-    return dict(ti=ti, x0=x0, v0=v0, f=f, fd=fd, m=m, t0=t0, lists=lists, cm=cm, xk=xk, vk=vk, mk=mk,
+    return dict(ti=ti, x0=x0, v0=v0, f=f, fd=fd, m=m, t0=t0, lists=lists, cm=cm, xk=xk, vk=vk, mk=mk, n_single=ns,
                 pofs=np.array(pofs, dtype=np.int32), plist=np.array(plist, dtype=np.int32), slot=slot,
                 active=active, xp=xp, vp=vp)
 
@@ -117,6 +118,136 @@ def _numpy_corrections(S):
     return np.array(out_a), np.array(out_j)
 
 
+def _reference_routines(S):
+    """CMFIRR_COR (cmfirr_cor.f:1-136) and CMFIRR_UCOR (cmfirr_ucor.f:1-116)
+    as nbint_cor.f:40-79 calls them, statement by statement in the
+    routines' own order and control flow: a perturbed c.m. body gets
+    CMFIRR_COR over its first component's perturber list (and no
+    CMFIRR_UCOR, nbint_cor.f:66-75); any other body CMFIRR_UCOR over the
+    c.m. bodies at the end of its ascending neighbour list
+    (nbint_cor.f:77-79).  X, XDOT are the predicted bodies (jpred_int.f),
+    the components of perturbed pairs stand for X(J1), X(J2).  Returns the
+    corrections alone (FIRR, FD starting at zero)."""
+    xp, vp, m, slot = S["xp"], S["vp"], S["m"], S["slot"]
+    N = S["n_single"]       # bodies 0 .. N-1 are singles, the rest c.m. bodies
+    out_a, out_j = [], []
+
+    def pert(j):            # LIST(1,J1) > 0: the pair of c.m. body j (0-based) is perturbed
+        return slot[j] >= 0
+
+    for a in S["active"]:
+        I = a - 1
+        firr = [0.0, 0.0, 0.0]
+        fd = [0.0, 0.0, 0.0]
+        row = S["lists"][I]
+        nnb0 = int(row[0])
+        if nnb0 == 0:                       # nbint_cor.f:44-55 is the caller's own force
+            out_a.append(firr)
+            out_j.append(fd)
+            continue
+        if pert(I):
+            # CMFIRR_COR(I, I1, FIRR, FD)
+            p = slot[I]
+            x1, x2 = S["xk"][p]
+            v1, v2 = S["vk"][p]
+            b1, b2 = S["mk"][p]
+            for J in S["plist"][S["pofs"][p]:S["pofs"][p + 1]] - 1:
+                K = J
+                xk = [None, None]
+                vk = [None, None]
+                bk = [None, None]
+                if slot[J] >= 0:            # J > N with LIST(1,J1) > 0
+                    q = slot[J]
+                    xk = [S["xk"][q][0], S["xk"][q][1]]
+                    vk = [S["vk"][q][0], S["vk"][q][1]]
+                    bk = [S["mk"][q][0], S["mk"][q][1]]
+                    K = -1                  # K = J1
+                if K == J:
+                    xk[0], vk[0], bk[0] = xp[J], vp[J], m[J]
+                A1 = xp[J][0] - xp[I][0]
+                A2 = xp[J][1] - xp[I][1]
+                A3 = xp[J][2] - xp[I][2]
+                RIJ2 = A1 * A1 + A2 * A2 + A3 * A3
+                DV = [vp[J][0] - vp[I][0], vp[J][1] - vp[I][1], vp[J][2] - vp[I][2]]
+                DR2I = 1.0 / RIJ2
+                DR3I = m[J] * DR2I * np.sqrt(DR2I)
+                DRDV = 3.0 * (A1 * DV[0] + A2 * DV[1] + A3 * DV[2]) * DR2I
+                FCM = [A1 * DR3I, A2 * DR3I, A3 * DR3I]
+                FCMD = [(DV[0] - A1 * DRDV) * DR3I, (DV[1] - A2 * DRDV) * DR3I, (DV[2] - A3 * DRDV) * DR3I]
+                comp = 0
+                while True:                 # label 20
+                    FP, FPD = [0.0] * 6, [0.0] * 6
+                    for half, (xc, vc) in enumerate(((x1, v1), (x2, v2))):
+                        dr2 = 0.0
+                        drdv = 0.0
+                        dx = [0.0] * 3
+                        dv = [0.0] * 3
+                        for L in range(3):
+                            dx[L] = xk[comp][L] - xc[L]
+                            dv[L] = vk[comp][L] - vc[L]
+                            dr2 = dr2 + dx[L] ** 2
+                            drdv = drdv + dx[L] * dv[L]
+                        dr2i = 1.0 / dr2
+                        dr3i = bk[comp] * dr2i * np.sqrt(dr2i)
+                        drdv = 3.0 * drdv * dr2i
+                        for L in range(3):
+                            FP[L + 3 * half] = dx[L] * dr3i
+                            FPD[L + 3 * half] = (dv[L] - dx[L] * drdv) * dr3i
+                    for L in range(3):
+                        firr[L] = firr[L] + ((b1 * FP[L] + b2 * FP[L + 3]) / m[I] - FCM[L])
+                        fd[L] = fd[L] + ((b1 * FPD[L] + b2 * FPD[L + 3]) / m[I] - FCMD[L])
+                    if K == -1 and comp == 0:   # the perturber's second component, no c.m. term
+                        FCM = [0.0, 0.0, 0.0]
+                        FCMD = [0.0, 0.0, 0.0]
+                        comp = 1
+                        continue
+                    break
+        else:
+            # CMFIRR_UCOR(I, NNB0, LIST(1,I), FIRR, FD): the c.m. neighbours
+            # sit at the end of the ascending list
+            klist = row[1:1 + nnb0] - 1
+            nnb2 = nnb0                     # the list up to its last single
+            while nnb2 >= 1 and klist[nnb2 - 1] >= N:
+                nnb2 -= 1
+            for J in klist[nnb2:]:
+                if not pert(J):             # unperturbed binary: a single particle
+                    continue
+                q = slot[J]
+                A1 = xp[J][0] - xp[I][0]
+                A2 = xp[J][1] - xp[I][1]
+                A3 = xp[J][2] - xp[I][2]
+                RIJ2 = A1 * A1 + A2 * A2 + A3 * A3
+                DV = [vp[J][0] - vp[I][0], vp[J][1] - vp[I][1], vp[J][2] - vp[I][2]]
+                DR2I = 1.0 / RIJ2
+                DR3I = m[J] * DR2I * np.sqrt(DR2I)
+                DRDV = 3.0 * (A1 * DV[0] + A2 * DV[1] + A3 * DV[2]) * DR2I
+                FCM = [A1 * DR3I, A2 * DR3I, A3 * DR3I]
+                FCMD = [(DV[0] - A1 * DRDV) * DR3I, (DV[1] - A2 * DRDV) * DR3I, (DV[2] - A3 * DRDV) * DR3I]
+                FP, FPD = [0.0] * 6, [0.0] * 6
+                for half in range(2):
+                    dr2 = 0.0
+                    drdv = 0.0
+                    dx = [0.0] * 3
+                    dv = [0.0] * 3
+                    for L in range(3):
+                        dx[L] = S["xk"][q][half][L] - xp[I][L]
+                        dv[L] = S["vk"][q][half][L] - vp[I][L]
+                        dr2 = dr2 + dx[L] ** 2
+                        drdv = drdv + dx[L] * dv[L]
+                    dr2i = 1.0 / dr2
+                    dr3i = S["mk"][q][half] * dr2i * np.sqrt(dr2i)
+                    drdv = 3.0 * drdv * dr2i
+                    for L in range(3):
+                        FP[L + 3 * half] = dx[L] * dr3i
+                        FPD[L + 3 * half] = (dv[L] - dx[L] * drdv) * dr3i
+                for L in range(3):
+                    firr[L] = firr[L] + (FP[L] + FP[L + 3] - FCM[L])
+                    fd[L] = fd[L] + (FPD[L] + FPD[L + 3] - FCMD[L])
+        out_a.append(firr)
+        out_j.append(fd)
+    return np.array(out_a), np.array(out_j)
+
+
 def _oracle_corrections(orc, S, acc=None, jrk=None):
     ni = len(S["active"])
     acc = np.zeros((ni, 3)) if acc is None else acc
@@ -134,6 +265,22 @@ def test_oracle_corrections_match_direct_evaluation(orc):
     scale_j = np.abs(nj).max()
     np.testing.assert_allclose(ca, na, rtol=0, atol=1e-9 * scale_a)
     np.testing.assert_allclose(cj, nj, rtol=0, atol=1e-9 * scale_j)
+
+
+@pytest.mark.parametrize("seed", [11, 14])
+def test_oracle_corrections_equal_the_reference_routines(orc, seed):
+    """The oracle's corrections against CMFIRR_COR / CMFIRR_UCOR restated
+    statement by statement (their control flow and operation order): the
+    same values, bit for bit.  The system has perturbers that are perturbed
+    pairs themselves (CMFIRR_COR's second pass, GO TO 20), unperturbed c.m.
+    neighbours (skipped by CMFIRR_UCOR) and bodies whose lists end in c.m.
+    bodies only."""
+    S = _system(seed)
+    ca, cj = _oracle_corrections(orc, S)
+    ra, rj = _reference_routines(S)
+    assert np.abs(ra).max() > 0
+    np.testing.assert_array_equal(ca, ra)
+    np.testing.assert_array_equal(cj, rj)
 
 
 def test_oracle_corrections_vanish_for_components_at_the_cm(orc):
