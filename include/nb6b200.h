@@ -271,7 +271,7 @@ void nb6_blocks_active_(int *nact, int *addr, double *rows);
 void nb6_irr_tune_(int *chunks);
 /* Form of the device block clock for the following nb6_blocks_run_ calls
  * (no reference counterpart): *persistent = 0 (the default) runs each block
- * as a CUDA graph of three launches; 1 (or environment NB6_BLK_PERSIST=1)
+ * as a CUDA graph of two launches; 1 (or environment NB6_BLK_PERSIST=1)
  * runs a whole call as one cooperative launch that loops over blocks, with
  * two grid-wide barriers per block.  Both give the same results bit for
  * bit. */

@@ -111,7 +111,13 @@ NB6_DEV void cm_pair(const double *xi, const double *vi, const double *xj, const
 // term (cmfirr_ucor.f:14-116); for i itself the c.m. of a perturbed pair,
 // the perturbation terms over its perturber list are added instead
 // (cmfirr_cor.f:13-130).  An empty list gets no corrections.
-template <bool KS, bool CG = false>
+// DEEP: the ids of two rounds are loaded with the list header and the
+// records of both rounds before their arithmetic -- fewer dependent round
+// trips for one body's walk (the block clock's small blocks are bound by
+// that latency) at the cost of registers (the bulk calls keep the plain
+// walk's occupancy).  Each lane sums its entries l = lane, lane + 32, ...
+// in that order either way, so both forms give the same bits.
+template <bool KS, bool CG = false, bool DEEP = false>
 NB6_DEV void irr_force_warp(int i, int lane, double ti, const Rec *__restrict__ rec,
                             const int *__restrict__ lists, int ls, int nmax, const KsArgs &ks, double *a,
                             double *jd, int &nnbid) {
@@ -126,11 +132,7 @@ NB6_DEV void irr_force_warp(int i, int lane, double ti, const Rec *__restrict__ 
     double ax = 0, ay = 0, az = 0, jx = 0, jy = 0, jz = 0;
     double rmin = 1.0e300;
     int jmin = 0x7fffffff;
-    for (int l = lane; l < nnb; l += 32) {
-        const int j = row[1 + l];
-        if (j < 0 || j >= nmax) continue;   // ids are checked at set_list time
-        Rec rj;
-        load_rec<CG>(rec + j, rj);
+    auto add = [&](const Rec &rj, int j) {
         double xj[3], vj[3];
         predict(rj, ti, xj, vj);
         const double dxd = xj[0] - xi[0], dyd = xj[1] - xi[1], dzd = xj[2] - xi[2];
@@ -152,7 +154,7 @@ NB6_DEV void irr_force_warp(int i, int lane, double ti, const Rec *__restrict__ 
                 jy += fd[1];
                 jz += fd[2];
             }
-            continue;
+            return;
         }
         // The list walk is bound by the record gathers, not by arithmetic,
         // so the pair math stays in FP64 (nbint.F:143-158).
@@ -167,6 +169,33 @@ NB6_DEV void irr_force_warp(int i, int lane, double ti, const Rec *__restrict__ 
         jx += mr3 * (dvx + al * dxd);
         jy += mr3 * (dvy + al * dyd);
         jz += mr3 * (dvz + al * dzd);
+    };
+    if (DEEP) {
+        int jn0 = 1 + lane < ls ? row[1 + lane] : -1;
+        int jn1 = 33 + lane < ls ? row[33 + lane] : -1;
+        for (int base = 0; base < nnb; base += 64) {
+            const int j0 = base + lane < nnb ? jn0 : -1;
+            const int j1 = base + 32 + lane < nnb ? jn1 : -1;
+            if (base + 64 < nnb) {
+                const int l = base + 65 + lane;
+                jn0 = l < ls ? row[l] : -1;
+                jn1 = l + 32 < ls ? row[l + 32] : -1;
+            }
+            const bool v0 = j0 >= 0 && j0 < nmax, v1 = j1 >= 0 && j1 < nmax;   // ids are checked at set_list time
+            Rec r0, r1;
+            if (v0) load_rec<CG>(rec + j0, r0);
+            if (v1) load_rec<CG>(rec + j1, r1);
+            if (v0) add(r0, j0);
+            if (v1) add(r1, j1);
+        }
+    } else {
+        for (int l = lane; l < nnb; l += 32) {
+            const int j = row[1 + l];
+            if (j < 0 || j >= nmax) continue;   // ids are checked at set_list time
+            Rec rj;
+            load_rec<CG>(rec + j, rj);
+            add(rj, j);
+        }
     }
     if (KS && pi >= 0 && nnb > 0) {
         // i is the c.m. of a perturbed pair: perturbation of its components
@@ -730,23 +759,29 @@ __global__ void reg_corrector_kernel(int ni, const int *__restrict__ addr, const
 
 // ----------------------------------------------------------------------------
 // Device block clock (nb6_blocks_run_): blocks of irregular steps run back to
-// back on the device, each as three launches of one CUDA graph --
-//   blk_collect  the active set {i : tn_i == block time} (next_tlist.f picks
-//                the same set from its level lists), or a stop when the
+// back on the device, each as two launches of one CUDA graph --
+//   blk_collect  first the new records of the block before (see blk_step),
+//                then the active set {i : tn_i == block time} (next_tlist.f
+//                picks the same set from its level lists), or a stop when the
 //                block time passes the caller's limit; also the earliest tn
 //                of the other bodies, which this block leaves as they are;
-//   blk_irr      the neighbour force of every active body (irr_force_warp);
-//   blk_corr     the irregular corrector of every active body (the same
-//                correct_irr_body as nb6_irr_correct_), then, in the last CTA
-//                to finish, the block's bookkeeping, the next block time (the
-//                earlier of the others' earliest tn and the block's new
-//                ones) and a stop when a body is due a regular step (the
-//                host runs the regular part).
+//   blk_step     one warp per active body: its neighbour force
+//                (irr_force_warp), then on lane 0 its irregular corrector
+//                (correct_state, as nb6_irr_correct_ does), with the body's
+//                new aux and tn written in place and its new record kept in
+//                its corrector row until the next blk_collect -- other warps
+//                of this block still read the old record of i as a
+//                neighbour, predicted from its old state, as the host does;
+//                then, in the last CTA to finish, the block's bookkeeping,
+//                the next block time (the earlier of the others' earliest tn
+//                and the block's new ones) and a stop when a body is due a
+//                regular step (the host runs the regular part).
 // The first block time of a run is the minimum over every body (blk_min,
-// launched once per run).
-// A stopped control block turns every later launch into an early return, so
-// the host enqueues many blocks and synchronises once.  No kernel waits on
-// another: the ordering is the stream's, the last-CTA test is one atomic.
+// launched once per run); blk_flush writes the last block's records when a
+// run ends.  A stopped control block turns every later launch into an early
+// return, so the host enqueues many blocks and synchronises once.  No
+// kernel waits on another: the ordering is the stream's, the last-CTA test
+// is one atomic.
 // ----------------------------------------------------------------------------
 struct BlockCtl {
     unsigned long long tmin_bits[2];  // per parity: the block time, min tn (bits of a non-negative double)
@@ -757,7 +792,7 @@ struct BlockCtl {
     int stop;                         // 0 run; 1 a regular-due block's irregular part is done; 2 block time > tlimit;
                                       // 3 the run's block limit reached
     int regdue;                       // the running block has a regular-due body
-    unsigned cta_done;                // blk_corr CTAs finished (last-CTA test)
+    unsigned cta_done;                // blk_step CTAs finished (last-CTA test)
     long long blocks, irr_steps;      // since the last reset by the host
     double tlimit, tblock;            // run limit; time of the last block done
     int last_nact;
@@ -767,6 +802,10 @@ struct BlockCtl {
     // holds the last block's active set
     unsigned bar_count, bar_gen;
     int last_parity;
+    // graph form: the block whose new records blk_collect still has to write
+    // (its active count, act[] half and time; pend_na = 0: none)
+    int pend_na, pend_parity;
+    double pend_t;
 };
 
 constexpr int BLK_NT = 256;
@@ -810,9 +849,33 @@ __global__ void __launch_bounds__(BLK_NT) blk_min(int n, const double *__restric
     if (threadIdx.x == 0) atomicMin(&c->tmin_bits[p], m);
 }
 
+// The new records of the block before (x0, v0, F, FDOT from its corrector
+// rows, t0 = its time); act holds both halves.
+NB6_DEV void blk_scatter_pending(const BlockCtl *c, const int *__restrict__ act, int n,
+                                 const double *__restrict__ rows, Rec *__restrict__ rec) {
+    const int na = c->pend_na;
+    if (na <= 0) return;
+    const int *ap = act + (size_t)c->pend_parity * n;
+    const double t = c->pend_t;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < na; k += gridDim.x * blockDim.x) {
+        const double *o = rows + (size_t)k * 24;
+        Rec *r = rec + ap[k];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            r->x[d] = o[d];
+            r->v[d] = o[3 + d];
+            r->f[d] = o[12 + d];
+            r->fd[d] = o[15 + d];
+        }
+        r->t0 = t;
+    }
+}
+
 __global__ void __launch_bounds__(BLK_NT) blk_collect(int n, const double *__restrict__ tn, BlockCtl *c,
-                                                      int *__restrict__ act) {
+                                                      int *__restrict__ act, const double *__restrict__ rows,
+                                                      Rec *__restrict__ rec) {
     blk_enter();
+    blk_scatter_pending(c, act, n, rows, rec);
     if (c->stop) return;
     if (c->blocks >= c->blimit) {  // every thread reads the same count: all return
         if (blockIdx.x == 0 && threadIdx.x == 0) c->stop = 3;
@@ -825,6 +888,7 @@ __global__ void __launch_bounds__(BLK_NT) blk_collect(int n, const double *__res
         return;
     }
     const int lane = threadIdx.x & 31;
+    act += (size_t)c->parity * n;   // this block's half
     unsigned long long m2 = ~0ull;  // the others' earliest time (they keep it through this block)
     // the next times are loaded U per thread at once, all in flight together
     // (one pass for up to U x grid threads bodies), then tested
@@ -860,53 +924,42 @@ __global__ void __launch_bounds__(BLK_NT) blk_collect(int n, const double *__res
 
 template <bool KS>
 __global__ void __launch_bounds__(IRR_WARPS * 32)
-    blk_irr(const BlockCtl *c, const int *__restrict__ act, const Rec *__restrict__ rec,
-            const int *__restrict__ lists, int ls, int nmax, KsArgs ks, double *__restrict__ out) {
+    blk_step(BlockCtl *c, const int *__restrict__ act, int n, const Rec *__restrict__ rec, Aux *__restrict__ aux,
+             const int *__restrict__ lists, int ls, KsArgs ks, HermiteParams hp, double *__restrict__ rows,
+             double *__restrict__ tn, int *__restrict__ reg, double *__restrict__ regxv) {
     blk_enter();
+    if (blockIdx.x == 0 && threadIdx.x == 0) c->pend_na = 0;   // blk_collect has written them
     if (c->stop) return;
     const int p = c->parity, na = c->nact[p];
     const double t = __longlong_as_double((long long)c->tmin_bits[p]);
+    const int *ap = act + (size_t)p * n;
     const int lane = threadIdx.x & 31;
-    for (int k = blockIdx.x * IRR_WARPS + (threadIdx.x >> 5); k < na; k += gridDim.x * IRR_WARPS) {
-        double a[3], jd[3];
-        int id;
-        irr_force_warp<KS>(act[k], lane, t, rec, lists, ls, nmax, ks, a, jd, id);
-        if (lane == 0) {
-            double *o = out + (size_t)k * 8;
-            o[0] = a[0];
-            o[1] = a[1];
-            o[2] = a[2];
-            o[3] = jd[0];
-            o[4] = jd[1];
-            o[5] = jd[2];
-            o[6] = (double)id;
-            o[7] = 0.0;
-        }
-    }
-}
-
-__global__ void __launch_bounds__(BLK_NT)
-    blk_corr(BlockCtl *c, const int *__restrict__ act, const double *__restrict__ force, Rec *__restrict__ rec,
-             Aux *__restrict__ aux, HermiteParams hp, double *__restrict__ rows, double *__restrict__ tn,
-             int *__restrict__ reg, double *__restrict__ regxv) {
-    blk_enter();
-    if (c->stop) return;
-    const int p = c->parity, na = c->nact[p];
-    const double t = __longlong_as_double((long long)c->tmin_bits[p]);
     bool due = false;
-    unsigned long long mact = ~0ull;  // earliest new tn of this thread's bodies
-    for (int k = blockIdx.x * BLK_NT + threadIdx.x; k < na; k += gridDim.x * BLK_NT) {
-        double *o = rows + (size_t)k * 24;
-        const int i = act[k];
-        if (correct_irr_body(i, t, force + (size_t)k * 8, rec, aux, hp, o, tn)) {
-            due = true;
-            const int q = atomicAdd(&c->nreg, 1);  // (q < na <= nmax)
-            reg[q] = i;
-            for (int d = 0; d < 6; ++d) regxv[6 * (size_t)q + d] = o[d];  // x0, v0
+    unsigned long long mact = ~0ull;  // earliest new tn of this CTA's bodies
+    for (int k = blockIdx.x * IRR_WARPS + (threadIdx.x >> 5); k < na; k += gridDim.x * IRR_WARPS) {
+        const int i = ap[k];
+        double fk[8];
+        int id;
+        irr_force_warp<KS, false, !KS>(i, lane, t, rec, lists, ls, n, ks, fk, fk + 3, id);
+        if (lane == 0) {
+            fk[6] = (double)id;
+            fk[7] = 0.0;
+            Rec r = rec[i];
+            Aux x = aux[i];
+            double *o = rows + (size_t)k * 24;
+            if (correct_state(r, x, t, fk, hp, o)) {
+                due = true;
+                const int q = atomicAdd(&c->nreg, 1);  // (q < na <= n)
+                reg[q] = i;
+                for (int d = 0; d < 6; ++d) regxv[6 * (size_t)q + d] = o[d];  // x0, v0
+            }
+            aux[i] = x;
+            const double tnew = dadd(r.t0, x.step);
+            tn[i] = tnew;
+            mact = min(mact, (unsigned long long)__double_as_longlong(tnew));
         }
-        mact = min(mact, (unsigned long long)__double_as_longlong(tn[i]));
     }
-    mact = cta_min(mact);
+    mact = cta_min<IRR_WARPS * 32>(mact);
     if (threadIdx.x == 0) atomicMin(&c->mact_bits[p], mact);
     if (__syncthreads_or(due) && threadIdx.x == 0) atomicOr(&c->regdue, 1);
     if (threadIdx.x == 0) {
@@ -919,6 +972,10 @@ __global__ void __launch_bounds__(BLK_NT)
             c->irr_steps += na;
             c->tblock = t;
             c->last_nact = na;
+            c->last_parity = p;
+            c->pend_na = na;
+            c->pend_parity = p;
+            c->pend_t = t;
             // the next block's time: the earliest of the bodies outside this
             // block (unchanged by it) and of this block's new times
             c->tmin_bits[q] = min(atomicAdd(&c->m2_bits[p], 0ull), atomicAdd(&c->mact_bits[p], 0ull));
@@ -929,6 +986,12 @@ __global__ void __launch_bounds__(BLK_NT)
             if (atomicExch(&c->regdue, 0)) c->stop = 1;
         }
     }
+}
+
+// The last block's new records, when a run ends.
+__global__ void blk_flush(BlockCtl *c, const int *__restrict__ act, int n, const double *__restrict__ rows,
+                          Rec *__restrict__ rec) {
+    blk_scatter_pending(c, act, n, rows, rec);
 }
 
 // ----------------------------------------------------------------------------
@@ -942,13 +1005,13 @@ __global__ void __launch_bounds__(BLK_NT)
 //      tn[i] written in place and the new record kept in the body's out
 //      row until phase A of the next block -- other warps of this block
 //      still read the old record of i as a neighbour, predicted from its
-//      old state, exactly as blk_irr does before blk_corr runs.
-// The last CTA at the barrier after B does blk_corr's bookkeeping.  Data
+//      old state, exactly as in the graph form's blk_step.
+// The last CTA at the barrier after B does blk_step's bookkeeping.  Data
 // written by other CTAs of the launch (records, tn, aux, the active set,
 // out rows) is read through L2 only (ld.global.cg), after the barrier's
 // fences.  The active set alternates between two halves of act[] (phase A
 // reads the previous block's half while it writes the next one).
-// Results are those of the three-kernel form, bit for bit.
+// Results are those of the graph form, bit for bit.
 // ----------------------------------------------------------------------------
 #ifndef PB_THREADS
 #define PB_THREADS 256
@@ -1114,7 +1177,7 @@ __global__ void __launch_bounds__(NT, 1)
         if (threadIdx.x == 0) atomicMin(&c->mact_bits[p], mact);
         if (__syncthreads_or(due) && threadIdx.x == 0) atomicOr(&c->regdue, 1);
         const bool go = grid_sync(c, status, [&] {
-            // the block is done (blk_corr's last-CTA bookkeeping)
+            // the block is done (blk_step's last-CTA bookkeeping)
             const int q = p ^ 1;
             c->blocks += 1;
             c->irr_steps += na;
@@ -1299,11 +1362,11 @@ struct IrrState {
     DevBuf<double> tn;
     bool clock_dirty = true;
     DevBuf<int> bact;                 // active set of the running block
-    DevBuf<double> bforce, brows;     // its force rows [nmax][8], corrector rows [nmax][24]
+    DevBuf<double> brows;             // its corrector rows [nmax][24]
     DevBuf<BlockCtl> bctl;
     HostBuf<BlockCtl> hctl;
     cudaGraphExec_t bgraph = nullptr;
-    const void *bgraph_key[8] = {};   // buffers and pair-table flag the graph was made with
+    const void *bgraph_key[11] = {};  // buffers, size and pair table the graph was made with
     int blk_batch = 16;               // blocks per synchronisation
     int blk_unroll = 0;               // blocks per graph (NB6_BLK_UNROLL, default 4)
     bool blk_pdl = true;              // programmatic edges between the block kernels (NB6_BLK_PDL=0: off)
@@ -1410,7 +1473,6 @@ void irr_close_impl() {
     I.bsort.release();
     I.bsortxv.release();
     I.bsort_tmp.release();
-    I.bforce.release();
     I.brows.release();
     I.bctl.release();
     I.hctl.release();
@@ -1925,8 +1987,9 @@ bool blocks_persist(cudaStream_t st, int max_blocks, BlockCtl &h) {
 
 bool blocks_graph(cudaStream_t st) {
     const KsArgs ks = ks_args();
-    const void *key[8] = {I.bact.ptr, I.bforce.ptr, I.brows.ptr, I.bctl.ptr, I.tn.ptr, I.breg.ptr, I.bregxv.ptr,
-                          ks.slot ? (const void *)I.ks_slot.ptr : nullptr};
+    const void *key[11] = {I.bact.ptr, I.brows.ptr, I.bctl.ptr, I.tn.ptr, I.breg.ptr, I.bregxv.ptr, I.rec.ptr,
+                           I.aux.ptr, I.lists.ptr, ks.slot ? (const void *)I.ks_slot.ptr : nullptr,
+                           reinterpret_cast<const void *>((size_t)I.nmax)};
     // (a pair table's layout depends on its size: with one set, capture anew)
     if (I.bgraph && memcmp(key, I.bgraph_key, sizeof(key)) == 0 && !ks.slot) return true;
     if (I.bgraph) {
@@ -1934,13 +1997,13 @@ bool blocks_graph(cudaStream_t st) {
         I.bgraph = nullptr;
     }
     const int sms = nb6_num_sms();
-    // blk_irr: one resident wave of CTAs (they stride over the active set)
-    int irr_occ = 0;
+    // blk_step: one resident wave of CTAs (they stride over the active set)
+    int step_occ = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &irr_occ, ks.slot ? (const void *)blk_irr<true> : (const void *)blk_irr<false>, IRR_WARPS * 32, 0) !=
-            cudaSuccess ||
-        irr_occ < 1)
-        irr_occ = 4;
+            &step_occ, ks.slot ? (const void *)blk_step<true> : (const void *)blk_step<false>, IRR_WARPS * 32,
+            0) != cudaSuccess ||
+        step_occ < 1)
+        step_occ = 4;
     cudaGraph_t g = nullptr;
     if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return false;
     // blk_unroll blocks back to back; with blk_pdl every kernel after the
@@ -1961,23 +2024,17 @@ bool blocks_graph(cudaStream_t st) {
     bool ok = true;
     for (int u = 0; u < I.blk_unroll && ok; ++u) {
         cudaLaunchConfig_t c0 = cfg(sms * 4, BLK_NT, u == 0);
-        ok = cudaLaunchKernelEx(&c0, blk_collect, I.nmax, (const double *)I.tn.ptr, I.bctl.ptr, I.bact.ptr) ==
-             cudaSuccess;
-        cudaLaunchConfig_t c1 = cfg(sms * irr_occ, IRR_WARPS * 32, false);
-        const BlockCtl *cc = I.bctl.ptr;
+        ok = cudaLaunchKernelEx(&c0, blk_collect, I.nmax, (const double *)I.tn.ptr, I.bctl.ptr, I.bact.ptr,
+                                (const double *)I.brows.ptr, I.rec.ptr) == cudaSuccess;
+        cudaLaunchConfig_t c1 = cfg(sms * step_occ, IRR_WARPS * 32, false);
         const int *ca = I.bact.ptr, *cl = I.lists.ptr;
         const Rec *cr = I.rec.ptr;
         if (ok && ks.slot)
-            ok = cudaLaunchKernelEx(&c1, blk_irr<true>, cc, ca, cr, cl, I.lmax, I.nmax, ks, I.bforce.ptr) ==
-                 cudaSuccess;
+            ok = cudaLaunchKernelEx(&c1, blk_step<true>, I.bctl.ptr, ca, I.nmax, cr, I.aux.ptr, cl, I.lmax, ks, I.hp,
+                                    I.brows.ptr, I.tn.ptr, I.breg.ptr, I.bregxv.ptr) == cudaSuccess;
         else if (ok)
-            ok = cudaLaunchKernelEx(&c1, blk_irr<false>, cc, ca, cr, cl, I.lmax, I.nmax, ks, I.bforce.ptr) ==
-                 cudaSuccess;
-        cudaLaunchConfig_t c2 = cfg(sms * 2, BLK_NT, false);
-        if (ok)
-            ok = cudaLaunchKernelEx(&c2, blk_corr, I.bctl.ptr, ca, (const double *)I.bforce.ptr, I.rec.ptr,
-                                    I.aux.ptr, I.hp, I.brows.ptr, I.tn.ptr, I.breg.ptr, I.bregxv.ptr) ==
-                 cudaSuccess;
+            ok = cudaLaunchKernelEx(&c1, blk_step<false>, I.bctl.ptr, ca, I.nmax, cr, I.aux.ptr, cl, I.lmax, ks,
+                                    I.hp, I.brows.ptr, I.tn.ptr, I.breg.ptr, I.bregxv.ptr) == cudaSuccess;
     }
     if (cudaStreamEndCapture(st, &g) != cudaSuccess || !g || !ok) {
         if (g) cudaGraphDestroy(g);
@@ -2015,7 +2072,6 @@ void blocks_run_impl(double tlimit, int max_blocks, int *reason, long long *nblo
     cudaStream_t st = nb6_stream();
     irr_flush(st);
     I.bact.reserve((size_t)I.nmax * 2);
-    I.bforce.reserve((size_t)I.nmax * 8);
     I.brows.reserve((size_t)I.nmax * 24);
     I.breg.reserve((size_t)I.nmax);
     I.bregxv.reserve((size_t)I.nmax * 6);
@@ -2043,7 +2099,7 @@ void blocks_run_impl(double tlimit, int max_blocks, int *reason, long long *nblo
     }
     NB6_CUDA_CHECK(cudaMemcpyAsync(I.bctl.ptr, &h, sizeof(BlockCtl), cudaMemcpyHostToDevice, st));
     // the first block's time from every body; each later one comes from the
-    // block before it (blk_collect and blk_corr)
+    // block before it (blk_collect and blk_step)
     blk_min<<<nb6_num_sms() * 4, BLK_NT, 0, st>>>(I.nmax, I.tn.ptr, I.bctl.ptr);
     NB6_CUDA_CHECK(cudaGetLastError());
     if (I.blk_persist && blocks_persist(st, max_blocks, h)) {
@@ -2058,7 +2114,6 @@ void blocks_run_impl(double tlimit, int max_blocks, int *reason, long long *nblo
         I.num_steps += (unsigned long long)h.irr_steps;
         return;
     }
-    I.bact_last = I.bact.ptr;
     if (!blocks_graph(st)) {
         fprintf(stderr, "nb6_blocks_run: the block graph could not be built\n");
         nb6_fatal(NB6_ERR_CUDA);
@@ -2078,6 +2133,15 @@ void blocks_run_impl(double tlimit, int max_blocks, int *reason, long long *nblo
         if (h.stop || done >= max_blocks) break;
         batch = std::min(batch * 2, 256);
     }
+    // the last block's new records (the next run starts from a fresh
+    // control block)
+    if (h.pend_na > 0) {
+        blk_flush<<<std::min((h.pend_na + 255) / 256, nb6_num_sms() * 4), 256, 0, st>>>(
+            I.bctl.ptr, I.bact.ptr, I.nmax, (const double *)I.brows.ptr, I.rec.ptr);
+        NB6_CUDA_CHECK(cudaGetLastError());
+        NB6_CUDA_CHECK(cudaStreamSynchronize(st));
+    }
+    I.bact_last = I.bact.ptr + (size_t)h.last_parity * I.nmax;
     // next run's first batch: about twice this run's length
     I.blk_batch = (int)std::max<long long>(2, std::min<long long>(128, 2 * done));
     *reason = h.stop == 3 ? 0 : h.stop;

@@ -279,7 +279,7 @@ class ForceLib:
 
     def blocks_mode(self, persistent: bool) -> None:
         """nb6_blocks_mode_: 1 one persistent launch per nb6_blocks_run_ call,
-        0 (the default) a graph of three launches per block (same results)."""
+        0 (the default) a graph of two launches per block (same results)."""
         self.lib.nb6_blocks_mode_(_ci(1 if persistent else 0))
 
     def blocks_active(self, nmax: int) -> tuple[np.ndarray, np.ndarray]:
