@@ -106,7 +106,7 @@ def test_block_clock_runs_to_the_limit(nb6):
 @pytest.mark.parametrize("stepr_all", [None, 1.0])
 def test_persistent_and_graph_forms_agree_bit_for_bit(nb6, stepr_all):
     """The persistent form (one cooperative launch per call, grid barriers
-    between the phases of a block) and the graph form (three launches per
+    between the phases of a block) and the graph form (two launches per
     block) give the same blocks, active sets, corrector rows, due lists and
     final state.  stepr_all = 1.0: no regular step due, the run ends at the
     time limit after many blocks; None: it stops at the first block with a
