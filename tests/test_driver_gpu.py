@@ -42,10 +42,10 @@ def test_energy_drift_t10_within_10pct_of_reference(orc):
     Single realisations are chaotic and the drivers integrate single stars
     without KS regularisation, so one seed's drift is set by its closest
     encounters: across these seeds max |dE/E| spans three decades on either
-    backend.  The contract's 10% is therefore stated over the sample, on the
-    median of max |dE/E|; with 8 seeds the median's own scatter is tens of
-    per cent, so the test fails only on a drift clearly above the
-    reference's (more than 1.5 times its median) and prints both medians."""
+    backend.  The contract's 10% is therefore stated over the sample: the
+    median of max |dE/E| over the seeds may exceed the reference's median by
+    at most 10% (measured: 3.4e-6 against 1.4e-5, a quarter of it).  Both
+    medians are printed."""
     from nb6b200 import drive, ics
     ours, ref = _backends(orc)
     mo, mr = [], []
@@ -58,4 +58,4 @@ def test_energy_drift_t10_within_10pct_of_reference(orc):
         mr.append(rr.de_max)
     med_o, med_r = float(np.median(mo)), float(np.median(mr))
     print(f"\nT=10 max |dE/E| median over {len(SEEDS)} seeds: ours {med_o:.3e}  reference {med_r:.3e}")
-    assert med_o <= 1.5 * med_r
+    assert med_o <= 1.10 * med_r
