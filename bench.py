@@ -417,6 +417,18 @@ def irregular_leg(lib, m, x, v, h2, dtr, args, nsample: int = 65536):
     return out
 
 
+def tuned_table():
+    """The regular-force autotuner's choices in this process, as
+    "log2 N_active/log2 N_j/m_flag: variant" strings."""
+    import ctypes as C
+    from nb6b200 import load_cdll
+    lib = load_cdll()
+    n, cap = C.c_int(0), C.c_int(256)
+    buf = (C.c_int * (4 * 256))()
+    lib.nb6_regf_tuned_(C.byref(n), C.byref(cap), buf)
+    return [f"{buf[4 * k]}/{buf[4 * k + 1]}/{buf[4 * k + 2]}: {buf[4 * k + 3]}" for k in range(min(n.value, 256))]
+
+
 def northstar_leg(m, x, v, rs, args):
     """N-body time per wall second of the block-step drivers on this GPU,
     the plain GPU method against the batched, device-resident form:
@@ -457,8 +469,11 @@ def northstar_leg(m, x, v, rs, args):
                   "reg_steps": plain.stats["reg_steps"], "irr_steps": plain.stats["irr_steps"]},
         "batched_device": {"wall_s": wb, "wall_with_startup_s": t_batch, "nbody_time_per_wall_s": t3 / wb,
                            "dE": float(batch.de_max[0]), "reg_calls": batch.stats["reg_calls"],
-                           "reg_steps": batch.stats["reg_steps"], "irr_steps": batch.stats["irr_steps"]},
+                           "reg_steps": batch.stats["reg_steps"], "irr_steps": batch.stats["irr_steps"],
+                           "wall_block_runs_s": batch.stats["wall_irr"],
+                           "wall_regular_s": batch.stats["wall_reg"]},
         "speedup": wp / wb,
+        "autotuner": tuned_table(),
         "dE_ratio_batched_over_plain": float(batch.de_max[0]) / plain.de_max if plain.de_max > 0 else None}
     cls = make_clusters(args.ns_clusters)
     sizes = np.array([c.n for c in cls])

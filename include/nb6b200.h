@@ -133,6 +133,10 @@ void nb6_regf_tune_(int *variant, int *nslices);
  * (default, or NB6_AUTOTUNE=0 in the environment for off), 0 off, -1 clears
  * the cached choices. */
 void nb6_regf_autotune_(int *flag);
+/* The autotuner's choices so far (no reference counterpart): *n buckets,
+ * out[4k..4k+3] = (log2 N_active, log2 N_j, m_flag, variant) for the first
+ * *cap of them, ascending. */
+void nb6_regf_tuned_(int *n, int *cap, int *out);
 /* Regular-force calls (gpunb_regf_, nb6_regf_device_) are submitted as one
  * CUDA graph launch each: the graph of a call kind is built once and its
  * nodes re-parameterised per call.  flag 1 = on (default; NB6_GRAPHS=0 in

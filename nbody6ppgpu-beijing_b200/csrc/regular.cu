@@ -2883,6 +2883,23 @@ void nb6_regf_autotune_(int *flag) {
     R.autotune = *flag ? 1 : 0;
 }
 
+// The autotuner's choices so far: *n = number of buckets; out[4k..4k+3] =
+// (log2 N_active, log2 N_j, m_flag, variant) of bucket k, for the first
+// *cap buckets (ascending).
+void nb6_regf_tuned_(int *n, int *cap, int *out) {
+    int k = 0;
+    for (const auto &e : R.tuned) {
+        if (k < *cap) {
+            out[4 * k] = e.first.li;
+            out[4 * k + 1] = e.first.lj;
+            out[4 * k + 2] = e.first.mf;
+            out[4 * k + 3] = e.second;
+        }
+        ++k;
+    }
+    *n = k;
+}
+
 // Spatial ordering of the j set for the tile kernels: 1 on (default;
 // NB6_JSORT=0 in the environment for off), 0 off, other values query.
 // Returns the setting.

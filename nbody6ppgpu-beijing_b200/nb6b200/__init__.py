@@ -26,7 +26,7 @@ ABI_SYMBOLS = (
     "gpuirr_open_", "gpuirr_close_", "gpuirr_set_jp_", "gpuirr_set_list_",
     "nb6_set_abort_on_error_", "nb6_last_status_", "nb6_device_",
     "nb6_regf_device_", "nb6_regf_outputs_", "nb6_regf_last_kernel_ms_", "nb6_regf_tune_",
-    "nb6_regf_last_geometry_", "nb6_regf_autotune_", "nb6_regf_graphs_", "nb6_regf_jsort_", "nb6_regf_seg_",
+    "nb6_regf_last_geometry_", "nb6_regf_autotune_", "nb6_regf_tuned_", "nb6_regf_graphs_", "nb6_regf_jsort_", "nb6_regf_seg_",
     "nb6_irr_predict_send_", "nb6_irr_last_kernel_ms_", "nb6_regf_proposals_",
     "nb6_hermite_open_", "nb6_hermite_set_", "nb6_irr_correct_", "nb6_regf_correct_", "nb6_hermite_get_", "nb6_ks_set_", "nb6_blocks_run_", "nb6_blocks_mode_", "nb6_irr_tune_", "nb6_blocks_active_", "nb6_blocks_regular_",
     "nb6_mlp_size_", "nb6_mlp_init_", "nb6_mlp_set_", "nb6_mlp_get_", "nb6_mlp_grad_",
