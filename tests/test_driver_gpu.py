@@ -44,8 +44,10 @@ def test_energy_drift_t10_within_10pct_of_reference(orc):
     encounters: across these seeds max |dE/E| spans three decades on either
     backend.  The contract's 10% is therefore stated over the sample: the
     median of max |dE/E| over the seeds may exceed the reference's median by
-    at most 10% (measured: 3.4e-6 against 1.4e-5, a quarter of it).  Both
-    medians are printed."""
+    at most 10% (measured: 3.4e-6 and 7.3e-6 in two runs against 1.4e-5;
+    the library's own median moves with the autotuner's kernel choices,
+    which change the last bits and so the orbits).  Both medians are
+    printed."""
     from nb6b200 import drive, ics
     ours, ref = _backends(orc)
     mo, mr = [], []
