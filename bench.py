@@ -156,7 +156,7 @@ class Clocks:
         load = [s for s, w in zip(sm, pw) if w > 0.3 * max(pw)] or sm
         return {"sm_mhz": float(np.median(load)), "sm_max_mhz": float(max(smax)),
                 "reasons": sorted(reasons), "samples": len(sm),
-                "power_w_max": float(max(pw))}
+                "power_w_max": float(max(pw)), "sm_mhz_min": float(min(sm))}
 
 
 def reduce_max(value: float, pg, device=None) -> float:
@@ -813,7 +813,10 @@ def main():
     # device-resident drivers (rank 0)
     ns = None
     if rank == 0 and not args.no_northstar:
+        ns_clk = Clocks(local)
+        ns_clk.start()
         ns = northstar_leg(m, x, v, rs, args)
+        ns["clocks"] = ns_clk.stop()
     # the reference's own GPU code on this GPU, same workload (rank 0)
     ref_gpu = None
     if rank == 0 and not args.no_ref_gpu:
