@@ -1447,11 +1447,14 @@ void irr_open_impl(int nmax, int lmax, int rank) {
         fprintf(stderr, "# Opening IRR lib. GPU ver. - rank: %d; nmax: %d, lmax: %d\n", rank, nmax, lmax);
 }
 
+void irr_profile_impl(int rank);
+
 void irr_close_impl() {
     if (!I.open) {
         fprintf(stderr, "irr_simd: it is already close\n");
         return;
     }
+    if (getenv("NB6_VERBOSE")) irr_profile_impl(0);   // the counters of the session
     I.open = false;
     I.rec.release();
     I.lists.release();
