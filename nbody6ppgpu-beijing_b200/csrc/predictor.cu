@@ -55,17 +55,57 @@ NB6_DEV void pred3(double s, const double *__restrict__ x0, const double *__rest
     }
 }
 
+// Two bodies per thread: their six coordinates of each array are three
+// 16-byte loads (the arrays are (n, 3) FP64 from cudaMalloc, so body 2p
+// starts on a 16-byte boundary) and the results three 16-byte stores; the
+// arithmetic is pred3's, operation for operation.
+NB6_DEV void load6(const double *__restrict__ a, size_t p, double *o) {
+    const double2 *q = reinterpret_cast<const double2 *>(a) + 3 * p;
+    const double2 u = __ldg(q), v = __ldg(q + 1), w = __ldg(q + 2);
+    o[0] = u.x; o[1] = u.y; o[2] = v.x; o[3] = v.y; o[4] = w.x; o[5] = w.y;
+}
+
+NB6_DEV void store6(double *__restrict__ a, size_t p, const double *o) {
+    double2 *q = reinterpret_cast<double2 *>(a) + 3 * p;
+    q[0] = make_double2(o[0], o[1]);
+    q[1] = make_double2(o[2], o[3]);
+    q[2] = make_double2(o[4], o[5]);
+}
+
 __global__ void predict_kernel(int n, double time, const double *__restrict__ t0,
                                const double *__restrict__ x0, const double *__restrict__ x0dot,
                                const double *__restrict__ f, const double *__restrict__ fdot,
                                double *__restrict__ xp, double *__restrict__ vp) {
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    const size_t npair = (size_t)n / 2;
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < npair;
+         p += (size_t)gridDim.x * blockDim.x) {
+        const double2 tt = __ldg(reinterpret_cast<const double2 *>(t0) + p);
+        double X0[6], VD[6], FF[6], FD[6], x[6], v[6];
+        load6(x0, p, X0);
+        load6(x0dot, p, VD);
+        load6(f, p, FF);
+        load6(fdot, p, FD);
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            const double s = time - (b ? tt.y : tt.x), s1 = 1.5 * s, s2 = 2.0 * s;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const int c = 3 * b + k;
+                x[c] = ((FD[c] * s + FF[c]) * s + VD[c]) * s + X0[c];
+                v[c] = (FD[c] * s1 + FF[c]) * s2 + VD[c];
+            }
+        }
+        store6(xp, p, x);
+        store6(vp, p, v);
+    }
+    if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {   // an odd last body
+        const size_t j = (size_t)n - 1;
         double x[3], v[3];
-        pred3(time - t0[j], x0, x0dot, f, fdot, (size_t)j, x, v);
+        pred3(time - t0[j], x0, x0dot, f, fdot, j, x, v);
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            xp[3 * (size_t)j + k] = x[k];
-            vp[3 * (size_t)j + k] = v[k];
+            xp[3 * j + k] = x[k];
+            vp[3 * j + k] = v[k];
         }
     }
 }
@@ -236,7 +276,7 @@ void nb6_predict_device_(double *time, double **d_x, double **d_xdot) {
     cudaStream_t st = nb6_stream();
     NB6_CUDA_CHECK(cudaEventRecord(S.ev0, st));
     if (n > 0)
-        predict_kernel<<<grid_for(n), 256, 0, st>>>((int)n, *time, S.t0.ptr, S.x0.ptr, S.x0dot.ptr,
+        predict_kernel<<<grid_for((n + 1) / 2), 256, 0, st>>>((int)n, *time, S.t0.ptr, S.x0.ptr, S.x0dot.ptr,
                                                     S.f.ptr, S.fdot.ptr, S.xp.ptr, S.vp.ptr);
     NB6_CUDA_CHECK(cudaGetLastError());
     NB6_CUDA_CHECK(cudaEventRecord(S.ev1, st));
