@@ -1934,8 +1934,9 @@ static void regf_prepare(int ni, const double *d_h2, const double *d_dtr, const 
         // time each candidate three times and keep its best (after one
         // untimed warm-up launch); neighbour counters are reset before every
         // trial
-        float best = 1e30f;
+        float best = 1e30f, tdefault = 1e30f;
         int bestv = variant;
+        const int vdefault = default_variant(nt);
         for (int c = -1; c < ncand; ++c) {
             const int v = cands[c < 0 ? 0 : c];
             Plan p = make_plan(v, nt, R.nj, R.ntile, mf, 0);
@@ -1959,6 +1960,13 @@ static void regf_prepare(int ni, const double *d_h2, const double *d_dtr, const 
                 best = vbest;
                 bestv = v;
             }
+            if (c >= 0 && v == vdefault) tdefault = vbest;
+        }
+        // timings within 3% are a tie, and a tie keeps the default: the
+        // choice then no longer flips between processes on timing noise
+        if (tdefault <= 1.03f * best) {
+            bestv = vdefault;
+            best = tdefault;
         }
         R.nbcnt_dirty = true;
         R.tuned[key] = bestv;
