@@ -161,3 +161,81 @@ def test_persistent_form_in_the_ensemble_driver_bit_for_bit(nb6):
         np.testing.assert_array_equal(a.x[c], b.x[c])
         np.testing.assert_array_equal(a.v[c], b.v[c])
     np.testing.assert_array_equal(a.energy, b.energy)
+
+
+def _ks_table(S, seed, npair=25):
+    """Perturbed pairs among the bodies the neighbour lists hold (the first
+    200), components about each c.m. body's position, random perturbers."""
+    cl = S["cl"]
+    n = cl.n
+    rng = np.random.default_rng(seed)
+    cm = np.sort(rng.choice(200, npair, replace=False)) + 1
+    m = cl.mass[cm - 1]
+    q = rng.uniform(0.2, 0.8, npair)
+    d = rng.normal(size=(npair, 3))
+    d *= (2e-3 / np.linalg.norm(d, axis=1))[:, None]
+    dv = rng.normal(size=(npair, 3)) * 0.3
+    x, v = cl.pos[cm - 1], cl.vel[cm - 1]
+    xk = np.stack([x + (1 - q)[:, None] * d, x - q[:, None] * d], axis=1)
+    vk = np.stack([v + (1 - q)[:, None] * dv, v - q[:, None] * dv], axis=1)
+    mk = np.stack([q * m, (1 - q) * m], axis=1)
+    pofs, plist = [0], []
+    for p in range(npair):
+        k = int(rng.integers(0, 20))
+        others = np.delete(np.arange(1, n + 1), cm[p] - 1)
+        plist.extend(rng.choice(others, k, replace=False).tolist())
+        pofs.append(len(plist))
+    return cm, xk, vk, mk, np.array(pofs, dtype=np.int32), np.array(plist, dtype=np.int32)
+
+
+def test_block_clock_with_ks_pairs_equals_corrector_call(nb6):
+    """With a KS pair table set, a block of the device clock (the corrected
+    neighbour walk inside blk_step) gives nb6_irr_correct_'s rows for the
+    same active set, bit for bit."""
+    S = _state(9)
+    n = S["cl"].n
+    table = _ks_table(S, 9)
+    tmin = (S["t0"] + S["step"]).min()
+    act_host = np.nonzero(S["t0"] + S["step"] == tmin)[0] + 1
+    assert np.intersect1d(act_host, table[0]).size > 0 or len(act_host) > 20
+    _open(nb6, S)
+    try:
+        nb6.ks_set(*table)
+        r1 = nb6.blocks_run(1.0, 1)
+        addr, rows = nb6.blocks_active(n)
+    finally:
+        nb6.irr_close(0)
+    assert r1["blocks"] == 1 and r1["nact"] == len(act_host)
+    _open(nb6, S)
+    try:
+        nb6.ks_set(*table)
+        ref = nb6.irr_correct(tmin, act_host)
+        nb6.ks_set([], [], [], [], [0], [])
+        plain = nb6.irr_correct(tmin, act_host)
+    finally:
+        nb6.irr_close(0)
+    order = np.argsort(addr)
+    np.testing.assert_array_equal(addr[order], act_host)
+    np.testing.assert_array_equal(rows[order], ref)
+    assert np.any(ref[:, 6:9] != plain[:, 6:9])          # the pairs changed some forces
+
+
+def test_block_clock_forms_agree_with_ks_pairs(nb6):
+    """The persistent and graph forms with a KS pair table set (their
+    corrected walks) over a run of many blocks: same final state."""
+    S = _state(10)
+    S["stepr"][:] = 1.0
+    n = S["cl"].n
+    table = _ks_table(S, 10)
+    out = {}
+    for persistent in (True, False):
+        _open(nb6, S)
+        try:
+            nb6.ks_set(*table)
+            nb6.blocks_mode(persistent)
+            out[persistent] = (nb6.blocks_run(0.125, 100000), nb6.hermite_get(1, n))
+        finally:
+            nb6.blocks_mode(False)
+            nb6.irr_close(0)
+    assert out[True][0] == out[False][0] and out[True][0]["blocks"] > 10
+    np.testing.assert_array_equal(out[True][1], out[False][1])
