@@ -27,6 +27,9 @@ Reported on one JSON line (rank 0):
 --impl reference runs the reference's CPU library (the timed CPU arm).
 Multi-GPU (torchrun, --gpus N): every rank evaluates its own cluster of the
 same size (independent clusters, weak scaling), no data-path collective.
+cpu_baseline, err_vs_fp64 and the irregular, predictor, end-to-end driver
+and reference-GPU legs run at N = 1 only (on rank 0); at N > 1 the line
+carries the scaled regular-force figures alone.
 """
 from __future__ import annotations
 
@@ -758,7 +761,7 @@ def main():
                # one rsqrt per pair against the nominal 16 MUFU results per SM
                # per clock at the GPU's maximum SM clock
                "frac_mufu_peak": float(n) * n / (pot_ms * 1e-3) / mufu_peak_per_s()}
-        if rank == 0:
+        if rank == 0 and world == 1:
             import oracle
             i0 = int(np.random.default_rng(9).integers(1, n - 64))
             po = oracle.pot(m, x, i0, 64)
@@ -784,20 +787,23 @@ def main():
     # irregular store, one irr_simd_firr_vec_ over the sample; 60 flops per
     # list pair (irr.avx.cpp:411).  The reference's irr.avx.cpp runs the
     # identical calls on the host cores.
+    # the diagnostic legs below run on rank 0 of a one-GPU run only: with N
+    # replicas they would only hold the other GPUs while rank 0 works alone
+    solo = rank == 0 and world == 1
     irr = None
-    if not args.no_irr and rank == 0:
+    if not args.no_irr and solo:
         irr = irregular_leg(lib, m, x, v, h2, dtr, args)
 
     # the Hermite predictor over the same bodies (rank 0)
     pred = None
-    if not args.no_pred and rank == 0:
+    if not args.no_pred and solo:
         pred = predictor_leg(lib, m, x, v, flush_l2)
 
     # accuracy against the FP64 oracle on calls of the timed shape (chunks of
     # 1024 i, so the same tuned kernel and its far-tile path run; rank 0)
     err = None
     cpu = None
-    if rank == 0:
+    if solo:
         if not args.no_err:
             err = fp64_error_leg(lib, m, x, v, h2, dtr, args)
         if not args.no_cpu_baseline:
@@ -812,14 +818,14 @@ def main():
     # configs 3 and 4 end to end: the plain GPU method against the batched,
     # device-resident drivers (rank 0)
     ns = None
-    if rank == 0 and not args.no_northstar:
+    if solo and not args.no_northstar:
         ns_clk = Clocks(local)
         ns_clk.start()
         ns = northstar_leg(m, x, v, rs, args)
         ns["clocks"] = ns_clk.stop()
     # the reference's own GPU code on this GPU, same workload (rank 0)
     ref_gpu = None
-    if rank == 0 and not args.no_ref_gpu:
+    if solo and not args.no_ref_gpu:
         ref_gpu = reference_gpu_rate(m, x, v, rs, dtr, args, seconds=5.0)
     achieved = FLOPS_PER_PAIR * args.chunk * n / (kernel_ms * 1e-3) / 1e12
     nominal = 2 * 128 * 148 * (clk.get("sm_max_mhz") or 1965.0) * 1e6 / 1e12
