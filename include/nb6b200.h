@@ -273,6 +273,16 @@ void nb6_blocks_active_(int *nact, int *addr, double *rows);
  * later launches run; 1 gives one launch over every body, then one download
  * and copy. */
 void nb6_irr_tune_(int *chunks);
+/* Neighbour gathers of irr_simd_firr_vec_ and nb6_irr_correct_ (no
+ * reference counterpart): *mode = 1 (the default, or environment
+ * NB6_IRR_PV) predicts every record set so far to the call's time once per
+ * call, into 64-byte bodies (x, m, v), and walks the lists over those when
+ * the call's list entries (active bodies x the mean list length) number at
+ * least 8 per body set; 2 always does;
+ * 0 never does (each lane then predicts each neighbour from its 128-byte
+ * record).  Both walks give the same bits.  Calls with a KS pair table
+ * (nb6_ks_set_) always take the record walk. */
+void nb6_irr_pv_(int *mode);
 /* Form of the device block clock for the following nb6_blocks_run_ calls
  * (no reference counterpart): *persistent = 0 (the default) runs each block
  * as a CUDA graph of two launches; 1 (or environment NB6_BLK_PERSIST=1)

@@ -103,6 +103,28 @@ NB6_DEV void cm_pair(const double *xi, const double *vi, const double *xj, const
     }
 }
 
+// The lanes' sums reduced into every lane; the nearest neighbour is the
+// smallest r2, the smallest index on ties (1-based, -1 for an empty list).
+NB6_DEV void irr_warp_finish(double ax, double ay, double az, double jx, double jy, double jz, double rmin, int jmin,
+                             int nnb, double *a, double *jd, int &nnbid) {
+    a[0] = warp_sum_d(ax);
+    a[1] = warp_sum_d(ay);
+    a[2] = warp_sum_d(az);
+    jd[0] = warp_sum_d(jx);
+    jd[1] = warp_sum_d(jy);
+    jd[2] = warp_sum_d(jz);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double r2 = __shfl_xor_sync(0xffffffffu, rmin, o);
+        const int j2 = __shfl_xor_sync(0xffffffffu, jmin, o);
+        if (r2 < rmin || (r2 == rmin && j2 < jmin)) {
+            rmin = r2;
+            jmin = j2;
+        }
+    }
+    nnbid = (nnb > 0 && jmin != 0x7fffffff) ? jmin + 1 : -1;
+}
+
 // One warp, one active particle i: neighbour force, jerk and nearest
 // neighbour (1-based, -1 for an empty list), reduced into every lane.
 // With a KS pair table the force includes the c.m. corrections NBINT_COR
@@ -230,22 +252,105 @@ NB6_DEV void irr_force_warp(int i, int lane, double ti, const Rec *__restrict__ 
             }
         }
     }
-    a[0] = warp_sum_d(ax);
-    a[1] = warp_sum_d(ay);
-    a[2] = warp_sum_d(az);
-    jd[0] = warp_sum_d(jx);
-    jd[1] = warp_sum_d(jy);
-    jd[2] = warp_sum_d(jz);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        const double r2 = __shfl_xor_sync(0xffffffffu, rmin, o);
-        const int j2 = __shfl_xor_sync(0xffffffffu, jmin, o);
-        if (r2 < rmin || (r2 == rmin && j2 < jmin)) {
-            rmin = r2;
-            jmin = j2;
+    irr_warp_finish(ax, ay, az, jx, jy, jz, rmin, jmin, nnb, a, jd, nnbid);
+}
+
+// A body predicted to the time of one call: x, m, v in 64 bytes, so a
+// neighbour gather moves two 32-byte sectors instead of the record's four.
+struct Pv {
+    double x[3], m, v[3], pad;
+};
+
+// One thread per body: every record predicted to ti by predict(), the
+// function the record walk applies to each neighbour, so the predicted set
+// holds the same bits the record walk computes.
+__global__ void irr_predict_set(int n, double ti, const Rec *__restrict__ rec, Pv *__restrict__ pv) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    Rec r;
+    load_rec(rec + j, r);
+    double x[3], v[3];
+    predict(r, ti, x, v);
+    double2 *q = reinterpret_cast<double2 *>(pv + j);
+    q[0] = make_double2(x[0], x[1]);
+    q[1] = make_double2(x[2], r.m);
+    q[2] = make_double2(v[0], v[1]);
+    q[3] = make_double2(v[2], 0.0);
+}
+
+NB6_DEV void load_pv(const Pv *__restrict__ p, double *x, double *v, double &m) {
+    const double2 *q = reinterpret_cast<const double2 *>(p);
+    const double2 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2), d = __ldg(q + 3);
+    x[0] = a.x;
+    x[1] = a.y;
+    x[2] = b.x;
+    m = b.y;
+    v[0] = c.x;
+    v[1] = c.y;
+    v[2] = d.x;
+}
+
+// irr_force_warp without a pair table, over the predicted set: the same
+// pair terms in the same order per lane, so the same bits.  DEEP as in
+// irr_force_warp (two rounds of ids and bodies loaded before their
+// arithmetic).
+template <bool DEEP>
+NB6_DEV void irr_force_warp_pv(int i, int lane, const Pv *__restrict__ pv, const int *__restrict__ lists, int ls,
+                               int nmax, double *a, double *jd, int &nnbid) {
+    double xi[3], vi[3], mi;
+    load_pv(pv + i, xi, vi, mi);
+    const int *row = lists + (size_t)i * ls;
+    const int nnb = row[0];
+    double ax = 0, ay = 0, az = 0, jx = 0, jy = 0, jz = 0;
+    double rmin = 1.0e300;
+    int jmin = 0x7fffffff;
+    auto add = [&](const double *xj, const double *vj, double m, int j) {
+        const double dxd = xj[0] - xi[0], dyd = xj[1] - xi[1], dzd = xj[2] - xi[2];
+        const double r2d = dxd * dxd + dyd * dyd + dzd * dzd;
+        if (r2d < rmin || (r2d == rmin && j < jmin)) {
+            rmin = r2d;
+            jmin = j;
+        }
+        const double dvx = vj[0] - vi[0], dvy = vj[1] - vi[1], dvz = vj[2] - vi[2];
+        const double rinv = rsqrt(r2d);
+        const double rinv2 = rinv * rinv;
+        const double mr3 = m * rinv * rinv2;
+        const double al = -3.0 * (dxd * dvx + dyd * dvy + dzd * dvz) * rinv2;
+        ax += mr3 * dxd;
+        ay += mr3 * dyd;
+        az += mr3 * dzd;
+        jx += mr3 * (dvx + al * dxd);
+        jy += mr3 * (dvy + al * dyd);
+        jz += mr3 * (dvz + al * dzd);
+    };
+    if (DEEP) {
+        int jn0 = 1 + lane < ls ? row[1 + lane] : -1;
+        int jn1 = 33 + lane < ls ? row[33 + lane] : -1;
+        for (int base = 0; base < nnb; base += 64) {
+            const int j0 = base + lane < nnb ? jn0 : -1;
+            const int j1 = base + 32 + lane < nnb ? jn1 : -1;
+            if (base + 64 < nnb) {
+                const int l = base + 65 + lane;
+                jn0 = l < ls ? row[l] : -1;
+                jn1 = l + 32 < ls ? row[l + 32] : -1;
+            }
+            const bool v0 = j0 >= 0 && j0 < nmax, v1 = j1 >= 0 && j1 < nmax;   // ids are checked at set_list time
+            double x0[3], w0[3], m0 = 0, x1[3], w1[3], m1 = 0;
+            if (v0) load_pv(pv + j0, x0, w0, m0);
+            if (v1) load_pv(pv + j1, x1, w1, m1);
+            if (v0) add(x0, w0, m0, j0);
+            if (v1) add(x1, w1, m1, j1);
+        }
+    } else {
+        for (int l = lane; l < nnb; l += 32) {
+            const int j = row[1 + l];
+            if (j < 0 || j >= nmax) continue;   // ids are checked at set_list time
+            double xj[3], vj[3], m;
+            load_pv(pv + j, xj, vj, m);
+            add(xj, vj, m, j);
         }
     }
-    nnbid = (nnb > 0 && jmin != 0x7fffffff) ? jmin + 1 : -1;
+    irr_warp_finish(ax, ay, az, jx, jy, jz, rmin, jmin, nnb, a, jd, nnbid);
 }
 
 // out row k = (ax, ay, az, jx, jy, jz, nnbid, 0) (the correctors' rows),
@@ -253,18 +358,23 @@ NB6_DEV void irr_force_warp(int i, int lane, double ti, const Rec *__restrict__ 
 // (doubles) | nnbid[ni] | nnb[ni] (ints), one download per call and plain
 // block copies into the caller's arrays.
 // KS: with the pair table (a separate instance: the corrections double the
-// registers of the plain walk).
-template <bool KS>
+// registers of the plain walk).  PV (no pair table): 1 = the walk over the
+// predicted set pv, 2 = the same two rounds deep; 0 = over the records.
+template <bool KS, int PV = 0>
 __global__ void __launch_bounds__(IRR_WARPS * 32)
     irr_kernel(int ni, const int *__restrict__ addr, double ti, const Rec *__restrict__ rec,
-               const int *__restrict__ lists, int ls, int nmax, KsArgs ks, double *__restrict__ out,
-               double *__restrict__ fv) {
+               const Pv *__restrict__ pv, const int *__restrict__ lists, int ls, int nmax, KsArgs ks,
+               double *__restrict__ out, double *__restrict__ fv) {
+    static_assert(!(KS && PV), "the predicted-set walk has no pair table");
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int k = blockIdx.x * IRR_WARPS + warp;
     if (k >= ni) return;
     double a[3], jd[3];
     int id;
-    irr_force_warp<KS>(addr[k] - 1, lane, ti, rec, lists, ls, nmax, ks, a, jd, id);
+    if (PV)
+        irr_force_warp_pv<PV == 2>(addr[k] - 1, lane, pv, lists, ls, nmax, a, jd, id);
+    else
+        irr_force_warp<KS>(addr[k] - 1, lane, ti, rec, lists, ls, nmax, ks, a, jd, id);
     if (lane == 0 && !out) {
         // the caller's layout, in the blocks of the output staging:
         // acc[ni][3] | jrk[ni][3] (doubles) | nnbid[ni] | nnb[ni] (ints)
@@ -1332,6 +1442,7 @@ struct IrrState {
     HostBuf<double> hout;
     std::vector<int> jp_slot, list_slot;  // staged slot per particle, -1 if none
     std::vector<int> nnb_host;            // list lengths, for the profile counters
+    long long nnb_total = 0;              // their sum
     std::vector<int> flush_off;           // latest list entry per particle, per flush
     int njp = 0, nlist = 0;
     size_t list_words = 0;
@@ -1341,6 +1452,11 @@ struct IrrState {
     cudaStream_t cst = nullptr;                // downloads of the chunks' results
     cudaEvent_t evk[IRR_CHUNKS] = {}, evc[IRR_CHUNKS] = {};   // chunk kernel / download done
     int chunks_max = IRR_CHUNKS;               // nb6_irr_tune_
+    DevBuf<Pv> pv;                             // the predicted set of the running call, nmax bodies
+    bool pv_zeroed = false;                    // pv cleared since open (bodies never set stay zero)
+    int pv_mode = -1;                          // nb6_irr_pv_ / NB6_IRR_PV: 0 never, 1 by size, 2 always
+    int pv_deep = -1;                          // NB6_IRR_PV_DEEP=1: the two-round walk over the set
+    int addr_hi = 0;                           // 1 + the highest address set (records above are zero)
     // device-resident corrector state (nb6_hermite_open_)
     bool hermite = false;
     HermiteParams hp{};
@@ -1403,14 +1519,52 @@ KsArgs ks_args() {
     return k;
 }
 
-// out: rows of 8 doubles; or, out null, the caller's layout in fv
-void launch_irr_kernel(int ni, const int *daddr, double ti, double *out, cudaStream_t st, double *fv = nullptr) {
+// The predicted set for a call at ti over ni active bodies, or null when
+// the record walk serves the call: with a pair table, or when the call's
+// list entries (ni x the mean list length) number fewer than 8 per body
+// set.  The prediction pass reads every record set so far and writes its
+// 64-byte body (192 bytes per body) and saves 64 bytes per list entry; on
+// a B200 it paid at 16 entries per body set and lost at 3 to 4.
+const Pv *irr_predicted_set(int ni, double ti, cudaStream_t st) {
+    if (I.pv_mode < 0) {
+        const char *e = getenv("NB6_IRR_PV");
+        I.pv_mode = e ? atoi(e) : 1;
+    }
+    if (I.pv_deep < 0) {
+        const char *e = getenv("NB6_IRR_PV_DEEP");
+        I.pv_deep = e && atoi(e) == 1 ? 1 : 0;
+    }
+    const int n = I.addr_hi;
+    if (I.ks_npair > 0 || I.pv_mode == 0 || n <= 0) return nullptr;
+    if (I.pv_mode == 1 && (double)ni * (double)I.nnb_total < 8.0 * (double)n * (double)n) return nullptr;
+    if (!I.pv_zeroed) {
+        // every address the lists or the active set can name (< nmax) has a
+        // body; those never set keep the zeros that predict() makes of
+        // their zero records
+        I.pv.reserve((size_t)I.nmax);
+        NB6_CUDA_CHECK(cudaMemsetAsync(I.pv.ptr, 0, sizeof(Pv) * (size_t)I.nmax, st));
+        I.pv_zeroed = true;
+    }
+    irr_predict_set<<<(n + 255) / 256, 256, 0, st>>>(n, ti, I.rec.ptr, I.pv.ptr);
+    return I.pv.ptr;
+}
+
+// out: rows of 8 doubles; or, out null, the caller's layout in fv.  pv: the
+// call's predicted set (irr_predicted_set), null for the record walk.
+void launch_irr_kernel(int ni, const int *daddr, double ti, double *out, cudaStream_t st, double *fv = nullptr,
+                       const Pv *pv = nullptr) {
     const KsArgs ks = ks_args();
     const dim3 grid((ni + IRR_WARPS - 1) / IRR_WARPS), block(IRR_WARPS * 32);
+    const Rec *rec = I.rec.ptr;
+    const int *lists = I.lists.ptr;
     if (ks.slot)
-        irr_kernel<true><<<grid, block, 0, st>>>(ni, daddr, ti, I.rec.ptr, I.lists.ptr, I.lmax, I.nmax, ks, out, fv);
+        irr_kernel<true><<<grid, block, 0, st>>>(ni, daddr, ti, rec, nullptr, lists, I.lmax, I.nmax, ks, out, fv);
+    else if (pv && I.pv_deep == 1)
+        irr_kernel<false, 2><<<grid, block, 0, st>>>(ni, daddr, ti, rec, pv, lists, I.lmax, I.nmax, ks, out, fv);
+    else if (pv)
+        irr_kernel<false, 1><<<grid, block, 0, st>>>(ni, daddr, ti, rec, pv, lists, I.lmax, I.nmax, ks, out, fv);
     else
-        irr_kernel<false><<<grid, block, 0, st>>>(ni, daddr, ti, I.rec.ptr, I.lists.ptr, I.lmax, I.nmax, ks, out, fv);
+        irr_kernel<false><<<grid, block, 0, st>>>(ni, daddr, ti, rec, nullptr, lists, I.lmax, I.nmax, ks, out, fv);
 }
 
 __global__ void ks_scatter_slots(int npair, const int *__restrict__ cm, int *__restrict__ slot) {
@@ -1439,7 +1593,10 @@ void irr_open_impl(int nmax, int lmax, int rank) {
     I.jp_slot.assign(nmax, -1);
     I.list_slot.assign(nmax, -1);
     I.nnb_host.assign(nmax, 0);
+    I.nnb_total = 0;
     I.njp = I.nlist = 0;
+    I.addr_hi = 0;
+    I.pv_zeroed = false;
     I.list_words = 0;
     I.time_grav = 0;
     I.num_inter = I.num_fcall = I.num_steps = 0;
@@ -1457,6 +1614,7 @@ void irr_close_impl() {
     if (getenv("NB6_VERBOSE")) irr_profile_impl(0);   // the counters of the session
     I.open = false;
     I.rec.release();
+    I.pv.release();
     I.lists.release();
     I.dstage_rec.release();
     I.dints.release();
@@ -1519,6 +1677,7 @@ void irr_set_jp_impl(int a, const double *pos, const double *vel, const double *
         nb6_fatal(NB6_ERR_BAD_ARG);
         return;
     }
+    if (a + 1 > I.addr_hi) I.addr_hi = a + 1;
     int s = I.jp_slot[a];
     if (s < 0) {
         s = I.njp++;
@@ -1585,17 +1744,44 @@ void irr_set_list_impl(int a, const int *nblist) {
     e[1] = nnb;
     for (int l = 0; l < nnb; ++l) e[2 + l] = nblist[1 + l] - 1;
     I.list_slot[a] = (int)I.list_words;
+    I.nnb_total += nnb - I.nnb_host[a];
     I.nnb_host[a] = nnb;
     I.list_words = need;
     I.nlist++;
 }
 
 // Small stagings are read by the kernels straight from pinned host memory
-// (mapped under unified addressing), which saves the copy launches that
-// dominate a block's irregular call; large ones (start-up, many actives)
-// go through one bulk DMA copy each.
-constexpr size_t ZERO_COPY_MAX = 1 << 20;
-size_t zero_copy_bytes() { return nb6_uva() ? ZERO_COPY_MAX : 0; }
+// (mapped under unified addressing), and small results written straight
+// into it, which saves the copy launches that dominate a small call; large
+// ones go through one bulk DMA copy each.  The limits differ by access:
+//   records (ZC_REC_MAX)   read once, coalesced, by the scatter kernel;
+//   integers (ZC_INTS_MAX) the active addresses among them, read one per
+//                          warp at the head of each walk, so each warp
+//                          waits a PCIe round trip;
+//   results (ZC_OUT_MAX)   written in 8-byte pieces per body.
+// Measured on a B200 (irr_simd_firr_vec_, lists of 64 in a Plummer
+// N = 262,144): results written to host memory cost 0.24 ms per call at
+// 16,384 bodies against 0.11 ms through a device buffer and one download,
+// and the same at 256 bodies; addresses read from host memory cost 0.34 ms
+// at 65,536 bodies against 0.25 ms uploaded, and won at 4,096.
+// NB6_ZC_REC, NB6_ZC_INTS and NB6_ZC_OUT (bytes) override them.
+constexpr size_t ZC_REC_MAX = 1 << 20, ZC_INTS_MAX = 32 << 10, ZC_OUT_MAX = 16 << 10;
+size_t zc_limit(const char *name, size_t def) {
+    const char *e = getenv(name);
+    return nb6_uva() ? (e ? (size_t)atoll(e) : def) : 0;
+}
+size_t zero_copy_rec_bytes() {
+    static const size_t lim = zc_limit("NB6_ZC_REC", ZC_REC_MAX);
+    return lim;
+}
+size_t zero_copy_ints_bytes() {
+    static const size_t lim = zc_limit("NB6_ZC_INTS", ZC_INTS_MAX);
+    return lim;
+}
+size_t zero_copy_out_bytes() {
+    static const size_t lim = zc_limit("NB6_ZC_OUT", ZC_OUT_MAX);
+    return lim;
+}
 
 // Upload and scatter everything staged since the last flush, with the
 // active addresses of a force call (active may be null): the records and
@@ -1644,14 +1830,14 @@ const int *irr_flush(cudaStream_t st, const int *active = nullptr, int ni = 0) {
     if (ni) memcpy(h + njp + ne, active, sizeof(int) * ni);
     if (I.list_words) memcpy(h + njp + ne + ni, I.hstage_list.ptr, sizeof(int) * I.list_words);
     const Rec *drec = I.hstage_rec.ptr;
-    if (njp && sizeof(Rec) * (size_t)njp > zero_copy_bytes()) {
+    if (njp && sizeof(Rec) * (size_t)njp > zero_copy_rec_bytes()) {
         I.dstage_rec.reserve(njp);
         NB6_CUDA_CHECK(cudaMemcpyAsync(I.dstage_rec.ptr, I.hstage_rec.ptr, sizeof(Rec) * njp,
                                        cudaMemcpyHostToDevice, st));
         drec = I.dstage_rec.ptr;
     }
     const int *d = h;
-    if (sizeof(int) * nint > zero_copy_bytes()) {
+    if (sizeof(int) * nint > zero_copy_ints_bytes()) {
         NB6_CUDA_CHECK(cudaMemcpyAsync(I.dints.ptr, h, sizeof(int) * nint, cudaMemcpyHostToDevice, st));
         d = I.dints.ptr;
     }
@@ -1705,7 +1891,7 @@ void irr_firr_vec_impl(double ti, int ni, const int *addr, double (*acc)[3], dou
     const size_t nd = 7 * (size_t)ni;   // 6 ni doubles + 2 ni ints
     const size_t bytes = sizeof(double) * nd;
     I.hout.reserve(nd);
-    const bool direct = bytes <= zero_copy_bytes();
+    const bool direct = bytes <= zero_copy_out_bytes();
     double *out = I.hout.ptr;
     if (!direct) {
         I.dout.reserve(nd);
@@ -1726,9 +1912,10 @@ void irr_firr_vec_impl(double ti, int ni, const int *addr, double (*acc)[3], dou
     CopyPool *pool = direct ? nullptr : &nb6_copy_pool();
     auto chunk_lo = [&](int c) { return (int)((long long)ni * c / nch); };
     NB6_CUDA_CHECK(cudaEventRecord(I.ev0, st));
+    const Pv *pv = irr_predicted_set(ni, ti, st);
     for (int c = 0; c < nch; ++c) {
         const int a = chunk_lo(c), m = chunk_lo(c + 1) - a;
-        launch_irr_kernel(m, daddr + a, ti, nullptr, st, out + 7 * (size_t)a);
+        launch_irr_kernel(m, daddr + a, ti, nullptr, st, out + 7 * (size_t)a, pv);
         NB6_CUDA_CHECK(cudaGetLastError());
         if (!direct) {
             NB6_CUDA_CHECK(cudaEventRecord(I.evk[c], st));
@@ -1858,7 +2045,7 @@ void irr_correct_impl(double time, int ni, const int *addr, double *out) {
     const int *daddr = irr_flush(st, addr, ni);
     const size_t rowd = 24;
     I.hout.reserve((size_t)ni * rowd);
-    const bool direct = sizeof(double) * rowd * (size_t)ni <= zero_copy_bytes();
+    const bool direct = sizeof(double) * rowd * (size_t)ni <= zero_copy_out_bytes();
     // forces of all active bodies into a device buffer, then the corrector
     I.dout.reserve((size_t)ni * (8 + (direct ? 0 : rowd)));
     double *force = I.dout.ptr;
@@ -1868,7 +2055,7 @@ void irr_correct_impl(double time, int ni, const int *addr, double *out) {
         NB6_CUDA_CHECK(cudaEventCreate(&I.ev1));
     }
     NB6_CUDA_CHECK(cudaEventRecord(I.ev0, st));
-    launch_irr_kernel(ni, daddr, time, force, st);
+    launch_irr_kernel(ni, daddr, time, force, st, nullptr, irr_predicted_set(ni, time, st));
     NB6_CUDA_CHECK(cudaGetLastError());
     NB6_CUDA_CHECK(cudaEventRecord(I.ev1, st));
     irr_apply_corrector<<<(ni + 127) / 128, 128, 0, st>>>(ni, daddr, time, force, I.rec.ptr, I.aux.ptr, I.hp, o,
@@ -2291,7 +2478,7 @@ void regf_correct_impl(double time, int ni, const int *addr, int *iseg, int nseg
     p.acpar = I.acpar.ptr;
     const size_t rowd = 32;
     I.hout.reserve((size_t)ni * rowd);
-    const bool direct = sizeof(double) * rowd * (size_t)ni <= zero_copy_bytes();
+    const bool direct = sizeof(double) * rowd * (size_t)ni <= zero_copy_out_bytes();
     double *o = I.hout.ptr;
     if (!direct) {
         I.dout.reserve((size_t)ni * rowd);
@@ -2311,7 +2498,11 @@ void regf_correct_impl(double time, int ni, const int *addr, int *iseg, int nseg
     if (nb6_check_dev_status() != 0) return;
     memcpy(out, I.hout.ptr, sizeof(double) * rowd * ni);
     for (int k = 0; k < ni; ++k)
-        if (out[rowd * k + 28] == 0.0) I.nnb_host[addr[k] - 1] = (int)out[rowd * k + 27];
+        if (out[rowd * k + 28] == 0.0) {
+            const int nn = (int)out[rowd * k + 27];
+            I.nnb_total += nn - I.nnb_host[addr[k] - 1];
+            I.nnb_host[addr[k] - 1] = nn;
+        }
     const double t4 = nb6_wtime();
     I.time_grav += t4 - t0;
     I.rc_calls++;
@@ -2559,6 +2750,7 @@ void nb6_ks_set_(int *npair, int *cm, double *xk, double *vk, double *mk, int *p
 // made on the device, bit for bit the same).
 void nb6_blocks_mode_(int *persistent) { I.blk_persist = *persistent ? 1 : 0; }
 
+void nb6_irr_pv_(int *mode) { I.pv_mode = (*mode >= 0 && *mode <= 2) ? *mode : 1; }
 void nb6_irr_tune_(int *chunks) { I.chunks_max = (*chunks >= 1 && *chunks <= IRR_CHUNKS) ? *chunks : IRR_CHUNKS; }
 
 void nb6_blocks_run_(double *tlimit, int *max_blocks, int *reason, long long *nblocks, long long *nirr,

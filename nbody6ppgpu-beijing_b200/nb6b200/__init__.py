@@ -28,7 +28,7 @@ ABI_SYMBOLS = (
     "nb6_regf_device_", "nb6_regf_outputs_", "nb6_regf_last_kernel_ms_", "nb6_regf_tune_",
     "nb6_regf_last_geometry_", "nb6_regf_autotune_", "nb6_regf_tuned_", "nb6_regf_graphs_", "nb6_regf_jsort_", "nb6_regf_seg_",
     "nb6_irr_predict_send_", "nb6_irr_last_kernel_ms_", "nb6_regf_proposals_",
-    "nb6_hermite_open_", "nb6_hermite_set_", "nb6_irr_correct_", "nb6_regf_correct_", "nb6_hermite_get_", "nb6_ks_set_", "nb6_blocks_run_", "nb6_blocks_mode_", "nb6_irr_tune_", "nb6_blocks_active_", "nb6_blocks_regular_",
+    "nb6_hermite_open_", "nb6_hermite_set_", "nb6_irr_correct_", "nb6_regf_correct_", "nb6_hermite_get_", "nb6_ks_set_", "nb6_blocks_run_", "nb6_blocks_mode_", "nb6_irr_tune_", "nb6_irr_pv_", "nb6_blocks_active_", "nb6_blocks_regular_",
     "nb6_mlp_size_", "nb6_mlp_init_", "nb6_mlp_set_", "nb6_mlp_get_", "nb6_mlp_grad_",
     "nb6_mlp_train_", "nb6_mlp_predict_", "nb6_mlp_enable_",
     "nb6_sync_", "nb6_stream_",

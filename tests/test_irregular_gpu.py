@@ -120,6 +120,47 @@ def test_irregular_large_call_in_chunks(nb6, orc):
         nb6.irr_close(0)
 
 
+def test_predicted_set_walk_equals_record_walk_bit_for_bit(nb6, orc):
+    """The walk over the predicted set (every record predicted to the call's
+    time once, nb6_irr_pv_ 2) and the walk that predicts each neighbour from
+    its record (nb6_irr_pv_ 0) give the same bits, for a small and a large
+    call; the default (1) picks one of them by size."""
+    import ctypes as C
+    from nb6b200 import ics
+    n, lmax = 20000, 72
+    rng = np.random.default_rng(33)
+    cl = ics.plummer(n, seed=33)
+    lists = np.zeros((n, lmax), dtype=np.int32)
+    for i in range(n):
+        ids = np.unique((i + rng.integers(1, n, int(rng.integers(0, lmax)))) % n) + 1
+        lists[i, 0] = len(ids)
+        lists[i, 1:1 + len(ids)] = ids
+    g = {"x0": cl.pos, "v0": cl.vel, "acc2": rng.normal(size=(n, 3)) * 0.5,
+         "jrk6": rng.normal(size=(n, 3)) * 0.2, "mass": cl.mass,
+         "t0": -rng.integers(0, 16, n) / 2048.0, "lists": lists}
+    load_state(nb6, g)
+    ti = 3.0 / 4096
+    mode = lambda k: nb6.lib.nb6_irr_pv_(C.byref(C.c_int(k)))    # noqa: E731
+    try:
+        for ni in (97, 15000):
+            addr = np.sort(rng.choice(n, ni, replace=False) + 1).astype(np.int32)
+            res = {}
+            for k in (0, 2, 1):
+                mode(k)
+                res[k] = [a.copy() for a in nb6.irr_firr_vec(ti, addr)]
+            for k in (2, 1):
+                for a, b in zip(res[k], res[0]):
+                    np.testing.assert_array_equal(a, b)
+            oa, oj, oid = orc.firr(ti, addr, g["x0"], g["v0"], g["acc2"], g["jrk6"], g["mass"], g["t0"], lists)
+            ok = lists[addr - 1, 0] > 0
+            assert rel_err_vec(res[2][0][ok], oa[ok]).max() <= 1e-6
+            assert rel_err_vec(res[2][1][ok], oj[ok]).max() <= 1e-5
+            np.testing.assert_array_equal(res[2][2], oid)
+    finally:
+        mode(1)
+        nb6.irr_close(0)
+
+
 def test_irregular_updates_between_calls(nb6, orc):
     """set_jp / set_list after a firr call take effect on the next call; a
     second set of the same particle before a flush wins."""
