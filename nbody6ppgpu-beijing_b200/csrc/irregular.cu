@@ -291,10 +291,7 @@ NB6_DEV void load_pv(const Pv *__restrict__ p, double *x, double *v, double &m) 
 }
 
 // irr_force_warp without a pair table, over the predicted set: the same
-// pair terms in the same order per lane, so the same bits.  DEEP as in
-// irr_force_warp (two rounds of ids and bodies loaded before their
-// arithmetic).
-template <bool DEEP>
+// pair terms in the same order per lane, so the same bits.
 NB6_DEV void irr_force_warp_pv(int i, int lane, const Pv *__restrict__ pv, const int *__restrict__ lists, int ls,
                                int nmax, double *a, double *jd, int &nnbid) {
     double xi[3], vi[3], mi;
@@ -323,32 +320,12 @@ NB6_DEV void irr_force_warp_pv(int i, int lane, const Pv *__restrict__ pv, const
         jy += mr3 * (dvy + al * dyd);
         jz += mr3 * (dvz + al * dzd);
     };
-    if (DEEP) {
-        int jn0 = 1 + lane < ls ? row[1 + lane] : -1;
-        int jn1 = 33 + lane < ls ? row[33 + lane] : -1;
-        for (int base = 0; base < nnb; base += 64) {
-            const int j0 = base + lane < nnb ? jn0 : -1;
-            const int j1 = base + 32 + lane < nnb ? jn1 : -1;
-            if (base + 64 < nnb) {
-                const int l = base + 65 + lane;
-                jn0 = l < ls ? row[l] : -1;
-                jn1 = l + 32 < ls ? row[l + 32] : -1;
-            }
-            const bool v0 = j0 >= 0 && j0 < nmax, v1 = j1 >= 0 && j1 < nmax;   // ids are checked at set_list time
-            double x0[3], w0[3], m0 = 0, x1[3], w1[3], m1 = 0;
-            if (v0) load_pv(pv + j0, x0, w0, m0);
-            if (v1) load_pv(pv + j1, x1, w1, m1);
-            if (v0) add(x0, w0, m0, j0);
-            if (v1) add(x1, w1, m1, j1);
-        }
-    } else {
-        for (int l = lane; l < nnb; l += 32) {
-            const int j = row[1 + l];
-            if (j < 0 || j >= nmax) continue;   // ids are checked at set_list time
-            double xj[3], vj[3], m;
-            load_pv(pv + j, xj, vj, m);
-            add(xj, vj, m, j);
-        }
+    for (int l = lane; l < nnb; l += 32) {
+        const int j = row[1 + l];
+        if (j < 0 || j >= nmax) continue;   // ids are checked at set_list time
+        double xj[3], vj[3], m;
+        load_pv(pv + j, xj, vj, m);
+        add(xj, vj, m, j);
     }
     irr_warp_finish(ax, ay, az, jx, jy, jz, rmin, jmin, nnb, a, jd, nnbid);
 }
@@ -358,9 +335,9 @@ NB6_DEV void irr_force_warp_pv(int i, int lane, const Pv *__restrict__ pv, const
 // (doubles) | nnbid[ni] | nnb[ni] (ints), one download per call and plain
 // block copies into the caller's arrays.
 // KS: with the pair table (a separate instance: the corrections double the
-// registers of the plain walk).  PV (no pair table): 1 = the walk over the
-// predicted set pv, 2 = the same two rounds deep; 0 = over the records.
-template <bool KS, int PV = 0>
+// registers of the plain walk).  PV (no pair table): the walk over the
+// predicted set pv instead of the records.
+template <bool KS, bool PV = false>
 __global__ void __launch_bounds__(IRR_WARPS * 32)
     irr_kernel(int ni, const int *__restrict__ addr, double ti, const Rec *__restrict__ rec,
                const Pv *__restrict__ pv, const int *__restrict__ lists, int ls, int nmax, KsArgs ks,
@@ -372,7 +349,7 @@ __global__ void __launch_bounds__(IRR_WARPS * 32)
     double a[3], jd[3];
     int id;
     if (PV)
-        irr_force_warp_pv<PV == 2>(addr[k] - 1, lane, pv, lists, ls, nmax, a, jd, id);
+        irr_force_warp_pv(addr[k] - 1, lane, pv, lists, ls, nmax, a, jd, id);
     else
         irr_force_warp<KS>(addr[k] - 1, lane, ti, rec, lists, ls, nmax, ks, a, jd, id);
     if (lane == 0 && !out) {
@@ -1455,7 +1432,6 @@ struct IrrState {
     DevBuf<Pv> pv;                             // the predicted set of the running call, nmax bodies
     bool pv_zeroed = false;                    // pv cleared since open (bodies never set stay zero)
     int pv_mode = -1;                          // nb6_irr_pv_ / NB6_IRR_PV: 0 never, 1 by size, 2 always
-    int pv_deep = -1;                          // NB6_IRR_PV_DEEP=1: the two-round walk over the set
     int addr_hi = 0;                           // 1 + the highest address set (records above are zero)
     // device-resident corrector state (nb6_hermite_open_)
     bool hermite = false;
@@ -1530,10 +1506,6 @@ const Pv *irr_predicted_set(int ni, double ti, cudaStream_t st) {
         const char *e = getenv("NB6_IRR_PV");
         I.pv_mode = e ? atoi(e) : 1;
     }
-    if (I.pv_deep < 0) {
-        const char *e = getenv("NB6_IRR_PV_DEEP");
-        I.pv_deep = e && atoi(e) == 1 ? 1 : 0;
-    }
     const int n = I.addr_hi;
     if (I.ks_npair > 0 || I.pv_mode == 0 || n <= 0) return nullptr;
     if (I.pv_mode == 1 && (double)ni * (double)I.nnb_total < 8.0 * (double)n * (double)n) return nullptr;
@@ -1559,10 +1531,8 @@ void launch_irr_kernel(int ni, const int *daddr, double ti, double *out, cudaStr
     const int *lists = I.lists.ptr;
     if (ks.slot)
         irr_kernel<true><<<grid, block, 0, st>>>(ni, daddr, ti, rec, nullptr, lists, I.lmax, I.nmax, ks, out, fv);
-    else if (pv && I.pv_deep == 1)
-        irr_kernel<false, 2><<<grid, block, 0, st>>>(ni, daddr, ti, rec, pv, lists, I.lmax, I.nmax, ks, out, fv);
     else if (pv)
-        irr_kernel<false, 1><<<grid, block, 0, st>>>(ni, daddr, ti, rec, pv, lists, I.lmax, I.nmax, ks, out, fv);
+        irr_kernel<false, true><<<grid, block, 0, st>>>(ni, daddr, ti, rec, pv, lists, I.lmax, I.nmax, ks, out, fv);
     else
         irr_kernel<false><<<grid, block, 0, st>>>(ni, daddr, ti, rec, nullptr, lists, I.lmax, I.nmax, ks, out, fv);
 }
