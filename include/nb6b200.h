@@ -278,7 +278,7 @@ void nb6_irr_tune_(int *chunks);
  * NB6_IRR_PV) predicts every record set so far to the call's time once per
  * call, into 64-byte bodies (x, m, v), and walks the lists over those when
  * the call's list entries (active bodies x the mean list length) number at
- * least 8 per body set; 2 always does;
+ * least 4 per body set; 2 always does;
  * 0 never does (each lane then predicts each neighbour from its 128-byte
  * record).  Both walks give the same bits.  Calls with a KS pair table
  * (nb6_ks_set_) always take the record walk. */

@@ -261,21 +261,58 @@ struct Pv {
     double x[3], m, v[3], pad;
 };
 
-// One thread per body: every record predicted to ti by predict(), the
-// function the record walk applies to each neighbour, so the predicted set
-// holds the same bits the record walk computes.
-__global__ void irr_predict_set(int n, double ti, const Rec *__restrict__ rec, Pv *__restrict__ pv) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= n) return;
-    Rec r;
-    load_rec(rec + j, r);
-    double x[3], v[3];
-    predict(r, ti, x, v);
-    double2 *q = reinterpret_cast<double2 *>(pv + j);
-    q[0] = make_double2(x[0], x[1]);
-    q[1] = make_double2(x[2], r.m);
-    q[2] = make_double2(v[0], v[1]);
-    q[3] = make_double2(v[2], 0.0);
+// Every record predicted to ti by predict(), the function the record walk
+// applies to each neighbour, so the predicted set holds the same bits the
+// record walk computes.  A CTA takes PS_NT consecutive records: the threads
+// read them as consecutive 16-byte pieces into shared memory, each thread
+// predicts one record from there, and the 64-byte bodies leave through
+// shared memory the same way, so every global access of a warp is one
+// contiguous 512-byte run.  The 16-byte pieces are stored XOR-swizzled so
+// that a quarter-warp's accesses fall in distinct bank groups.
+constexpr int PS_NT = 128;
+__global__ void __launch_bounds__(PS_NT) irr_predict_set(int n, double ti, const Rec *__restrict__ rec,
+                                                        Pv *__restrict__ pv) {
+    __shared__ double2 sm[PS_NT * 8];   // PS_NT records of 8 pieces; later PS_NT bodies of 4
+    const int t = threadIdx.x;
+    const int b0 = blockIdx.x * PS_NT;
+    const int nb = min(PS_NT, n - b0);
+    const double2 *src = reinterpret_cast<const double2 *>(rec + b0);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int q = t + PS_NT * k;   // piece q & 7 of record q >> 3
+        if (q < nb * 8) sm[(q & ~7) | ((q & 7) ^ ((q >> 3) & 7))] = __ldg(src + q);
+    }
+    __syncthreads();
+    double x[3], v[3], m = 0.0;
+    if (t < nb) {
+        const int sw = t & 7;
+        const double2 a = sm[t * 8 + (0 ^ sw)], b = sm[t * 8 + (1 ^ sw)], c = sm[t * 8 + (2 ^ sw)];
+        const double2 d = sm[t * 8 + (3 ^ sw)], e = sm[t * 8 + (4 ^ sw)], f = sm[t * 8 + (5 ^ sw)];
+        const double2 g = sm[t * 8 + (6 ^ sw)];
+        Rec r;   // the piece order of load_rec
+        r.x[0] = a.x; r.x[1] = a.y; r.x[2] = b.x;
+        r.v[0] = b.y; r.v[1] = c.x; r.v[2] = c.y;
+        r.f[0] = d.x; r.f[1] = d.y; r.f[2] = e.x;
+        r.fd[0] = e.y; r.fd[1] = f.x; r.fd[2] = f.y;
+        r.m = g.x; r.t0 = g.y;
+        predict(r, ti, x, v);
+        m = r.m;
+    }
+    __syncthreads();
+    if (t < nb) {
+        const int sw = (t >> 1) & 3;
+        sm[t * 4 + (0 ^ sw)] = make_double2(x[0], x[1]);
+        sm[t * 4 + (1 ^ sw)] = make_double2(x[2], m);
+        sm[t * 4 + (2 ^ sw)] = make_double2(v[0], v[1]);
+        sm[t * 4 + (3 ^ sw)] = make_double2(v[2], 0.0);
+    }
+    __syncthreads();
+    double2 *dst = reinterpret_cast<double2 *>(pv + b0);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int q = t + PS_NT * k;   // piece q & 3 of body q >> 2
+        if (q < nb * 4) dst[q] = sm[(q & ~3) | ((q & 3) ^ ((q >> 3) & 3))];
+    }
 }
 
 NB6_DEV void load_pv(const Pv *__restrict__ p, double *x, double *v, double &m) {
@@ -1497,10 +1534,12 @@ KsArgs ks_args() {
 
 // The predicted set for a call at ti over ni active bodies, or null when
 // the record walk serves the call: with a pair table, or when the call's
-// list entries (ni x the mean list length) number fewer than 8 per body
+// list entries (ni x the mean list length) number fewer than 4 per body
 // set.  The prediction pass reads every record set so far and writes its
 // 64-byte body (192 bytes per body) and saves 64 bytes per list entry; on
-// a B200 it paid at 16 entries per body set and lost at 3 to 4.
+// a B200 (lists of 64 in a Plummer N = 262,144) the call took 7% less time
+// at 4 entries per body set, 16% less at 16, the same at 2 and 9% more at
+// 1.
 const Pv *irr_predicted_set(int ni, double ti, cudaStream_t st) {
     if (I.pv_mode < 0) {
         const char *e = getenv("NB6_IRR_PV");
@@ -1508,7 +1547,7 @@ const Pv *irr_predicted_set(int ni, double ti, cudaStream_t st) {
     }
     const int n = I.addr_hi;
     if (I.ks_npair > 0 || I.pv_mode == 0 || n <= 0) return nullptr;
-    if (I.pv_mode == 1 && (double)ni * (double)I.nnb_total < 8.0 * (double)n * (double)n) return nullptr;
+    if (I.pv_mode == 1 && (double)ni * (double)I.nnb_total < 4.0 * (double)n * (double)n) return nullptr;
     if (!I.pv_zeroed) {
         // every address the lists or the active set can name (< nmax) has a
         // body; those never set keep the zeros that predict() makes of
@@ -1517,7 +1556,7 @@ const Pv *irr_predicted_set(int ni, double ti, cudaStream_t st) {
         NB6_CUDA_CHECK(cudaMemsetAsync(I.pv.ptr, 0, sizeof(Pv) * (size_t)I.nmax, st));
         I.pv_zeroed = true;
     }
-    irr_predict_set<<<(n + 255) / 256, 256, 0, st>>>(n, ti, I.rec.ptr, I.pv.ptr);
+    irr_predict_set<<<(n + PS_NT - 1) / PS_NT, PS_NT, 0, st>>>(n, ti, I.rec.ptr, I.pv.ptr);
     return I.pv.ptr;
 }
 
