@@ -1504,7 +1504,6 @@ struct IrrState {
     DevBuf<int> breg;                 // regular-due bodies of the running block
     DevBuf<double> bregxv;            // their x0, v0
     DevBuf<int> bsort;                // [sorted addresses | slots in | slots out], 3 x nmax
-    DevBuf<double> bsortxv;           // x0, v0 in address order
     DevBuf<char> bsort_tmp;
     long long rc_calls = 0;           // nb6_regf_correct_ calls and their host-side phases
     double rc_t[4] = {0, 0, 0, 0};
@@ -1641,7 +1640,6 @@ void irr_close_impl() {
     I.breg.release();
     I.bregxv.release();
     I.bsort.release();
-    I.bsortxv.release();
     I.bsort_tmp.release();
     I.brows.release();
     I.bctl.release();
@@ -2375,12 +2373,37 @@ __global__ void iota_kernel(int n, int *v) {
 
 // The due list in address order: 1-based addresses and the x0, v0 rows
 // permuted to match.
-__global__ void due_gather(int n, int *__restrict__ addr, const int *__restrict__ slot,
-                           const double *__restrict__ xv, double *__restrict__ out) {
+// keys: sorted 0-based addresses, slot: their append slots; out: 1-based
+// addresses and each body's x0, v0 in that order
+__global__ void due_gather(int n, const int *__restrict__ keys, const int *__restrict__ slot,
+                           const double *__restrict__ xv, int *__restrict__ addr, double *__restrict__ out) {
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        addr[k] += 1;
+        addr[k] = keys[k] + 1;
         const double *src = xv + 6 * (size_t)slot[k];
         for (int d = 0; d < 6; ++d) out[6 * (size_t)k + d] = src[d];
+    }
+}
+
+// The same for a short due list in one launch: one CTA holds the n keys in
+// shared memory and each key's place is the number of keys before it in
+// (key, slot) order, so the result is the sort's.
+constexpr int DUE_RANK_MAX = 2048, DUE_RANK_NT = 1024;
+__global__ void __launch_bounds__(DUE_RANK_NT) due_rank(int n, const int *__restrict__ keys,
+                                                        const double *__restrict__ xv, int *__restrict__ addr,
+                                                        double *__restrict__ out) {
+    __shared__ int sk[DUE_RANK_MAX];
+    for (int q = threadIdx.x; q < n; q += DUE_RANK_NT) sk[q] = keys[q];
+    __syncthreads();
+    for (int q = threadIdx.x; q < n; q += DUE_RANK_NT) {
+        const int k = sk[q];
+        int r = 0;
+        for (int p = 0; p < n; ++p) {
+            const int kp = sk[p];
+            r += (kp < k) | ((kp == k) & (p < q));
+        }
+        addr[r] = k + 1;
+        const double *src = xv + 6 * (size_t)q;
+        for (int d = 0; d < 6; ++d) out[6 * (size_t)r + d] = src[d];
     }
 }
 
@@ -2393,26 +2416,40 @@ void blocks_regular_impl(int *nreg, int *addr, double *xv) {
     *nreg = nr;
     if (nr <= 0) return;
     cudaStream_t st = nb6_stream();
-    // ascending addresses (the device appends in no particular order): a
-    // radix sort of (address, slot) on the device
-    I.bsort.reserve(3 * (size_t)nr);
-    I.bsortxv.reserve(6 * (size_t)nr);
-    int *keys_out = I.bsort.ptr, *vals_in = I.bsort.ptr + nr, *vals_out = I.bsort.ptr + 2 * (size_t)nr;
-    const int g = std::min((nr + 255) / 256, nb6_num_sms() * 4);
-    iota_kernel<<<g, 256, 0, st>>>(nr, vals_in);
-    int bits = 1;
-    while (bits < 31 && (1 << bits) < I.nmax) ++bits;
-    size_t tmp = 0;
-    NB6_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(nullptr, tmp, I.breg.ptr, keys_out, vals_in, vals_out, nr, 0, bits,
-                                                   st));
-    I.bsort_tmp.reserve(tmp + 16);
-    NB6_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(I.bsort_tmp.ptr, tmp, I.breg.ptr, keys_out, vals_in, vals_out, nr,
-                                                   0, bits, st));
-    due_gather<<<g, 256, 0, st>>>(nr, keys_out, vals_out, I.bregxv.ptr, I.bsortxv.ptr);
+    // ascending addresses (the device appends in no particular order), then
+    // [x0, v0 of each | 1-based addresses] in one device block, one
+    // download into pinned staging and two copies into the caller's arrays.
+    // Up to NB6_DUE_SORT_MIN bodies (default 2,048) one launch ranks the
+    // keys; longer lists take a radix sort of (address, slot).
+    const size_t nd = 6 * (size_t)nr + ((size_t)nr + 1) / 2;
+    I.dout.reserve(nd);
+    I.hout.reserve(nd);
+    double *dxv = I.dout.ptr;
+    int *daddr = reinterpret_cast<int *>(I.dout.ptr + 6 * (size_t)nr);
+    const char *e = getenv("NB6_DUE_SORT_MIN");
+    const int rank_max = std::min(DUE_RANK_MAX, e ? atoi(e) : DUE_RANK_MAX);
+    if (nr <= rank_max) {
+        due_rank<<<1, DUE_RANK_NT, 0, st>>>(nr, I.breg.ptr, I.bregxv.ptr, daddr, dxv);
+    } else {
+        I.bsort.reserve(3 * (size_t)nr);
+        int *keys_out = I.bsort.ptr, *vals_in = I.bsort.ptr + nr, *vals_out = I.bsort.ptr + 2 * (size_t)nr;
+        const int g = std::min((nr + 255) / 256, nb6_num_sms() * 4);
+        iota_kernel<<<g, 256, 0, st>>>(nr, vals_in);
+        int bits = 1;
+        while (bits < 31 && (1 << bits) < I.nmax) ++bits;
+        size_t tmp = 0;
+        NB6_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(nullptr, tmp, I.breg.ptr, keys_out, vals_in, vals_out, nr, 0,
+                                                       bits, st));
+        I.bsort_tmp.reserve(tmp + 16);
+        NB6_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(I.bsort_tmp.ptr, tmp, I.breg.ptr, keys_out, vals_in, vals_out,
+                                                       nr, 0, bits, st));
+        due_gather<<<g, 256, 0, st>>>(nr, keys_out, vals_out, I.bregxv.ptr, daddr, dxv);
+    }
     NB6_CUDA_CHECK(cudaGetLastError());
-    NB6_CUDA_CHECK(cudaMemcpyAsync(addr, keys_out, sizeof(int) * nr, cudaMemcpyDeviceToHost, st));
-    NB6_CUDA_CHECK(cudaMemcpyAsync(xv, I.bsortxv.ptr, sizeof(double) * 6 * (size_t)nr, cudaMemcpyDeviceToHost, st));
+    NB6_CUDA_CHECK(cudaMemcpyAsync(I.hout.ptr, I.dout.ptr, sizeof(double) * nd, cudaMemcpyDeviceToHost, st));
     NB6_CUDA_CHECK(cudaStreamSynchronize(st));
+    memcpy(xv, I.hout.ptr, sizeof(double) * 6 * (size_t)nr);
+    memcpy(addr, I.hout.ptr + 6 * (size_t)nr, sizeof(int) * (size_t)nr);
 }
 
 void hermite_get_impl(int a0, int n, double *out) {

@@ -47,7 +47,12 @@ def _open(nb6, S):
     nb6.hermite_set_all(S["fi"], S["fid"], S["fr"], S["frd"], S["step"], np.zeros(n), S["stepr"], cl.rs)
 
 
-def test_block_clock_first_block_equals_host_choice_and_corrector(nb6):
+@pytest.mark.parametrize("due_sort_min", [None, "0"])
+def test_block_clock_first_block_equals_host_choice_and_corrector(nb6, monkeypatch, due_sort_min):
+    """due_sort_min "0": the due list through the radix sort instead of the
+    one-launch ranking."""
+    if due_sort_min is not None:
+        monkeypatch.setenv("NB6_DUE_SORT_MIN", due_sort_min)
     S = _state(5)
     n = S["cl"].n
     tmin = (S["t0"] + S["step"]).min()
