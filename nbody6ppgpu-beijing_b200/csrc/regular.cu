@@ -1932,9 +1932,12 @@ static void regf_prepare(int ni, const double *d_h2, const double *d_dtr, const 
         if (L.hin)
             NB6_CUDA_CHECK(cudaMemcpyAsync(R.iin.ptr, L.hin, L.in_bytes, cudaMemcpyHostToDevice, st));
         // time each candidate three times and keep its best (after one
-        // untimed warm-up launch); neighbour counters are reset before every
-        // trial
-        float best = 1e30f, tdefault = 1e30f;
+        // warm-up launch whose time is not compared); when the warm-up took
+        // 2 ms or more, once: the noise of so long a launch is well inside
+        // the 3% tie below, and the trials of a large bucket would
+        // otherwise cost ~16 such launches.  Neighbour counters are reset
+        // before every trial.
+        float best = 1e30f, tdefault = 1e30f, twarm = 0.f;
         int bestv = variant;
         const int vdefault = default_variant(nt);
         for (int c = -1; c < ncand; ++c) {
@@ -1944,7 +1947,8 @@ static void regf_prepare(int ni, const double *d_h2, const double *d_dtr, const 
             t.nslices = p.nslices;
             t.ni = t.ni_pad = nt;
             float vbest = 1e30f;
-            for (int rep = 0; rep < (c < 0 ? 1 : 3); ++rep) {
+            const int reps = c < 0 ? 1 : (twarm >= 2.0f ? 1 : 3);
+            for (int rep = 0; rep < reps; ++rep) {
                 NB6_CUDA_CHECK(cudaMemsetAsync(R.nbcnt.ptr, 0, sizeof(int) * nt, st));
                 NB6_CUDA_CHECK(cudaEventRecord(R.tev0, st));
                 if (mf) launch_plan<true>(p, t, st);
@@ -1956,6 +1960,7 @@ static void regf_prepare(int ni, const double *d_h2, const double *d_dtr, const 
                 NB6_CUDA_CHECK(cudaEventElapsedTime(&ms, R.tev0, R.tev1));
                 vbest = std::min(vbest, ms);
             }
+            if (c < 0) twarm = vbest;
             if (c >= 0 && vbest < best) {
                 best = vbest;
                 bestv = v;
